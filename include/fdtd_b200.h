@@ -1,0 +1,231 @@
+/*
+ * fdtd_b200.h -- C ABI of the B200 FDTD time-stepping library (libfdtd_b200.so).
+ *
+ * Two groups of entry points:
+ *
+ *  1. The fused step engine (fdtd_engine_*): binds the compiled solver-scene
+ *     tensors of one simulation, packs them into its internal padded layout and
+ *     advances whole step ranges with one fused kernel per time step.  It
+ *     replaces the per-step kernel sequence of the reference's step driver,
+ *     witwin/maxwell/fdtd/runtime/stepping.py:1740-1815 (_field_update_block)
+ *     and :2289-2345 (the solve loop), and the host-side running-DFT loop of
+ *     witwin/maxwell/fdtd/observers.py:577-659.
+ *
+ *  2. Per-op entry points (fdtd_op_*) with the semantics of the reference's
+ *     torch ops witwin_maxwell_fdtd_cuda::<name>, schemas at
+ *     witwin/maxwell/fdtd/cuda/extension.cpp:2059-2196, so that the reference's
+ *     NativeFDTDModule (witwin/maxwell/fdtd/cuda/backend.py:89-115) can be
+ *     re-pointed op by op.
+ *
+ * Conventions: every array argument is a device pointer to float32 data in
+ * C-contiguous [X][Y][Z] order (z fastest) unless stated otherwise; shapes are
+ * passed as plain ints; `stream` is a cudaStream_t (NULL = legacy default).
+ * Every function returns 0 on success or a negative status:
+ */
+#ifndef FDTD_B200_H
+#define FDTD_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define FDTD_OK 0
+#define FDTD_ERR_INVALID_ARG (-1)
+#define FDTD_ERR_CUDA (-2)
+#define FDTD_ERR_UNSUPPORTED (-3)
+#define FDTD_ERR_STATE (-4)
+#define FDTD_ERR_TIMEOUT (-5)
+
+/* Boundary codes, witwin/maxwell/fdtd/boundary/common.py:5-10. */
+#define FDTD_BND_NONE 0
+#define FDTD_BND_PML 1
+#define FDTD_BND_PERIODIC 2
+#define FDTD_BND_BLOCH 3
+#define FDTD_BND_PEC 4
+#define FDTD_BND_PMC 5
+
+/* Last error message of the calling thread (engine-independent). */
+const char* fdtd_last_error(void);
+/* Library version string. */
+const char* fdtd_version(void);
+
+/* ------------------------------------------------------------------------ */
+/* 1. Fused step engine                                                       */
+/* ------------------------------------------------------------------------ */
+typedef struct fdtd_engine fdtd_engine;
+
+typedef struct {
+  int nx, ny, nz;       /* node counts per axis, CPML cells included (scene.py:1260-1281) */
+  double dt;            /* time step (fdtd/solver.py:145-159) */
+  int boundary[6];      /* x_lo, x_hi, y_lo, y_hi, z_lo, z_hi boundary codes */
+  int pml_lo[3];        /* CPML slab length on the low face of each axis (0 = none) */
+  int pml_hi[3];        /* CPML slab length on the high face of each axis */
+  int sample_block;     /* monitor samples buffered between DFT flushes (0 = 32) */
+  int tile_rows;        /* y rows per CTA (0 = default) */
+  int chunk_planes;     /* x planes per CTA (0 = default) */
+} fdtd_grid_desc;
+
+/* Create an engine on the current CUDA device.  Replaces FDTD.init_field,
+ * witwin/maxwell/fdtd/runtime/stepping.py:1624-1654 (field allocation). */
+int fdtd_engine_create(const fdtd_grid_desc* desc, void* stream, fdtd_engine** out);
+int fdtd_engine_destroy(fdtd_engine* h);
+
+/* Per-axis inverse spacings: inv_e has N entries (dual), inv_h N-1 (primal),
+ * witwin/maxwell/fdtd/runtime/initialization.py:131-139. */
+int fdtd_engine_set_spacing(fdtd_engine* h, int axis, const float* inv_e, const float* inv_h);
+
+/* CPML (b, c, 1/kappa) profiles of one axis, witwin/maxwell/fdtd/boundary/cpml.py:114-210
+ * and :398-402: *_e have N entries, *_h have N-1. */
+int fdtd_engine_set_cpml(fdtd_engine* h, int axis, const float* b_e, const float* c_e, const float* ik_e,
+                         const float* b_h, const float* c_h, const float* ik_h);
+
+/* Update coefficients of component comp (0..2 = Ex..Ez, 3..5 = Hx..Hz) in the
+ * reference's Yee shape, or NULL with the uniform scalar value
+ * (witwin/maxwell/fdtd/runtime/materials.py:942-1008, :1550-1574). */
+int fdtd_engine_set_coefficients(fdtd_engine* h, int comp, const float* decay, float decay_uniform,
+                                 const float* curl, float curl_uniform);
+
+/* Copy a field component between the reference Yee-shaped tensor and the
+ * engine's current state (witwin/maxwell/fdtd/runtime/stepping.py:1625-1630). */
+int fdtd_engine_pack_field(fdtd_engine* h, int comp, const float* src);
+int fdtd_engine_unpack_field(fdtd_engine* h, int comp, float* dst);
+
+/* Copy a CPML psi array in the reference's slab-compressed layout
+ * (witwin/maxwell/fdtd/boundary/cpml.py:218-333); which = 0 for the a-axis
+ * array, 1 for the b-axis array of component comp (e.g. Hx: psi_hx_y, psi_hx_z). */
+int fdtd_engine_pack_psi(fdtd_engine* h, int comp, int which, const float* src);
+int fdtd_engine_unpack_psi(fdtd_engine* h, int comp, int which, float* dst);
+
+/* One Debye (kind 0), Drude (1) or Lorentz (2) pole on E component comp over
+ * the box [i0,i1)x[j0,j1)x[k0,k1); drive and inv_eps are box-dense
+ * (witwin/maxwell/fdtd/runtime/materials.py:530-589, dispersive.cu:18-83).
+ * Returns the pole id in *pole_id. */
+int fdtd_engine_add_pole(fdtd_engine* h, int comp, int kind, const int* box, const float* drive,
+                         const float* inv_eps, float decay, float restoring, int* pole_id);
+int fdtd_engine_pole_state(fdtd_engine* h, int pole_id, float* pol_out, float* cur_out);
+
+/* Soft source patch: comp gets coeff[cell] * signal[n] added at step n
+ * (witwin/maxwell/fdtd/cuda/kernels/sources.cu:135-154; the signal table
+ * holds the host-evaluated waveform, excitation/temporal.py:408-491). */
+int fdtd_engine_add_patch(fdtd_engine* h, int comp, const int* box, const float* coeff, const float* signal,
+                          int n_signal, float scale);
+
+/* 1-D incident line for TFSF (witwin/maxwell/fdtd/excitation/spatial.py:311-469):
+ * the engine precomputes its whole history for n_steps steps.  Coefficient
+ * vectors: e_decay/e_curl have n_e entries, h_decay/h_curl n_e-1; source
+ * holds the FP32 source value for each step.  Returns the line id. */
+int fdtd_engine_add_aux_line(fdtd_engine* h, int n_e, const float* e_decay, const float* e_curl,
+                             const float* h_decay, const float* h_curl, int source_index,
+                             const float* source, int n_steps, int* line_id);
+/* TFSF face correction: comp gets coeff[cell] * line[sample_index[coord]] * scale,
+ * sampling the line's E history (sample_kind 0) or H history (1)
+ * (witwin/maxwell/fdtd/cuda/kernels/sources.cu:485-545, excitation/tfsf_apply.py:136-264). */
+int fdtd_engine_add_line_patch(fdtd_engine* h, int comp, const int* box, const float* coeff, int line_id,
+                               int sample_kind, const int* sample_index, int sample_axis, float scale);
+
+/* Monitor sample region of component comp over box; *base receives the first
+ * slot of the region in the DFT accumulator vector. */
+int fdtd_engine_add_sample_region(fdtd_engine* h, int comp, const int* box, int64_t* base);
+
+/* Running DFT of all sample regions (witwin/maxwell/fdtd/observers.py:577-659,
+ * spectral.py:165-232): omega (host, rad/s, n_freq entries) and the host
+ * window weight per step (n_steps entries, FP64).  Phases are reduced in FP64
+ * on the GPU; H regions carry the -omega*dt/2 retard (spectral.py:197-220). */
+int fdtd_engine_set_dft(fdtd_engine* h, int n_freq, const double* omega, int n_steps, const double* window);
+/* Read the accumulated DFT: re/im device arrays of n_freq * n_samples floats,
+ * [freq][slot] order, unscaled (scale 2/sum(window) is applied by the caller). */
+int fdtd_engine_read_dft(fdtd_engine* h, float* re, float* im);
+
+/* Freeze the scene description and build device tables.  Must precede stepping. */
+int fdtd_engine_finalize(fdtd_engine* h);
+/* Advance steps [n0, n1).  One fused kernel per step, a DFT flush every
+ * sample_block steps and at the end of the range. */
+int fdtd_engine_step_range(fdtd_engine* h, int n0, int n1);
+/* Flush buffered monitor samples into the DFT accumulators now. */
+int fdtd_engine_flush(fdtd_engine* h);
+
+/* Checkpoints of the full time-stepping state (fields, psi, ADE state),
+ * witwin/maxwell/fdtd/checkpoint.py:365-568. */
+int fdtd_engine_checkpoint_save(fdtd_engine* h, int slot);
+int fdtd_engine_checkpoint_load(fdtd_engine* h, int slot);
+
+/* Tile shape selection: time the candidate (tile_rows, chunk_planes) pairs on
+ * the bound scene (state is saved and restored) and keep the fastest. */
+int fdtd_engine_autotune(fdtd_engine* h, int* tile_rows, int* chunk_planes);
+/* Launch configuration and launch count bookkeeping. */
+int fdtd_engine_info(fdtd_engine* h, int* tile_rows, int* chunk_planes, int* grid_x, int* grid_y,
+                     int* block, int64_t* launches);
+/* Average device time of one fused step kernel over `reps` back-to-back
+ * launches at step index n (CUDA events on the engine stream).  The launches
+ * advance the field state like steps do but record no monitor samples. */
+int fdtd_engine_time_kernel(fdtd_engine* h, int n, int reps, float* ms);
+/* Device time of the last step_range in milliseconds (CUDA events). */
+int fdtd_engine_last_ms(fdtd_engine* h, float* ms);
+
+/* ------------------------------------------------------------------------ */
+/* 2. Per-op entry points (reference op semantics)                           */
+/* ------------------------------------------------------------------------ */
+
+/* Magnetic update of component comp (0 Hx, 1 Hy, 2 Hz) over an (nx, ny, nz)
+ * H array; mode 0 = standard (update_magnetic_h*_standard), 1 = dense CPML
+ * (update_magnetic_h*_cpml), 2 = slab-compressed CPML
+ * (update_magnetic_h*_cpml_compressed); witwin/maxwell/fdtd/cuda/kernels/magnetic.cu:20-212.
+ * first/second are the b-axis / a-axis E sources (Hx: Ey, Ez; Hy: Ex, Ez; Hz: Ex, Ey).
+ * decay/curl may be NULL to use the uniform scalars. slab = {a_low, a_high_start,
+ * a_high_len, b_low, b_high_start, b_high_len}. */
+int fdtd_op_update_magnetic(int comp, int mode, int nx, int ny, int nz, float* field, const float* first,
+                            const float* second, const float* decay, const float* curl, float decay_u,
+                            float curl_u, const float* inv_a, const float* inv_b, float* psi_a, float* psi_b,
+                            const float* ika, const float* ba, const float* ca, const float* ikb,
+                            const float* bb, const float* cb, const int* slab, void* stream);
+
+/* Electric update of component comp (0 Ex, 1 Ey, 2 Ez) with boundary-mode-aware
+ * backward differences; modes = {a_low, a_high, b_low, b_high} boundary codes;
+ * witwin/maxwell/fdtd/cuda/kernels/electric.cu:242-941 (update_electric_e*_{standard,cpml,cpml_compressed}).
+ * first/second: Ex: Hy, Hz; Ey: Hx, Hz; Ez: Hx, Hy. */
+int fdtd_op_update_electric(int comp, int mode, int nx, int ny, int nz, float* field, const float* first,
+                            const float* second, const float* decay, const float* curl, float decay_u,
+                            float curl_u, const float* inv_a, const float* inv_b, const int* modes,
+                            float* psi_a, float* psi_b, const float* ika, const float* ba, const float* ca,
+                            const float* ikb, const float* bb, const float* cb, const int* slab, void* stream);
+
+/* ADE ops, witwin/maxwell/fdtd/cuda/kernels/dispersive.cu:18-83
+ * (update_debye_current, update_drude_current, update_lorentz_current, apply_polarization_current). */
+int fdtd_op_update_debye(int64_t n, const float* e, const float* drive, float decay, float dt, float* pol,
+                         float* cur, void* stream);
+int fdtd_op_update_drude(int64_t n, const float* e, const float* drive, float decay, float* cur, void* stream);
+int fdtd_op_update_lorentz(int64_t n, const float* e, const float* drive, float decay, float restoring,
+                           float dt, float* pol, float* cur, void* stream);
+int fdtd_op_apply_polarization(int64_t n, const float* cur, const float* inv_eps, float dt, float* e,
+                               void* stream);
+
+/* add_source_patch (sources.cu:135-154): field[off + idx] += signal * patch[idx],
+ * cells outside the field are skipped.  fshape/pshape/offset are int[3]. */
+int fdtd_op_add_source_patch(float* field, const int* fshape, const float* patch, const int* pshape,
+                             const int* offset, float signal, void* stream);
+/* add_scaled_line_source_patch (sources.cu:485-545): value = coeff * incident[sample_idx[a]] * scale. */
+int fdtd_op_add_line_patch(float* field, const int* fshape, const float* coeff, const int* pshape,
+                           const int* offset, const float* incident, const int64_t* sample_idx, int axis,
+                           float scale, void* stream);
+/* Auxiliary 1-D grid (sources.cu:803-839). */
+int fdtd_op_aux_magnetic(int n_e, float* h, const float* e, const float* h_decay, const float* h_curl,
+                         void* stream);
+int fdtd_op_aux_electric(int n_e, float* e, const float* h, const float* e_decay, const float* e_curl,
+                         int source_index, float source_value, void* stream);
+/* Observers (observers.cu:7-78) and the batched full-field DFT (spectral.cu:9-146). */
+int fdtd_op_point_observers(const float* field, const int* fshape, int n_points, const int* pi, const int* pj,
+                            const int* pk, float* re, float* im, float wcos, float wsin, void* stream);
+int fdtd_op_plane_observer(const float* field, const int* fshape, int axis, int index, float* re, float* im,
+                           float wcos, float wsin, void* stream);
+int fdtd_op_dft_volume(int64_t n, int n_freq, const float* field, float* re, float* im, const float* wcos,
+                       const float* wsin, void* stream);
+/* PEC face clamp (boundary.cu:69-168). */
+int fdtd_op_clamp_face(float* field, const int* fshape, int axis, int side, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* FDTD_B200_H */

@@ -1,0 +1,351 @@
+"""CPU oracle for the FDTD hot path -- test infrastructure, not product code.
+
+``OracleSimulation`` steps a compiled scene on the CPU with the reference's
+per-step kernel order (witwin/maxwell/fdtd/runtime/stepping.py:1740-1815 and
+:2289-2345), calling the plain-C restatements of the reference's per-op kernels
+in ``fdtd_oracle.c`` on full Yee-shaped arrays:
+
+    H update (CPML slab psi)           magnetic.cu:145-212
+    TFSF H correction, aux H advance   tfsf_apply.py:228-264, sources.cu:803-839
+    ADE advance from E^n               dispersive.cu:18-70, materials.py:665-703
+    E update (boundary modes, CPML)    electric.cu:242-311, 647-941
+    TFSF E correction, aux E advance   tfsf_apply.py:237-264
+    soft sources                       sources.cu:135-154, temporal.py:408-491
+    ADE subtraction E -= dt J / eps    dispersive.cu:72-83, materials.py:911
+    monitor running DFT                observers.py:577-659, spectral.py:165-232
+
+The DFT phase follows the reference's observer path: a float64 rotation
+recurrence per frequency, H samples rotated by -omega*dt/2, result scaled by
+2/sum(window).  Precision "f64" is the accuracy oracle; "f32" is the FP32
+restatement used as the CPU baseline.  Only tests, smoke() and the benchmark's
+CPU-baseline leg use this module.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import subprocess
+from concurrent.futures import ThreadPoolExecutor
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+_LIBS: dict = {}
+_vp = ctypes.c_void_p
+
+COMPONENTS = ("Ex", "Ey", "Ez", "Hx", "Hy", "Hz")
+
+
+def build(force: bool = False) -> None:
+    """Compile the two oracle libraries with the committed Makefile."""
+    libs = [HERE / "liboracle_f64.so", HERE / "liboracle_f32.so"]
+    src = HERE / "fdtd_oracle.c"
+    if not force and all(p.exists() and p.stat().st_mtime >= src.stat().st_mtime for p in libs):
+        return
+    subprocess.run(["make", "-s", "-C", str(HERE)], check=True)
+
+
+def load(precision: str = "f64") -> ctypes.CDLL:
+    if precision not in ("f64", "f32"):
+        raise ValueError(precision)
+    if precision not in _LIBS:
+        path = HERE / f"liboracle_{precision}.so"
+        if not path.exists():
+            build()
+        lib = ctypes.CDLL(str(path))
+        real = ctypes.c_double if precision == "f64" else ctypes.c_float
+        i, i64 = ctypes.c_int, ctypes.c_int64
+        lib.oracle_real_size.restype = i
+        lib.oracle_h_update.argtypes = [i, i, i, i, i, i, i] + [_vp] * 15 + [i] * 6
+        lib.oracle_e_update.argtypes = [i, i, i, i, i, i, i] + [_vp] * 7 + [i] * 4 + [_vp] * 8 + [i] * 6
+        lib.oracle_debye.argtypes = [i64, i64, _vp, _vp, real, real, _vp, _vp]
+        lib.oracle_drude.argtypes = [i64, i64, _vp, _vp, real, _vp]
+        lib.oracle_lorentz.argtypes = [i64, i64, _vp, _vp, real, real, real, _vp, _vp]
+        lib.oracle_apply_polarization.argtypes = [i64, i64, _vp, _vp, real, _vp]
+        lib.oracle_add_patch.argtypes = [i, i, i, _vp, i, i, i, _vp, i, i, i, real]
+        lib.oracle_add_line_patch.argtypes = [i, i, i, _vp, i, i, i, _vp, _vp, _vp, i, i, i, i, real]
+        lib.oracle_aux_magnetic.argtypes = [i, _vp, _vp, _vp, _vp]
+        lib.oracle_aux_electric.argtypes = [i, _vp, _vp, _vp, _vp, i, real]
+        lib.oracle_point_observers.argtypes = [i, i, _vp, i, _vp, _vp, _vp, _vp, _vp, real, real]
+        lib.oracle_plane_observer.argtypes = [i, i, i, _vp, i, i, _vp, _vp, real, real]
+        lib.oracle_dft_volume.argtypes = [i64, i64, i64, i, _vp, _vp, _vp, _vp, _vp]
+        lib.oracle_clamp_face.argtypes = [i, i, i, _vp, i, i]
+        _LIBS[precision] = lib
+    return _LIBS[precision]
+
+
+def _p(a):
+    return None if a is None else a.ctypes.data_as(_vp)
+
+
+def component_shape(name, nodes):
+    nx, ny, nz = nodes
+    return {
+        "Ex": (nx - 1, ny, nz), "Ey": (nx, ny - 1, nz), "Ez": (nx, ny, nz - 1),
+        "Hx": (nx, ny - 1, nz - 1), "Hy": (nx - 1, ny, nz - 1), "Hz": (nx - 1, ny - 1, nz),
+    }[name]
+
+
+# (a-axis, b-axis, first, second) per component, magnetic.cu:20-212 / electric.cu:242-941
+_H_SPEC = {"Hx": (1, 2, "Ey", "Ez"), "Hy": (0, 2, "Ex", "Ez"), "Hz": (0, 1, "Ex", "Ey")}
+_E_SPEC = {"Ex": (1, 2, "Hy", "Hz"), "Ey": (0, 2, "Hx", "Hz"), "Ez": (0, 1, "Hx", "Hy")}
+
+
+class OracleSimulation:
+    def __init__(self, compiled, precision: str = "f64", threads: int | None = None):
+        self.cs = compiled
+        self.precision = precision
+        self.lib = load(precision)
+        self.dtype = np.float64 if precision == "f64" else np.float32
+        self.threads = max(1, int(threads or os.cpu_count() or 1))
+        self.pool = ThreadPoolExecutor(self.threads) if self.threads > 1 else None
+        cs = compiled
+        dt = self.dtype
+        nodes = cs.nodes
+        self.fields = {n: np.zeros(component_shape(n, nodes), dt) for n in COMPONENTS}
+        self.decay = {}
+        self.curl = {}
+        for n in COMPONENTS:
+            shape = component_shape(n, nodes)
+            du, cu = cs.uniform[n]
+            self.decay[n] = (np.full(shape, du, dt) if cs.decay[n] is None else cs.decay[n].astype(dt))
+            self.curl[n] = (np.full(shape, cu, dt) if cs.curl[n] is None else cs.curl[n].astype(dt))
+        self.inv_e = [a.astype(dt) for a in cs.inv_e]
+        self.inv_h = [a.astype(dt) for a in cs.inv_h]
+        self.cp = {k: [a.astype(dt) for a in v] for k, v in cs.cpml.items()}
+        self.cpml = any(cs.pml_lo) or any(cs.pml_hi)
+        # slab psi in the reference's compressed layout (cpml.py:218-333)
+        self.psi = {}
+        self.slab = {}
+        for n in COMPONENTS:
+            spec = _H_SPEC.get(n) or _E_SPEC[n]
+            shape = component_shape(n, nodes)
+            for which, axis in enumerate(spec[:2]):
+                size = shape[axis]
+                low = min(cs.pml_lo[axis], size)
+                high = min(cs.pml_hi[axis], max(size - low, 0))
+                cshape = list(shape)
+                cshape[axis] = low + high
+                self.psi[(n, which)] = np.zeros(cshape, dt)
+                self.slab[(n, which)] = (low, size - high, high)
+        # ADE: full-volume drive / state per pole component (materials.py:530-662)
+        self.poles = []
+        for pole in cs.poles:
+            shape = component_shape(pole.component, nodes)
+            b = pole.box
+            sl = (slice(b[0], b[1]), slice(b[2], b[3]), slice(b[4], b[5]))
+            drive = np.zeros(shape, dt)
+            drive[sl] = pole.drive
+            inv_eps = (1.0 / cs.eps[pole.component]).astype(np.float32).astype(dt)
+            inv_eps[sl] = pole.inv_eps
+            self.poles.append({
+                "comp": pole.component, "kind": pole.kind, "decay": pole.decay, "restoring": pole.restoring,
+                "drive": drive, "inv_eps": inv_eps, "P": np.zeros(shape, dt), "J": np.zeros(shape, dt),
+            })
+        self.patches = [(p.component, p.box, p.coeff.astype(dt), p.signal) for p in cs.patches]
+        self.aux = None
+        if cs.aux_line is not None:
+            a = cs.aux_line
+            ne = a.e_decay.size
+            self.aux = {
+                "e": np.zeros(ne, dt), "h": np.zeros(ne - 1, dt),
+                "ed": a.e_decay.astype(dt), "ec": a.e_curl.astype(dt),
+                "hd": a.h_decay.astype(dt), "hc": a.h_curl.astype(dt),
+                "src": a.source_index, "signal": a.source,
+            }
+        self.lines = [
+            (lp.component, lp.box, lp.coeff.astype(dt), lp.sample_kind, lp.sample_axis,
+             lp.sample_index.astype(np.int64), lp.scale)
+            for lp in cs.line_patches
+        ]
+        # monitor running DFT state (observers.py:409-659)
+        self.freqs = np.asarray(cs.frequencies, dtype=np.float64)
+        nf = self.freqs.size
+        self.acc = []
+        for reg in cs.regions:
+            b = reg.box
+            shape = (nf, b[1] - b[0], b[3] - b[2], b[5] - b[4])
+            self.acc.append([np.zeros(shape, dt), np.zeros(shape, dt)])
+        omega = 2.0 * np.pi * self.freqs
+        self.phase_step_cos = np.cos(omega * cs.dt)
+        self.phase_step_sin = np.sin(omega * cs.dt)
+        self.h_off_cos = np.cos(-0.5 * omega * cs.dt)
+        self.h_off_sin = np.sin(-0.5 * omega * cs.dt)
+        self.phase_cos = np.ones(nf)
+        self.phase_sin = np.zeros(nf)
+        self.window_sum = 0.0
+        self.step = 0
+
+    # ------------------------------------------------------------------ utils
+    def _split(self, nx, fn):
+        if self.pool is None or nx < 2 * self.threads:
+            fn(0, nx)
+            return
+        edges = np.linspace(0, nx, self.threads + 1).astype(int)
+        futures = [self.pool.submit(fn, int(a), int(b)) for a, b in zip(edges[:-1], edges[1:]) if b > a]
+        for f in futures:
+            f.result()
+
+    def _split_flat(self, n, fn):
+        if self.pool is None or n < 1 << 16:
+            fn(0, n)
+            return
+        edges = np.linspace(0, n, self.threads + 1).astype(np.int64)
+        futures = [self.pool.submit(fn, int(a), int(b)) for a, b in zip(edges[:-1], edges[1:]) if b > a]
+        for f in futures:
+            f.result()
+
+    # ------------------------------------------------------------------- ops
+    def update_h(self):
+        F = self.fields
+        mode = 2 if self.cpml else 0
+        for n, (A, B, first, second) in _H_SPEC.items():
+            shape = F[n].shape
+            pa, pb = self.psi[(n, 0)], self.psi[(n, 1)]
+            sa, sb = self.slab[(n, 0)], self.slab[(n, 1)]
+            cp = self.cp
+            args = (n, A, B, first, second, pa, pb, sa, sb)
+
+            def run(i0, i1, n=n, A=A, B=B, first=first, second=second, pa=pa, pb=pb, sa=sa, sb=sb, shape=shape):
+                self.lib.oracle_h_update(
+                    i0, i1, "xyz".index(n[1]), mode, shape[0], shape[1], shape[2], _p(F[n]), _p(F[first]),
+                    _p(F[second]), _p(self.decay[n]), _p(self.curl[n]), _p(self.inv_h[A]), _p(self.inv_h[B]),
+                    _p(pa), _p(pb), _p(cp["ik_h"][A]), _p(cp["b_h"][A]), _p(cp["c_h"][A]), _p(cp["ik_h"][B]),
+                    _p(cp["b_h"][B]), _p(cp["c_h"][B]), sa[0], sa[1], sa[2], sb[0], sb[1], sb[2])
+
+            del args
+            self._split(shape[0], run)
+
+    def update_e(self):
+        F = self.fields
+        mode = 2 if self.cpml else 0
+        bnd = self.cs.boundary
+        for n, (A, B, first, second) in _E_SPEC.items():
+            shape = F[n].shape
+            pa, pb = self.psi[(n, 0)], self.psi[(n, 1)]
+            sa, sb = self.slab[(n, 0)], self.slab[(n, 1)]
+            cp = self.cp
+
+            def run(i0, i1, n=n, A=A, B=B, first=first, second=second, pa=pa, pb=pb, sa=sa, sb=sb, shape=shape):
+                self.lib.oracle_e_update(
+                    i0, i1, "xyz".index(n[1]), mode, shape[0], shape[1], shape[2], _p(F[n]), _p(F[first]),
+                    _p(F[second]), _p(self.decay[n]), _p(self.curl[n]), _p(self.inv_e[A]), _p(self.inv_e[B]),
+                    bnd[2 * A], bnd[2 * A + 1], bnd[2 * B], bnd[2 * B + 1], _p(pa), _p(pb), _p(cp["ik_e"][A]),
+                    _p(cp["b_e"][A]), _p(cp["c_e"][A]), _p(cp["ik_e"][B]), _p(cp["b_e"][B]), _p(cp["c_e"][B]),
+                    sa[0], sa[1], sa[2], sb[0], sb[1], sb[2])
+
+            self._split(shape[0], run)
+
+    def advance_ade(self):
+        F = self.fields
+        dt = self.cs.dt
+        for p in self.poles:
+            e = F[p["comp"]]
+            n = e.size
+            if p["kind"] == 0:
+                self._split_flat(n, lambda a, b, p=p, e=e: self.lib.oracle_debye(
+                    a, b, _p(e), _p(p["drive"]), p["decay"], dt, _p(p["P"]), _p(p["J"])))
+            elif p["kind"] == 1:
+                self._split_flat(n, lambda a, b, p=p, e=e: self.lib.oracle_drude(
+                    a, b, _p(e), _p(p["drive"]), p["decay"], _p(p["J"])))
+            else:
+                self._split_flat(n, lambda a, b, p=p, e=e: self.lib.oracle_lorentz(
+                    a, b, _p(e), _p(p["drive"]), p["decay"], p["restoring"], dt, _p(p["P"]), _p(p["J"])))
+
+    def apply_ade(self):
+        F = self.fields
+        dt = self.cs.dt
+        for p in self.poles:
+            e = F[p["comp"]]
+            self._split_flat(e.size, lambda a, b, p=p, e=e: self.lib.oracle_apply_polarization(
+                a, b, _p(p["J"]), _p(p["inv_eps"]), dt, _p(e)))
+
+    def _line_corrections(self, magnetic: bool):
+        if self.aux is None:
+            return
+        sample = self.aux["e"] if magnetic else self.aux["h"]
+        for comp, box, coeff, kind, axis, idx, scale in self.lines:
+            if (comp[0] == "H") != magnetic:
+                continue
+            f = self.fields[comp]
+            pshape = coeff.shape
+            self.lib.oracle_add_line_patch(f.shape[0], f.shape[1], f.shape[2], _p(f), pshape[0], pshape[1], pshape[2],
+                                           _p(coeff), _p(sample), _p(idx), axis, box[0], box[2], box[4], scale)
+
+    def step_once(self):
+        n = self.step
+        F = self.fields
+        self.update_h()
+        if self.aux is not None:
+            self._line_corrections(True)
+            a = self.aux
+            self.lib.oracle_aux_magnetic(a["e"].size, _p(a["h"]), _p(a["e"]), _p(a["hd"]), _p(a["hc"]))
+        self.advance_ade()
+        self.update_e()
+        if self.aux is not None:
+            self._line_corrections(False)
+            a = self.aux
+            self.lib.oracle_aux_electric(a["e"].size, _p(a["e"]), _p(a["h"]), _p(a["ed"]), _p(a["ec"]), a["src"],
+                                         float(a["signal"][n]))
+        for comp, box, coeff, signal in self.patches:
+            f = F[comp]
+            self.lib.oracle_add_patch(f.shape[0], f.shape[1], f.shape[2], _p(f), coeff.shape[0], coeff.shape[1],
+                                      coeff.shape[2], _p(coeff), box[0], box[2], box[4], float(signal[n]))
+        self.apply_ade()
+        if self.aux is None:
+            self._clamp_pec()
+        self._accumulate(n)
+        self.step += 1
+
+    def _clamp_pec(self):
+        bnd = self.cs.boundary
+        # enforce_pec_boundaries (stepping.py:1450): tangential E on PEC faces
+        for n, (A, B, _, _) in _E_SPEC.items():
+            f = self.fields[n]
+            for axis in (A, B):
+                for side in (0, 1):
+                    if bnd[2 * axis + side] == 4:
+                        self.lib.oracle_clamp_face(f.shape[0], f.shape[1], f.shape[2], _p(f), axis, side)
+
+    def _accumulate(self, n):
+        cs = self.cs
+        if self.freqs.size == 0 or not cs.regions:
+            return
+        w = float(cs.window[n])
+        wc = w * self.phase_cos
+        ws = w * self.phase_sin
+        hc = wc * self.h_off_cos - ws * self.h_off_sin
+        hs = ws * self.h_off_cos + wc * self.h_off_sin
+        dt = self.dtype
+        for reg, (re, im) in zip(cs.regions, self.acc):
+            b = reg.box
+            v = self.fields[reg.component][b[0]:b[1], b[2]:b[3], b[4]:b[5]]
+            ccos, csin = (wc, ws) if reg.component[0] == "E" else (hc, hs)
+            for f in range(self.freqs.size):
+                re[f] += v * dt(ccos[f])
+                im[f] += v * dt(csin[f])
+        self.window_sum += w
+        nc = self.phase_cos * self.phase_step_cos - self.phase_sin * self.phase_step_sin
+        ns = self.phase_sin * self.phase_step_cos + self.phase_cos * self.phase_step_sin
+        self.phase_cos, self.phase_sin = nc, ns
+
+    def run(self, steps: int):
+        for _ in range(int(steps)):
+            self.step_once()
+        return self
+
+    def monitor_results(self) -> dict:
+        cs = self.cs
+        scale = 2.0 / self.window_sum if self.window_sum > 0 else 0.0
+        out: dict = {}
+        for reg, (re, im) in zip(cs.regions, self.acc):
+            fidx = [cs.frequencies.index(f) for f in cs.monitor_frequencies[reg.monitor]]
+            data = (re[fidx].astype(np.float64) + 1j * im[fidx].astype(np.float64)) * scale
+            out.setdefault(reg.monitor, {})[reg.component] = data
+        return out
+
+    def close(self):
+        if self.pool is not None:
+            self.pool.shutdown()
+            self.pool = None

@@ -1,0 +1,205 @@
+"""GPU parity of the fused step engine against the CPU oracle and the reference goldens.
+
+Tolerance: relative L2 <= 1e-5 for FP32 fields and monitor spectra against the
+FP32 oracle (same arithmetic, different summation order / FMA contraction), and
+against the reference's own 60-step golden run; FP64-oracle agreement is
+asserted at 1e-4 (it measures FP32 rounding growth, not a semantic difference).
+"""
+from __future__ import annotations
+
+import importlib.util
+import sys
+from pathlib import Path
+
+import numpy as np
+import pytest
+import torch
+
+from conftest import load_package
+from oracle import oracle as orc
+
+pytestmark = pytest.mark.gpu
+GOLDEN = Path(__file__).resolve().parent / "golden"
+FIELDS = ("Ex", "Ey", "Ez", "Hx", "Hy", "Hz")
+TOL = 1e-5
+
+
+def rel_l2(a, b) -> float:
+    a = np.asarray(a, dtype=np.float64)
+    b = np.asarray(b, dtype=np.float64)
+    den = np.linalg.norm(b.ravel())
+    return float(np.linalg.norm((a - b).ravel()) / den) if den > 0 else float(np.linalg.norm(a.ravel()))
+
+
+def _golden_module():
+    spec = importlib.util.spec_from_file_location("make_golden", GOLDEN / "make_golden.py")
+    mg = importlib.util.module_from_spec(spec)
+    sys.modules["make_golden"] = mg
+    spec.loader.exec_module(mg)
+    return mg
+
+
+def _run_engine(cs, steps, **kw):
+    wm = load_package()
+    solver = wm.solver.B200FDTD(cs, **kw).init_field()
+    solver.step_range(0, steps)
+    fields = {n: solver.field(n).cpu().numpy() for n in FIELDS}
+    mons = {k: {c: v.cpu().numpy() for c, v in d.items()} for k, d in solver.monitor_results().items()}
+    return solver, fields, mons
+
+
+def test_engine_matches_reference_golden_run():
+    """Fused engine (FP32) vs the reference's Torch ops (FP64) on the golden scene."""
+    wm = load_package()
+    mg = _golden_module()
+    gold = dict(np.load(GOLDEN / "steps.npz"))
+    steps = int(gold["steps"])
+    cs = wm.compile_scene(mg.golden_scene(), steps)
+    solver, fields, mons = _run_engine(cs, steps)
+    for n in FIELDS:
+        assert rel_l2(fields[n], gold[f"field_{n}"]) < TOL, n
+    scale = 2.0 / float(gold["window_sum"])
+    re, im = solver.raw_dft()
+    re, im = re.cpu().numpy(), im.cpu().numpy()
+    for i, (reg, base) in enumerate(zip(cs.regions, solver.region_base)):
+        b = reg.box
+        count = (b[1] - b[0]) * (b[3] - b[2]) * (b[5] - b[4])
+        g_re = gold[f"dft_{i}_re"].reshape(len(cs.frequencies), -1)
+        g_im = gold[f"dft_{i}_im"].reshape(len(cs.frequencies), -1)
+        assert rel_l2(re[:, base:base + count], g_re) < TOL, reg
+        assert rel_l2(im[:, base:base + count], g_im) < TOL, reg
+    del scale
+    solver.close()
+
+
+def _c1_scene(wm, cells=64, pml=10):
+    """64^3 cells, 10-cell CPML, eps 4 box, Ez dipole, z-plane + point monitors at 3 frequencies."""
+    sc = wm.Scene(cells=(cells,) * 3, spacing=25e-9, pml_cells=pml)
+    sc.structures.append(wm.Structure(wm.Box((20, 20, 20), (44, 44, 44)), wm.Medium(eps_r=4.0)))
+    sc.sources.append(wm.PointDipole((20, 32, 32), "Ez", wm.GaussianPulse(300e12, 100e12), width=25e-9))
+    freqs = (250e12, 300e12, 350e12)
+    sc.monitors.append(wm.PlaneMonitor("plane_z44", 2, 44, frequencies=freqs))
+    sc.monitors.append(wm.PointMonitor("point", (44, 32, 32), frequencies=freqs))
+    return sc
+
+
+def test_engine_matches_oracle_small_plain_config():
+    """Plain FP32 64^3 config (CPML, dielectric box, dipole, plane + point DFT), 1000 steps."""
+    wm = load_package()
+    steps = 1000
+    cs = wm.compile_scene(_c1_scene(wm), steps)
+    solver, fields, mons = _run_engine(cs, steps)
+    ref32 = orc.OracleSimulation(cs, "f32").run(steps)
+    for n in FIELDS:
+        assert rel_l2(fields[n], ref32.fields[n]) < TOL, n
+    rm = ref32.monitor_results()
+    for name, comps in rm.items():
+        for comp, r in comps.items():
+            assert rel_l2(mons[name][comp], r) < TOL, (name, comp)
+    ref32.close()
+    solver.close()
+
+
+def test_engine_dispersive_tfsf_against_fp64_oracle():
+    """Lorentz sphere + Drude slab + TFSF plane wave + flux planes, FP32 engine vs FP64 oracle."""
+    wm = load_package()
+    steps = 400
+    sc = wm.Scene(cells=(48, 40, 40), spacing=25e-9, pml_cells=8)
+    sc.structures.append(wm.Structure(wm.Sphere((26, 20, 20), 8.0), wm.Medium.lorentz(2.0, 3.0, 250e12, 20e12)))
+    sc.structures.append(wm.Structure(wm.Box((12, 0, 0), (16, 40, 40)), wm.Medium.drude(2e15 / (2 * np.pi), 1e14 / (2 * np.pi))))
+    sc.sources.append(wm.PlaneWaveTFSF((1, 0, 0), (0, 0, 1), wm.GaussianPulse(300e12, 100e12), (10, 10, 10), (38, 30, 30)))
+    freqs = tuple(np.linspace(200e12, 400e12, 5))
+    sc.monitors.append(wm.flux_monitor("flux_lo", 2, 14, freqs))
+    sc.monitors.append(wm.flux_monitor("flux_hi", 2, 26, freqs))
+    for face in wm.closed_box_monitor("box", (12, 12, 12), (36, 28, 28), freqs):
+        sc.monitors.append(face)
+    cs = wm.compile_scene(sc, steps)
+    solver, fields, mons = _run_engine(cs, steps)
+    ref32 = orc.OracleSimulation(cs, "f32").run(steps)
+    ref64 = orc.OracleSimulation(cs, "f64").run(steps)
+    for n in FIELDS:
+        assert rel_l2(fields[n], ref32.fields[n]) < TOL, n
+        assert rel_l2(fields[n], ref64.fields[n]) < 1e-4, n
+    for p_idx in range(len(cs.poles)):
+        pol, cur = solver.pole_state(p_idx)
+        b = cs.poles[p_idx].box
+        sl = (slice(b[0], b[1]), slice(b[2], b[3]), slice(b[4], b[5]))
+        assert rel_l2(cur.cpu().numpy(), ref32.poles[p_idx]["J"][sl]) < TOL
+    r32 = ref32.monitor_results()
+    for name, comps in r32.items():
+        for comp, r in comps.items():
+            assert rel_l2(mons[name][comp], r) < TOL, (name, comp)
+    ref32.close()
+    ref64.close()
+    solver.close()
+
+
+@pytest.mark.parametrize("tiles", [(1, 8), (3, 16), (6, 5), (13, 64)])
+def test_tile_shape_does_not_change_results(tiles):
+    """Every (tile_rows, chunk_planes) decomposition gives bit-identical fields."""
+    wm = load_package()
+    steps = 50
+    cs = wm.compile_scene(_c1_scene(wm, cells=40, pml=6), steps)
+    _, base, _ = _run_engine(cs, steps, tile_rows=4, chunk_planes=32)
+    _, other, _ = _run_engine(cs, steps, tile_rows=tiles[0], chunk_planes=tiles[1])
+    for n in FIELDS:
+        np.testing.assert_array_equal(other[n], base[n])
+
+
+def test_checkpoint_roundtrip_and_autotune_restore_state():
+    wm = load_package()
+    steps = 60
+    cs = wm.compile_scene(_c1_scene(wm, cells=32, pml=6), steps)
+    solver = wm.solver.B200FDTD(cs).init_field()
+    solver.step_range(0, 20)
+    solver.checkpoint_save(0)
+    solver.step_range(20, 40)
+    after = {n: solver.field(n).cpu().numpy() for n in FIELDS}
+    solver.checkpoint_load(0)
+    solver.autotune()  # times candidate tiles, then restores the saved state
+    solver.step_range(20, 40)
+    again = {n: solver.field(n).cpu().numpy() for n in FIELDS}
+    for n in FIELDS:
+        np.testing.assert_array_equal(again[n], after[n])
+    solver.close()
+
+
+def test_tfsf_total_field_stays_inside_box():
+    """Plane wave in vacuum: the scattered-field region stays empty (leakage < 1e-3 of the TF field)."""
+    wm = load_package()
+    steps = 300
+    sc = wm.Scene(cells=(48, 32, 32), spacing=25e-9, pml_cells=8)
+    sc.sources.append(wm.PlaneWaveTFSF((1, 0, 0), (0, 0, 1), wm.GaussianPulse(300e12, 100e12), (12, 11, 11), (36, 21, 21)))
+    cs = wm.compile_scene(sc, steps)
+    _, fields, _ = _run_engine(cs, steps - 100)
+    ez = fields["Ez"]
+    inside = np.abs(ez[14:34, 13:19, 13:19]).max()
+    outside = max(np.abs(ez[:, :9, :]).max(), np.abs(ez[:, 24:, :]).max(), np.abs(ez[:, :, :9]).max())
+    assert inside > 0.1
+    assert outside < 1e-3 * inside
+
+
+def test_engine_rejects_bad_inputs():
+    wm = load_package()
+    lib = wm._lib.load()
+    import ctypes
+
+    desc = wm._lib.FdtdGridDesc()
+    desc.nx = desc.ny = desc.nz = 2
+    desc.dt = 1e-17
+    handle = ctypes.c_void_p()
+    rc = lib.fdtd_engine_create(ctypes.byref(desc), None, ctypes.byref(handle))
+    assert rc == -1 and b"at least 3" in lib.fdtd_last_error()
+    desc.nx = desc.ny = desc.nz = 10
+    desc.boundary[0] = 3  # Bloch face: not supported by the fused engine
+    rc = lib.fdtd_engine_create(ctypes.byref(desc), None, ctypes.byref(handle))
+    assert rc == -3
+    desc.boundary[0] = 1
+    rc = lib.fdtd_engine_create(ctypes.byref(desc), None, ctypes.byref(handle))
+    assert rc == 0
+    # stepping before finalize is a state error, not a crash
+    assert lib.fdtd_engine_step_range(handle, 0, 1) == -4
+    box = wm._lib.int_array([0, 20, 0, 1, 0, 1])
+    dummy = torch.zeros(64, device="cuda")
+    assert lib.fdtd_engine_add_patch(handle, 0, box, dummy.data_ptr(), dummy.data_ptr(), 1, 1.0) == -1
+    assert lib.fdtd_engine_destroy(handle) == 0

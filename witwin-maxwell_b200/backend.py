@@ -1,0 +1,262 @@
+"""NativeFDTDModule-compatible per-op surface backed by libfdtd_b200.so.
+
+The reference dispatches every hot-path kernel through
+``solver.fdtd_module.<camelCaseName>(**kwargs).launchRaw()``
+(witwin/maxwell/fdtd/cuda/backend.py:73-115, name table :3583-).  This module
+exposes the same names and keyword arguments for the forward hot-path ops, so a
+reference solver can be re-pointed op by op (``solver.fdtd_module =
+NativeFDTDModule()``).  Tensors must be float32 (index tensors int32/int64),
+contiguous and on one CUDA device; every launch goes on torch's current stream
+of that device, as in the reference (launch.h:14-20).  Unknown names raise
+AttributeError, invalid arguments raise ValueError, as the reference does.
+"""
+from __future__ import annotations
+
+import ctypes
+
+import torch
+
+from . import _lib
+
+_AXIS = {"x": 0, "y": 1, "z": 2}
+# component -> (a-axis, b-axis, first source, second source)
+_H_SPEC = {"Hx": ("y", "z", "Ey", "Ez"), "Hy": ("x", "z", "Ex", "Ez"), "Hz": ("x", "y", "Ex", "Ey")}
+_E_SPEC = {"Ex": ("y", "z", "Hy", "Hz"), "Ey": ("x", "z", "Hx", "Hz"), "Ez": ("x", "y", "Hx", "Hy")}
+
+
+def _check_tensor(t: torch.Tensor, name: str, dtype=torch.float32) -> None:
+    if not isinstance(t, torch.Tensor):
+        raise ValueError(f"{name} must be a tensor")
+    if t.device.type != "cuda":
+        raise ValueError(f"{name} must be a CUDA tensor")
+    if t.dtype != dtype:
+        raise ValueError(f"{name} must be {dtype}")
+    if not t.is_contiguous():
+        raise ValueError(f"{name} must be contiguous")
+
+
+def _stream(t: torch.Tensor) -> ctypes.c_void_p:
+    return ctypes.c_void_p(torch.cuda.current_stream(t.device).cuda_stream)
+
+
+def _uniform(value, tensor):
+    """(pointer, scalar) for an optional uniform coefficient (common.cuh:16-44)."""
+    if value is None:
+        return _lib.ptr(tensor), 0.0
+    return None, float(value)
+
+
+def _magnetic(comp: str, mode: int):
+    A, B, first, second = _H_SPEC[comp]
+    U, V = A.upper(), B.upper()
+
+    def run(**kw):
+        field = kw[comp]
+        for key in (comp, first, second, f"{comp}Decay", f"{comp}Curl"):
+            _check_tensor(kw[key], key)
+        nx, ny, nz = field.shape
+        dec_p, dec_u = _uniform(kw.get("uniformDecay"), kw[f"{comp}Decay"])
+        cur_p, cur_u = _uniform(kw.get("uniformCurl"), kw[f"{comp}Curl"])
+        psi_a = psi_b = ika = ba = ca = ikb = bb = cb = None
+        slab = None
+        if mode:
+            psi_a, psi_b = kw[f"Psi{comp}{U}"], kw[f"Psi{comp}{V}"]
+            ika, ba, ca = kw[f"InvKappa{comp}{U}"], kw[f"By{comp}{U}"], kw[f"Cy{comp}{U}"]
+            ikb, bb, cb = kw[f"InvKappa{comp}{V}"], kw[f"By{comp}{V}"], kw[f"Cy{comp}{V}"]
+            for t, n in ((psi_a, "psi_a"), (psi_b, "psi_b")):
+                _check_tensor(t, n)
+        if mode == 2:
+            slab = _lib.int_array([
+                kw[f"psi{comp}{U}LowLength"], kw[f"psi{comp}{U}HighStart"], kw[f"psi{comp}{U}HighLength"],
+                kw[f"psi{comp}{V}LowLength"], kw[f"psi{comp}{V}HighStart"], kw[f"psi{comp}{V}HighLength"],
+            ])
+        lib = _lib.load()
+        _lib.check(lib.fdtd_op_update_magnetic(
+            "xyz".index(comp[1]), mode, nx, ny, nz, _lib.ptr(field), _lib.ptr(kw[first]), _lib.ptr(kw[second]),
+            dec_p, cur_p, dec_u, cur_u, _lib.ptr(kw[f"invD{A}"]), _lib.ptr(kw[f"invD{B}"]), _lib.ptr(psi_a),
+            _lib.ptr(psi_b), _lib.ptr(ika), _lib.ptr(ba), _lib.ptr(ca), _lib.ptr(ikb), _lib.ptr(bb), _lib.ptr(cb),
+            slab, _stream(field)), f"update magnetic {comp}")
+
+    return run
+
+
+def _electric(comp: str, mode: int):
+    A, B, first, second = _E_SPEC[comp]
+    U, V = A.upper(), B.upper()
+
+    def run(**kw):
+        field = kw[comp]
+        for key in (comp, first, second, f"{comp}Decay", f"{comp}Curl"):
+            _check_tensor(kw[key], key)
+        nx, ny, nz = field.shape
+        dec_p, dec_u = _uniform(kw.get("uniformDecay"), kw[f"{comp}Decay"])
+        cur_p, cur_u = _uniform(kw.get("uniformCurl"), kw[f"{comp}Curl"])
+        modes = _lib.int_array([kw[f"{A}LowBoundaryMode"], kw[f"{A}HighBoundaryMode"],
+                                kw[f"{B}LowBoundaryMode"], kw[f"{B}HighBoundaryMode"]])
+        psi_a = psi_b = ika = ba = ca = ikb = bb = cb = None
+        slab = None
+        if mode:
+            psi_a, psi_b = kw[f"Psi{comp}{U}"], kw[f"Psi{comp}{V}"]
+            ika, ba, ca = kw[f"InvKappa{comp}{U}"], kw[f"B{comp}{U}"], kw[f"C{comp}{U}"]
+            ikb, bb, cb = kw[f"InvKappa{comp}{V}"], kw[f"B{comp}{V}"], kw[f"C{comp}{V}"]
+        if mode == 2:
+            slab = _lib.int_array([
+                kw[f"psi{comp}{U}LowLength"], kw[f"psi{comp}{U}HighStart"], kw[f"psi{comp}{U}HighLength"],
+                kw[f"psi{comp}{V}LowLength"], kw[f"psi{comp}{V}HighStart"], kw[f"psi{comp}{V}HighLength"],
+            ])
+        lib = _lib.load()
+        _lib.check(lib.fdtd_op_update_electric(
+            "xyz".index(comp[1]), mode, nx, ny, nz, _lib.ptr(field), _lib.ptr(kw[first]), _lib.ptr(kw[second]),
+            dec_p, cur_p, dec_u, cur_u, _lib.ptr(kw[f"invD{A}"]), _lib.ptr(kw[f"invD{B}"]), modes, _lib.ptr(psi_a),
+            _lib.ptr(psi_b), _lib.ptr(ika), _lib.ptr(ba), _lib.ptr(ca), _lib.ptr(ikb), _lib.ptr(bb), _lib.ptr(cb),
+            slab, _stream(field)), f"update electric {comp}")
+
+    return run
+
+
+def _debye(*, ElectricField, Polarization, PolarizationCurrent, DebyeDrive, decay, dt):
+    _lib.check(_lib.load().fdtd_op_update_debye(ElectricField.numel(), _lib.ptr(ElectricField), _lib.ptr(DebyeDrive),
+                                                float(decay), float(dt), _lib.ptr(Polarization),
+                                                _lib.ptr(PolarizationCurrent), _stream(ElectricField)), "debye")
+
+
+def _drude(*, ElectricField, PolarizationCurrent, DrudeDrive, decay):
+    _lib.check(_lib.load().fdtd_op_update_drude(ElectricField.numel(), _lib.ptr(ElectricField), _lib.ptr(DrudeDrive),
+                                                float(decay), _lib.ptr(PolarizationCurrent), _stream(ElectricField)), "drude")
+
+
+def _lorentz(*, ElectricField, Polarization, PolarizationCurrent, LorentzDrive, decay, restoring, dt):
+    _lib.check(_lib.load().fdtd_op_update_lorentz(ElectricField.numel(), _lib.ptr(ElectricField), _lib.ptr(LorentzDrive),
+                                                  float(decay), float(restoring), float(dt), _lib.ptr(Polarization),
+                                                  _lib.ptr(PolarizationCurrent), _stream(ElectricField)), "lorentz")
+
+
+def _apply_polarization(*, ElectricField, PolarizationCurrent, InvPermittivity, dt):
+    _lib.check(_lib.load().fdtd_op_apply_polarization(ElectricField.numel(), _lib.ptr(PolarizationCurrent),
+                                                      _lib.ptr(InvPermittivity), float(dt), _lib.ptr(ElectricField),
+                                                      _stream(ElectricField)), "apply polarization")
+
+
+def _add_source_patch(*, field, sourcePatch, offsetI, offsetJ, offsetK, signal):
+    _check_tensor(field, "field")
+    _check_tensor(sourcePatch, "sourcePatch")
+    _lib.check(_lib.load().fdtd_op_add_source_patch(
+        _lib.ptr(field), _lib.int_array(field.shape), _lib.ptr(sourcePatch), _lib.int_array(sourcePatch.shape),
+        _lib.int_array([offsetI, offsetJ, offsetK]), float(signal), _stream(field)), "add source patch")
+
+
+def _add_line_patch(*, field, coeffPatch, incidentField, sampleIndices, sampleAxisCode, offsetI, offsetJ, offsetK, scale):
+    _check_tensor(field, "field")
+    idx = sampleIndices.to(dtype=torch.int64).contiguous()
+    _lib.check(_lib.load().fdtd_op_add_line_patch(
+        _lib.ptr(field), _lib.int_array(field.shape), _lib.ptr(coeffPatch), _lib.int_array(coeffPatch.shape),
+        _lib.int_array([offsetI, offsetJ, offsetK]), _lib.ptr(incidentField), _lib.ptr(idx), int(sampleAxisCode),
+        float(scale), _stream(field)), "add line patch")
+
+
+def _aux_magnetic(*, Magnetic, Electric, MagneticDecay, MagneticCurl):
+    _lib.check(_lib.load().fdtd_op_aux_magnetic(Electric.numel(), _lib.ptr(Magnetic), _lib.ptr(Electric),
+                                                _lib.ptr(MagneticDecay), _lib.ptr(MagneticCurl), _stream(Magnetic)), "aux H")
+
+
+def _aux_electric(*, Electric, Magnetic, ElectricDecay, ElectricCurl, sourceIndex, sourceValue):
+    _lib.check(_lib.load().fdtd_op_aux_electric(Electric.numel(), _lib.ptr(Electric), _lib.ptr(Magnetic),
+                                                _lib.ptr(ElectricDecay), _lib.ptr(ElectricCurl), int(sourceIndex),
+                                                float(sourceValue), _stream(Electric)), "aux E")
+
+
+def _point_observers(*, field, pointI, pointJ, pointK, realAccum, imagAccum, weightedCos, weightedSin):
+    pi, pj, pk = (t.to(dtype=torch.int32).contiguous() for t in (pointI, pointJ, pointK))
+    _lib.check(_lib.load().fdtd_op_point_observers(
+        _lib.ptr(field), _lib.int_array(field.shape), int(pi.numel()), _lib.ptr(pi), _lib.ptr(pj), _lib.ptr(pk),
+        _lib.ptr(realAccum), _lib.ptr(imagAccum), float(weightedCos), float(weightedSin), _stream(field)), "point observers")
+
+
+def _plane_observer(*, field, planeRealAccum, planeImagAccum, axisCode, planeIndex, weightedCos, weightedSin):
+    _lib.check(_lib.load().fdtd_op_plane_observer(
+        _lib.ptr(field), _lib.int_array(field.shape), int(axisCode), int(planeIndex), _lib.ptr(planeRealAccum),
+        _lib.ptr(planeImagAccum), float(weightedCos), float(weightedSin), _stream(field)), "plane observer")
+
+
+def _dft_batched(*, Ex, Ey, Ez, ExRealAccum, ExImagAccum, EyRealAccum, EyImagAccum, EzRealAccum, EzImagAccum,
+                 weightedCos, weightedSin):
+    lib = _lib.load()
+    nf = int(weightedCos.numel())
+    for f, re, im in ((Ex, ExRealAccum, ExImagAccum), (Ey, EyRealAccum, EyImagAccum), (Ez, EzRealAccum, EzImagAccum)):
+        _lib.check(lib.fdtd_op_dft_volume(f.numel(), nf, _lib.ptr(f), _lib.ptr(re), _lib.ptr(im), _lib.ptr(weightedCos),
+                                          _lib.ptr(weightedSin), _stream(f)), "running DFT")
+
+
+def _clamp_face(*, field, axis, side):
+    _lib.check(_lib.load().fdtd_op_clamp_face(_lib.ptr(field), _lib.int_array(field.shape), int(axis), int(side),
+                                              _stream(field)), "clamp face")
+
+
+_KERNELS = {}
+for _c in ("Hx", "Hy", "Hz"):
+    _KERNELS[f"updateMagneticField{_c}Standard3D"] = _magnetic(_c, 0)
+    _KERNELS[f"updateMagneticField{_c}3D"] = _magnetic(_c, 1)
+    _KERNELS[f"updateMagneticField{_c}CpmlCompressed3D"] = _magnetic(_c, 2)
+for _c in ("Ex", "Ey", "Ez"):
+    _KERNELS[f"updateElectricField{_c}Standard3D"] = _electric(_c, 0)
+    _KERNELS[f"updateElectricField{_c}Cpml3D"] = _electric(_c, 1)
+    _KERNELS[f"updateElectricField{_c}CpmlCompressed3D"] = _electric(_c, 2)
+_KERNELS.update({
+    "updateDebyeCurrent3D": _debye,
+    "updateDrudeCurrent3D": _drude,
+    "updateLorentzCurrent3D": _lorentz,
+    "applyPolarizationCurrent3D": _apply_polarization,
+    "addSourcePatch3D": _add_source_patch,
+    "addScaledLineSourcePatch3D": _add_line_patch,
+    "updateAuxiliaryMagnetic1D": _aux_magnetic,
+    "updateAuxiliaryElectric1D": _aux_electric,
+    "accumulatePointObservers3D": _point_observers,
+    "accumulatePlaneObserver3D": _plane_observer,
+    "accumulateRunningDftYee3DBatched": _dft_batched,
+    "clampFieldFace3D": _clamp_face,
+})
+
+
+class _Launch:
+    __slots__ = ("kernel", "kwargs")
+
+    def __init__(self, kernel, kwargs):
+        self.kernel = kernel
+        self.kwargs = kwargs
+
+    def launchRaw(self):  # noqa: N802 - the reference's kernel-module API
+        # Strided views are made contiguous and written back, as the reference
+        # does for its in-place kernels (backend.py:54-70).
+        write_back = []
+        kwargs = dict(self.kwargs)
+        for key, value in kwargs.items():
+            if isinstance(value, torch.Tensor) and not value.is_contiguous():
+                contiguous = value.contiguous()
+                kwargs[key] = contiguous
+                write_back.append((value, contiguous))
+        self.kernel(**kwargs)
+        for original, contiguous in write_back:
+            original.copy_(contiguous)
+
+
+class NativeFDTDModule:
+    """``fdtd_module`` drop-in: ``module.<name>(**kwargs).launchRaw()``."""
+
+    def __getattr__(self, name: str):
+        kernel = _KERNELS.get(name)
+        if kernel is None:
+            raise AttributeError(f"B200 FDTD backend does not implement kernel {name!r}.")
+
+        def bind(**kwargs):
+            return _Launch(kernel, kwargs)
+
+        bind.__name__ = name
+        object.__setattr__(self, name, bind)
+        return bind
+
+
+def get_native_fdtd_module() -> NativeFDTDModule:
+    if not torch.cuda.is_available():
+        raise RuntimeError("the B200 FDTD backend requires a CUDA device")
+    _lib.load()
+    return NativeFDTDModule()

@@ -1,0 +1,1101 @@
+// Host side of the fused step engine and its C ABI (include/fdtd_b200.h).
+//
+// The engine owns its device state in an internal padded layout: every field
+// component lives in an [NX][NY][P] array (P = NZ rounded up to a multiple of
+// 4 so each z row starts on a 16-byte boundary and can be read as float4),
+// cells outside a component's Yee extent are held at zero.  CPML psi arrays
+// are kept only on their slabs; ADE state only on the pole boxes.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/fdtd_b200.h"
+#include "engine.cuh"
+
+namespace fdtdb200 {
+__global__ void fused_step_kernel(const StepParams p, int n, int slot);
+}
+
+using namespace fdtdb200;
+
+namespace {
+
+thread_local std::string g_last_error;
+
+int fail(int code, const std::string& msg) {
+  g_last_error = msg;
+  return code;
+}
+
+}  // namespace
+
+void fdtdb200::set_last_error(const std::string& msg) { g_last_error = msg; }
+
+namespace {
+
+int cuda_fail(cudaError_t err, const char* what) {
+  return fail(FDTD_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(err));
+}
+
+#define CUDA_TRY(expr)                              \
+  do {                                              \
+    cudaError_t err__ = (expr);                     \
+    if (err__ != cudaSuccess) return cuda_fail(err__, #expr); \
+  } while (0)
+
+int axis_a(int comp) { return comp == 0 ? 1 : 0; }
+int axis_b(int comp) { return comp == 2 ? 1 : 2; }
+
+// Yee extent of component comp (0..2 E, 3..5 H) on a node grid.
+void comp_extent(int comp, int NX, int NY, int NZ, int ext[3]) {
+  const int c = comp % 3;
+  const bool is_h = comp >= 3;
+  int n[3] = {NX, NY, NZ};
+  for (int a = 0; a < 3; ++a) {
+    // E component c is half-cell (N-1) along its own axis; H component c is
+    // half-cell along the two other axes.
+    const bool half = is_h ? (a != c) : (a == c);
+    ext[a] = half ? n[a] - 1 : n[a];
+  }
+}
+
+__global__ void pack_kernel(float* dst, const float* src, int sx, int sy, int sz, int NY, int P) {
+  const int64_t total = static_cast<int64_t>(sx) * sy * sz;
+  for (int64_t x = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; x < total;
+       x += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    const int k = static_cast<int>(x % sz);
+    const int64_t r = x / sz;
+    const int j = static_cast<int>(r % sy);
+    const int i = static_cast<int>(r / sy);
+    dst[(static_cast<int64_t>(i) * NY + j) * P + k] = src[x];
+  }
+}
+
+__global__ void unpack_kernel(float* dst, const float* src, int sx, int sy, int sz, int NY, int P) {
+  const int64_t total = static_cast<int64_t>(sx) * sy * sz;
+  for (int64_t x = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; x < total;
+       x += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    const int k = static_cast<int>(x % sz);
+    const int64_t r = x / sz;
+    const int j = static_cast<int>(r % sy);
+    const int i = static_cast<int>(r / sy);
+    dst[x] = src[(static_cast<int64_t>(i) * NY + j) * P + k];
+  }
+}
+
+// Precompute the history of a 1-D incident line (one block, sequential in time).
+// Restates AuxiliaryGrid1D.advance_magnetic / advance_electric,
+// witwin/maxwell/fdtd/excitation/spatial.py:443-462 and sources.cu:803-839.
+__global__ void aux_history_kernel(int ne, const float* e_decay, const float* e_curl, const float* h_decay,
+                                   const float* h_curl, int src_index, const float* source, int n_steps,
+                                   float* e_hist, float* h_hist, float* e, float* h) {
+  for (int x = threadIdx.x; x < ne; x += blockDim.x) {
+    e[x] = 0.0f;
+    if (x < ne - 1) h[x] = 0.0f;
+  }
+  __syncthreads();
+  for (int n = 0; n < n_steps; ++n) {
+    for (int x = threadIdx.x; x < ne; x += blockDim.x) e_hist[static_cast<int64_t>(n) * ne + x] = e[x];
+    for (int x = threadIdx.x; x < ne - 1; x += blockDim.x) h[x] = h_decay[x] * h[x] - h_curl[x] * (e[x + 1] - e[x]);
+    __syncthreads();
+    for (int x = threadIdx.x; x < ne - 1; x += blockDim.x) h_hist[static_cast<int64_t>(n) * ne + x] = h[x];
+    for (int x = threadIdx.x; x < ne; x += blockDim.x) {
+      if (x >= 1 && x < ne - 1 && x != src_index) e[x] = e_decay[x] * e[x] - e_curl[x] * (h[x] - h[x - 1]);
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      e[ne - 1] = 0.0f;
+      if (src_index >= 0 && src_index < ne) e[src_index] = source[n];
+    }
+    __syncthreads();
+  }
+}
+
+// DFT weights in FP64: phase = omega * (n [- 1/2]) * dt reduced modulo 2*pi in
+// double precision, window applied, stored as float2 (cos, sin).
+__global__ void dft_weight_kernel(int n_freq, int n_steps, const double* omega, const double* window, double dt,
+                                  float2* w_e, float2* w_h) {
+  const int64_t total = static_cast<int64_t>(n_freq) * n_steps;
+  const double two_pi = 6.283185307179586476925286766559;
+  for (int64_t x = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; x < total;
+       x += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    const int n = static_cast<int>(x / n_freq);
+    const int f = static_cast<int>(x % n_freq);
+    const double w = window[n];
+    double pe = fmod(omega[f] * dt * static_cast<double>(n), two_pi);
+    double ph = fmod(omega[f] * dt * (static_cast<double>(n) - 0.5), two_pi);
+    double se, ce, sh, ch;
+    sincos(pe, &se, &ce);
+    sincos(ph, &sh, &ch);
+    w_e[x] = make_float2(static_cast<float>(w * ce), static_cast<float>(w * se));
+    w_h[x] = make_float2(static_cast<float>(w * ch), static_cast<float>(w * sh));
+  }
+}
+
+struct RegionFlush {
+  int64_t base;
+  int64_t count;
+  int is_h;
+};
+
+// acc[f][slot] += sum_m sample[m][slot] * w[n_base + m][f], with Kahan
+// compensation of the accumulator update.
+__global__ void dft_flush_kernel(const float* samples, int64_t n_samples, int cnt, int n_base, int n_freq,
+                                 const float2* w_e, const float2* w_h, const RegionFlush* regions,
+                                 float* acc_re, float* acc_im, float* cmp_re, float* cmp_im) {
+  extern __shared__ float2 sw[];  // [cnt][n_freq]
+  const RegionFlush rg = regions[blockIdx.y];
+  const float2* w = rg.is_h ? w_h : w_e;
+  for (int x = threadIdx.x; x < cnt * n_freq; x += blockDim.x) {
+    sw[x] = w[static_cast<int64_t>(n_base) * n_freq + x];
+  }
+  __syncthreads();
+  for (int64_t p = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; p < rg.count;
+       p += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    const int64_t slot = rg.base + p;
+    float s[64];
+#pragma unroll 8
+    for (int m = 0; m < cnt; ++m) s[m] = samples[static_cast<int64_t>(m) * n_samples + slot];
+    for (int f = 0; f < n_freq; ++f) {
+      float re = 0.0f, im = 0.0f;
+#pragma unroll 8
+      for (int m = 0; m < cnt; ++m) {
+        const float2 ww = sw[m * n_freq + f];
+        re = fmaf(s[m], ww.x, re);
+        im = fmaf(s[m], ww.y, im);
+      }
+      const int64_t a = static_cast<int64_t>(f) * n_samples + slot;
+      {
+        const float y = re - cmp_re[a];
+        const float t = acc_re[a] + y;
+        cmp_re[a] = (t - acc_re[a]) - y;
+        acc_re[a] = t;
+      }
+      {
+        const float y = im - cmp_im[a];
+        const float t = acc_im[a] + y;
+        cmp_im[a] = (t - acc_im[a]) - y;
+        acc_im[a] = t;
+      }
+    }
+  }
+}
+
+}  // namespace
+
+struct DevBuf {
+  float* ptr = nullptr;
+  size_t n = 0;
+};
+
+struct PoleHost {
+  PoleTerm t;
+  float *drive = nullptr, *inv_eps = nullptr, *pol = nullptr, *cur = nullptr;
+  int64_t count = 0;
+};
+
+struct AuxLine {
+  int ne = 0, n_steps = 0;
+  float* e_hist = nullptr;
+  float* h_hist = nullptr;
+};
+
+struct Checkpoint {
+  std::vector<float*> bufs;
+  bool valid = false;
+};
+
+struct fdtd_engine {
+  fdtd_grid_desc desc{};
+  cudaStream_t stream = nullptr;
+  int NX = 0, NY = 0, NZ = 0, P = 0, SZ = 0;
+  int64_t plane = 0, vol = 0;
+  int TY = 0, CX = 0;
+  int cur = 0;  // index of the buffer holding the current state
+  float* E[2][3] = {};
+  float* H[2][3] = {};
+  float* psiE[3][2] = {};
+  float* psiH[2][3][2] = {};
+  int64_t psi_count[3] = {0, 0, 0};  // per axis element count of one slab array
+  float* ecoef[6][2] = {};           // [comp][decay, curl] padded arrays (nullptr = uniform)
+  float ucoef[6][2] = {};
+  float* inv_e[3] = {};
+  float* inv_h[3] = {};
+  float* eb[3] = {};
+  float* ec[3] = {};
+  float* eik[3] = {};
+  float* hb[3] = {};
+  float* hc[3] = {};
+  float* hik[3] = {};
+  bool cpml = false;
+  std::vector<InjectionTerm> terms;
+  std::vector<float*> owned;
+  std::vector<PoleHost> poles;
+  std::vector<SampleRegion> regions;
+  std::vector<AuxLine> lines;
+  int64_t n_samples = 0, n_samples_e = 0;
+  // device tables
+  InjectionTerm* d_terms = nullptr;
+  int* d_term_ptr = nullptr;
+  int* d_term_ids = nullptr;
+  PoleTerm* d_poles = nullptr;
+  SampleRegion* d_regions = nullptr;
+  int* d_region_ptr = nullptr;
+  int* d_region_ids = nullptr;
+  RegionFlush* d_flush = nullptr;
+  int n_flush = 0;
+  int64_t max_region = 0;
+  float* samples = nullptr;
+  int M = 32;
+  int pending = 0;
+  int pending_base = 0;
+  // DFT
+  int n_freq = 0, dft_steps = 0;
+  float2* w_e = nullptr;
+  float2* w_h = nullptr;
+  float *acc_re = nullptr, *acc_im = nullptr, *cmp_re = nullptr, *cmp_im = nullptr;
+  bool finalized = false;
+  int64_t launches = 0;
+  float last_ms = 0.0f;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  std::vector<Checkpoint> checkpoints;
+};
+
+namespace {
+
+int dev_alloc(fdtd_engine* h, float** out, size_t n) {
+  if (n == 0) {
+    *out = nullptr;
+    return 0;
+  }
+  CUDA_TRY(cudaMalloc(out, n * sizeof(float)));
+  CUDA_TRY(cudaMemsetAsync(*out, 0, n * sizeof(float), h->stream));
+  h->owned.push_back(*out);
+  return 0;
+}
+
+int dev_copy(fdtd_engine* h, float** out, const float* src, size_t n) {
+  int rc = dev_alloc(h, out, n);
+  if (rc) return rc;
+  if (n) CUDA_TRY(cudaMemcpyAsync(*out, src, n * sizeof(float), cudaMemcpyDefault, h->stream));
+  return 0;
+}
+
+int64_t slab_elems(const fdtd_engine* h, int axis) {
+  const int L = h->desc.pml_lo[axis] + h->desc.pml_hi[axis];
+  if (L == 0) return 0;
+  if (axis == 0) return static_cast<int64_t>(L) * h->NY * h->P;
+  if (axis == 1) return static_cast<int64_t>(h->NX) * L * h->P;
+  return static_cast<int64_t>(h->NX) * h->NY * L;
+}
+
+bool box_ok(const fdtd_engine* h, int comp, const int* box) {
+  int ext[3];
+  comp_extent(comp, h->NX, h->NY, h->NZ, ext);
+  for (int a = 0; a < 3; ++a) {
+    if (box[2 * a] < 0 || box[2 * a + 1] > ext[a] || box[2 * a] >= box[2 * a + 1]) return false;
+  }
+  return true;
+}
+
+void fill_params(const fdtd_engine* h, StepParams& p) {
+  std::memset(&p, 0, sizeof(p));
+  p.NX = h->NX;
+  p.NY = h->NY;
+  p.NZ = h->NZ;
+  p.P = h->P;
+  p.SZ = h->SZ;
+  p.TY = h->TY;
+  p.CX = h->CX;
+  p.Q = h->P / 4;
+  p.ROWS = h->TY + 2;
+  const int src = h->cur, dst = 1 - h->cur;
+  for (int c = 0; c < 3; ++c) {
+    p.Ein[c] = h->E[src][c];
+    p.Eout[c] = h->E[dst][c];
+    p.Hin[c] = h->H[src][c];
+    p.Hout[c] = h->H[dst][c];
+    p.edecay[c] = h->ecoef[c][0];
+    p.ecurl[c] = h->ecoef[c][1];
+    p.edecay_u[c] = h->ucoef[c][0];
+    p.ecurl_u[c] = h->ucoef[c][1];
+    p.hdecay[c] = h->ecoef[3 + c][0];
+    p.hcurl[c] = h->ecoef[3 + c][1];
+    p.hdecay_u[c] = h->ucoef[3 + c][0];
+    p.hcurl_u[c] = h->ucoef[3 + c][1];
+    p.inv_e[c] = h->inv_e[c];
+    p.inv_h[c] = h->inv_h[c];
+    p.eb[c] = h->eb[c];
+    p.ec[c] = h->ec[c];
+    p.eik[c] = h->eik[c];
+    p.hb[c] = h->hb[c];
+    p.hc[c] = h->hc[c];
+    p.hik[c] = h->hik[c];
+    p.slab_lo[c] = h->desc.pml_lo[c];
+    p.slab_hi[c] = h->desc.pml_hi[c];
+    for (int w = 0; w < 2; ++w) {
+      p.psiE[c][w] = h->psiE[c][w];
+      p.psiHin[c][w] = h->psiH[src][c][w];
+      p.psiHout[c][w] = h->psiH[dst][c][w];
+    }
+  }
+  for (int f = 0; f < 6; ++f) p.bnd[f] = h->desc.boundary[f];
+  p.cpml = h->cpml ? 1 : 0;
+  p.terms = h->d_terms;
+  p.term_plane_ptr = h->d_term_ptr;
+  p.term_plane_ids = h->d_term_ids;
+  p.n_terms = static_cast<int>(h->terms.size());
+  p.poles = h->d_poles;
+  p.n_poles = static_cast<int>(h->poles.size());
+  p.regions = h->d_regions;
+  p.region_plane_ptr = h->d_region_ptr;
+  p.region_plane_ids = h->d_region_ids;
+  p.n_regions = static_cast<int>(h->regions.size());
+  p.samples = h->samples;
+  p.n_samples = h->n_samples;
+  p.sample_block = h->M;
+}
+
+size_t smem_bytes(int TY, int P) { return sizeof(float) * 6 * static_cast<size_t>(TY + 2) * (P + 8); }
+int block_threads(int TY, int P) { return ((TY + 2) * (P / 4) + 31) / 32 * 32; }
+
+bool tile_fits(int TY, int P) {
+  return TY >= 1 && block_threads(TY, P) <= 512 && smem_bytes(TY, P) <= 200 * 1024;
+}
+
+void default_tiles(fdtd_engine* h) {
+  const int Q = h->P / 4;
+  int TY = h->desc.tile_rows;
+  if (TY <= 0) {
+    TY = std::max(1, 512 / Q - 2);
+    TY = std::min(TY, std::max(1, h->NY));
+  }
+  while (TY > 1 && !tile_fits(TY, h->P)) --TY;
+  int CX = h->desc.chunk_planes;
+  if (CX <= 0) {
+    // Aim for about 4 CTAs per SM over the whole grid.
+    const int ny_tiles = (h->NY + TY - 1) / TY;
+    const int want_chunks = std::max(1, (148 * 4 + ny_tiles - 1) / ny_tiles);
+    CX = std::max(8, (h->NX + want_chunks - 1) / want_chunks);
+  }
+  h->TY = TY;
+  h->CX = CX;
+}
+
+int launch_step(fdtd_engine* h, int n, int slot) {
+  StepParams p;
+  fill_params(h, p);
+  const dim3 grid((h->NY + h->TY - 1) / h->TY, (h->NX + h->CX - 1) / h->CX);
+  const int threads = block_threads(h->TY, h->P);
+  const size_t smem = smem_bytes(h->TY, h->P);
+  fused_step_kernel<<<grid, threads, smem, h->stream>>>(p, n, slot);
+  cudaError_t err = cudaGetLastError();
+  if (err != cudaSuccess) return cuda_fail(err, "fused_step_kernel launch");
+  ++h->launches;
+  h->cur = 1 - h->cur;
+  return 0;
+}
+
+int flush_samples(fdtd_engine* h) {
+  if (h->pending == 0) return 0;
+  if (h->n_freq > 0 && h->n_flush > 0 && h->n_samples > 0) {
+    if (h->pending_base + h->pending > h->dft_steps)
+      return fail(FDTD_ERR_STATE, "DFT weight table shorter than the stepped range");
+    const int threads = 256;
+    const int gx = static_cast<int>(std::min<int64_t>((h->max_region + threads - 1) / threads, 4096));
+    const dim3 grid(std::max(gx, 1), h->n_flush);
+    const size_t smem = sizeof(float2) * static_cast<size_t>(h->pending) * h->n_freq;
+    dft_flush_kernel<<<grid, threads, smem, h->stream>>>(h->samples, h->n_samples, h->pending, h->pending_base,
+                                                           h->n_freq, h->w_e, h->w_h, h->d_flush, h->acc_re,
+                                                           h->acc_im, h->cmp_re, h->cmp_im);
+    cudaError_t err = cudaGetLastError();
+    if (err != cudaSuccess) return cuda_fail(err, "dft_flush_kernel launch");
+    ++h->launches;
+  }
+  h->pending_base += h->pending;
+  h->pending = 0;
+  return 0;
+}
+
+template <typename T>
+int upload_vec(fdtd_engine* h, T** dptr, const std::vector<T>& v) {
+  if (*dptr) cudaFree(*dptr);
+  *dptr = nullptr;
+  if (v.empty()) return 0;
+  CUDA_TRY(cudaMalloc(dptr, v.size() * sizeof(T)));
+  CUDA_TRY(cudaMemcpyAsync(*dptr, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice, h->stream));
+  return 0;
+}
+
+// CSR over x planes of the boxes [i0, i1).
+template <typename T>
+void build_plane_csr(int NX, const std::vector<T>& items, std::vector<int>& ptr, std::vector<int>& ids) {
+  ptr.assign(NX + 1, 0);
+  for (const auto& t : items)
+    for (int i = t.i0; i < t.i1; ++i) ptr[i + 1]++;
+  for (int i = 0; i < NX; ++i) ptr[i + 1] += ptr[i];
+  ids.assign(ptr[NX], 0);
+  std::vector<int> fill(ptr.begin(), ptr.end() - 1);
+  for (size_t x = 0; x < items.size(); ++x)
+    for (int i = items[x].i0; i < items[x].i1; ++i) ids[fill[i]++] = static_cast<int>(x);
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* fdtd_last_error(void) { return g_last_error.c_str(); }
+const char* fdtd_version(void) { return "fdtd_b200 0.1.0 (sm_100a)"; }
+
+int fdtd_engine_create(const fdtd_grid_desc* desc, void* stream, fdtd_engine** out) {
+  if (!desc || !out) return fail(FDTD_ERR_INVALID_ARG, "null descriptor or output pointer");
+  *out = nullptr;
+  if (desc->nx < 3 || desc->ny < 3 || desc->nz < 3)
+    return fail(FDTD_ERR_INVALID_ARG, "grid needs at least 3 nodes per axis");
+  if (!(desc->dt > 0.0)) return fail(FDTD_ERR_INVALID_ARG, "dt must be positive");
+  for (int f = 0; f < 6; ++f) {
+    const int b = desc->boundary[f];
+    if (b != FDTD_BND_NONE && b != FDTD_BND_PML && b != FDTD_BND_PEC)
+      return fail(FDTD_ERR_UNSUPPORTED,
+                  "fused engine supports NONE, PML and PEC faces; periodic, Bloch and PMC faces use the per-op path");
+  }
+  const int n[3] = {desc->nx, desc->ny, desc->nz};
+  for (int a = 0; a < 3; ++a) {
+    if (desc->pml_lo[a] < 0 || desc->pml_hi[a] < 0 || desc->pml_lo[a] + desc->pml_hi[a] > n[a] - 1)
+      return fail(FDTD_ERR_INVALID_ARG, "CPML slab lengths exceed the axis");
+  }
+  fdtd_engine* h = new fdtd_engine();
+  h->desc = *desc;
+  h->stream = static_cast<cudaStream_t>(stream);
+  h->NX = desc->nx;
+  h->NY = desc->ny;
+  h->NZ = desc->nz;
+  h->P = (desc->nz + 3) / 4 * 4;
+  h->SZ = desc->pml_lo[2] + desc->pml_hi[2];
+  h->plane = static_cast<int64_t>(h->NY) * h->P;
+  h->vol = h->plane * h->NX;
+  h->M = desc->sample_block > 0 ? std::min(desc->sample_block, 64) : 32;
+  h->cpml = false;
+  for (int a = 0; a < 3; ++a)
+    if (desc->pml_lo[a] + desc->pml_hi[a] > 0) h->cpml = true;
+  if (!tile_fits(1, h->P)) {
+    delete h;
+    return fail(FDTD_ERR_UNSUPPORTED, "z extent too large for one CTA row");
+  }
+  int rc = 0;
+  for (int b = 0; b < 2 && !rc; ++b)
+    for (int c = 0; c < 3 && !rc; ++c) {
+      rc = dev_alloc(h, &h->E[b][c], h->vol);
+      if (!rc) rc = dev_alloc(h, &h->H[b][c], h->vol);
+    }
+  for (int c = 0; c < 3 && !rc; ++c) {
+    const int ax[2] = {axis_a(c), axis_b(c)};
+    for (int w = 0; w < 2 && !rc; ++w) {
+      const int64_t cnt = slab_elems(h, ax[w]);
+      rc = dev_alloc(h, &h->psiE[c][w], cnt);
+      if (!rc) rc = dev_alloc(h, &h->psiH[0][c][w], cnt);
+      if (!rc) rc = dev_alloc(h, &h->psiH[1][c][w], cnt);
+    }
+  }
+  for (int c = 0; c < 6; ++c) {
+    h->ucoef[c][0] = 1.0f;
+    h->ucoef[c][1] = 0.0f;
+  }
+  if (!rc) {
+    cudaError_t e1 = cudaEventCreate(&h->ev0);
+    cudaError_t e2 = cudaEventCreate(&h->ev1);
+    if (e1 != cudaSuccess || e2 != cudaSuccess) rc = cuda_fail(e1 != cudaSuccess ? e1 : e2, "cudaEventCreate");
+  }
+  if (rc) {
+    fdtd_engine_destroy(h);
+    return rc;
+  }
+  default_tiles(h);
+  *out = h;
+  return 0;
+}
+
+int fdtd_engine_destroy(fdtd_engine* h) {
+  if (!h) return 0;
+  cudaStreamSynchronize(h->stream);
+  for (float* p : h->owned) cudaFree(p);
+  for (auto& pl : h->poles) {
+    cudaFree(pl.drive);
+    cudaFree(pl.inv_eps);
+    cudaFree(pl.pol);
+    cudaFree(pl.cur);
+  }
+  for (auto& l : h->lines) {
+    cudaFree(l.e_hist);
+    cudaFree(l.h_hist);
+  }
+  for (auto& ck : h->checkpoints)
+    for (float* p : ck.bufs) cudaFree(p);
+  cudaFree(h->d_terms);
+  cudaFree(h->d_term_ptr);
+  cudaFree(h->d_term_ids);
+  cudaFree(h->d_poles);
+  cudaFree(h->d_regions);
+  cudaFree(h->d_region_ptr);
+  cudaFree(h->d_region_ids);
+  cudaFree(h->d_flush);
+  cudaFree(h->samples);
+  cudaFree(h->w_e);
+  cudaFree(h->w_h);
+  cudaFree(h->acc_re);
+  cudaFree(h->acc_im);
+  cudaFree(h->cmp_re);
+  cudaFree(h->cmp_im);
+  if (h->ev0) cudaEventDestroy(h->ev0);
+  if (h->ev1) cudaEventDestroy(h->ev1);
+  delete h;
+  return 0;
+}
+
+int fdtd_engine_set_spacing(fdtd_engine* h, int axis, const float* inv_e, const float* inv_h) {
+  if (!h || axis < 0 || axis > 2 || !inv_e || !inv_h) return fail(FDTD_ERR_INVALID_ARG, "bad spacing arguments");
+  const int n[3] = {h->NX, h->NY, h->NZ};
+  int rc = dev_copy(h, &h->inv_e[axis], inv_e, n[axis]);
+  if (!rc) rc = dev_copy(h, &h->inv_h[axis], inv_h, n[axis] - 1);
+  return rc;
+}
+
+int fdtd_engine_set_cpml(fdtd_engine* h, int axis, const float* b_e, const float* c_e, const float* ik_e,
+                         const float* b_h, const float* c_h, const float* ik_h) {
+  if (!h || axis < 0 || axis > 2 || !b_e || !c_e || !ik_e || !b_h || !c_h || !ik_h)
+    return fail(FDTD_ERR_INVALID_ARG, "bad CPML profile arguments");
+  const int n[3] = {h->NX, h->NY, h->NZ};
+  int rc = dev_copy(h, &h->eb[axis], b_e, n[axis]);
+  if (!rc) rc = dev_copy(h, &h->ec[axis], c_e, n[axis]);
+  if (!rc) rc = dev_copy(h, &h->eik[axis], ik_e, n[axis]);
+  if (!rc) rc = dev_copy(h, &h->hb[axis], b_h, n[axis] - 1);
+  if (!rc) rc = dev_copy(h, &h->hc[axis], c_h, n[axis] - 1);
+  if (!rc) rc = dev_copy(h, &h->hik[axis], ik_h, n[axis] - 1);
+  return rc;
+}
+
+int fdtd_engine_set_coefficients(fdtd_engine* h, int comp, const float* decay, float decay_uniform,
+                                 const float* curl, float curl_uniform) {
+  if (!h || comp < 0 || comp > 5) return fail(FDTD_ERR_INVALID_ARG, "bad coefficient arguments");
+  if (h->finalized) return fail(FDTD_ERR_STATE, "engine already finalized");
+  int ext[3];
+  comp_extent(comp, h->NX, h->NY, h->NZ, ext);
+  const float* src[2] = {decay, curl};
+  h->ucoef[comp][0] = decay_uniform;
+  h->ucoef[comp][1] = curl_uniform;
+  for (int w = 0; w < 2; ++w) {
+    if (!src[w]) {
+      h->ecoef[comp][w] = nullptr;
+      continue;
+    }
+    int rc = dev_alloc(h, &h->ecoef[comp][w], h->vol);
+    if (rc) return rc;
+    pack_kernel<<<1024, 256, 0, h->stream>>>(h->ecoef[comp][w], src[w], ext[0], ext[1], ext[2], h->NY, h->P);
+    CUDA_TRY(cudaGetLastError());
+  }
+  return 0;
+}
+
+int fdtd_engine_pack_field(fdtd_engine* h, int comp, const float* src) {
+  if (!h || comp < 0 || comp > 5 || !src) return fail(FDTD_ERR_INVALID_ARG, "bad pack arguments");
+  int ext[3];
+  comp_extent(comp, h->NX, h->NY, h->NZ, ext);
+  float* dst = comp < 3 ? h->E[h->cur][comp] : h->H[h->cur][comp - 3];
+  pack_kernel<<<1024, 256, 0, h->stream>>>(dst, src, ext[0], ext[1], ext[2], h->NY, h->P);
+  CUDA_TRY(cudaGetLastError());
+  return 0;
+}
+
+int fdtd_engine_unpack_field(fdtd_engine* h, int comp, float* dst) {
+  if (!h || comp < 0 || comp > 5 || !dst) return fail(FDTD_ERR_INVALID_ARG, "bad unpack arguments");
+  int ext[3];
+  comp_extent(comp, h->NX, h->NY, h->NZ, ext);
+  const float* src = comp < 3 ? h->E[h->cur][comp] : h->H[h->cur][comp - 3];
+  unpack_kernel<<<1024, 256, 0, h->stream>>>(dst, src, ext[0], ext[1], ext[2], h->NY, h->P);
+  CUDA_TRY(cudaGetLastError());
+  return 0;
+}
+
+static int psi_geometry(fdtd_engine* h, int comp, int which, float** buf, int shape[3], int* pitch_y,
+                        int* pitch_z) {
+  const int c = comp % 3;
+  const int axis = which == 0 ? axis_a(c) : axis_b(c);
+  int ext[3];
+  comp_extent(comp, h->NX, h->NY, h->NZ, ext);
+  const int L = h->desc.pml_lo[axis] + h->desc.pml_hi[axis];
+  shape[0] = ext[0];
+  shape[1] = ext[1];
+  shape[2] = ext[2];
+  shape[axis] = L;
+  *buf = comp < 3 ? h->psiE[c][which] : h->psiH[h->cur][c][which];
+  // internal pitches: x slab [L][NY][P], y slab [NX][L][P], z slab [NX][NY][L]
+  *pitch_y = axis == 1 ? L : h->NY;
+  *pitch_z = axis == 2 ? L : h->P;
+  return L;
+}
+
+int fdtd_engine_pack_psi(fdtd_engine* h, int comp, int which, const float* src) {
+  if (!h || comp < 0 || comp > 5 || which < 0 || which > 1 || !src)
+    return fail(FDTD_ERR_INVALID_ARG, "bad psi pack arguments");
+  float* buf;
+  int shape[3], py, pz;
+  if (psi_geometry(h, comp, which, &buf, shape, &py, &pz) == 0) return 0;
+  pack_kernel<<<1024, 256, 0, h->stream>>>(buf, src, shape[0], shape[1], shape[2], py, pz);
+  CUDA_TRY(cudaGetLastError());
+  return 0;
+}
+
+int fdtd_engine_unpack_psi(fdtd_engine* h, int comp, int which, float* dst) {
+  if (!h || comp < 0 || comp > 5 || which < 0 || which > 1 || !dst)
+    return fail(FDTD_ERR_INVALID_ARG, "bad psi unpack arguments");
+  float* buf;
+  int shape[3], py, pz;
+  if (psi_geometry(h, comp, which, &buf, shape, &py, &pz) == 0) return 0;
+  unpack_kernel<<<1024, 256, 0, h->stream>>>(dst, buf, shape[0], shape[1], shape[2], py, pz);
+  CUDA_TRY(cudaGetLastError());
+  return 0;
+}
+
+int fdtd_engine_add_pole(fdtd_engine* h, int comp, int kind, const int* box, const float* drive,
+                         const float* inv_eps, float decay, float restoring, int* pole_id) {
+  if (!h || comp < 0 || comp > 2 || kind < 0 || kind > 2 || !box || !drive || !inv_eps)
+    return fail(FDTD_ERR_INVALID_ARG, "bad pole arguments");
+  if (h->finalized) return fail(FDTD_ERR_STATE, "engine already finalized");
+  if (!box_ok(h, comp, box)) return fail(FDTD_ERR_INVALID_ARG, "pole box outside the component extent");
+  PoleHost ph;
+  ph.count = static_cast<int64_t>(box[1] - box[0]) * (box[3] - box[2]) * (box[5] - box[4]);
+  CUDA_TRY(cudaMalloc(&ph.drive, ph.count * sizeof(float)));
+  CUDA_TRY(cudaMalloc(&ph.inv_eps, ph.count * sizeof(float)));
+  CUDA_TRY(cudaMalloc(&ph.pol, ph.count * sizeof(float)));
+  CUDA_TRY(cudaMalloc(&ph.cur, ph.count * sizeof(float)));
+  CUDA_TRY(cudaMemcpyAsync(ph.drive, drive, ph.count * sizeof(float), cudaMemcpyDefault, h->stream));
+  CUDA_TRY(cudaMemcpyAsync(ph.inv_eps, inv_eps, ph.count * sizeof(float), cudaMemcpyDefault, h->stream));
+  CUDA_TRY(cudaMemsetAsync(ph.pol, 0, ph.count * sizeof(float), h->stream));
+  CUDA_TRY(cudaMemsetAsync(ph.cur, 0, ph.count * sizeof(float), h->stream));
+  PoleTerm& t = ph.t;
+  t.comp = comp;
+  t.kind = kind;
+  t.i0 = box[0];
+  t.i1 = box[1];
+  t.j0 = box[2];
+  t.j1 = box[3];
+  t.k0 = box[4];
+  t.k1 = box[5];
+  t.decay = decay;
+  t.restoring = restoring;
+  t.dt = static_cast<float>(h->desc.dt);
+  t.inv_dt = static_cast<float>(1.0 / h->desc.dt);
+  t.drive = ph.drive;
+  t.inv_eps = ph.inv_eps;
+  t.pol = ph.pol;
+  t.cur = ph.cur;
+  h->poles.push_back(ph);
+  if (pole_id) *pole_id = static_cast<int>(h->poles.size()) - 1;
+  return 0;
+}
+
+int fdtd_engine_pole_state(fdtd_engine* h, int pole_id, float* pol_out, float* cur_out) {
+  if (!h || pole_id < 0 || pole_id >= static_cast<int>(h->poles.size()))
+    return fail(FDTD_ERR_INVALID_ARG, "bad pole id");
+  const PoleHost& ph = h->poles[pole_id];
+  if (pol_out) CUDA_TRY(cudaMemcpyAsync(pol_out, ph.pol, ph.count * sizeof(float), cudaMemcpyDefault, h->stream));
+  if (cur_out) CUDA_TRY(cudaMemcpyAsync(cur_out, ph.cur, ph.count * sizeof(float), cudaMemcpyDefault, h->stream));
+  return 0;
+}
+
+int fdtd_engine_add_patch(fdtd_engine* h, int comp, const int* box, const float* coeff, const float* signal,
+                          int n_signal, float scale) {
+  if (!h || comp < 0 || comp > 5 || !box || !coeff || !signal || n_signal <= 0)
+    return fail(FDTD_ERR_INVALID_ARG, "bad patch arguments");
+  if (h->finalized) return fail(FDTD_ERR_STATE, "engine already finalized");
+  if (!box_ok(h, comp, box)) return fail(FDTD_ERR_INVALID_ARG, "patch box outside the component extent");
+  InjectionTerm t{};
+  t.comp = comp;
+  t.i0 = box[0];
+  t.i1 = box[1];
+  t.j0 = box[2];
+  t.j1 = box[3];
+  t.k0 = box[4];
+  t.k1 = box[5];
+  const int64_t cnt = static_cast<int64_t>(t.i1 - t.i0) * (t.j1 - t.j0) * (t.k1 - t.k0);
+  float* c = nullptr;
+  float* s = nullptr;
+  int rc = dev_copy(h, &c, coeff, cnt);
+  if (!rc) rc = dev_copy(h, &s, signal, n_signal);
+  if (rc) return rc;
+  t.coeff = c;
+  t.signal = s;
+  t.aux_len = n_signal;  // bound of the signal table
+  t.scale = scale;
+  h->terms.push_back(t);
+  return 0;
+}
+
+int fdtd_engine_add_aux_line(fdtd_engine* h, int n_e, const float* e_decay, const float* e_curl,
+                             const float* h_decay, const float* h_curl, int source_index, const float* source,
+                             int n_steps, int* line_id) {
+  if (!h || n_e < 4 || !e_decay || !e_curl || !h_decay || !h_curl || !source || n_steps <= 0)
+    return fail(FDTD_ERR_INVALID_ARG, "bad auxiliary line arguments");
+  AuxLine l;
+  l.ne = n_e;
+  l.n_steps = n_steps;
+  CUDA_TRY(cudaMalloc(&l.e_hist, sizeof(float) * static_cast<size_t>(n_steps) * n_e));
+  CUDA_TRY(cudaMalloc(&l.h_hist, sizeof(float) * static_cast<size_t>(n_steps) * n_e));
+  float *ed, *ecu, *hd, *hcu, *src, *e, *hh;
+  int rc = dev_copy(h, &ed, e_decay, n_e);
+  if (!rc) rc = dev_copy(h, &ecu, e_curl, n_e);
+  if (!rc) rc = dev_copy(h, &hd, h_decay, n_e - 1);
+  if (!rc) rc = dev_copy(h, &hcu, h_curl, n_e - 1);
+  if (!rc) rc = dev_copy(h, &src, source, n_steps);
+  if (!rc) rc = dev_alloc(h, &e, n_e);
+  if (!rc) rc = dev_alloc(h, &hh, n_e);
+  if (rc) return rc;
+  aux_history_kernel<<<1, 256, 0, h->stream>>>(n_e, ed, ecu, hd, hcu, source_index, src, n_steps, l.e_hist,
+                                               l.h_hist, e, hh);
+  CUDA_TRY(cudaGetLastError());
+  h->lines.push_back(l);
+  if (line_id) *line_id = static_cast<int>(h->lines.size()) - 1;
+  return 0;
+}
+
+int fdtd_engine_add_line_patch(fdtd_engine* h, int comp, const int* box, const float* coeff, int line_id,
+                               int sample_kind, const int* sample_index, int sample_axis, float scale) {
+  if (!h || comp < 0 || comp > 5 || !box || !coeff || !sample_index || sample_axis < 0 || sample_axis > 2 ||
+      line_id < 0 || line_id >= static_cast<int>(h->lines.size()) || sample_kind < 0 || sample_kind > 1)
+    return fail(FDTD_ERR_INVALID_ARG, "bad line patch arguments");
+  if (h->finalized) return fail(FDTD_ERR_STATE, "engine already finalized");
+  if (!box_ok(h, comp, box)) return fail(FDTD_ERR_INVALID_ARG, "line patch box outside the component extent");
+  InjectionTerm t{};
+  t.comp = comp;
+  t.i0 = box[0];
+  t.i1 = box[1];
+  t.j0 = box[2];
+  t.j1 = box[3];
+  t.k0 = box[4];
+  t.k1 = box[5];
+  const int64_t cnt = static_cast<int64_t>(t.i1 - t.i0) * (t.j1 - t.j0) * (t.k1 - t.k0);
+  const int axis_len = box[2 * sample_axis + 1] - box[2 * sample_axis];
+  float* c = nullptr;
+  int rc = dev_copy(h, &c, coeff, cnt);
+  if (rc) return rc;
+  int* idx = nullptr;
+  CUDA_TRY(cudaMalloc(&idx, sizeof(int) * axis_len));
+  CUDA_TRY(cudaMemcpyAsync(idx, sample_index, sizeof(int) * axis_len, cudaMemcpyDefault, h->stream));
+  h->owned.push_back(reinterpret_cast<float*>(idx));
+  const AuxLine& l = h->lines[line_id];
+  t.coeff = c;
+  t.signal = nullptr;
+  t.aux_hist = sample_kind == 0 ? l.e_hist : l.h_hist;
+  t.sample_index = idx;
+  t.aux_len = l.ne;
+  t.sample_axis = sample_axis;
+  t.scale = scale;
+  h->terms.push_back(t);
+  return 0;
+}
+
+int fdtd_engine_add_sample_region(fdtd_engine* h, int comp, const int* box, int64_t* base) {
+  if (!h || comp < 0 || comp > 5 || !box) return fail(FDTD_ERR_INVALID_ARG, "bad sample region arguments");
+  if (h->finalized) return fail(FDTD_ERR_STATE, "engine already finalized");
+  if (!box_ok(h, comp, box)) return fail(FDTD_ERR_INVALID_ARG, "sample region outside the component extent");
+  SampleRegion r{};
+  r.comp = comp;
+  r.i0 = box[0];
+  r.i1 = box[1];
+  r.j0 = box[2];
+  r.j1 = box[3];
+  r.k0 = box[4];
+  r.k1 = box[5];
+  r.base = h->n_samples;
+  h->n_samples += static_cast<int64_t>(r.i1 - r.i0) * (r.j1 - r.j0) * (r.k1 - r.k0);
+  h->regions.push_back(r);
+  if (base) *base = r.base;
+  return 0;
+}
+
+int fdtd_engine_set_dft(fdtd_engine* h, int n_freq, const double* omega, int n_steps, const double* window) {
+  if (!h || n_freq <= 0 || n_freq > 256 || !omega || n_steps <= 0 || !window)
+    return fail(FDTD_ERR_INVALID_ARG, "bad DFT arguments");
+  h->n_freq = n_freq;
+  h->dft_steps = n_steps;
+  cudaFree(h->w_e);
+  cudaFree(h->w_h);
+  CUDA_TRY(cudaMalloc(&h->w_e, sizeof(float2) * static_cast<size_t>(n_freq) * n_steps));
+  CUDA_TRY(cudaMalloc(&h->w_h, sizeof(float2) * static_cast<size_t>(n_freq) * n_steps));
+  double *d_omega = nullptr, *d_window = nullptr;
+  CUDA_TRY(cudaMalloc(&d_omega, sizeof(double) * n_freq));
+  CUDA_TRY(cudaMalloc(&d_window, sizeof(double) * n_steps));
+  CUDA_TRY(cudaMemcpyAsync(d_omega, omega, sizeof(double) * n_freq, cudaMemcpyHostToDevice, h->stream));
+  CUDA_TRY(cudaMemcpyAsync(d_window, window, sizeof(double) * n_steps, cudaMemcpyHostToDevice, h->stream));
+  dft_weight_kernel<<<256, 256, 0, h->stream>>>(n_freq, n_steps, d_omega, d_window, h->desc.dt, h->w_e, h->w_h);
+  CUDA_TRY(cudaGetLastError());
+  CUDA_TRY(cudaStreamSynchronize(h->stream));
+  cudaFree(d_omega);
+  cudaFree(d_window);
+  return 0;
+}
+
+int fdtd_engine_finalize(fdtd_engine* h) {
+  if (!h) return fail(FDTD_ERR_INVALID_ARG, "null engine");
+  if (h->finalized) return 0;
+  for (int a = 0; a < 3; ++a) {
+    if (!h->inv_e[a] || !h->inv_h[a]) return fail(FDTD_ERR_STATE, "spacing not set on every axis");
+    if (h->cpml && (!h->eb[a] || !h->hb[a])) return fail(FDTD_ERR_STATE, "CPML profile not set on every axis");
+  }
+  std::vector<int> ptr, ids;
+  int rc = upload_vec(h, &h->d_terms, h->terms);
+  if (rc) return rc;
+  build_plane_csr(h->NX, h->terms, ptr, ids);
+  if (!ids.empty()) {
+    rc = upload_vec(h, &h->d_term_ptr, ptr);
+    if (!rc) rc = upload_vec(h, &h->d_term_ids, ids);
+    if (rc) return rc;
+  } else {
+    rc = upload_vec(h, &h->d_term_ptr, ptr);
+    if (rc) return rc;
+  }
+  std::vector<PoleTerm> pv;
+  for (const auto& ph : h->poles) pv.push_back(ph.t);
+  rc = upload_vec(h, &h->d_poles, pv);
+  if (rc) return rc;
+  rc = upload_vec(h, &h->d_regions, h->regions);
+  if (rc) return rc;
+  build_plane_csr(h->NX, h->regions, ptr, ids);
+  rc = upload_vec(h, &h->d_region_ptr, ptr);
+  if (!rc && !ids.empty()) rc = upload_vec(h, &h->d_region_ids, ids);
+  if (rc) return rc;
+  std::vector<RegionFlush> fl;
+  for (const auto& r : h->regions) {
+    RegionFlush f;
+    f.base = r.base;
+    f.count = static_cast<int64_t>(r.i1 - r.i0) * (r.j1 - r.j0) * (r.k1 - r.k0);
+    f.is_h = r.comp >= 3 ? 1 : 0;
+    fl.push_back(f);
+    h->max_region = std::max(h->max_region, f.count);
+  }
+  rc = upload_vec(h, &h->d_flush, fl);
+  if (rc) return rc;
+  h->n_flush = static_cast<int>(fl.size());
+  if (h->n_samples > 0) {
+    CUDA_TRY(cudaMalloc(&h->samples, sizeof(float) * static_cast<size_t>(h->M) * h->n_samples));
+    if (h->n_freq > 0) {
+      const size_t acc = static_cast<size_t>(h->n_freq) * h->n_samples;
+      CUDA_TRY(cudaMalloc(&h->acc_re, sizeof(float) * acc));
+      CUDA_TRY(cudaMalloc(&h->acc_im, sizeof(float) * acc));
+      CUDA_TRY(cudaMalloc(&h->cmp_re, sizeof(float) * acc));
+      CUDA_TRY(cudaMalloc(&h->cmp_im, sizeof(float) * acc));
+      CUDA_TRY(cudaMemsetAsync(h->acc_re, 0, sizeof(float) * acc, h->stream));
+      CUDA_TRY(cudaMemsetAsync(h->acc_im, 0, sizeof(float) * acc, h->stream));
+      CUDA_TRY(cudaMemsetAsync(h->cmp_re, 0, sizeof(float) * acc, h->stream));
+      CUDA_TRY(cudaMemsetAsync(h->cmp_im, 0, sizeof(float) * acc, h->stream));
+    }
+  }
+  CUDA_TRY(cudaFuncSetAttribute(fused_step_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
+  CUDA_TRY(cudaStreamSynchronize(h->stream));
+  h->finalized = true;
+  return 0;
+}
+
+int fdtd_engine_step_range(fdtd_engine* h, int n0, int n1) {
+  if (!h) return fail(FDTD_ERR_INVALID_ARG, "null engine");
+  if (!h->finalized) return fail(FDTD_ERR_STATE, "engine not finalized");
+  if (n1 < n0 || n0 < 0) return fail(FDTD_ERR_INVALID_ARG, "bad step range");
+  for (const auto& t : h->terms) {
+    if (t.signal && n1 > t.aux_len) return fail(FDTD_ERR_INVALID_ARG, "source signal table shorter than the range");
+  }
+  for (const auto& l : h->lines) {
+    if (n1 > l.n_steps) return fail(FDTD_ERR_INVALID_ARG, "incident line history shorter than the range");
+  }
+  if (h->n_samples > 0 && h->n_freq > 0 && n1 > h->dft_steps)
+    return fail(FDTD_ERR_INVALID_ARG, "DFT weight table shorter than the range");
+  CUDA_TRY(cudaEventRecord(h->ev0, h->stream));
+  for (int n = n0; n < n1; ++n) {
+    if (h->pending == 0) h->pending_base = n;
+    if (h->pending_base + h->pending != n) {
+      int rc = flush_samples(h);
+      if (rc) return rc;
+      h->pending_base = n;
+    }
+    int rc = launch_step(h, n, h->pending);
+    if (rc) return rc;
+    if (h->n_samples > 0) {
+      ++h->pending;
+      if (h->pending == h->M) {
+        rc = flush_samples(h);
+        if (rc) return rc;
+      }
+    }
+  }
+  CUDA_TRY(cudaEventRecord(h->ev1, h->stream));
+  CUDA_TRY(cudaEventSynchronize(h->ev1));
+  CUDA_TRY(cudaEventElapsedTime(&h->last_ms, h->ev0, h->ev1));
+  return 0;
+}
+
+int fdtd_engine_flush(fdtd_engine* h) {
+  if (!h) return fail(FDTD_ERR_INVALID_ARG, "null engine");
+  return flush_samples(h);
+}
+
+int fdtd_engine_read_dft(fdtd_engine* h, float* re, float* im) {
+  if (!h || !re || !im) return fail(FDTD_ERR_INVALID_ARG, "bad DFT read arguments");
+  if (!h->acc_re) return fail(FDTD_ERR_STATE, "no DFT accumulators");
+  int rc = flush_samples(h);
+  if (rc) return rc;
+  const size_t bytes = sizeof(float) * static_cast<size_t>(h->n_freq) * h->n_samples;
+  CUDA_TRY(cudaMemcpyAsync(re, h->acc_re, bytes, cudaMemcpyDefault, h->stream));
+  CUDA_TRY(cudaMemcpyAsync(im, h->acc_im, bytes, cudaMemcpyDefault, h->stream));
+  return 0;
+}
+
+static void state_buffers(fdtd_engine* h, std::vector<std::pair<float*, size_t>>& out) {
+  const int c0 = h->cur;
+  for (int c = 0; c < 3; ++c) {
+    out.push_back({h->E[c0][c], static_cast<size_t>(h->vol)});
+    out.push_back({h->H[c0][c], static_cast<size_t>(h->vol)});
+  }
+  for (int c = 0; c < 3; ++c) {
+    const int ax[2] = {axis_a(c), axis_b(c)};
+    for (int w = 0; w < 2; ++w) {
+      const size_t n = static_cast<size_t>(slab_elems(h, ax[w]));
+      if (n == 0) continue;
+      out.push_back({h->psiE[c][w], n});
+      out.push_back({h->psiH[c0][c][w], n});
+    }
+  }
+  for (auto& ph : h->poles) {
+    out.push_back({ph.pol, static_cast<size_t>(ph.count)});
+    out.push_back({ph.cur, static_cast<size_t>(ph.count)});
+  }
+}
+
+int fdtd_engine_checkpoint_save(fdtd_engine* h, int slot) {
+  if (!h || slot < 0 || slot > 1 << 20) return fail(FDTD_ERR_INVALID_ARG, "bad checkpoint slot");
+  if (static_cast<int>(h->checkpoints.size()) <= slot) h->checkpoints.resize(slot + 1);
+  std::vector<std::pair<float*, size_t>> bufs;
+  state_buffers(h, bufs);
+  Checkpoint& ck = h->checkpoints[slot];
+  if (ck.bufs.size() != bufs.size()) {
+    for (float* p : ck.bufs) cudaFree(p);
+    ck.bufs.assign(bufs.size(), nullptr);
+    for (size_t x = 0; x < bufs.size(); ++x) CUDA_TRY(cudaMalloc(&ck.bufs[x], bufs[x].second * sizeof(float)));
+  }
+  for (size_t x = 0; x < bufs.size(); ++x)
+    CUDA_TRY(cudaMemcpyAsync(ck.bufs[x], bufs[x].first, bufs[x].second * sizeof(float), cudaMemcpyDeviceToDevice,
+                             h->stream));
+  ck.valid = true;
+  return 0;
+}
+
+int fdtd_engine_checkpoint_load(fdtd_engine* h, int slot) {
+  if (!h || slot < 0 || slot >= static_cast<int>(h->checkpoints.size()) || !h->checkpoints[slot].valid)
+    return fail(FDTD_ERR_INVALID_ARG, "no checkpoint in that slot");
+  std::vector<std::pair<float*, size_t>> bufs;
+  state_buffers(h, bufs);
+  Checkpoint& ck = h->checkpoints[slot];
+  for (size_t x = 0; x < bufs.size(); ++x)
+    CUDA_TRY(cudaMemcpyAsync(bufs[x].first, ck.bufs[x], bufs[x].second * sizeof(float), cudaMemcpyDeviceToDevice,
+                             h->stream));
+  return 0;
+}
+
+int fdtd_engine_autotune(fdtd_engine* h, int* tile_rows, int* chunk_planes) {
+  if (!h || !h->finalized) return fail(FDTD_ERR_STATE, "engine not finalized");
+  int rc = flush_samples(h);
+  if (rc) return rc;
+  const int next_step = h->pending_base;
+  // Save the state into a private checkpoint, time the candidates (their steps
+  // write scratch samples into slot 0 and advance the state), then restore.
+  const int slot = static_cast<int>(h->checkpoints.size());
+  rc = fdtd_engine_checkpoint_save(h, slot);
+  if (rc) return rc;
+  const int Q = h->P / 4;
+  std::vector<int> tys;
+  for (int ty : {1, 2, 3, 4, 6, 8, 12, 16, 24, 32, 48})
+    if (tile_fits(ty, h->P) && ty <= h->NY && (ty + 2) * Q >= 64) tys.push_back(ty);
+  if (tys.empty()) tys.push_back(h->TY);
+  const int cxs[] = {8, 16, 32, 64, 128};
+  float best = 1e30f;
+  int best_ty = h->TY, best_cx = h->CX;
+  for (int ty : tys) {
+    for (int cx : cxs) {
+      if (cx > 2 * h->NX) continue;
+      h->TY = ty;
+      h->CX = cx;
+      const int reps = 3;
+      rc = launch_step(h, 0, 0);
+      if (rc) return rc;
+      CUDA_TRY(cudaEventRecord(h->ev0, h->stream));
+      for (int r = 0; r < reps; ++r) {
+        rc = launch_step(h, 0, 0);
+        if (rc) return rc;
+      }
+      CUDA_TRY(cudaEventRecord(h->ev1, h->stream));
+      CUDA_TRY(cudaEventSynchronize(h->ev1));
+      float ms = 0.0f;
+      CUDA_TRY(cudaEventElapsedTime(&ms, h->ev0, h->ev1));
+      if (ms < best) {
+        best = ms;
+        best_ty = ty;
+        best_cx = cx;
+      }
+    }
+  }
+  h->TY = best_ty;
+  h->CX = best_cx;
+  rc = fdtd_engine_checkpoint_load(h, slot);
+  if (rc) return rc;
+  for (float* p : h->checkpoints[slot].bufs) cudaFree(p);
+  h->checkpoints.pop_back();
+  h->pending = 0;
+  h->pending_base = next_step;
+  if (tile_rows) *tile_rows = best_ty;
+  if (chunk_planes) *chunk_planes = best_cx;
+  return 0;
+}
+
+int fdtd_engine_time_kernel(fdtd_engine* h, int n, int reps, float* ms) {
+  if (!h || !ms || reps <= 0 || n < 0) return fail(FDTD_ERR_INVALID_ARG, "bad time_kernel arguments");
+  if (!h->finalized) return fail(FDTD_ERR_STATE, "engine not finalized");
+  for (const auto& t : h->terms)
+    if (t.signal && n >= t.aux_len) return fail(FDTD_ERR_INVALID_ARG, "step index beyond the source table");
+  for (const auto& l : h->lines)
+    if (n >= l.n_steps) return fail(FDTD_ERR_INVALID_ARG, "step index beyond the incident line history");
+  const int slot = h->pending < h->M ? h->pending : 0;
+  CUDA_TRY(cudaEventRecord(h->ev0, h->stream));
+  for (int r = 0; r < reps; ++r) {
+    int rc = launch_step(h, n, slot);
+    if (rc) return rc;
+  }
+  CUDA_TRY(cudaEventRecord(h->ev1, h->stream));
+  CUDA_TRY(cudaEventSynchronize(h->ev1));
+  float total = 0.0f;
+  CUDA_TRY(cudaEventElapsedTime(&total, h->ev0, h->ev1));
+  *ms = total / static_cast<float>(reps);
+  return 0;
+}
+
+int fdtd_engine_info(fdtd_engine* h, int* tile_rows, int* chunk_planes, int* grid_x, int* grid_y, int* block,
+                     int64_t* launches) {
+  if (!h) return fail(FDTD_ERR_INVALID_ARG, "null engine");
+  if (tile_rows) *tile_rows = h->TY;
+  if (chunk_planes) *chunk_planes = h->CX;
+  if (grid_x) *grid_x = (h->NY + h->TY - 1) / h->TY;
+  if (grid_y) *grid_y = (h->NX + h->CX - 1) / h->CX;
+  if (block) *block = block_threads(h->TY, h->P);
+  if (launches) *launches = h->launches;
+  return 0;
+}
+
+int fdtd_engine_last_ms(fdtd_engine* h, float* ms) {
+  if (!h || !ms) return fail(FDTD_ERR_INVALID_ARG, "bad arguments");
+  *ms = h->last_ms;
+  return 0;
+}
+
+}  // extern "C"

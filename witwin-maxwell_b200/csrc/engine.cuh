@@ -1,0 +1,92 @@
+// Internal data structures of the fused FDTD step engine.
+#pragma once
+
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include "common.cuh"
+
+namespace fdtdb200 {
+
+// A dense patch over an axis-aligned box of one field component that is added
+// to that component every step.  The added value is coeff[cell] * s, where s is
+// either signal[n] (a soft source whose waveform the host evaluated in FP64) or
+// aux_hist[n * aux_len + sample_index[coord along sample_axis]] (a TFSF face
+// correction that reads the 1-D incident line).
+struct InjectionTerm {
+  int comp;  // 0..2 = Ex..Ez (applied in the E phase), 3..5 = Hx..Hz (H phase)
+  int i0, i1, j0, j1, k0, k1;
+  const float* coeff;     // [i1-i0][j1-j0][k1-k0]
+  const float* signal;    // per-step scalar table, or nullptr
+  const float* aux_hist;  // per-step incident line history, or nullptr
+  const int* sample_index;
+  int aux_len;
+  int sample_axis;
+  float scale;
+};
+
+// One Debye/Drude/Lorentz pole acting on one E component over a box.
+struct PoleTerm {
+  int comp;  // 0..2
+  int kind;  // 0 Debye, 1 Drude, 2 Lorentz
+  int i0, i1, j0, j1, k0, k1;
+  float decay, restoring, dt, inv_dt;
+  const float* drive;    // box-dense
+  const float* inv_eps;  // box-dense (1/eps of the component, absolute)
+  float* pol;            // box-dense polarisation (Debye, Lorentz)
+  float* cur;            // box-dense current
+};
+
+// A box of one component whose values are written into the per-step sample
+// ring buffer that feeds the batched monitor DFT.
+struct SampleRegion {
+  int comp;  // 0..5
+  int i0, i1, j0, j1, k0, k1;
+  int64_t base;  // first sample slot of the region
+};
+
+struct StepParams {
+  int NX, NY, NZ, P, SZ;  // node counts, padded z pitch, z-slab row length
+  int TY, CX, Q, ROWS;    // tile rows, planes per chunk, float4 per row, thread rows (TY + 2)
+  const float* Ein[3];
+  float* Eout[3];
+  const float* Hin[3];
+  float* Hout[3];
+  const float* ecurl[3];
+  const float* edecay[3];
+  float ecurl_u[3], edecay_u[3];
+  const float* hcurl[3];
+  const float* hdecay[3];
+  float hcurl_u[3], hdecay_u[3];
+  const float* inv_e[3];
+  const float* inv_h[3];
+  const float* eb[3];
+  const float* ec[3];
+  const float* eik[3];
+  const float* hb[3];
+  const float* hc[3];
+  const float* hik[3];
+  int slab_lo[3], slab_hi[3];
+  float* psiE[3][2];
+  const float* psiHin[3][2];
+  float* psiHout[3][2];
+  int bnd[6];
+  int cpml;
+  // injection / ADE / sampling
+  const InjectionTerm* terms;
+  const int* term_plane_ptr;  // [NX + 1] CSR over planes
+  const int* term_plane_ids;
+  int n_terms;
+  const PoleTerm* poles;
+  int n_poles;
+  const SampleRegion* regions;
+  const int* region_plane_ptr;
+  const int* region_plane_ids;
+  int n_regions;
+  float* samples;  // [M][n_samples]
+  int64_t n_samples;
+  int sample_block;  // M
+};
+
+}  // namespace fdtdb200

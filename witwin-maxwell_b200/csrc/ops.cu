@@ -1,0 +1,478 @@
+// Per-op kernels with the semantics of the reference's torch ops
+// (witwin/maxwell/fdtd/cuda/extension.cpp:2059-2196).  They let a caller
+// re-point the reference's NativeFDTDModule op by op; the fused engine is the
+// fast path.  Each kernel is one thread per output element over a flattened
+// index (z fastest), 256-thread blocks, launched on the caller's stream.
+#include <cuda_runtime.h>
+
+#include <string>
+
+#include "../../include/fdtd_b200.h"
+#include "common.cuh"
+
+using namespace fdtdb200;
+
+namespace {
+
+int op_fail(int code, const char* msg) {
+  set_last_error(msg);
+  return code;
+}
+
+int op_launch_check(const char* what) {
+  cudaError_t err = cudaGetLastError();
+  if (err != cudaSuccess) {
+    set_last_error(std::string(what) + ": " + cudaGetErrorString(err));
+    return FDTD_ERR_CUDA;
+  }
+  return 0;
+}
+
+constexpr int kThreads = 256;
+
+unsigned blocks_for(int64_t n) {
+  int64_t b = (n + kThreads - 1) / kThreads;
+  if (b < 1) b = 1;
+  if (b > (1 << 20)) b = 1 << 20;
+  return static_cast<unsigned>(b);
+}
+
+__device__ __forceinline__ void unflatten(int64_t x, int ny, int nz, int& i, int& j, int& k) {
+  k = static_cast<int>(x % nz);
+  const int64_t r = x / nz;
+  j = static_cast<int>(r % ny);
+  i = static_cast<int>(r / ny);
+}
+
+struct CpmlArgs {
+  float* psi_a;
+  float* psi_b;
+  const float *ika, *ba, *ca, *ikb, *bb, *cb;
+  int a_low, a_hstart, a_hlen, b_low, b_hstart, b_hlen;
+};
+
+__device__ __forceinline__ float psi_advance(int mode, float* psi, const float* b, const float* c, int axis, int i,
+                                             int j, int k, int ny, int nz, int coord, int low, int hstart,
+                                             int hlen, float d) {
+  int64_t o;
+  if (mode == 1) {
+    o = off3(i, j, k, ny, nz);
+  } else {
+    const int local = slab_local(coord, low, hstart, hlen);
+    if (local < 0) return 0.0f;
+    const int clen = low + hlen;
+    o = axis == 0 ? off3(local, j, k, ny, nz) : (axis == 1 ? off3(i, local, k, clen, nz) : off3(i, j, local, ny, clen));
+  }
+  const float v = b[coord] * psi[o] + c[coord] * d;
+  psi[o] = v;
+  return v;
+}
+
+// witwin/maxwell/fdtd/cuda/kernels/magnetic.cu:20-212
+__global__ void op_magnetic_kernel(int comp, int mode, int nx, int ny, int nz, float* field, const float* first,
+                                   const float* second, const float* decay, const float* curl, float decay_u,
+                                   float curl_u, const float* inv_a, const float* inv_b, CpmlArgs cp) {
+  const int64_t total = static_cast<int64_t>(nx) * ny * nz;
+  const int A = comp == 0 ? 1 : 0, B = comp == 2 ? 1 : 2;
+  const int sy2 = ny + (A == 1), sz2 = nz + (A == 2);
+  const int sy1 = ny + (B == 1), sz1 = nz + (B == 2);
+  for (int64_t x = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; x < total;
+       x += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    int i, j, k;
+    unflatten(x, ny, nz, i, j, k);
+    const int ca_ = A == 0 ? i : (A == 1 ? j : k);
+    const int cb_ = B == 0 ? i : (B == 1 ? j : k);
+    const float da = (second[off3(i + (A == 0), j + (A == 1), k + (A == 2), sy2, sz2)] - second[off3(i, j, k, sy2, sz2)]) * inv_a[ca_];
+    const float db = (first[off3(i + (B == 0), j + (B == 1), k + (B == 2), sy1, sz1)] - first[off3(i, j, k, sy1, sz1)]) * inv_b[cb_];
+    float ea = da, eb = db;
+    if (mode != 0) {
+      const float pa = psi_advance(mode, cp.psi_a, cp.ba, cp.ca, A, i, j, k, ny, nz, ca_, cp.a_low, cp.a_hstart, cp.a_hlen, da);
+      const float pb = psi_advance(mode, cp.psi_b, cp.bb, cp.cb, B, i, j, k, ny, nz, cb_, cp.b_low, cp.b_hstart, cp.b_hlen, db);
+      ea = da * cp.ika[ca_] + pa;
+      eb = db * cp.ikb[cb_] + pb;
+    }
+    const float c = comp == 1 ? (eb - ea) : (ea - eb);
+    const float dv = decay ? decay[x] : decay_u;
+    const float cv = curl ? curl[x] : curl_u;
+    field[x] = field[x] * dv - cv * c;
+  }
+}
+
+__device__ __forceinline__ float bdiff(const float* src, int axis, int i, int j, int k, int tsize, int sy, int sz,
+                                       int lo, int hi, const float* inv) {
+  const int coord = axis == 0 ? i : (axis == 1 ? j : k);
+  const float iv = inv[coord];
+  if (coord == 0 || coord + 1 == tsize) {
+    const int last = tsize - 2;
+    const int64_t l = axis == 0 ? off3(0, j, k, sy, sz) : (axis == 1 ? off3(i, 0, k, sy, sz) : off3(i, j, 0, sy, sz));
+    const int64_t h = axis == 0 ? off3(last, j, k, sy, sz) : (axis == 1 ? off3(i, last, k, sy, sz) : off3(i, j, last, sy, sz));
+    const int mode = coord == 0 ? lo : hi;
+    if (mode == BND_PERIODIC) return (src[l] - src[h]) * iv;
+    if (mode == BND_PMC) return coord == 0 ? 2.0f * src[l] * iv : -2.0f * src[h] * iv;
+    return 0.0f;
+  }
+  const int64_t cur = off3(i, j, k, sy, sz);
+  const int64_t prv = axis == 0 ? off3(i - 1, j, k, sy, sz) : (axis == 1 ? off3(i, j - 1, k, sy, sz) : off3(i, j, k - 1, sy, sz));
+  return (src[cur] - src[prv]) * iv;
+}
+
+// witwin/maxwell/fdtd/cuda/kernels/electric.cu:18-119, 242-311, 462-941
+__global__ void op_electric_kernel(int comp, int mode, int nx, int ny, int nz, float* field, const float* first,
+                                   const float* second, const float* decay, const float* curl, float decay_u,
+                                   float curl_u, const float* inv_a, const float* inv_b, int a_lo, int a_hi,
+                                   int b_lo, int b_hi, CpmlArgs cp) {
+  const int64_t total = static_cast<int64_t>(nx) * ny * nz;
+  const int A = comp == 0 ? 1 : 0, B = comp == 2 ? 1 : 2;
+  const int sy2 = ny - (A == 1), sz2 = nz - (A == 2);
+  const int sy1 = ny - (B == 1), sz1 = nz - (B == 2);
+  const int size_a = A == 0 ? nx : (A == 1 ? ny : nz);
+  const int size_b = B == 0 ? nx : (B == 1 ? ny : nz);
+  for (int64_t x = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; x < total;
+       x += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    int i, j, k;
+    unflatten(x, ny, nz, i, j, k);
+    const int ca_ = A == 0 ? i : (A == 1 ? j : k);
+    const int cb_ = B == 0 ? i : (B == 1 ? j : k);
+    const bool pec = (ca_ == 0 && a_lo == BND_PEC) || (ca_ + 1 == size_a && a_hi == BND_PEC) ||
+                     (cb_ == 0 && b_lo == BND_PEC) || (cb_ + 1 == size_b && b_hi == BND_PEC);
+    if (pec) {
+      field[x] = 0.0f;
+      continue;
+    }
+    const bool ina = (ca_ == 0 && (a_lo == BND_NONE || a_lo == BND_PML)) ||
+                     (ca_ + 1 == size_a && (a_hi == BND_NONE || a_hi == BND_PML));
+    const bool inb = (cb_ == 0 && (b_lo == BND_NONE || b_lo == BND_PML)) ||
+                     (cb_ + 1 == size_b && (b_hi == BND_NONE || b_hi == BND_PML));
+    if (ina || inb) continue;
+    const float da = bdiff(second, A, i, j, k, size_a, sy2, sz2, a_lo, a_hi, inv_a);
+    const float db = bdiff(first, B, i, j, k, size_b, sy1, sz1, b_lo, b_hi, inv_b);
+    float ea = da, eb = db;
+    if (mode != 0) {
+      const float pa = psi_advance(mode, cp.psi_a, cp.ba, cp.ca, A, i, j, k, ny, nz, ca_, cp.a_low, cp.a_hstart, cp.a_hlen, da);
+      const float pb = psi_advance(mode, cp.psi_b, cp.bb, cp.cb, B, i, j, k, ny, nz, cb_, cp.b_low, cp.b_hstart, cp.b_hlen, db);
+      ea = da * cp.ika[ca_] + pa;
+      eb = db * cp.ikb[cb_] + pb;
+    }
+    const float c = comp == 1 ? (eb - ea) : (ea - eb);
+    const float dv = decay ? decay[x] : decay_u;
+    const float cv = curl ? curl[x] : curl_u;
+    field[x] = field[x] * dv + cv * c;
+  }
+}
+
+__global__ void op_debye_kernel(int64_t n, const float* e, const float* drive, float decay, float inv_dt, float* pol,
+                                float* cur) {
+  for (int64_t x = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; x < n;
+       x += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    const float prev = pol[x];
+    const float next = decay * prev + drive[x] * e[x];
+    pol[x] = next;
+    cur[x] = (next - prev) * inv_dt;
+  }
+}
+
+__global__ void op_drude_kernel(int64_t n, const float* e, const float* drive, float decay, float* cur) {
+  for (int64_t x = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; x < n;
+       x += static_cast<int64_t>(gridDim.x) * blockDim.x)
+    cur[x] = decay * cur[x] + drive[x] * e[x];
+}
+
+__global__ void op_lorentz_kernel(int64_t n, const float* e, const float* drive, float decay, float restoring,
+                                  float dt, float* pol, float* cur) {
+  for (int64_t x = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; x < n;
+       x += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    const float pj = cur[x], pp = pol[x];
+    const float nj = decay * pj - restoring * pp + drive[x] * e[x];
+    cur[x] = nj;
+    pol[x] = pp + dt * nj;
+  }
+}
+
+__global__ void op_apply_pol_kernel(int64_t n, const float* cur, const float* inv_eps, float dt, float* e) {
+  for (int64_t x = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; x < n;
+       x += static_cast<int64_t>(gridDim.x) * blockDim.x)
+    e[x] -= dt * cur[x] * inv_eps[x];
+}
+
+__global__ void op_patch_kernel(float* field, int fx, int fy, int fz, const float* patch, int px, int py, int pz,
+                                int oi, int oj, int ok, float signal) {
+  const int64_t total = static_cast<int64_t>(px) * py * pz;
+  for (int64_t x = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; x < total;
+       x += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    int i, j, k;
+    unflatten(x, py, pz, i, j, k);
+    const int gi = oi + i, gj = oj + j, gk = ok + k;
+    if (gi < 0 || gj < 0 || gk < 0 || gi >= fx || gj >= fy || gk >= fz) continue;
+    field[off3(gi, gj, gk, fy, fz)] += signal * patch[x];
+  }
+}
+
+__global__ void op_line_patch_kernel(float* field, int fx, int fy, int fz, const float* coeff, int px, int py, int pz,
+                                     int oi, int oj, int ok, const float* inc, const int64_t* sidx, int axis,
+                                     float scale) {
+  const int64_t total = static_cast<int64_t>(px) * py * pz;
+  for (int64_t x = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; x < total;
+       x += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    int i, j, k;
+    unflatten(x, py, pz, i, j, k);
+    const int gi = oi + i, gj = oj + j, gk = ok + k;
+    if (gi < 0 || gj < 0 || gk < 0 || gi >= fx || gj >= fy || gk >= fz) continue;
+    const int a = axis == 0 ? i : (axis == 1 ? j : k);
+    field[off3(gi, gj, gk, fy, fz)] += coeff[x] * inc[sidx[a]] * scale;
+  }
+}
+
+__global__ void op_aux_h_kernel(int ne, float* h, const float* e, const float* hd, const float* hc) {
+  const int x = blockIdx.x * blockDim.x + threadIdx.x;
+  if (x < ne - 1) h[x] = hd[x] * h[x] - hc[x] * (e[x + 1] - e[x]);
+}
+
+__global__ void op_aux_e_kernel(int ne, float* e, const float* h, const float* ed, const float* ec, int src,
+                                float value) {
+  const int x = blockIdx.x * blockDim.x + threadIdx.x;
+  if (x >= ne) return;
+  if (x == src) {
+    e[x] = value;
+  } else if (x == ne - 1) {
+    e[x] = 0.0f;
+  } else if (x >= 1) {
+    e[x] = ed[x] * e[x] - ec[x] * (h[x] - h[x - 1]);
+  }
+}
+
+__global__ void op_points_kernel(const float* field, int fy, int fz, int np, const int* pi, const int* pj,
+                                 const int* pk, float* re, float* im, float wc, float ws) {
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= np) return;
+  const float v = field[off3(pi[p], pj[p], pk[p], fy, fz)];
+  re[p] += v * wc;
+  im[p] += v * ws;
+}
+
+__global__ void op_plane_kernel(const float* field, int fx, int fy, int fz, int axis, int index, float* re, float* im,
+                                float wc, float ws) {
+  const int da = axis == 0 ? fy : fx;
+  const int db = axis == 2 ? fy : fz;
+  const int64_t total = static_cast<int64_t>(da) * db;
+  for (int64_t x = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; x < total;
+       x += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    const int a = static_cast<int>(x / db), b = static_cast<int>(x % db);
+    int64_t o;
+    if (axis == 0) o = off3(index, a, b, fy, fz);
+    else if (axis == 1) o = off3(a, index, b, fy, fz);
+    else o = off3(a, b, index, fy, fz);
+    const float v = field[o];
+    re[x] += v * wc;
+    im[x] += v * ws;
+  }
+}
+
+__global__ void op_dft_volume_kernel(int64_t n, int nf, const float* field, float* re, float* im, const float* wc,
+                                     const float* ws) {
+  for (int64_t x = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; x < n;
+       x += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    const float v = field[x];
+    for (int f = 0; f < nf; ++f) {
+      re[static_cast<int64_t>(f) * n + x] += v * wc[f];
+      im[static_cast<int64_t>(f) * n + x] += v * ws[f];
+    }
+  }
+}
+
+__global__ void op_clamp_kernel(float* field, int fx, int fy, int fz, int axis, int side) {
+  const int n[3] = {fx, fy, fz};
+  const int idx = side == 0 ? 0 : n[axis] - 1;
+  const int da = axis == 0 ? fy : fx;
+  const int db = axis == 2 ? fy : fz;
+  const int64_t total = static_cast<int64_t>(da) * db;
+  for (int64_t x = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; x < total;
+       x += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    const int a = static_cast<int>(x / db), b = static_cast<int>(x % db);
+    int64_t o;
+    if (axis == 0) o = off3(idx, a, b, fy, fz);
+    else if (axis == 1) o = off3(a, idx, b, fy, fz);
+    else o = off3(a, b, idx, fy, fz);
+    field[o] = 0.0f;
+  }
+}
+
+CpmlArgs make_cpml(float* psi_a, float* psi_b, const float* ika, const float* ba, const float* ca, const float* ikb,
+                   const float* bb, const float* cb, const int* slab) {
+  CpmlArgs c{};
+  c.psi_a = psi_a;
+  c.psi_b = psi_b;
+  c.ika = ika;
+  c.ba = ba;
+  c.ca = ca;
+  c.ikb = ikb;
+  c.bb = bb;
+  c.cb = cb;
+  if (slab) {
+    c.a_low = slab[0];
+    c.a_hstart = slab[1];
+    c.a_hlen = slab[2];
+    c.b_low = slab[3];
+    c.b_hstart = slab[4];
+    c.b_hlen = slab[5];
+  }
+  return c;
+}
+
+bool cpml_args_ok(int mode, float* psi_a, float* psi_b, const float* ika, const float* ba, const float* ca,
+                  const float* ikb, const float* bb, const float* cb, const int* slab) {
+  if (mode == 0) return true;
+  if (!psi_a || !psi_b || !ika || !ba || !ca || !ikb || !bb || !cb) return false;
+  return mode == 1 || slab != nullptr;
+}
+
+}  // namespace
+
+extern "C" {
+
+int fdtd_op_update_magnetic(int comp, int mode, int nx, int ny, int nz, float* field, const float* first,
+                            const float* second, const float* decay, const float* curl, float decay_u,
+                            float curl_u, const float* inv_a, const float* inv_b, float* psi_a, float* psi_b,
+                            const float* ika, const float* ba, const float* ca, const float* ikb,
+                            const float* bb, const float* cb, const int* slab, void* stream) {
+  if (comp < 0 || comp > 2 || mode < 0 || mode > 2 || nx <= 0 || ny <= 0 || nz <= 0 || !field || !first ||
+      !second || !inv_a || !inv_b)
+    return op_fail(FDTD_ERR_INVALID_ARG, "update_magnetic: bad arguments");
+  if (!cpml_args_ok(mode, psi_a, psi_b, ika, ba, ca, ikb, bb, cb, slab))
+    return op_fail(FDTD_ERR_INVALID_ARG, "update_magnetic: missing CPML arguments");
+  const int64_t n = static_cast<int64_t>(nx) * ny * nz;
+  op_magnetic_kernel<<<blocks_for(n), kThreads, 0, static_cast<cudaStream_t>(stream)>>>(
+      comp, mode, nx, ny, nz, field, first, second, decay, curl, decay_u, curl_u, inv_a, inv_b,
+      make_cpml(psi_a, psi_b, ika, ba, ca, ikb, bb, cb, slab));
+  return op_launch_check("update_magnetic");
+}
+
+int fdtd_op_update_electric(int comp, int mode, int nx, int ny, int nz, float* field, const float* first,
+                            const float* second, const float* decay, const float* curl, float decay_u,
+                            float curl_u, const float* inv_a, const float* inv_b, const int* modes,
+                            float* psi_a, float* psi_b, const float* ika, const float* ba, const float* ca,
+                            const float* ikb, const float* bb, const float* cb, const int* slab, void* stream) {
+  if (comp < 0 || comp > 2 || mode < 0 || mode > 2 || nx < 2 || ny < 2 || nz < 2 || !field || !first || !second ||
+      !inv_a || !inv_b || !modes)
+    return op_fail(FDTD_ERR_INVALID_ARG, "update_electric: bad arguments");
+  for (int m = 0; m < 4; ++m)
+    if (modes[m] == BND_BLOCH) return op_fail(FDTD_ERR_UNSUPPORTED, "update_electric: Bloch faces need the complex kernels");
+  if (!cpml_args_ok(mode, psi_a, psi_b, ika, ba, ca, ikb, bb, cb, slab))
+    return op_fail(FDTD_ERR_INVALID_ARG, "update_electric: missing CPML arguments");
+  const int64_t n = static_cast<int64_t>(nx) * ny * nz;
+  op_electric_kernel<<<blocks_for(n), kThreads, 0, static_cast<cudaStream_t>(stream)>>>(
+      comp, mode, nx, ny, nz, field, first, second, decay, curl, decay_u, curl_u, inv_a, inv_b, modes[0],
+      modes[1], modes[2], modes[3], make_cpml(psi_a, psi_b, ika, ba, ca, ikb, bb, cb, slab));
+  return op_launch_check("update_electric");
+}
+
+int fdtd_op_update_debye(int64_t n, const float* e, const float* drive, float decay, float dt, float* pol,
+                         float* cur, void* stream) {
+  if (n < 0 || !e || !drive || !pol || !cur || !(dt > 0.0f)) return op_fail(FDTD_ERR_INVALID_ARG, "update_debye: bad arguments");
+  if (n == 0) return 0;
+  op_debye_kernel<<<blocks_for(n), kThreads, 0, static_cast<cudaStream_t>(stream)>>>(n, e, drive, decay, 1.0f / dt, pol, cur);
+  return op_launch_check("update_debye");
+}
+
+int fdtd_op_update_drude(int64_t n, const float* e, const float* drive, float decay, float* cur, void* stream) {
+  if (n < 0 || !e || !drive || !cur) return op_fail(FDTD_ERR_INVALID_ARG, "update_drude: bad arguments");
+  if (n == 0) return 0;
+  op_drude_kernel<<<blocks_for(n), kThreads, 0, static_cast<cudaStream_t>(stream)>>>(n, e, drive, decay, cur);
+  return op_launch_check("update_drude");
+}
+
+int fdtd_op_update_lorentz(int64_t n, const float* e, const float* drive, float decay, float restoring,
+                           float dt, float* pol, float* cur, void* stream) {
+  if (n < 0 || !e || !drive || !pol || !cur) return op_fail(FDTD_ERR_INVALID_ARG, "update_lorentz: bad arguments");
+  if (n == 0) return 0;
+  op_lorentz_kernel<<<blocks_for(n), kThreads, 0, static_cast<cudaStream_t>(stream)>>>(n, e, drive, decay, restoring, dt, pol, cur);
+  return op_launch_check("update_lorentz");
+}
+
+int fdtd_op_apply_polarization(int64_t n, const float* cur, const float* inv_eps, float dt, float* e,
+                               void* stream) {
+  if (n < 0 || !cur || !inv_eps || !e) return op_fail(FDTD_ERR_INVALID_ARG, "apply_polarization: bad arguments");
+  if (n == 0) return 0;
+  op_apply_pol_kernel<<<blocks_for(n), kThreads, 0, static_cast<cudaStream_t>(stream)>>>(n, cur, inv_eps, dt, e);
+  return op_launch_check("apply_polarization");
+}
+
+int fdtd_op_add_source_patch(float* field, const int* fshape, const float* patch, const int* pshape,
+                             const int* offset, float signal, void* stream) {
+  if (!field || !fshape || !patch || !pshape || !offset) return op_fail(FDTD_ERR_INVALID_ARG, "add_source_patch: bad arguments");
+  const int64_t n = static_cast<int64_t>(pshape[0]) * pshape[1] * pshape[2];
+  if (n <= 0) return 0;
+  op_patch_kernel<<<blocks_for(n), kThreads, 0, static_cast<cudaStream_t>(stream)>>>(
+      field, fshape[0], fshape[1], fshape[2], patch, pshape[0], pshape[1], pshape[2], offset[0], offset[1], offset[2], signal);
+  return op_launch_check("add_source_patch");
+}
+
+int fdtd_op_add_line_patch(float* field, const int* fshape, const float* coeff, const int* pshape,
+                           const int* offset, const float* incident, const int64_t* sample_idx, int axis,
+                           float scale, void* stream) {
+  if (!field || !fshape || !coeff || !pshape || !offset || !incident || !sample_idx || axis < 0 || axis > 2)
+    return op_fail(FDTD_ERR_INVALID_ARG, "add_line_patch: bad arguments");
+  const int64_t n = static_cast<int64_t>(pshape[0]) * pshape[1] * pshape[2];
+  if (n <= 0) return 0;
+  op_line_patch_kernel<<<blocks_for(n), kThreads, 0, static_cast<cudaStream_t>(stream)>>>(
+      field, fshape[0], fshape[1], fshape[2], coeff, pshape[0], pshape[1], pshape[2], offset[0], offset[1],
+      offset[2], incident, sample_idx, axis, scale);
+  return op_launch_check("add_line_patch");
+}
+
+int fdtd_op_aux_magnetic(int n_e, float* h, const float* e, const float* h_decay, const float* h_curl,
+                         void* stream) {
+  if (n_e < 2 || !h || !e || !h_decay || !h_curl) return op_fail(FDTD_ERR_INVALID_ARG, "aux_magnetic: bad arguments");
+  op_aux_h_kernel<<<blocks_for(n_e), kThreads, 0, static_cast<cudaStream_t>(stream)>>>(n_e, h, e, h_decay, h_curl);
+  return op_launch_check("aux_magnetic");
+}
+
+int fdtd_op_aux_electric(int n_e, float* e, const float* h, const float* e_decay, const float* e_curl,
+                         int source_index, float source_value, void* stream) {
+  if (n_e < 2 || !h || !e || !e_decay || !e_curl) return op_fail(FDTD_ERR_INVALID_ARG, "aux_electric: bad arguments");
+  // Interior cells read h only, so a single pass is race free.
+  op_aux_e_kernel<<<blocks_for(n_e), kThreads, 0, static_cast<cudaStream_t>(stream)>>>(n_e, e, h, e_decay, e_curl,
+                                                                                         source_index, source_value);
+  return op_launch_check("aux_electric");
+}
+
+int fdtd_op_point_observers(const float* field, const int* fshape, int n_points, const int* pi, const int* pj,
+                            const int* pk, float* re, float* im, float wcos, float wsin, void* stream) {
+  if (!field || !fshape || n_points < 0 || !pi || !pj || !pk || !re || !im)
+    return op_fail(FDTD_ERR_INVALID_ARG, "point_observers: bad arguments");
+  if (n_points == 0) return 0;
+  op_points_kernel<<<blocks_for(n_points), kThreads, 0, static_cast<cudaStream_t>(stream)>>>(
+      field, fshape[1], fshape[2], n_points, pi, pj, pk, re, im, wcos, wsin);
+  return op_launch_check("point_observers");
+}
+
+int fdtd_op_plane_observer(const float* field, const int* fshape, int axis, int index, float* re, float* im,
+                           float wcos, float wsin, void* stream) {
+  if (!field || !fshape || axis < 0 || axis > 2 || !re || !im || index < 0 || index >= fshape[axis])
+    return op_fail(FDTD_ERR_INVALID_ARG, "plane_observer: bad arguments");
+  const int da = axis == 0 ? fshape[1] : fshape[0];
+  const int db = axis == 2 ? fshape[1] : fshape[2];
+  op_plane_kernel<<<blocks_for(static_cast<int64_t>(da) * db), kThreads, 0, static_cast<cudaStream_t>(stream)>>>(
+      field, fshape[0], fshape[1], fshape[2], axis, index, re, im, wcos, wsin);
+  return op_launch_check("plane_observer");
+}
+
+int fdtd_op_dft_volume(int64_t n, int n_freq, const float* field, float* re, float* im, const float* wcos,
+                       const float* wsin, void* stream) {
+  if (n < 0 || n_freq <= 0 || !field || !re || !im || !wcos || !wsin)
+    return op_fail(FDTD_ERR_INVALID_ARG, "dft_volume: bad arguments");
+  if (n == 0) return 0;
+  op_dft_volume_kernel<<<blocks_for(n), kThreads, 0, static_cast<cudaStream_t>(stream)>>>(n, n_freq, field, re, im, wcos, wsin);
+  return op_launch_check("dft_volume");
+}
+
+int fdtd_op_clamp_face(float* field, const int* fshape, int axis, int side, void* stream) {
+  if (!field || !fshape || axis < 0 || axis > 2 || side < 0 || side > 1)
+    return op_fail(FDTD_ERR_INVALID_ARG, "clamp_face: bad arguments");
+  const int da = axis == 0 ? fshape[1] : fshape[0];
+  const int db = axis == 2 ? fshape[1] : fshape[2];
+  op_clamp_kernel<<<blocks_for(static_cast<int64_t>(da) * db), kThreads, 0, static_cast<cudaStream_t>(stream)>>>(
+      field, fshape[0], fshape[1], fshape[2], axis, side);
+  return op_launch_check("clamp_face");
+}
+
+}  // extern "C"

@@ -1,0 +1,777 @@
+"""Scene description and compilation into the solver-scene tensors of the hot path.
+
+The reference compiles a ``witwin.maxwell.Scene`` (through the ``witwin.core``
+geometry layer) into per-Yee-component tensors: permittivities, update
+coefficients, CPML profiles, ADE drive templates, source patches and monitor
+index sets (witwin/maxwell/scene.py:1260-1481, fdtd/runtime/materials.py,
+fdtd/boundary/cpml.py, fdtd/excitation/*, fdtd/observers.py).  This module
+produces the same tensors for scenes built from axis-aligned boxes and spheres
+on a uniform grid, which is what the FDTD hot path consumes.  Geometry
+rasterisation is node-based (a node is inside a structure or not) followed by
+the reference's node-to-Yee-component averaging
+(fdtd/runtime/materials.py:399-407); the reference's subpixel smoothing of
+arbitrary geometry belongs to the scene compiler and is not part of this
+package.
+
+Everything here is host-side numpy in float64 with float32 results, as in the
+reference.  Cell-index coordinates are node indices of the full grid
+(CPML cells included): node i sits at x = i * dx.
+"""
+from __future__ import annotations
+
+import math
+from dataclasses import dataclass, field
+from typing import Sequence
+
+import numpy as np
+
+# CODATA 2018 constants, witwin/maxwell/constants.py:24-36.
+EPSILON_0 = 8.8541878128e-12
+MU_0 = 1.25663706212e-6
+C_0 = 299792458.0
+ETA_0 = 376.730313668
+
+BOUNDARY_NONE = 0
+BOUNDARY_PML = 1
+BOUNDARY_PERIODIC = 2
+BOUNDARY_BLOCH = 3
+BOUNDARY_PEC = 4
+BOUNDARY_PMC = 5
+
+COMPONENTS = ("Ex", "Ey", "Ez", "Hx", "Hy", "Hz")
+COMP_INDEX = {name: idx for idx, name in enumerate(COMPONENTS)}
+
+# Default CPML grading, witwin/maxwell/fdtd/boundary/cpml.py:9-21.
+DEFAULT_CPML_CONFIG = {"grading_order": 3.0, "kappa_max": 1.0, "alpha_max": 0.0, "reflection": 1e-6}
+# Point dipole reference width, witwin/maxwell/sources.py:21.
+POINT_DIPOLE_REFERENCE_WIDTH = 0.02
+# TFSF auxiliary line absorber, witwin/maxwell/fdtd/excitation/tfsf_state.py:46.
+TFSF_ABSORBER_CELLS = 20
+
+
+def component_shape(name: str, nodes: Sequence[int]) -> tuple[int, int, int]:
+    """Yee shape of a component on a node grid (witwin/maxwell/fdtd/runtime/stepping.py:1625-1630)."""
+    nx, ny, nz = (int(v) for v in nodes)
+    return {
+        "Ex": (nx - 1, ny, nz),
+        "Ey": (nx, ny - 1, nz),
+        "Ez": (nx, ny, nz - 1),
+        "Hx": (nx, ny - 1, nz - 1),
+        "Hy": (nx - 1, ny, nz - 1),
+        "Hz": (nx - 1, ny - 1, nz),
+    }[name]
+
+
+# --------------------------------------------------------------------------
+# Source time functions (witwin/maxwell/sources.py:181-330, waveforms.py:30-61)
+# --------------------------------------------------------------------------
+@dataclass(frozen=True)
+class GaussianPulse:
+    frequency: float
+    fwidth: float
+    amplitude: float = 1.0
+    phase: float = 0.0
+    delay: float | None = None
+    kind: str = "gaussian_pulse"
+
+    @property
+    def sigma_t(self) -> float:
+        return 1.0 / (2.0 * math.pi * self.fwidth)
+
+    @property
+    def resolved_delay(self) -> float:
+        return 6.0 * self.sigma_t if self.delay is None else float(self.delay)
+
+    def evaluate(self, t: float) -> float:
+        tau = float(t) - self.resolved_delay
+        envelope = math.exp(-0.5 * (tau / self.sigma_t) ** 2)
+        return self.amplitude * envelope * math.cos(2.0 * math.pi * self.frequency * tau + self.phase)
+
+    @property
+    def characteristic_frequency(self) -> float:
+        return max(self.frequency, self.frequency + 3.0 * self.fwidth)
+
+
+@dataclass(frozen=True)
+class CW:
+    frequency: float
+    amplitude: float = 1.0
+    phase: float = 0.0
+    kind: str = "cw"
+
+    def evaluate(self, t: float) -> float:
+        return self.amplitude * math.cos(2.0 * math.pi * self.frequency * float(t) + self.phase)
+
+    @property
+    def characteristic_frequency(self) -> float:
+        return self.frequency
+
+
+@dataclass(frozen=True)
+class CustomSourceTime:
+    """Sampled waveform table, linear interpolation, zero outside (waveforms.py:63-66)."""
+
+    times: tuple[float, ...]
+    amplitudes: tuple[float, ...]
+    frequency: float = 0.0
+    kind: str = "custom"
+
+    def evaluate(self, t: float) -> float:
+        return float(np.interp(float(t), self.times, self.amplitudes, left=0.0, right=0.0))
+
+    @property
+    def characteristic_frequency(self) -> float:
+        return self.frequency
+
+
+def ramped_cw(frequency: float, ramp_steps: int, dt: float, total_steps: int, amplitude: float = 1.0) -> CustomSourceTime:
+    """CW with a raised-cosine ramp over the first ``ramp_steps`` steps, as a sampled table."""
+    times = np.arange(total_steps + 1, dtype=np.float64) * dt
+    ramp = np.where(
+        np.arange(total_steps + 1) < ramp_steps,
+        0.5 * (1.0 - np.cos(np.pi * np.arange(total_steps + 1) / max(ramp_steps, 1))),
+        1.0,
+    )
+    values = amplitude * ramp * np.cos(2.0 * np.pi * frequency * times)
+    return CustomSourceTime(tuple(times.tolist()), tuple(values.tolist()), frequency=frequency)
+
+
+# --------------------------------------------------------------------------
+# Media (witwin/maxwell/media.py:125-215, 1050-1113)
+# --------------------------------------------------------------------------
+@dataclass(frozen=True)
+class DebyePole:
+    delta_eps: float
+    tau: float
+
+
+@dataclass(frozen=True)
+class DrudePole:
+    plasma_frequency: float  # Hz; 2*pi applied at compile (media.py:149-155)
+    gamma: float  # Hz
+
+
+@dataclass(frozen=True)
+class LorentzPole:
+    delta_eps: float
+    resonance_frequency: float  # Hz
+    gamma: float  # Hz
+
+
+@dataclass(frozen=True)
+class Medium:
+    eps_r: float = 1.0
+    poles: tuple = ()
+    eps_diag: tuple[float, float, float] | None = None  # diagonal anisotropy (eps_xx, eps_yy, eps_zz)
+
+    @staticmethod
+    def debye(eps_inf: float, delta_eps: float, tau: float) -> "Medium":
+        return Medium(eps_r=eps_inf, poles=(DebyePole(delta_eps, tau),))
+
+    @staticmethod
+    def drude(plasma_frequency: float, gamma: float, eps_inf: float = 1.0) -> "Medium":
+        return Medium(eps_r=eps_inf, poles=(DrudePole(plasma_frequency, gamma),))
+
+    @staticmethod
+    def lorentz(eps_inf: float, delta_eps: float, resonance_frequency: float, gamma: float) -> "Medium":
+        return Medium(eps_r=eps_inf, poles=(LorentzPole(delta_eps, resonance_frequency, gamma),))
+
+    def axis_eps(self, axis: int) -> float:
+        return float(self.eps_diag[axis]) if self.eps_diag is not None else float(self.eps_r)
+
+
+# --------------------------------------------------------------------------
+# Geometry in node-index coordinates
+# --------------------------------------------------------------------------
+@dataclass(frozen=True)
+class Box:
+    """Cells [lo, hi) per axis, i.e. nodes lo..hi inclusive."""
+
+    lo: tuple[float, float, float]
+    hi: tuple[float, float, float]
+
+    def node_mask(self, nodes: Sequence[int]) -> np.ndarray:
+        axes = [np.arange(n, dtype=np.float64) for n in nodes]
+        m = [(a >= lo) & (a <= hi) for a, lo, hi in zip(axes, self.lo, self.hi)]
+        return m[0][:, None, None] & m[1][None, :, None] & m[2][None, None, :]
+
+
+@dataclass(frozen=True)
+class Sphere:
+    center: tuple[float, float, float]
+    radius: float
+
+    def node_mask(self, nodes: Sequence[int]) -> np.ndarray:
+        x = np.arange(nodes[0], dtype=np.float64)[:, None, None] - self.center[0]
+        y = np.arange(nodes[1], dtype=np.float64)[None, :, None] - self.center[1]
+        z = np.arange(nodes[2], dtype=np.float64)[None, None, :] - self.center[2]
+        return x * x + y * y + z * z <= self.radius * self.radius
+
+
+@dataclass(frozen=True)
+class Structure:
+    geometry: object
+    medium: Medium
+
+
+@dataclass(frozen=True)
+class MaterialRegion:
+    """Design region with per-cell relative permittivity (witwin/maxwell/scene.py:567-610).
+
+    ``eps_r`` holds one value per cell of ``box`` (shape hi - lo); node values
+    take the cell's value for the cell whose low corner is the node.
+    """
+
+    lo: tuple[int, int, int]
+    hi: tuple[int, int, int]
+    eps_r: np.ndarray
+
+
+# --------------------------------------------------------------------------
+# Sources and monitors
+# --------------------------------------------------------------------------
+@dataclass(frozen=True)
+class PointDipole:
+    position: tuple[float, float, float]  # node-index coordinates
+    polarization: str  # "Ex" | "Ey" | "Ez"
+    source_time: object
+    width: float | None = None  # metres; default POINT_DIPOLE_REFERENCE_WIDTH
+
+
+@dataclass(frozen=True)
+class PlaneWaveTFSF:
+    """Axis-aligned plane wave injected through a TFSF box (or slab along the propagation axis)."""
+
+    direction: tuple[int, int, int]  # e.g. (1, 0, 0)
+    polarization: tuple[float, float, float]  # e.g. (0, 0, 1)
+    source_time: object
+    lower: tuple[int, int, int]  # TF box node indices
+    upper: tuple[int, int, int]
+    slab: bool = False
+
+
+@dataclass(frozen=True)
+class PlaneMonitor:
+    name: str
+    axis: int
+    index: int
+    components: tuple[str, ...] = ("Ex", "Ey", "Ez", "Hx", "Hy", "Hz")
+    frequencies: tuple[float, ...] = ()
+    lo: tuple[int, int] | None = None  # in-plane bounds (optional finite plane)
+    hi: tuple[int, int] | None = None
+
+
+@dataclass(frozen=True)
+class PointMonitor:
+    name: str
+    index: tuple[int, int, int]
+    components: tuple[str, ...] = ("Ex", "Ey", "Ez", "Hx", "Hy", "Hz")
+    frequencies: tuple[float, ...] = ()
+
+
+def tangential_components(axis: int) -> tuple[str, ...]:
+    """Tangential field components of a monitor plane (witwin/maxwell/monitors.py:71-77)."""
+    return {0: ("Ey", "Ez", "Hy", "Hz"), 1: ("Ex", "Ez", "Hx", "Hz"), 2: ("Ex", "Ey", "Hx", "Hy")}[axis]
+
+
+def flux_monitor(name: str, axis: int, index: int, frequencies, lo=None, hi=None) -> PlaneMonitor:
+    return PlaneMonitor(name, axis, index, tangential_components(axis), tuple(frequencies), lo, hi)
+
+
+def closed_box_monitor(name: str, lo: Sequence[int], hi: Sequence[int], frequencies) -> list[PlaneMonitor]:
+    """Six finite flux planes bounding [lo, hi] (witwin/maxwell/monitors.py:323-376)."""
+    faces = []
+    for axis in range(3):
+        others = [a for a in range(3) if a != axis]
+        plo = (int(lo[others[0]]), int(lo[others[1]]))
+        phi = (int(hi[others[0]]), int(hi[others[1]]))
+        for side, index in (("lo", lo[axis]), ("hi", hi[axis])):
+            faces.append(flux_monitor(f"{name}_{'xyz'[axis]}{side}", axis, int(index), frequencies, plo, phi))
+    return faces
+
+
+@dataclass
+class Scene:
+    """A uniform-grid scene: cells per axis (CPML included), spacing and content."""
+
+    cells: tuple[int, int, int]
+    spacing: float
+    pml_cells: int = 10
+    boundary: tuple[int, int, int, int, int, int] = (BOUNDARY_PML,) * 6
+    structures: list = field(default_factory=list)
+    material_regions: list = field(default_factory=list)
+    sources: list = field(default_factory=list)
+    monitors: list = field(default_factory=list)
+    courant: float = 0.99
+    dt: float | None = None
+
+    @property
+    def nodes(self) -> tuple[int, int, int]:
+        return tuple(int(c) + 1 for c in self.cells)
+
+    def resolve_dt(self) -> float:
+        # Courant-scaled 3-D stability limit, fdtd/solver.py:145-159 (dt2 term).
+        if self.dt is not None:
+            return float(self.dt)
+        d = float(self.spacing)
+        return float(self.courant) / (C_0 * math.sqrt(3.0 / (d * d)))
+
+    def pml_lengths(self) -> tuple[list[int], list[int]]:
+        lo = [self.pml_cells if self.boundary[2 * a] == BOUNDARY_PML else 0 for a in range(3)]
+        hi = [self.pml_cells if self.boundary[2 * a + 1] == BOUNDARY_PML else 0 for a in range(3)]
+        return lo, hi
+
+
+# --------------------------------------------------------------------------
+# Compiled scene (the hot path's inputs)
+# --------------------------------------------------------------------------
+@dataclass
+class CompiledPole:
+    component: str  # "Ex" | "Ey" | "Ez"
+    kind: int  # 0 Debye, 1 Drude, 2 Lorentz
+    decay: float
+    restoring: float
+    box: tuple[int, int, int, int, int, int]
+    drive: np.ndarray  # box-dense float32
+    inv_eps: np.ndarray  # box-dense float32
+
+
+@dataclass
+class CompiledPatch:
+    component: str
+    box: tuple[int, int, int, int, int, int]
+    coeff: np.ndarray  # box-dense float32
+    signal: np.ndarray  # float32 per step
+
+
+@dataclass
+class CompiledLinePatch:
+    component: str
+    box: tuple[int, int, int, int, int, int]
+    coeff: np.ndarray
+    sample_kind: int  # 0 = incident E history, 1 = incident H history
+    sample_axis: int
+    sample_index: np.ndarray  # int32, one per coordinate along sample_axis
+    scale: float
+
+
+@dataclass
+class CompiledAuxLine:
+    e_decay: np.ndarray
+    e_curl: np.ndarray
+    h_decay: np.ndarray
+    h_curl: np.ndarray
+    source_index: int
+    source: np.ndarray  # float32 per step
+
+
+@dataclass
+class CompiledRegion:
+    monitor: str
+    component: str
+    box: tuple[int, int, int, int, int, int]
+
+
+@dataclass
+class CompiledScene:
+    nodes: tuple[int, int, int]
+    spacing: float
+    dt: float
+    time_steps: int
+    boundary: tuple[int, ...]
+    pml_lo: list[int]
+    pml_hi: list[int]
+    inv_e: list[np.ndarray]
+    inv_h: list[np.ndarray]
+    cpml: dict  # b_e, c_e, ik_e, b_h, c_h, ik_h -> list per axis
+    eps: dict  # Ex, Ey, Ez absolute permittivity (float32, Yee shapes)
+    decay: dict  # component -> array or None
+    curl: dict
+    uniform: dict  # component -> (decay_value | None, curl_value | None)
+    poles: list
+    patches: list
+    aux_line: CompiledAuxLine | None
+    line_patches: list
+    regions: list
+    frequencies: tuple[float, ...]
+    monitor_frequencies: dict
+    window: np.ndarray  # float64 per step
+    design: MaterialRegion | None = None
+
+    @property
+    def cells(self) -> int:
+        return int(np.prod([n - 1 for n in self.nodes]))
+
+
+def _avg_node_to_component(node: np.ndarray, name: str) -> np.ndarray:
+    """witwin/maxwell/fdtd/runtime/materials.py:399-407."""
+    if name == "Ex":
+        return 0.5 * (node[:-1, :, :] + node[1:, :, :])
+    if name == "Ey":
+        return 0.5 * (node[:, :-1, :] + node[:, 1:, :])
+    return 0.5 * (node[:, :, :-1] + node[:, :, 1:])
+
+
+def cpml_profile_1d(positions64, nodes64, thickness, dt, vacuum_constant, strength, impedance, config,
+                    *, high_positions64=None, apply_low=True, apply_high=True):
+    """(kappa, b, c) graded by physical depth, witwin/maxwell/fdtd/boundary/cpml.py:114-210."""
+    length = len(positions64)
+    thickness = int(thickness)
+    if thickness <= 0 or not (apply_low or apply_high):
+        return np.ones(length, np.float32), np.zeros(length, np.float32), np.zeros(length, np.float32)
+    nodes64 = np.asarray(nodes64, dtype=np.float64)
+
+    def interface(low):
+        cell_count = len(nodes64) - 1
+        if thickness <= cell_count:
+            return float(nodes64[thickness]) if low else float(nodes64[-1 - thickness])
+        extra = thickness - cell_count
+        if low:
+            return float(nodes64[-1]) + extra * float(nodes64[-1] - nodes64[-2])
+        return float(nodes64[0]) - extra * float(nodes64[1] - nodes64[0])
+
+    m = float(config["grading_order"])
+    kappa_max = float(config["kappa_max"])
+    alpha_max = float(config["alpha_max"])
+    reflection = float(config["reflection"])
+    sigma_numerator = -(m + 1.0) * math.log(reflection) / (2.0 * float(impedance))
+    positions = np.asarray(positions64, dtype=np.float64)
+    high_positions = positions if high_positions64 is None else np.asarray(high_positions64, dtype=np.float64)
+    depth_low = np.zeros(length)
+    depth_high = np.zeros(length)
+    sigma_max_low = sigma_max_high = 0.0
+    if apply_low:
+        low_interface = interface(True)
+        layer_low = low_interface - float(nodes64[0])
+        depth_low = np.clip((low_interface - positions) / layer_low, 0.0, 1.0)
+        sigma_max_low = sigma_numerator / layer_low * strength
+    if apply_high:
+        high_interface = interface(False)
+        layer_high = float(nodes64[-1]) - high_interface
+        depth_high = np.clip((high_positions - high_interface) / layer_high, 0.0, 1.0)
+        sigma_max_high = sigma_numerator / layer_high * strength
+    use_high = depth_high > depth_low
+    depth = np.where(use_high, depth_high, depth_low)
+    sigma_peak = np.where(use_high, sigma_max_high, sigma_max_low)
+    active = depth > 0.0
+    graded = np.zeros(length)
+    graded[active] = depth[active] ** m
+    sigma = sigma_peak * graded
+    kappa = np.ones(length)
+    kappa[active] = 1.0 + (kappa_max - 1.0) * graded[active]
+    alpha = np.zeros(length)
+    alpha[active] = alpha_max * (1.0 - depth[active])
+    decay = np.exp(-(sigma / kappa + alpha) * float(dt) / float(vacuum_constant))
+    denom = sigma + alpha * kappa
+    c = np.zeros(length)
+    mask = denom > 1e-12
+    c[mask] = sigma[mask] * (decay[mask] - 1.0) / (denom[mask] * kappa[mask])
+    return kappa.astype(np.float32), decay.astype(np.float32), c.astype(np.float32)
+
+
+def _source_signal(source_time, dt: float, steps: int) -> np.ndarray:
+    """Host-evaluated waveform per step at t_n = n*dt (excitation/temporal.py:408-491)."""
+    return np.asarray([source_time.evaluate(n * dt) for n in range(steps)], dtype=np.float64).astype(np.float32)
+
+
+def _dipole_patch(scene: Scene, src: PointDipole, eps: dict, dt: float):
+    """Normalised Gaussian point-dipole patch, witwin/maxwell/fdtd/excitation/injection.py:36-61, 214-396.
+
+    The reference evaluates the profile over the cutoff window (3 * max(width,
+    0.01 m), which covers the whole grid at optical scales) in float32; entries
+    that underflow to zero are cropped away here, which leaves the sum unchanged.
+    """
+    d = float(scene.spacing)
+    nodes = scene.nodes
+    width = POINT_DIPOLE_REFERENCE_WIDTH if src.width is None else float(src.width)
+    name = src.polarization
+    shape = component_shape(name, nodes)
+    axis = "xyz".index(name[1])
+    coords = []
+    for a in range(3):
+        base = np.arange(shape[a], dtype=np.float64) * d
+        if a == axis:
+            base = base + 0.5 * d
+        coords.append(base.astype(np.float32))
+    pos = [np.float32(p * d) for p in src.position]
+    dist_sq = ((coords[0][:, None, None] - pos[0]) ** 2 + (coords[1][None, :, None] - pos[1]) ** 2
+               + (coords[2][None, None, :] - pos[2]) ** 2).astype(np.float32)
+
+    def widths(c):
+        w = np.empty_like(c)
+        diffs = c[1:] - c[:-1]
+        w[0] = 0.5 * diffs[0]
+        w[-1] = 0.5 * diffs[-1]
+        w[1:-1] = 0.5 * (diffs[:-1] + diffs[1:])
+        return w
+
+    wv = [widths(c) for c in coords]
+    volumes = wv[0][:, None, None] * wv[1][None, :, None] * wv[2][None, None, :]
+    width_sq = np.float32(2.0 * width ** 2)
+    profile = np.exp(-dist_sq / width_sq).astype(np.float32)
+    mass = np.float32(np.sum(profile * volumes, dtype=np.float32))
+    profile = profile / max(mass, np.finfo(np.float32).eps)
+    patch = (np.float32(-dt) / eps[name]) * profile
+    patch = patch.astype(np.float32)
+    nz = np.nonzero(patch)
+    box = tuple(int(v) for a in range(3) for v in (nz[a].min(), nz[a].max() + 1))
+    coeff = patch[box[0]:box[1], box[2]:box[3], box[4]:box[5]].copy()
+    return box, coeff
+
+
+# TFSF face specs, witwin/maxwell/fdtd/excitation/tfsf_specs.py:46-333:
+# (field, incident, offsets, shape, sample_offsets, delta_axis, sign) built from lower/upper.
+def _tfsf_specs(lower, upper):
+    ix0, iy0, iz0 = lower
+    ix1, iy1, iz1 = upper
+    mag = [
+        ("Hy", "Ez", (ix0 - 1, iy0, iz0), (1, iy1 - iy0 + 1, iz1 - iz0), (ix0, iy0, iz0), 0, +1.0),
+        ("Hz", "Ey", (ix0 - 1, iy0, iz0), (1, iy1 - iy0, iz1 - iz0 + 1), (ix0, iy0, iz0), 0, -1.0),
+        ("Hy", "Ez", (ix1, iy0, iz0), (1, iy1 - iy0 + 1, iz1 - iz0), (ix1, iy0, iz0), 0, -1.0),
+        ("Hz", "Ey", (ix1, iy0, iz0), (1, iy1 - iy0, iz1 - iz0 + 1), (ix1, iy0, iz0), 0, +1.0),
+        ("Hx", "Ez", (ix0, iy0 - 1, iz0), (ix1 - ix0 + 1, 1, iz1 - iz0), (ix0, iy0, iz0), 1, -1.0),
+        ("Hz", "Ex", (ix0, iy0 - 1, iz0), (ix1 - ix0, 1, iz1 - iz0 + 1), (ix0, iy0, iz0), 1, +1.0),
+        ("Hx", "Ez", (ix0, iy1, iz0), (ix1 - ix0 + 1, 1, iz1 - iz0), (ix0, iy1, iz0), 1, +1.0),
+        ("Hz", "Ex", (ix0, iy1, iz0), (ix1 - ix0, 1, iz1 - iz0 + 1), (ix0, iy1, iz0), 1, -1.0),
+        ("Hx", "Ey", (ix0, iy0, iz0 - 1), (ix1 - ix0 + 1, iy1 - iy0, 1), (ix0, iy0, iz0), 2, +1.0),
+        ("Hy", "Ex", (ix0, iy0, iz0 - 1), (ix1 - ix0, iy1 - iy0 + 1, 1), (ix0, iy0, iz0), 2, -1.0),
+        ("Hx", "Ey", (ix0, iy0, iz1), (ix1 - ix0 + 1, iy1 - iy0, 1), (ix0, iy0, iz1), 2, -1.0),
+        ("Hy", "Ex", (ix0, iy0, iz1), (ix1 - ix0, iy1 - iy0 + 1, 1), (ix0, iy0, iz1), 2, +1.0),
+    ]
+    ele = [
+        ("Ey", "Hz", (ix0, iy0, iz0), (1, iy1 - iy0, iz1 - iz0 + 1), (ix0 - 1, iy0, iz0), 0, +1.0),
+        ("Ez", "Hy", (ix0, iy0, iz0), (1, iy1 - iy0 + 1, iz1 - iz0), (ix0 - 1, iy0, iz0), 0, -1.0),
+        ("Ey", "Hz", (ix1, iy0, iz0), (1, iy1 - iy0, iz1 - iz0 + 1), (ix1, iy0, iz0), 0, -1.0),
+        ("Ez", "Hy", (ix1, iy0, iz0), (1, iy1 - iy0 + 1, iz1 - iz0), (ix1, iy0, iz0), 0, +1.0),
+        ("Ex", "Hz", (ix0, iy0, iz0), (ix1 - ix0, 1, iz1 - iz0 + 1), (ix0, iy0 - 1, iz0), 1, -1.0),
+        ("Ez", "Hx", (ix0, iy0, iz0), (ix1 - ix0 + 1, 1, iz1 - iz0), (ix0, iy0 - 1, iz0), 1, +1.0),
+        ("Ex", "Hz", (ix0, iy1, iz0), (ix1 - ix0, 1, iz1 - iz0 + 1), (ix0, iy1, iz0), 1, +1.0),
+        ("Ez", "Hx", (ix0, iy1, iz0), (ix1 - ix0 + 1, 1, iz1 - iz0), (ix0, iy1, iz0), 1, -1.0),
+        ("Ex", "Hy", (ix0, iy0, iz0), (ix1 - ix0, iy1 - iy0 + 1, 1), (ix0, iy0, iz0 - 1), 2, +1.0),
+        ("Ey", "Hx", (ix0, iy0, iz0), (ix1 - ix0 + 1, iy1 - iy0, 1), (ix0, iy0, iz0 - 1), 2, -1.0),
+        ("Ex", "Hy", (ix0, iy0, iz1), (ix1 - ix0, iy1 - iy0 + 1, 1), (ix0, iy0, iz1), 2, -1.0),
+        ("Ey", "Hx", (ix0, iy0, iz1), (ix1 - ix0 + 1, iy1 - iy0, 1), (ix0, iy0, iz1), 2, +1.0),
+    ]
+    return ele, mag
+
+
+def _magnetic_unit_vector(direction, polarization):
+    """witwin/maxwell/fdtd/excitation/tfsf_specs.py:335-346."""
+    d, p = direction, polarization
+    mx = -(d[1] * p[2] - d[2] * p[1])
+    my = -(d[2] * p[0] - d[0] * p[2])
+    mz = -(d[0] * p[1] - d[1] * p[0])
+    mag = math.sqrt(mx * mx + my * my + mz * mz)
+    return {"Hx": mx / mag, "Hy": my / mag, "Hz": mz / mag}
+
+
+def _compile_tfsf(scene: Scene, src: PlaneWaveTFSF, curl: dict, dt: float, steps: int):
+    """Axis-aligned plane-wave TFSF (excitation/tfsf_state.py:293-357, spatial.py:311-469)."""
+    d = float(scene.spacing)
+    nodes = scene.nodes
+    axis = int(np.argmax(np.abs(src.direction)))
+    sign = 1 if src.direction[axis] > 0 else -1
+    if any(src.direction[a] != 0 for a in range(3) if a != axis):
+        raise ValueError("only axis-aligned plane waves are supported")
+    # 1-D incident line over the domain extent along the axis plus the absorber
+    # (tfsf_state.py:57-76): s_min = 0, ds = d.
+    s_span = (nodes[axis] - 1) * d
+    s_max = s_span + TFSF_ABSORBER_CELLS * d
+    ne = max(int(math.ceil(s_max / d)) + 1, 4)
+    eps_line = 1.0 / (ETA_0 * C_0)
+    mu_line = ETA_0 / C_0
+    sigma_e = np.zeros(ne, np.float32)
+    sigma_h = np.zeros(ne - 1, np.float32)
+    edge_e = min(TFSF_ABSORBER_CELLS, ne - 1)
+    edge_h = min(TFSF_ABSORBER_CELLS, ne - 1)
+    sigma_e[-edge_e:] = np.float32(0.35) * ((np.arange(edge_e, dtype=np.float32) + 1.0) / edge_e) ** 2
+    sigma_h[-edge_h:] = np.float32(0.35) * ((np.arange(edge_h, dtype=np.float32) + 0.5) / edge_h) ** 2
+    sf_e = (np.float32(0.5 * dt) * sigma_e / np.float32(eps_line)).astype(np.float32)
+    sf_h = (np.float32(0.5 * dt) * sigma_h / np.float32(mu_line)).astype(np.float32)
+    aux = CompiledAuxLine(
+        e_decay=((1.0 - sf_e) / (1.0 + sf_e)).astype(np.float32),
+        e_curl=(np.float32(dt / (eps_line * d)) / (1.0 + sf_e)).astype(np.float32),
+        h_decay=((1.0 - sf_h) / (1.0 + sf_h)).astype(np.float32),
+        h_curl=(np.float32(dt / (mu_line * d)) / (1.0 + sf_h)).astype(np.float32),
+        source_index=0,
+        source=_source_signal(src.source_time, dt, steps),
+    )
+    electric_vector = {"Ex": src.polarization[0], "Ey": src.polarization[1], "Ez": src.polarization[2]}
+    magnetic_vector = _magnetic_unit_vector(src.direction, src.polarization)
+    ele, mag = _tfsf_specs(src.lower, src.upper)
+    if src.slab:
+        # Slab injection keeps the two faces normal to the propagation axis
+        # (tfsf_specs.py:322-332).
+        ele = [s for s in ele if s[5] == axis]
+        mag = [s for s in mag if s[5] == axis]
+    out = []
+    for specs, vector, kind in ((mag, electric_vector, 0), (ele, magnetic_vector, 1)):
+        for fname, iname, offs, shape, soffs, delta_axis, sgn in specs:
+            scale = float(vector[iname])
+            if abs(sgn * scale) <= 1e-12:
+                continue
+            box = (offs[0], offs[0] + shape[0], offs[1], offs[1] + shape[1], offs[2], offs[2] + shape[2])
+            c = curl[fname]
+            c_arr = np.broadcast_to(c, component_shape(fname, nodes)) if np.ndim(c) == 0 else c
+            coeff = (sgn * (c_arr[box[0]:box[1], box[2]:box[3], box[4]:box[5]] / np.float32(d))).astype(np.float32)
+            start = soffs[axis]
+            length = shape[axis]
+            idx = np.arange(start, start + length, dtype=np.int64)
+            if sign < 0:
+                max_index = nodes[axis] - 1 if kind == 0 else nodes[axis] - 2
+                idx = max_index - idx
+            out.append(CompiledLinePatch(fname, box, np.ascontiguousarray(coeff), kind, axis,
+                                         idx.astype(np.int32), scale))
+    return aux, out
+
+
+def compile_scene(scene: Scene, time_steps: int) -> CompiledScene:
+    """Compile a scene into the solver tensors consumed by the FDTD step path."""
+    nodes = scene.nodes
+    d = float(scene.spacing)
+    dt = scene.resolve_dt()
+    pml_lo, pml_hi = scene.pml_lengths()
+    # --- grid: uniform spacing (scene.py:1245-1281) ---
+    inv_e = [np.full(n, 1.0 / d, dtype=np.float64).astype(np.float32) for n in nodes]
+    inv_h = [np.full(n - 1, 1.0 / d, dtype=np.float64).astype(np.float32) for n in nodes]
+    # --- materials: node rasterisation, then node -> component averaging ---
+    eps_node = [np.ones(nodes, dtype=np.float64) for _ in range(3)]
+    pole_weights = []  # list of (pole, node weight array)
+    for st in scene.structures:
+        mask = st.geometry.node_mask(nodes)
+        for a in range(3):
+            eps_node[a][mask] = st.medium.axis_eps(a)
+        for entry in pole_weights:
+            entry[1][mask] = 0.0
+        for pole in st.medium.poles:
+            w = np.zeros(nodes, dtype=np.float64)
+            w[mask] = 1.0
+            pole_weights.append((pole, w))
+    design = None
+    for region in scene.material_regions:
+        lo, hi = region.lo, region.hi
+        vals = np.asarray(region.eps_r, dtype=np.float64)
+        for a in range(3):
+            eps_node[a][lo[0]:hi[0], lo[1]:hi[1], lo[2]:hi[2]] = vals
+        design = region
+    eps = {}
+    for a, name in enumerate(("Ex", "Ey", "Ez")):
+        eps[name] = (EPSILON_0 * _avg_node_to_component(eps_node[a], name)).astype(np.float32)
+    # --- update coefficients (materials.py:942-1008): lossless, CPML not folded ---
+    decay, curl, uniform = {}, {}, {}
+    for name in ("Ex", "Ey", "Ez"):
+        c = (np.float32(dt) / eps[name]).astype(np.float32)
+        decay[name] = None
+        if float(c.min()) == float(c.max()):
+            curl[name] = None
+            uniform[name] = (1.0, float(c.flat[0]))
+        else:
+            curl[name] = c
+            uniform[name] = (1.0, None)
+    h_curl = float(np.float32(dt) / np.float32(MU_0))
+    for name in ("Hx", "Hy", "Hz"):
+        decay[name] = None
+        curl[name] = None
+        uniform[name] = (1.0, h_curl)
+    # --- CPML profiles (cpml.py:383-414) ---
+    eta0 = math.sqrt(MU_0 / EPSILON_0)
+    magnetic_strength = float(np.float32(MU_0 / EPSILON_0))
+    cp = {k: [] for k in ("b_e", "c_e", "ik_e", "b_h", "c_h", "ik_h")}
+    for a in range(3):
+        nodes64 = np.arange(nodes[a], dtype=np.float64) * d
+        half64 = nodes64[:-1] + 0.5 * d
+        apply_low = scene.boundary[2 * a] == BOUNDARY_PML
+        apply_high = scene.boundary[2 * a + 1] == BOUNDARY_PML
+        ke, be, ce = cpml_profile_1d(nodes64, nodes64, scene.pml_cells, dt, EPSILON_0, 1.0, eta0,
+                                     DEFAULT_CPML_CONFIG, apply_low=apply_low, apply_high=apply_high)
+        kh, bh, ch = cpml_profile_1d(half64, nodes64, scene.pml_cells, dt, MU_0, magnetic_strength, eta0,
+                                     DEFAULT_CPML_CONFIG, high_positions64=nodes64[1:], apply_low=apply_low,
+                                     apply_high=apply_high)
+        cp["b_e"].append(be)
+        cp["c_e"].append(ce)
+        cp["ik_e"].append((np.float32(1.0) / ke).astype(np.float32))
+        cp["b_h"].append(bh)
+        cp["c_h"].append(ch)
+        cp["ik_h"].append((np.float32(1.0) / kh).astype(np.float32))
+    # --- ADE templates (materials.py:530-589) ---
+    poles = []
+    for pole, w_node in pole_weights:
+        if isinstance(pole, DebyePole):
+            kind = 0
+            decay_v = (2.0 * pole.tau - dt) / (2.0 * pole.tau + dt)
+            restoring = 0.0
+            base = 2.0 * EPSILON_0 * pole.delta_eps * dt / (2.0 * pole.tau + dt)
+        elif isinstance(pole, DrudePole):
+            kind = 1
+            wp = 2.0 * math.pi * pole.plasma_frequency
+            g = 2.0 * math.pi * pole.gamma
+            denom = 2.0 + g * dt
+            decay_v = (2.0 - g * dt) / denom
+            restoring = 0.0
+            base = 2.0 * EPSILON_0 * wp * wp * dt / denom
+        else:
+            kind = 2
+            w0 = 2.0 * math.pi * pole.resonance_frequency
+            g = 2.0 * math.pi * pole.gamma
+            denom = 2.0 + g * dt
+            decay_v = (2.0 - g * dt) / denom
+            restoring = 2.0 * w0 * w0 * dt / denom
+            base = 2.0 * EPSILON_0 * pole.delta_eps * w0 * w0 * dt / denom
+        for name in ("Ex", "Ey", "Ez"):
+            weight = _avg_node_to_component(w_node, name).astype(np.float32)
+            nzi = np.nonzero(weight)
+            if nzi[0].size == 0:
+                continue
+            box = tuple(int(v) for a in range(3) for v in (nzi[a].min(), nzi[a].max() + 1))
+            sl = (slice(box[0], box[1]), slice(box[2], box[3]), slice(box[4], box[5]))
+            drive = (weight[sl] * np.float32(base)).astype(np.float32)
+            inv_eps = (np.float32(1.0) / eps[name][sl]).astype(np.float32)
+            poles.append(CompiledPole(name, kind, float(decay_v), float(restoring), box,
+                                      np.ascontiguousarray(drive), np.ascontiguousarray(inv_eps)))
+    # --- sources ---
+    patches, line_patches, aux_line = [], [], None
+    for src in scene.sources:
+        if isinstance(src, PointDipole):
+            box, coeff = _dipole_patch(scene, src, eps, dt)
+            patches.append(CompiledPatch(src.polarization, box, coeff, _source_signal(src.source_time, dt, time_steps)))
+        elif isinstance(src, PlaneWaveTFSF):
+            if aux_line is not None:
+                raise ValueError("one TFSF source per scene")
+            curl_full = {}
+            for name in COMPONENTS:
+                curl_full[name] = curl[name] if curl[name] is not None else np.float32(uniform[name][1])
+            aux_line, line_patches = _compile_tfsf(scene, src, curl_full, dt, time_steps)
+        else:
+            raise TypeError(f"unsupported source {type(src).__name__}")
+    # --- monitors ---
+    regions = []
+    freq_list = []
+    mon_freqs = {}
+    for mon in scene.monitors:
+        mon_freqs[mon.name] = tuple(float(f) for f in mon.frequencies)
+        for f in mon.frequencies:
+            if float(f) not in freq_list:
+                freq_list.append(float(f))
+        for comp in mon.components:
+            shape = component_shape(comp, nodes)
+            if isinstance(mon, PointMonitor):
+                i, j, k = mon.index
+                box = (i, i + 1, j, j + 1, k, k + 1)
+            else:
+                box = [0, shape[0], 0, shape[1], 0, shape[2]]
+                box[2 * mon.axis] = mon.index
+                box[2 * mon.axis + 1] = mon.index + 1
+                if mon.lo is not None:
+                    others = [a for a in range(3) if a != mon.axis]
+                    for o, lo_v, hi_v in zip(others, mon.lo, mon.hi):
+                        box[2 * o] = int(lo_v)
+                        box[2 * o + 1] = min(int(hi_v) + 1, shape[o])
+                box = tuple(box)
+            regions.append(CompiledRegion(mon.name, comp, box))
+    window = np.ones(time_steps, dtype=np.float64)  # pulses force window "none" (spectral.py:244-267)
+    return CompiledScene(
+        nodes=nodes, spacing=d, dt=dt, time_steps=time_steps, boundary=tuple(scene.boundary), pml_lo=pml_lo,
+        pml_hi=pml_hi, inv_e=inv_e, inv_h=inv_h, cpml=cp, eps=eps, decay=decay, curl=curl, uniform=uniform,
+        poles=poles, patches=patches, aux_line=aux_line, line_patches=line_patches, regions=regions,
+        frequencies=tuple(freq_list), monitor_frequencies=mon_freqs, window=window, design=design,
+    )

@@ -1,0 +1,100 @@
+"""Synthetic scenes of the benchmark workloads (seeded, uniform 25 nm grids).
+
+Each builder returns a ``Scene`` with the shapes, materials, sources and
+monitors of one workload; the grids are synthetic stand-ins for scenes the
+reference would compile from geometry.  Cell counts include the CPML cells.
+"""
+from __future__ import annotations
+
+import numpy as np
+
+from .scene import (
+    Box,
+    GaussianPulse,
+    Medium,
+    PlaneMonitor,
+    PlaneWaveTFSF,
+    PointDipole,
+    PointMonitor,
+    Scene,
+    Sphere,
+    Structure,
+    closed_box_monitor,
+    flux_monitor,
+)
+
+SPACING = 25e-9
+
+
+def plain_small(cells: int = 64, pml: int = 10) -> Scene:
+    """64^3 cells, 10-cell CPML, vacuum with a centred 24^3 eps_r=4 box, Ez dipole at
+    (20,32,32) with a 300/100 THz Gaussian pulse, z=44 plane + point monitor at 250/300/350 THz."""
+    sc = Scene(cells=(cells,) * 3, spacing=SPACING, pml_cells=pml)
+    lo = (cells - 24) // 2
+    sc.structures.append(Structure(Box((lo,) * 3, (lo + 24,) * 3), Medium(eps_r=4.0)))
+    sc.sources.append(PointDipole((20, cells // 2, cells // 2), "Ez", GaussianPulse(300e12, 100e12), width=SPACING))
+    freqs = (250e12, 300e12, 350e12)
+    sc.monitors.append(PlaneMonitor("plane_z", 2, lo + 24, frequencies=freqs))
+    sc.monitors.append(PointMonitor("point", (lo + 24, cells // 2, cells // 2), frequencies=freqs))
+    return sc
+
+
+def dispersive_256(cells: int = 256, pml: int = 12, n_freq: int = 16) -> Scene:
+    """256^3 cells, 12-cell CPML; radius-60 Lorentz sphere (eps_inf 2, delta_eps 3, 250 THz,
+    gamma 20 THz) at the centre; 40-cell Drude slab x in [40, 80) (omega_p 2e15 rad/s,
+    gamma 1e14 rad/s); x-normal Ez plane wave (300/100 THz pulse) through a TFSF box inset
+    2 cells inside the CPML; 16 frequencies 200-400 THz on two z-normal flux planes and a
+    closed six-face flux box."""
+    scale = cells / 256.0
+    sc = Scene(cells=(cells,) * 3, spacing=SPACING, pml_cells=pml)
+    c = cells / 2.0
+    sc.structures.append(Structure(Sphere((c, c, c), 60.0 * scale), Medium.lorentz(2.0, 3.0, 250e12, 20e12)))
+    x0, x1 = int(round(40 * scale)), int(round(80 * scale))
+    sc.structures.append(Structure(Box((x0, 0, 0), (x1, cells, cells)), Medium.drude(2e15 / (2 * np.pi), 1e14 / (2 * np.pi))))
+    lo = pml + 2
+    hi = cells - pml - 2
+    sc.sources.append(PlaneWaveTFSF((1, 0, 0), (0, 0, 1), GaussianPulse(300e12, 100e12), (lo,) * 3, (hi,) * 3))
+    freqs = tuple(np.linspace(200e12, 400e12, n_freq))
+    sc.monitors.append(flux_monitor("flux_z_lo", 2, int(round(40 * scale)), freqs))
+    sc.monitors.append(flux_monitor("flux_z_hi", 2, int(round(216 * scale)), freqs))
+    b0, b1 = int(round(28 * scale)), int(round(228 * scale))
+    sc.monitors.extend(closed_box_monitor("box", (b0,) * 3, (b1,) * 3, freqs))
+    return sc
+
+
+def algorithmic_bytes(compiled, *, kahan: bool = True, storage_bytes: int = 4) -> dict:
+    """Compulsory HBM bytes per cell-update of one leapfrog step (every state array read
+    once and written once), split into the fused step kernel's share and the whole step.
+
+    fields: 6 arrays R+W; coefficients: 4 B per non-uniform decay/curl array; CPML psi:
+    4 arrays per axis R+W over the slab fraction 2L/N; ADE: state arrays R+W over the
+    material cells; monitors: the per-step running-DFT read-modify-write of every
+    monitor point (F frequencies, re/im, x2 with Kahan compensation).  The fused kernel
+    itself writes one 4-byte sample per monitor point and step; the batched DFT flush
+    does the accumulator traffic.
+    """
+    nodes = compiled.nodes
+    cells = float(np.prod([n - 1 for n in nodes]))
+    s = float(storage_bytes)
+    out = {"fields": 6 * 2 * s}
+    nonuni = sum(1 for n in ("Ex", "Ey", "Ez", "Hx", "Hy", "Hz") for arr in (compiled.decay[n], compiled.curl[n]) if arr is not None)
+    out["coefficients"] = 4.0 * nonuni
+    psi = 0.0
+    for a in range(3):
+        L = compiled.pml_lo[a] + compiled.pml_hi[a]
+        psi += 4 * 2 * 4.0 * L / (nodes[a] - 1)
+    out["cpml_psi"] = psi
+    ade = 0.0
+    for p in compiled.poles:
+        region = float(np.count_nonzero(p.drive))
+        states = 2 if p.kind == 2 else 1
+        ade += region * states * 2 * s
+    out["ade"] = ade / cells
+    nf = len(compiled.frequencies)
+    points = sum((r.box[1] - r.box[0]) * (r.box[3] - r.box[2]) * (r.box[5] - r.box[4]) for r in compiled.regions)
+    out["monitor_dft"] = points * nf * 2 * 2 * 4.0 * (2 if kahan else 1) / cells
+    out["monitor_samples"] = points * 4.0 / cells
+    out["step_kernel"] = out["fields"] + out["coefficients"] + out["cpml_psi"] + out["ade"] + out["monitor_samples"]
+    out["total"] = out["fields"] + out["coefficients"] + out["cpml_psi"] + out["ade"] + out["monitor_dft"]
+    out["cells"] = cells
+    return out
