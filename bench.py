@@ -218,7 +218,7 @@ def run_b200_arm(args, wm, world, rank, local):
     device = torch.device("cuda", local)
     torch.cuda.set_device(device)
     total_steps = args.warmup + args.steps + 16
-    sc = wm.workloads.dispersive_256()
+    sc = wm.workloads.dispersive_256(cells=args.cells)
     t_compile = time.perf_counter()
     cs = wm.compile_scene(sc, total_steps)
     t_compile = time.perf_counter() - t_compile
@@ -261,7 +261,7 @@ def run_b200_arm(args, wm, world, rank, local):
         "dtype": "f32",
         "data": "synthetic",
         "config": {
-            "workload": WORKLOAD,
+            "workload": WORKLOAD if args.cells == 256 else f"{WORKLOAD} (scaled to {args.cells}^3 cells)",
             "cells": int(cells),
             "nodes": list(cs.nodes),
             "frequencies": len(cs.frequencies),
@@ -293,7 +293,8 @@ def run_b200_arm(args, wm, world, rank, local):
     del solver
     torch.cuda.empty_cache()
     # ---------------- end to end through the public API, host buffers ----------------
-    result["e2e"] = run_e2e(args, wm, cs, device, world)
+    if args.e2e:
+        result["e2e"] = run_e2e(args, wm, cs, device, world)
     if rank == 0 and args.cpu_baseline:
         try:
             threads = os.cpu_count() or 1
@@ -368,6 +369,9 @@ def main():
     ap.add_argument("--sample-block", type=int, default=32)
     ap.add_argument("--autotune", action="store_true")
     ap.add_argument("--no-cpu-baseline", dest="cpu_baseline", action="store_false")
+    ap.add_argument("--no-e2e", dest="e2e", action="store_false")
+    ap.add_argument("--cells", type=int, default=256,
+                    help="cells per axis of the (scaled) workload; 256 is the benchmark, smaller sizes are for profiling")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

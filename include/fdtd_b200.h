@@ -154,6 +154,13 @@ int fdtd_engine_checkpoint_load(fdtd_engine* h, int slot);
 /* Tile shape selection: time the candidate (tile_rows, chunk_planes) pairs on
  * the bound scene (state is saved and restored) and keep the fastest. */
 int fdtd_engine_autotune(fdtd_engine* h, int* tile_rows, int* chunk_planes);
+/* Launch configuration of the fused step kernel: the register budget variant
+ * (1: unconstrained, about 100 registers per thread; 3: at most 85, three
+ * 256-thread CTAs per SM; 2: at most 64, four CTAs per SM) and the number of x
+ * planes each warp marches through (chunk_planes, 0 keeps the current value).
+ * tile_rows is accepted for compatibility and ignored. */
+int fdtd_engine_set_launch(fdtd_engine* h, int variant, int tile_rows, int chunk_planes);
+int fdtd_engine_get_launch(fdtd_engine* h, int* variant, int* tile_rows, int* chunk_planes);
 /* Launch configuration and launch count bookkeeping. */
 int fdtd_engine_info(fdtd_engine* h, int* tile_rows, int* chunk_planes, int* grid_x, int* grid_y,
                      int* block, int64_t* launches);

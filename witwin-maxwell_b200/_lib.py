@@ -65,6 +65,8 @@ _SIGNATURES = {
     "fdtd_engine_info": ([_vp, _c_int_p, _c_int_p, _c_int_p, _c_int_p, _c_int_p, _c_i64_p], _i),
     "fdtd_engine_last_ms": ([_vp, ctypes.POINTER(_f)], _i),
     "fdtd_engine_time_kernel": ([_vp, _i, _i, ctypes.POINTER(_f)], _i),
+    "fdtd_engine_set_launch": ([_vp, _i, _i, _i], _i),
+    "fdtd_engine_get_launch": ([_vp, _c_int_p, _c_int_p, _c_int_p], _i),
     "fdtd_op_update_magnetic": (
         [_i, _i, _i, _i, _i, _vp, _vp, _vp, _vp, _vp, _f, _f, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _c_int_p, _vp],
         _i,

@@ -18,7 +18,8 @@
 #include "engine.cuh"
 
 namespace fdtdb200 {
-__global__ void fused_step_kernel(const StepParams p, int n, int slot);
+template <bool kCpml, bool kCoef, int kMinBlocks>
+__global__ void warp_step_kernel(const StepParams p, int n, int slot);
 }
 
 using namespace fdtdb200;
@@ -216,6 +217,7 @@ struct fdtd_engine {
   int NX = 0, NY = 0, NZ = 0, P = 0, SZ = 0;
   int64_t plane = 0, vol = 0;
   int TY = 0, CX = 0;
+  int variant = 1;  // fused kernel register budget: 1 = up to 128/thread, 2 = 64/thread
   int cur = 0;  // index of the buffer holding the current state
   float* E[2][3] = {};
   float* H[2][3] = {};
@@ -241,12 +243,16 @@ struct fdtd_engine {
   int64_t n_samples = 0, n_samples_e = 0;
   // device tables
   InjectionTerm* d_terms = nullptr;
-  int* d_term_ptr = nullptr;
-  int* d_term_ids = nullptr;
   PoleTerm* d_poles = nullptr;
   SampleRegion* d_regions = nullptr;
-  int* d_region_ptr = nullptr;
-  int* d_region_ids = nullptr;
+  BoxIndex term_ix[2] = {};
+  BoxIndex region_ix[2] = {};
+  int n_terms_ph[2] = {0, 0};
+  int n_regions_ph[2] = {0, 0};
+  int* d_pole_ptr = nullptr;
+  int* d_pole_ids = nullptr;
+  const int* d_plane_bits = nullptr;
+  std::vector<int*> index_bufs;
   RegionFlush* d_flush = nullptr;
   int n_flush = 0;
   int64_t max_region = 0;
@@ -313,7 +319,7 @@ void fill_params(const fdtd_engine* h, StepParams& p) {
   p.TY = h->TY;
   p.CX = h->CX;
   p.Q = h->P / 4;
-  p.ROWS = h->TY + 2;
+  p.ROWS = 1;
   const int src = h->cur, dst = 1 - h->cur;
   for (int c = 0; c < 3; ++c) {
     p.Ein[c] = h->E[src][c];
@@ -347,55 +353,65 @@ void fill_params(const fdtd_engine* h, StepParams& p) {
   for (int f = 0; f < 6; ++f) p.bnd[f] = h->desc.boundary[f];
   p.cpml = h->cpml ? 1 : 0;
   p.terms = h->d_terms;
-  p.term_plane_ptr = h->d_term_ptr;
-  p.term_plane_ids = h->d_term_ids;
-  p.n_terms = static_cast<int>(h->terms.size());
   p.poles = h->d_poles;
+  p.pole_plane_ptr = h->d_pole_ptr;
+  p.pole_plane_ids = h->d_pole_ids;
   p.n_poles = static_cast<int>(h->poles.size());
   p.regions = h->d_regions;
-  p.region_plane_ptr = h->d_region_ptr;
-  p.region_plane_ids = h->d_region_ids;
-  p.n_regions = static_cast<int>(h->regions.size());
+  p.plane_bits = reinterpret_cast<const unsigned*>(h->d_plane_bits);
+  for (int ph = 0; ph < 2; ++ph) {
+    p.term_index[ph] = h->term_ix[ph];
+    p.n_terms[ph] = h->n_terms_ph[ph];
+    p.region_index[ph] = h->region_ix[ph];
+    p.n_regions[ph] = h->n_regions_ph[ph];
+  }
   p.samples = h->samples;
   p.n_samples = h->n_samples;
   p.sample_block = h->M;
 }
 
-size_t smem_bytes(int TY, int P) { return sizeof(float) * 6 * static_cast<size_t>(TY + 2) * (P + 8); }
-int block_threads(int TY, int P) { return ((TY + 2) * (P / 4) + 31) / 32 * 32; }
-
-bool tile_fits(int TY, int P) {
-  return TY >= 1 && block_threads(TY, P) <= 512 && smem_bytes(TY, P) <= 200 * 1024;
-}
+constexpr int kWarpRows = 8;   // warps (y rows) per CTA of the step kernel
+constexpr int kWarpOut = 30;   // z cells produced per warp
 
 void default_tiles(fdtd_engine* h) {
-  const int Q = h->P / 4;
-  int TY = h->desc.tile_rows;
-  if (TY <= 0) {
-    TY = std::max(1, 512 / Q - 2);
-    TY = std::min(TY, std::max(1, h->NY));
-  }
-  while (TY > 1 && !tile_fits(TY, h->P)) --TY;
+  h->TY = 1;
   int CX = h->desc.chunk_planes;
   if (CX <= 0) {
-    // Aim for about 4 CTAs per SM over the whole grid.
-    const int ny_tiles = (h->NY + TY - 1) / TY;
-    const int want_chunks = std::max(1, (148 * 4 + ny_tiles - 1) / ny_tiles);
-    CX = std::max(8, (h->NX + want_chunks - 1) / want_chunks);
+    // about four resident warps per scheduler over the whole grid
+    const int64_t cols = static_cast<int64_t>((h->NY + kWarpRows - 1) / kWarpRows) * ((h->NZ + 29) / 30);
+    const int64_t want_chunks = std::max<int64_t>(1, (148 * 8 + cols - 1) / cols);
+    CX = static_cast<int>(std::max<int64_t>(16, (h->NX + want_chunks - 1) / want_chunks));
   }
-  h->TY = TY;
   h->CX = CX;
+}
+
+dim3 step_grid(const fdtd_engine* h) {
+  return dim3((h->NY + kWarpRows - 1) / kWarpRows, (h->NZ + kWarpOut - 1) / kWarpOut, (h->NX + h->CX - 1) / h->CX);
 }
 
 int launch_step(fdtd_engine* h, int n, int slot) {
   StepParams p;
   fill_params(h, p);
-  const dim3 grid((h->NY + h->TY - 1) / h->TY, (h->NX + h->CX - 1) / h->CX);
-  const int threads = block_threads(h->TY, h->P);
-  const size_t smem = smem_bytes(h->TY, h->P);
-  fused_step_kernel<<<grid, threads, smem, h->stream>>>(p, n, slot);
+  const dim3 grid = step_grid(h);
+  bool coef = false;
+  for (int c = 0; c < 6; ++c) coef = coef || h->ecoef[c][0] || h->ecoef[c][1];
+  const int block = kWarpRows * 32;
+#define FDTD_LAUNCH(CPML, COEF)                                                                  \
+  do {                                                                                           \
+    if (h->variant == 2) warp_step_kernel<CPML, COEF, 4><<<grid, block, 0, h->stream>>>(p, n, slot); \
+    else if (h->variant == 3) warp_step_kernel<CPML, COEF, 3><<<grid, block, 0, h->stream>>>(p, n, slot); \
+    else warp_step_kernel<CPML, COEF, 1><<<grid, block, 0, h->stream>>>(p, n, slot);            \
+  } while (0)
+  if (h->cpml) {
+    if (coef) FDTD_LAUNCH(true, true);
+    else FDTD_LAUNCH(true, false);
+  } else {
+    if (coef) FDTD_LAUNCH(false, true);
+    else FDTD_LAUNCH(false, false);
+  }
+#undef FDTD_LAUNCH
   cudaError_t err = cudaGetLastError();
-  if (err != cudaSuccess) return cuda_fail(err, "fused_step_kernel launch");
+  if (err != cudaSuccess) return cuda_fail(err, "warp_step_kernel launch");
   ++h->launches;
   h->cur = 1 - h->cur;
   return 0;
@@ -445,6 +461,58 @@ void build_plane_csr(int NX, const std::vector<T>& items, std::vector<int>& ptr,
     for (int i = items[x].i0; i < items[x].i1; ++i) ids[fill[i]++] = static_cast<int>(x);
 }
 
+int upload_ints(fdtd_engine* h, const std::vector<int>& v, const int** out) {
+  int* d = nullptr;
+  const size_t n = std::max<size_t>(v.size(), 1);
+  CUDA_TRY(cudaMalloc(&d, n * sizeof(int)));
+  CUDA_TRY(cudaMemsetAsync(d, 0, n * sizeof(int), h->stream));
+  if (!v.empty()) CUDA_TRY(cudaMemcpyAsync(d, v.data(), v.size() * sizeof(int), cudaMemcpyHostToDevice, h->stream));
+  h->index_bufs.push_back(d);
+  *out = d;
+  return 0;
+}
+
+// Build the per-axis CSR index of the selected items (see BoxIndex): each item
+// goes to the axis with the fewest planes / rows / float4 quads.
+template <typename T>
+int build_box_index(fdtd_engine* h, const std::vector<T>& items, const std::vector<int>& select, BoxIndex& out) {
+  const int dims[3] = {h->NX, h->NY, h->P};
+  std::vector<int> ptr[3], ids[3];
+  std::vector<int> axis_of(select.size());
+  for (size_t s = 0; s < select.size(); ++s) {
+    const T& t = items[select[s]];
+    const int ext[3] = {t.i1 - t.i0, t.j1 - t.j0, t.k1 - t.k0};
+    int a = 0;
+    if (ext[1] < ext[a]) a = 1;
+    if (ext[2] < ext[a]) a = 2;
+    axis_of[s] = a;
+  }
+  for (int a = 0; a < 3; ++a) {
+    ptr[a].assign(dims[a] + 1, 0);
+    for (size_t s = 0; s < select.size(); ++s) {
+      if (axis_of[s] != a) continue;
+      const T& t = items[select[s]];
+      const int lo = a == 0 ? t.i0 : (a == 1 ? t.j0 : t.k0);
+      const int hi = a == 0 ? t.i1 : (a == 1 ? t.j1 : t.k1);
+      for (int c = lo; c < hi; ++c) ptr[a][c + 1]++;
+    }
+    for (int c = 0; c < dims[a]; ++c) ptr[a][c + 1] += ptr[a][c];
+    ids[a].assign(ptr[a][dims[a]], 0);
+    std::vector<int> fill(ptr[a].begin(), ptr[a].end() - 1);
+    for (size_t s = 0; s < select.size(); ++s) {
+      if (axis_of[s] != a) continue;
+      const T& t = items[select[s]];
+      const int lo = a == 0 ? t.i0 : (a == 1 ? t.j0 : t.k0);
+      const int hi = a == 0 ? t.i1 : (a == 1 ? t.j1 : t.k1);
+      for (int c = lo; c < hi; ++c) ids[a][fill[c]++] = select[s];
+    }
+    int rc = upload_ints(h, ptr[a], &out.ptr[a]);
+    if (!rc) rc = upload_ints(h, ids[a], &out.ids[a]);
+    if (rc) return rc;
+  }
+  return 0;
+}
+
 }  // namespace
 
 extern "C" {
@@ -483,10 +551,6 @@ int fdtd_engine_create(const fdtd_grid_desc* desc, void* stream, fdtd_engine** o
   h->cpml = false;
   for (int a = 0; a < 3; ++a)
     if (desc->pml_lo[a] + desc->pml_hi[a] > 0) h->cpml = true;
-  if (!tile_fits(1, h->P)) {
-    delete h;
-    return fail(FDTD_ERR_UNSUPPORTED, "z extent too large for one CTA row");
-  }
   int rc = 0;
   for (int b = 0; b < 2 && !rc; ++b)
     for (int c = 0; c < 3 && !rc; ++c) {
@@ -537,12 +601,9 @@ int fdtd_engine_destroy(fdtd_engine* h) {
   for (auto& ck : h->checkpoints)
     for (float* p : ck.bufs) cudaFree(p);
   cudaFree(h->d_terms);
-  cudaFree(h->d_term_ptr);
-  cudaFree(h->d_term_ids);
   cudaFree(h->d_poles);
   cudaFree(h->d_regions);
-  cudaFree(h->d_region_ptr);
-  cudaFree(h->d_region_ids);
+  for (int* p : h->index_bufs) cudaFree(p);
   cudaFree(h->d_flush);
   cudaFree(h->samples);
   cudaFree(h->w_e);
@@ -783,11 +844,19 @@ int fdtd_engine_add_line_patch(fdtd_engine* h, int comp, const int* box, const f
   float* c = nullptr;
   int rc = dev_copy(h, &c, coeff, cnt);
   if (rc) return rc;
+  const AuxLine& l = h->lines[line_id];
+  // Every sample index must address a stored entry of the line history: E
+  // histories hold n_e values per step, H histories n_e - 1.
+  std::vector<int> host_idx(axis_len);
+  CUDA_TRY(cudaMemcpy(host_idx.data(), sample_index, sizeof(int) * axis_len, cudaMemcpyDefault));
+  const int limit = sample_kind == 0 ? l.ne : l.ne - 1;
+  for (int v : host_idx)
+    if (v < 0 || v >= limit) return fail(FDTD_ERR_INVALID_ARG, "line patch sample index outside the incident line");
   int* idx = nullptr;
   CUDA_TRY(cudaMalloc(&idx, sizeof(int) * axis_len));
-  CUDA_TRY(cudaMemcpyAsync(idx, sample_index, sizeof(int) * axis_len, cudaMemcpyDefault, h->stream));
+  CUDA_TRY(cudaMemcpyAsync(idx, host_idx.data(), sizeof(int) * axis_len, cudaMemcpyHostToDevice, h->stream));
+  CUDA_TRY(cudaStreamSynchronize(h->stream));
   h->owned.push_back(reinterpret_cast<float*>(idx));
-  const AuxLine& l = h->lines[line_id];
   t.coeff = c;
   t.signal = nullptr;
   t.aux_hist = sample_kind == 0 ? l.e_hist : l.h_hist;
@@ -847,28 +916,61 @@ int fdtd_engine_finalize(fdtd_engine* h) {
     if (!h->inv_e[a] || !h->inv_h[a]) return fail(FDTD_ERR_STATE, "spacing not set on every axis");
     if (h->cpml && (!h->eb[a] || !h->hb[a])) return fail(FDTD_ERR_STATE, "CPML profile not set on every axis");
   }
-  std::vector<int> ptr, ids;
   int rc = upload_vec(h, &h->d_terms, h->terms);
   if (rc) return rc;
-  build_plane_csr(h->NX, h->terms, ptr, ids);
-  if (!ids.empty()) {
-    rc = upload_vec(h, &h->d_term_ptr, ptr);
-    if (!rc) rc = upload_vec(h, &h->d_term_ids, ids);
-    if (rc) return rc;
-  } else {
-    rc = upload_vec(h, &h->d_term_ptr, ptr);
+  for (int ph = 0; ph < 2; ++ph) {
+    std::vector<int> sel;
+    for (size_t x = 0; x < h->terms.size(); ++x)
+      if ((h->terms[x].comp >= 3) == (ph == 1)) sel.push_back(static_cast<int>(x));
+    h->n_terms_ph[ph] = static_cast<int>(sel.size());
+    rc = build_box_index(h, h->terms, sel, h->term_ix[ph]);
     if (rc) return rc;
   }
   std::vector<PoleTerm> pv;
   for (const auto& ph : h->poles) pv.push_back(ph.t);
   rc = upload_vec(h, &h->d_poles, pv);
   if (rc) return rc;
+  {
+    std::vector<int> ptr, ids;
+    build_plane_csr(h->NX, pv, ptr, ids);
+    const int* dp = nullptr;
+    const int* di = nullptr;
+    rc = upload_ints(h, ptr, &dp);
+    if (!rc) rc = upload_ints(h, ids, &di);
+    if (rc) return rc;
+    h->d_pole_ptr = const_cast<int*>(dp);
+    h->d_pole_ids = const_cast<int*>(di);
+  }
   rc = upload_vec(h, &h->d_regions, h->regions);
   if (rc) return rc;
-  build_plane_csr(h->NX, h->regions, ptr, ids);
-  rc = upload_vec(h, &h->d_region_ptr, ptr);
-  if (!rc && !ids.empty()) rc = upload_vec(h, &h->d_region_ids, ids);
-  if (rc) return rc;
+  for (int ph = 0; ph < 2; ++ph) {
+    std::vector<int> sel;
+    for (size_t x = 0; x < h->regions.size(); ++x)
+      if ((h->regions[x].comp >= 3) == (ph == 1)) sel.push_back(static_cast<int>(x));
+    h->n_regions_ph[ph] = static_cast<int>(sel.size());
+    rc = build_box_index(h, h->regions, sel, h->region_ix[ph]);
+    if (rc) return rc;
+  }
+  {
+    // per-plane activity bits: planes whose x-indexed lists hold items
+    std::vector<int> bits(h->NX, 0);
+    auto mark_x = [&](const BoxIndex& ix, const std::vector<int>& ptr_host, unsigned flag) {
+      (void)ix;
+      for (int i = 0; i < h->NX; ++i)
+        if (ptr_host[i + 1] > ptr_host[i]) bits[i] |= static_cast<int>(flag);
+    };
+    for (int ph = 0; ph < 2; ++ph) {
+      std::vector<int> pt(h->NX + 1), pr(h->NX + 1);
+      CUDA_TRY(cudaMemcpy(pt.data(), h->term_ix[ph].ptr[0], sizeof(int) * (h->NX + 1), cudaMemcpyDeviceToHost));
+      CUDA_TRY(cudaMemcpy(pr.data(), h->region_ix[ph].ptr[0], sizeof(int) * (h->NX + 1), cudaMemcpyDeviceToHost));
+      mark_x(h->term_ix[ph], pt, ph == 1 ? kPlaneHTerms : kPlaneETerms);
+      mark_x(h->region_ix[ph], pr, ph == 1 ? kPlaneHRegions : kPlaneERegions);
+    }
+    for (const auto& ph : h->poles)
+      for (int i = ph.t.i0; i < ph.t.i1; ++i) bits[i] |= static_cast<int>(kPlanePoles);
+    rc = upload_ints(h, bits, &h->d_plane_bits);
+    if (rc) return rc;
+  }
   std::vector<RegionFlush> fl;
   for (const auto& r : h->regions) {
     RegionFlush f;
@@ -895,7 +997,9 @@ int fdtd_engine_finalize(fdtd_engine* h) {
       CUDA_TRY(cudaMemsetAsync(h->cmp_im, 0, sizeof(float) * acc, h->stream));
     }
   }
-  CUDA_TRY(cudaFuncSetAttribute(fused_step_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
+  // The flush stages cnt x n_freq float2 weights (at most 64 x 256 x 8 B).
+  CUDA_TRY(cudaFuncSetAttribute(dft_flush_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                static_cast<int>(sizeof(float2) * 64 * 256)));
   CUDA_TRY(cudaStreamSynchronize(h->stream));
   h->finalized = true;
   return 0;
@@ -1014,18 +1118,13 @@ int fdtd_engine_autotune(fdtd_engine* h, int* tile_rows, int* chunk_planes) {
   const int slot = static_cast<int>(h->checkpoints.size());
   rc = fdtd_engine_checkpoint_save(h, slot);
   if (rc) return rc;
-  const int Q = h->P / 4;
-  std::vector<int> tys;
-  for (int ty : {1, 2, 3, 4, 6, 8, 12, 16, 24, 32, 48})
-    if (tile_fits(ty, h->P) && ty <= h->NY && (ty + 2) * Q >= 64) tys.push_back(ty);
-  if (tys.empty()) tys.push_back(h->TY);
   const int cxs[] = {8, 16, 32, 64, 128};
   float best = 1e30f;
-  int best_ty = h->TY, best_cx = h->CX;
-  for (int ty : tys) {
+  int best_ty = 1, best_cx = h->CX, best_var = h->variant;
+  for (int var = 1; var <= 3; ++var) {
     for (int cx : cxs) {
       if (cx > 2 * h->NX) continue;
-      h->TY = ty;
+      h->variant = var;
       h->CX = cx;
       const int reps = 3;
       rc = launch_step(h, 0, 0);
@@ -1041,13 +1140,14 @@ int fdtd_engine_autotune(fdtd_engine* h, int* tile_rows, int* chunk_planes) {
       CUDA_TRY(cudaEventElapsedTime(&ms, h->ev0, h->ev1));
       if (ms < best) {
         best = ms;
-        best_ty = ty;
         best_cx = cx;
+        best_var = var;
       }
     }
   }
   h->TY = best_ty;
   h->CX = best_cx;
+  h->variant = best_var;
   rc = fdtd_engine_checkpoint_load(h, slot);
   if (rc) return rc;
   for (float* p : h->checkpoints[slot].bufs) cudaFree(p);
@@ -1080,14 +1180,32 @@ int fdtd_engine_time_kernel(fdtd_engine* h, int n, int reps, float* ms) {
   return 0;
 }
 
+int fdtd_engine_set_launch(fdtd_engine* h, int variant, int tile_rows, int chunk_planes) {
+  if (!h || variant < 1 || variant > 3 || tile_rows < 0 || chunk_planes < 0)
+    return fail(FDTD_ERR_INVALID_ARG, "bad launch configuration");
+  (void)tile_rows;  // the warp-granular kernel has no tile height
+  h->variant = variant;
+  if (chunk_planes > 0) h->CX = chunk_planes;
+  return 0;
+}
+
+int fdtd_engine_get_launch(fdtd_engine* h, int* variant, int* tile_rows, int* chunk_planes) {
+  if (!h) return fail(FDTD_ERR_INVALID_ARG, "null engine");
+  if (variant) *variant = h->variant;
+  if (tile_rows) *tile_rows = h->TY;
+  if (chunk_planes) *chunk_planes = h->CX;
+  return 0;
+}
+
 int fdtd_engine_info(fdtd_engine* h, int* tile_rows, int* chunk_planes, int* grid_x, int* grid_y, int* block,
                      int64_t* launches) {
   if (!h) return fail(FDTD_ERR_INVALID_ARG, "null engine");
   if (tile_rows) *tile_rows = h->TY;
   if (chunk_planes) *chunk_planes = h->CX;
-  if (grid_x) *grid_x = (h->NY + h->TY - 1) / h->TY;
-  if (grid_y) *grid_y = (h->NX + h->CX - 1) / h->CX;
-  if (block) *block = block_threads(h->TY, h->P);
+  const dim3 g = step_grid(h);
+  if (grid_x) *grid_x = static_cast<int>(g.x);
+  if (grid_y) *grid_y = static_cast<int>(g.y * g.z);
+  if (block) *block = kWarpRows * 32;
   if (launches) *launches = h->launches;
   return 0;
 }

@@ -46,6 +46,14 @@ struct SampleRegion {
   int64_t base;  // first sample slot of the region
 };
 
+// Per-axis CSR index of thin boxes: an item is listed along the axis where it
+// is thinnest (x: per plane i, y: per row j, z: per cell k), so a lane visits
+// only items that can contain its plane, row or z cell.
+struct BoxIndex {
+  const int* ptr[3];
+  const int* ids[3];
+};
+
 struct StepParams {
   int NX, NY, NZ, P, SZ;  // node counts, padded z pitch, z-slab row length
   int TY, CX, Q, ROWS;    // tile rows, planes per chunk, float4 per row, thread rows (TY + 2)
@@ -75,18 +83,27 @@ struct StepParams {
   int cpml;
   // injection / ADE / sampling
   const InjectionTerm* terms;
-  const int* term_plane_ptr;  // [NX + 1] CSR over planes
-  const int* term_plane_ids;
-  int n_terms;
+  BoxIndex term_index[2];  // [0] E-phase terms, [1] H-phase terms
+  int n_terms[2];
   const PoleTerm* poles;
+  const int* pole_plane_ptr;  // [NX + 1] CSR over planes
+  const int* pole_plane_ids;
   int n_poles;
   const SampleRegion* regions;
-  const int* region_plane_ptr;
-  const int* region_plane_ids;
-  int n_regions;
+  BoxIndex region_index[2];  // [0] E regions, [1] H regions
+  int n_regions[2];
   float* samples;  // [M][n_samples]
   int64_t n_samples;
   int sample_block;  // M
+  // Per-plane activity bits (kPlane* flags): which x-indexed lists hold items
+  // for plane i.  Lets a warp skip every lookup on planes that have none.
+  const unsigned* plane_bits;
 };
+
+constexpr unsigned kPlaneHTerms = 1u;
+constexpr unsigned kPlaneETerms = 2u;
+constexpr unsigned kPlaneHRegions = 4u;
+constexpr unsigned kPlaneERegions = 8u;
+constexpr unsigned kPlanePoles = 16u;
 
 }  // namespace fdtdb200

@@ -187,6 +187,14 @@ class B200FDTD:
         _lib.check(self.lib.fdtd_engine_autotune(self.handle, ctypes.byref(ty), ctypes.byref(cx)), "autotune")
         return ty.value, cx.value
 
+    def set_launch(self, variant: int, tile_rows: int = 0, chunk_planes: int = 0) -> None:
+        _lib.check(self.lib.fdtd_engine_set_launch(self.handle, int(variant), int(tile_rows), int(chunk_planes)), "set_launch")
+
+    def get_launch(self) -> tuple[int, int, int]:
+        v, ty, cx = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+        _lib.check(self.lib.fdtd_engine_get_launch(self.handle, ctypes.byref(v), ctypes.byref(ty), ctypes.byref(cx)), "get_launch")
+        return v.value, ty.value, cx.value
+
     def info(self) -> dict:
         vals = [ctypes.c_int() for _ in range(5)]
         launches = ctypes.c_int64()
@@ -194,6 +202,7 @@ class B200FDTD:
         keys = ("tile_rows", "chunk_planes", "grid_x", "grid_y", "block")
         out = {k: v.value for k, v in zip(keys, vals)}
         out["launches"] = launches.value
+        out["variant"] = self.get_launch()[0]
         return out
 
     def solve(self, time_steps: int | None = None) -> dict:
