@@ -18,7 +18,7 @@
 #include "engine.cuh"
 
 namespace fdtdb200 {
-template <bool kCpml, bool kCoef, int kMinBlocks>
+template <bool kCpml, bool kCoef, bool kUniform, int kMinBlocks>
 __global__ void warp_step_kernel(const StepParams p, int n, int slot);
 }
 
@@ -142,7 +142,31 @@ struct RegionFlush {
   int64_t base;
   int64_t count;
   int is_h;
+  int comp;
+  int i0, j0, k0, nj, nk;
 };
+
+// Copy the monitor cells of every sample region from the current fields into
+// sample slot `slot` (one CTA column per region; observers.cu:7-78 sample the
+// same values: E^{n+1} and H^{n+1/2} after all corrections of the step).
+struct FieldPtrs {
+  const float* f[6];
+};
+
+__global__ void sample_gather_kernel(const RegionFlush* regions, const FieldPtrs fields, int NY, int P,
+                                     float* samples, int64_t n_samples, int slot) {
+  const RegionFlush rg = regions[blockIdx.y];
+  const float* f = fields.f[rg.comp];
+  float* out = samples + static_cast<int64_t>(slot) * n_samples + rg.base;
+  for (int64_t x = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; x < rg.count;
+       x += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    const int lk = static_cast<int>(x % rg.nk);
+    const int64_t r = x / rg.nk;
+    const int lj = static_cast<int>(r % rg.nj);
+    const int li = static_cast<int>(r / rg.nj);
+    out[x] = __ldg(f + (static_cast<int64_t>(rg.i0 + li) * NY + rg.j0 + lj) * P + rg.k0 + lk);
+  }
+}
 
 // acc[f][slot] += sum_m sample[m][slot] * w[n_base + m][f], with Kahan
 // compensation of the accumulator update.
@@ -235,6 +259,8 @@ struct fdtd_engine {
   float* hc[3] = {};
   float* hik[3] = {};
   bool cpml = false;
+  bool uniform_grid = false;
+  float inv_e_u[3] = {0, 0, 0}, inv_h_u[3] = {0, 0, 0};
   std::vector<InjectionTerm> terms;
   std::vector<float*> owned;
   std::vector<PoleHost> poles;
@@ -336,6 +362,8 @@ void fill_params(const fdtd_engine* h, StepParams& p) {
     p.hcurl_u[c] = h->ucoef[3 + c][1];
     p.inv_e[c] = h->inv_e[c];
     p.inv_h[c] = h->inv_h[c];
+    p.inv_e_u[c] = h->inv_e_u[c];
+    p.inv_h_u[c] = h->inv_h_u[c];
     p.eb[c] = h->eb[c];
     p.ec[c] = h->ec[c];
     p.eik[c] = h->eik[c];
@@ -396,24 +424,47 @@ int launch_step(fdtd_engine* h, int n, int slot) {
   bool coef = false;
   for (int c = 0; c < 6; ++c) coef = coef || h->ecoef[c][0] || h->ecoef[c][1];
   const int block = kWarpRows * 32;
-#define FDTD_LAUNCH(CPML, COEF)                                                                  \
+#define FDTD_LAUNCH(CPML, COEF, UNI)                                                                  \
   do {                                                                                           \
-    if (h->variant == 2) warp_step_kernel<CPML, COEF, 4><<<grid, block, 0, h->stream>>>(p, n, slot); \
-    else if (h->variant == 3) warp_step_kernel<CPML, COEF, 3><<<grid, block, 0, h->stream>>>(p, n, slot); \
-    else warp_step_kernel<CPML, COEF, 1><<<grid, block, 0, h->stream>>>(p, n, slot);            \
+    if (h->variant == 2) warp_step_kernel<CPML, COEF, UNI, 4><<<grid, block, 0, h->stream>>>(p, n, slot); \
+    else if (h->variant == 3) warp_step_kernel<CPML, COEF, UNI, 3><<<grid, block, 0, h->stream>>>(p, n, slot); \
+    else warp_step_kernel<CPML, COEF, UNI, 1><<<grid, block, 0, h->stream>>>(p, n, slot);            \
   } while (0)
-  if (h->cpml) {
-    if (coef) FDTD_LAUNCH(true, true);
-    else FDTD_LAUNCH(true, false);
+  if (h->uniform_grid) {
+    if (h->cpml) {
+      if (coef) FDTD_LAUNCH(true, true, true);
+      else FDTD_LAUNCH(true, false, true);
+    } else {
+      if (coef) FDTD_LAUNCH(false, true, true);
+      else FDTD_LAUNCH(false, false, true);
+    }
   } else {
-    if (coef) FDTD_LAUNCH(false, true);
-    else FDTD_LAUNCH(false, false);
+    if (h->cpml) {
+      if (coef) FDTD_LAUNCH(true, true, false);
+      else FDTD_LAUNCH(true, false, false);
+    } else {
+      if (coef) FDTD_LAUNCH(false, true, false);
+      else FDTD_LAUNCH(false, false, false);
+    }
   }
 #undef FDTD_LAUNCH
   cudaError_t err = cudaGetLastError();
   if (err != cudaSuccess) return cuda_fail(err, "warp_step_kernel launch");
   ++h->launches;
   h->cur = 1 - h->cur;
+  if (h->n_flush > 0 && h->samples && slot >= 0) {
+    FieldPtrs fields;
+    for (int c = 0; c < 3; ++c) {
+      fields.f[c] = h->E[h->cur][c];
+      fields.f[3 + c] = h->H[h->cur][c];
+    }
+    const int gx = static_cast<int>(std::min<int64_t>((h->max_region + 255) / 256, 2048));
+    sample_gather_kernel<<<dim3(std::max(gx, 1), h->n_flush), 256, 0, h->stream>>>(
+        h->d_flush, fields, h->NY, h->P, h->samples, h->n_samples, slot);
+    err = cudaGetLastError();
+    if (err != cudaSuccess) return cuda_fail(err, "sample_gather_kernel launch");
+    ++h->launches;
+  }
   return 0;
 }
 
@@ -916,6 +967,21 @@ int fdtd_engine_finalize(fdtd_engine* h) {
     if (!h->inv_e[a] || !h->inv_h[a]) return fail(FDTD_ERR_STATE, "spacing not set on every axis");
     if (h->cpml && (!h->eb[a] || !h->hb[a])) return fail(FDTD_ERR_STATE, "CPML profile not set on every axis");
   }
+  {
+    // uniform grid: every inverse spacing of an axis (dual and primal) equal
+    bool uni = true;
+    const int nn[3] = {h->NX, h->NY, h->NZ};
+    for (int a = 0; a < 3 && uni; ++a) {
+      std::vector<float> ve(nn[a]), vh(nn[a] - 1);
+      CUDA_TRY(cudaMemcpy(ve.data(), h->inv_e[a], sizeof(float) * nn[a], cudaMemcpyDeviceToHost));
+      CUDA_TRY(cudaMemcpy(vh.data(), h->inv_h[a], sizeof(float) * (nn[a] - 1), cudaMemcpyDeviceToHost));
+      for (float v : ve) uni = uni && v == ve[0];
+      for (float v : vh) uni = uni && v == ve[0];
+      h->inv_e_u[a] = ve[0];
+      h->inv_h_u[a] = vh[0];
+    }
+    h->uniform_grid = uni;
+  }
   int rc = upload_vec(h, &h->d_terms, h->terms);
   if (rc) return rc;
   for (int ph = 0; ph < 2; ++ph) {
@@ -977,6 +1043,12 @@ int fdtd_engine_finalize(fdtd_engine* h) {
     f.base = r.base;
     f.count = static_cast<int64_t>(r.i1 - r.i0) * (r.j1 - r.j0) * (r.k1 - r.k0);
     f.is_h = r.comp >= 3 ? 1 : 0;
+    f.comp = r.comp;
+    f.i0 = r.i0;
+    f.j0 = r.j0;
+    f.k0 = r.k0;
+    f.nj = r.j1 - r.j0;
+    f.nk = r.k1 - r.k0;
     fl.push_back(f);
     h->max_region = std::max(h->max_region, f.count);
   }
@@ -1127,11 +1199,11 @@ int fdtd_engine_autotune(fdtd_engine* h, int* tile_rows, int* chunk_planes) {
       h->variant = var;
       h->CX = cx;
       const int reps = 3;
-      rc = launch_step(h, 0, 0);
+      rc = launch_step(h, 0, -1);
       if (rc) return rc;
       CUDA_TRY(cudaEventRecord(h->ev0, h->stream));
       for (int r = 0; r < reps; ++r) {
-        rc = launch_step(h, 0, 0);
+        rc = launch_step(h, 0, -1);
         if (rc) return rc;
       }
       CUDA_TRY(cudaEventRecord(h->ev1, h->stream));
@@ -1166,10 +1238,9 @@ int fdtd_engine_time_kernel(fdtd_engine* h, int n, int reps, float* ms) {
     if (t.signal && n >= t.aux_len) return fail(FDTD_ERR_INVALID_ARG, "step index beyond the source table");
   for (const auto& l : h->lines)
     if (n >= l.n_steps) return fail(FDTD_ERR_INVALID_ARG, "step index beyond the incident line history");
-  const int slot = h->pending < h->M ? h->pending : 0;
   CUDA_TRY(cudaEventRecord(h->ev0, h->stream));
   for (int r = 0; r < reps; ++r) {
-    int rc = launch_step(h, n, slot);
+    int rc = launch_step(h, n, -1);
     if (rc) return rc;
   }
   CUDA_TRY(cudaEventRecord(h->ev1, h->stream));

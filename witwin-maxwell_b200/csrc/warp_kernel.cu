@@ -11,6 +11,7 @@
 //     stored) and j; z+1 neighbours come from the next lane (__shfl_down),
 //   - computes E^{n+1}(i) for row j from the H of rows j, j-1, the H of the
 //     previous plane (registers) and the z-1 neighbour (__shfl_up).
+// Monitor samples are gathered by a separate kernel after the step.
 // Neighbour-row reads are L1/L2 hits (the warps of a block own consecutive
 // rows), so DRAM sees each field once per step.  E, H and the H CPML psi are
 // double-buffered across steps, so halo recomputation reads unmodified old
@@ -90,33 +91,17 @@ __device__ __forceinline__ void add_terms(const StepParams& p, int phase, int ba
   }
 }
 
-__device__ __forceinline__ void store_samples(const StepParams& p, int phase, int base, int slot, int i, int j, int k,
-                                              bool sx, bool sy, bool sz, float v0, float v1, float v2) {
-  const BoxIndex& ix = p.region_index[phase];
-  float* out = p.samples + static_cast<int64_t>(slot) * p.n_samples;
-  const int key[3] = {i, j, k};
-  const bool scan[3] = {sx, sy, sz};
-#pragma unroll
-  for (int a = 0; a < 3; ++a) {
-    if (!scan[a]) continue;
-    const int b = __ldg(ix.ptr[a] + key[a]), e = __ldg(ix.ptr[a] + key[a] + 1);
-    for (int x = b; x < e; ++x) {
-      const SampleRegion& r = p.regions[__ldg(ix.ids[a] + x)];
-      if (i < r.i0 || i >= r.i1 || j < r.j0 || j >= r.j1 || k < r.k0 || k >= r.k1) continue;
-      const int c = r.comp - base;
-      const float v = c == 0 ? v0 : (c == 1 ? v1 : v2);
-      out[r.base + (static_cast<int64_t>(i - r.i0) * (r.j1 - r.j0) + (j - r.j0)) * (r.k1 - r.k0) + (k - r.k0)] = v;
-    }
-  }
-}
-
 // Advance the ADE poles covering (i, j, k) from E^n and subtract dt J / eps.
-__device__ __forceinline__ void ade(const StepParams& p, int i, int j, int k, float e0, float e1, float e2, float& v0,
-                                    float& v1, float& v2) {
+// `lane_poles` has bit b set when pole b (b < 32) covers this lane's (j, k);
+// the plane list already restricts i.
+__device__ __forceinline__ void ade(const StepParams& p, unsigned lane_poles, int i, int j, int k, float e0, float e1,
+                                    float e2, float& v0, float& v1, float& v2) {
   const int b = __ldg(p.pole_plane_ptr + i), e = __ldg(p.pole_plane_ptr + i + 1);
   for (int x = b; x < e; ++x) {
-    const PoleTerm& pt = p.poles[__ldg(p.pole_plane_ids + x)];
-    if (j < pt.j0 || j >= pt.j1 || k < pt.k0 || k >= pt.k1) continue;
+    const int id = __ldg(p.pole_plane_ids + x);
+    if (id < 32 && !((lane_poles >> id) & 1u)) continue;
+    const PoleTerm& pt = p.poles[id];
+    if (id >= 32 && (j < pt.j0 || j >= pt.j1 || k < pt.k0 || k >= pt.k1)) continue;
     const int64_t o = (static_cast<int64_t>(i - pt.i0) * (pt.j1 - pt.j0) + (j - pt.j0)) * (pt.k1 - pt.k0) + (k - pt.k0);
     const int c = pt.comp;
     const float eo = c == 0 ? e0 : (c == 1 ? e1 : e2);
@@ -168,13 +153,14 @@ __device__ __forceinline__ Prof prof(const float* b, const float* c, const float
 
 // Lookup flags that do not change along the x march (bits of `lf`).
 constexpr unsigned kLfHTermYm = 1u, kLfHTermYc = 2u, kLfHTermZ = 4u, kLfETermY = 8u, kLfETermZ = 16u;
-constexpr unsigned kLfHRegY = 32u, kLfHRegZ = 64u, kLfERegY = 128u, kLfERegZ = 256u;
 
 }  // namespace
 
 // kCpml: the scene has CPML slabs.  kCoef: some decay/curl coefficient is a
 // per-cell array.  kMinBlocks trades registers for occupancy.
-template <bool kCpml, bool kCoef, int kMinBlocks>
+// kUniform: every axis has constant spacing, so the inverse spacings are the
+// scalars p.inv_e_u / p.inv_h_u.
+template <bool kCpml, bool kCoef, bool kUniform, int kMinBlocks>
 __global__ void __launch_bounds__(256, kMinBlocks) warp_step_kernel(const StepParams p, int n, int slot) {
   const int lane = threadIdx.x & 31;
   const int j = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
@@ -196,11 +182,11 @@ __global__ void __launch_bounds__(256, kMinBlocks) warp_step_kernel(const StepPa
   const bool hz_kok = k >= 0 && k < NZ - 1;  // Hx, Hy extent along z
   const bool ez_kok = k >= 0 && k < NZ;      // Ex, Ey (and Hz) extent along z
   const bool yc_ok = j < NY - 1;             // Hx, Hz extent along y (row j)
-  const float ihz = __ldg(p.inv_h[2] + (hz_kok ? k : 0));
-  const float iez = __ldg(p.inv_e[2] + (ez_kok ? k : 0));
-  const float ihy_m = __ldg(p.inv_h[1] + jm);
-  const float ihy_c = __ldg(p.inv_h[1] + (yc_ok ? j : 0));
-  const float iey = __ldg(p.inv_e[1] + j);
+  const float ihz = kUniform ? p.inv_h_u[2] : __ldg(p.inv_h[2] + (hz_kok ? k : 0));
+  const float iez = kUniform ? p.inv_e_u[2] : __ldg(p.inv_e[2] + (ez_kok ? k : 0));
+  const float ihy_m = kUniform ? p.inv_h_u[1] : __ldg(p.inv_h[1] + jm);
+  const float ihy_c = kUniform ? p.inv_h_u[1] : __ldg(p.inv_h[1] + (yc_ok ? j : 0));
+  const float iey = kUniform ? p.inv_e_u[1] : __ldg(p.inv_e[1] + j);
   const bool ylo = j == 0, yhi = j == NY - 1, zlo = k == 0, zhi = k == NZ - 1;
   const bool lane_edge = ylo || yhi || k <= 0 || k >= NZ - 1;
   int szh = -1, sze = -1, syh_m = -1, syh_c = -1, sye = -1;
@@ -227,13 +213,14 @@ __global__ void __launch_bounds__(256, kMinBlocks) warp_step_kernel(const StepPa
     if (list_nonempty(p.term_index[0], 1, j)) lf |= kLfETermY;
     if (kok && list_nonempty(p.term_index[0], 2, k)) lf |= kLfETermZ;
   }
-  if (p.n_regions[1]) {
-    if (list_nonempty(p.region_index[1], 1, j)) lf |= kLfHRegY;
-    if (kok && list_nonempty(p.region_index[1], 2, k)) lf |= kLfHRegZ;
-  }
-  if (p.n_regions[0]) {
-    if (list_nonempty(p.region_index[0], 1, j)) lf |= kLfERegY;
-    if (kok && list_nonempty(p.region_index[0], 2, k)) lf |= kLfERegZ;
+
+  unsigned lane_poles = 0;
+  if (p.n_poles && out_lane) {
+    const int np_ = min(p.n_poles, 32);
+    for (int b = 0; b < np_; ++b) {
+      const PoleTerm& pt = p.poles[b];
+      if (j >= pt.j0 && j < pt.j1 && k >= pt.k0 && k < pt.k1) lane_poles |= 1u << b;
+    }
   }
 
   // E^n(i) registers: row j-1 (x, y, z), row j (x, y, z), row j+1 (x, z)
@@ -268,28 +255,38 @@ __global__ void __launch_bounds__(256, kMinBlocks) warp_step_kernel(const StepPa
     const float np2 = ldz(p.Ein[2], on + rp, kok && jp_ok && inext);
     // H^{n-1/2}(i) of rows j-1 and j
     const float hm0 = ldz(p.Hin[0], o + rm, kok && jm_ok);
-    const float hm1 = ldz(p.Hin[1], o + rm, kok && jm_ok);
     const float hm2 = ldz(p.Hin[2], o + rm, kok && jm_ok);
     const float hc0 = ldz(p.Hin[0], o + rc, kok);
     const float hc1 = ldz(p.Hin[1], o + rc, kok);
     const float hc2 = ldz(p.Hin[2], o + rc, kok);
+    // E coefficient arrays of this plane, issued early so their latency hides
+    // behind the H update
+    float g0 = p.edecay_u[0], g1 = p.edecay_u[1], g2 = p.edecay_u[2];
+    float c0 = p.ecurl_u[0], c1 = p.ecurl_u[1], c2 = p.ecurl_u[2];
+    if (kCoef) {
+      const bool ld = own && out_lane;
+      if (p.ecurl[0]) c0 = ldz(p.ecurl[0], o + rc, ld);
+      if (p.ecurl[1]) c1 = ldz(p.ecurl[1], o + rc, ld);
+      if (p.ecurl[2]) c2 = ldz(p.ecurl[2], o + rc, ld);
+      if (p.edecay[0]) g0 = ldz(p.edecay[0], o + rc, ld);
+      if (p.edecay[1]) g1 = ldz(p.edecay[1], o + rc, ld);
+      if (p.edecay[2]) g2 = ldz(p.edecay[2], o + rc, ld);
+    }
     const bool ix_ok = i < NX - 1;
-    const float ihx = __ldg(p.inv_h[0] + (ix_ok ? i : 0));
-    // z+1 neighbours of rows j-1 and j
-    const float em0k = __shfl_down_sync(kFull, em0, 1);
+    const float ihx = kUniform ? p.inv_h_u[0] : __ldg(p.inv_h[0] + (ix_ok ? i : 0));
+    // z+1 neighbours of rows j-1 and j (the halo row needs Ey only: its Hy is unused)
     const float em1k = __shfl_down_sync(kFull, em1, 1);
     const float ec0k = __shfl_down_sync(kFull, ec0, 1);
     const float ec1k = __shfl_down_sync(kFull, ec1, 1);
 
-    // ---------------- H^{n+1/2}(i): halo row j-1, then row j ----------------
+    // ---------------- H^{n+1/2}(i): halo row j-1 (Hx, Hz), then row j ----------------
     // Hx: dEz/dy - dEy/dz; Hy: dEx/dz - dEz/dx; Hz: dEy/dx - dEx/dy
     float mxa = (ec2 - em2) * ihy_m, mxb = (em1k - em1) * ihz;
-    float mya = (nm2 - em2) * ihx, myb = (em0k - em0) * ihz;
     float mza = (nm1 - em1) * ihx, mzb = (ec0 - em0) * ihy_m;
     float cxa = (ep2 - ec2) * ihy_c, cxb = (ec1k - ec1) * ihz;
     float cya = (nc2 - ec2) * ihx, cyb = (ec0k - ec0) * ihz;
     float cza = (nc1 - ec1) * ihx, czb = (ep0 - ec0) * ihy_c;
-    const bool mx_ok = jm_ok && hz_kok, my_ok = jm_ok && ix_ok && hz_kok, mz_ok = jm_ok && ix_ok && ez_kok;
+    const bool mx_ok = jm_ok && hz_kok, mz_ok = jm_ok && ix_ok && ez_kok;
     const bool cx_ok = yc_ok && hz_kok, cy_ok = ix_ok && hz_kok, cz_ok = ix_ok && yc_ok && ez_kok;
     int sxh = -1, sxe = -1;
     if (kCpml) {
@@ -301,8 +298,6 @@ __global__ void __launch_bounds__(256, kMinBlocks) warp_step_kernel(const StepPa
         if (sxh >= 0) pxh = prof(p.hb[0], p.hc[0], p.hik[0], i);
         if (syh_m >= 0 && mx_ok) mxa = psi_step(mxa, pym.b, pym.c, pym.ik, p.psiHin[0][0], p.psiHout[0][0], yslab_off(p, i, syh_m, k), false);
         if (szh >= 0 && mx_ok) mxb = psi_step(mxb, pzh.b, pzh.c, pzh.ik, p.psiHin[0][1], p.psiHout[0][1], zslab_off(p, i, jm, szh), false);
-        if (sxh >= 0 && my_ok) mya = psi_step(mya, pxh.b, pxh.c, pxh.ik, p.psiHin[1][0], p.psiHout[1][0], xslab_off(p, sxh, jm, k), false);
-        if (szh >= 0 && my_ok) myb = psi_step(myb, pzh.b, pzh.c, pzh.ik, p.psiHin[1][1], p.psiHout[1][1], zslab_off(p, i, jm, szh), false);
         if (sxh >= 0 && mz_ok) mza = psi_step(mza, pxh.b, pxh.c, pxh.ik, p.psiHin[2][0], p.psiHout[2][0], xslab_off(p, sxh, jm, k), false);
         if (syh_m >= 0 && mz_ok) mzb = psi_step(mzb, pym.b, pym.c, pym.ik, p.psiHin[2][1], p.psiHout[2][1], yslab_off(p, i, syh_m, k), false);
         if (syh_c >= 0 && cx_ok) cxa = psi_step(cxa, pyc.b, pyc.c, pyc.ik, p.psiHin[0][0], p.psiHout[0][0], yslab_off(p, i, syh_c, k), wr);
@@ -315,17 +310,17 @@ __global__ void __launch_bounds__(256, kMinBlocks) warp_step_kernel(const StepPa
     }
     float dHx = p.hdecay_u[0], cHx = p.hcurl_u[0], dHy = p.hdecay_u[1], cHy = p.hcurl_u[1], dHz = p.hdecay_u[2],
           cHz = p.hcurl_u[2];
-    float dHxm = dHx, cHxm = cHx, dHym = dHy, cHym = cHy, dHzm = dHz, cHzm = cHz;
+    float dHxm = dHx, cHxm = cHx, dHzm = dHz, cHzm = cHz;
     if (kCoef) {
       if (p.hdecay[0]) { dHx = ldz(p.hdecay[0], o + rc, kok); dHxm = ldz(p.hdecay[0], o + rm, kok && jm_ok); }
       if (p.hcurl[0]) { cHx = ldz(p.hcurl[0], o + rc, kok); cHxm = ldz(p.hcurl[0], o + rm, kok && jm_ok); }
-      if (p.hdecay[1]) { dHy = ldz(p.hdecay[1], o + rc, kok); dHym = ldz(p.hdecay[1], o + rm, kok && jm_ok); }
-      if (p.hcurl[1]) { cHy = ldz(p.hcurl[1], o + rc, kok); cHym = ldz(p.hcurl[1], o + rm, kok && jm_ok); }
+      if (p.hdecay[1]) dHy = ldz(p.hdecay[1], o + rc, kok);
+      if (p.hcurl[1]) cHy = ldz(p.hcurl[1], o + rc, kok);
       if (p.hdecay[2]) { dHz = ldz(p.hdecay[2], o + rc, kok); dHzm = ldz(p.hdecay[2], o + rm, kok && jm_ok); }
       if (p.hcurl[2]) { cHz = ldz(p.hcurl[2], o + rc, kok); cHzm = ldz(p.hcurl[2], o + rm, kok && jm_ok); }
     }
     float hmx = mx_ok ? hm0 * dHxm - cHxm * (mxa - mxb) : 0.f;
-    float hmy = my_ok ? hm1 * dHym - cHym * (myb - mya) : 0.f;
+    float hmy = 0.f;
     float hmz = mz_ok ? hm2 * dHzm - cHzm * (mza - mzb) : 0.f;
     float hcx = cx_ok ? hc0 * dHx - cHx * (cxa - cxb) : 0.f;
     float hcy = cy_ok ? hc1 * dHy - cHy * (cyb - cya) : 0.f;
@@ -340,15 +335,13 @@ __global__ void __launch_bounds__(256, kMinBlocks) warp_step_kernel(const StepPa
       __stcg(p.Hout[0] + o + rc, hcx);
       __stcg(p.Hout[1] + o + rc, hcy);
       __stcg(p.Hout[2] + o + rc, hcz);
-      if ((pb & kPlaneHRegions) || (lf & (kLfHRegY | kLfHRegZ)))
-        store_samples(p, 1, 3, slot, i, j, k, pb & kPlaneHRegions, lf & kLfHRegY, lf & kLfHRegZ, hcx, hcy, hcz);
     }
 
     // ---------------- E^{n+1}(i), row j ----------------
     const float hxk = __shfl_up_sync(kFull, hcx, 1);
     const float hyk = __shfl_up_sync(kFull, hcy, 1);
     if (own && out_lane) {
-      const float iex = __ldg(p.inv_e[0] + i);
+      const float iex = kUniform ? p.inv_e_u[0] : __ldg(p.inv_e[0] + i);
       // Ex: dHz/dy - dHy/dz; Ey: dHx/dz - dHz/dx; Ez: dHy/dx - dHx/dy
       float d0a = (hcz - hmz) * iey, d0b = (hcy - hyk) * iez;
       float d1a = (hcz - hpz) * iex, d1b = (hcx - hxk) * iez;
@@ -370,29 +363,17 @@ __global__ void __launch_bounds__(256, kMinBlocks) warp_step_kernel(const StepPa
         if (sxe >= 0 && m2 == 0) d2a = psi_step(d2a, pxe.b, pxe.c, pxe.ik, p.psiE[2][0], p.psiE[2][0], xslab_off(p, sxe, j, k), true);
         if (sye >= 0 && m2 == 0) d2b = psi_step(d2b, pye.b, pye.c, pye.ik, p.psiE[2][1], p.psiE[2][1], yslab_off(p, i, sye, k), true);
       }
-      float g0 = p.edecay_u[0], g1 = p.edecay_u[1], g2 = p.edecay_u[2];
-      float c0 = p.ecurl_u[0], c1 = p.ecurl_u[1], c2 = p.ecurl_u[2];
-      if (kCoef) {
-        if (p.ecurl[0]) c0 = __ldg(p.ecurl[0] + o + rc);
-        if (p.ecurl[1]) c1 = __ldg(p.ecurl[1] + o + rc);
-        if (p.ecurl[2]) c2 = __ldg(p.ecurl[2] + o + rc);
-        if (p.edecay[0]) g0 = __ldg(p.edecay[0] + o + rc);
-        if (p.edecay[1]) g1 = __ldg(p.edecay[1] + o + rc);
-        if (p.edecay[2]) g2 = __ldg(p.edecay[2] + o + rc);
-      }
       float v0 = pick(m0, ec0 * g0 + c0 * (d0a - d0b), ec0);
       float v1 = pick(m1, ec1 * g1 + c1 * (d1b - d1a), ec1);
       float v2 = pick(m2, ec2 * g2 + c2 * (d2a - d2b), ec2);
       // ADE subtraction, TFSF electric corrections and soft sources: the
       // additive terms of witwin/maxwell/fdtd/runtime/stepping.py:2295-2320.
-      if (pb & kPlanePoles) ade(p, i, j, k, ec0, ec1, ec2, v0, v1, v2);
+      if (pb & kPlanePoles) ade(p, lane_poles, i, j, k, ec0, ec1, ec2, v0, v1, v2);
       if ((pb & kPlaneETerms) || (lf & (kLfETermY | kLfETermZ)))
         add_terms(p, 0, 0, n, i, j, k, pb & kPlaneETerms, lf & kLfETermY, lf & kLfETermZ, v0, v1, v2);
       __stcg(p.Eout[0] + o + rc, v0);
       __stcg(p.Eout[1] + o + rc, v1);
       __stcg(p.Eout[2] + o + rc, v2);
-      if ((pb & kPlaneERegions) || (lf & (kLfERegY | kLfERegZ)))
-        store_samples(p, 0, 0, slot, i, j, k, pb & kPlaneERegions, lf & kLfERegY, lf & kLfERegZ, v0, v1, v2);
     }
     hpz = hcz;
     hpy = hcy;
@@ -407,14 +388,18 @@ __global__ void __launch_bounds__(256, kMinBlocks) warp_step_kernel(const StepPa
   }
 }
 
-#define FDTD_INSTANTIATE(CPML, COEF)                                                  \
-  template __global__ void warp_step_kernel<CPML, COEF, 1>(const StepParams, int, int); \
-  template __global__ void warp_step_kernel<CPML, COEF, 3>(const StepParams, int, int); \
-  template __global__ void warp_step_kernel<CPML, COEF, 4>(const StepParams, int, int);
-FDTD_INSTANTIATE(false, false)
-FDTD_INSTANTIATE(false, true)
-FDTD_INSTANTIATE(true, false)
-FDTD_INSTANTIATE(true, true)
+#define FDTD_INSTANTIATE(CPML, COEF, UNI)                                                  \
+  template __global__ void warp_step_kernel<CPML, COEF, UNI, 1>(const StepParams, int, int); \
+  template __global__ void warp_step_kernel<CPML, COEF, UNI, 3>(const StepParams, int, int); \
+  template __global__ void warp_step_kernel<CPML, COEF, UNI, 4>(const StepParams, int, int);
+FDTD_INSTANTIATE(false, false, false)
+FDTD_INSTANTIATE(false, true, false)
+FDTD_INSTANTIATE(true, false, false)
+FDTD_INSTANTIATE(true, true, false)
+FDTD_INSTANTIATE(false, false, true)
+FDTD_INSTANTIATE(false, true, true)
+FDTD_INSTANTIATE(true, false, true)
+FDTD_INSTANTIATE(true, true, true)
 #undef FDTD_INSTANTIATE
 
 }  // namespace fdtdb200
