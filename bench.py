@@ -266,7 +266,7 @@ def run_b200_arm(args, wm, world, rank, local):
             "nodes": list(cs.nodes),
             "frequencies": len(cs.frequencies),
             "monitor_points": int(solver.n_samples),
-            "tile": [info1["tile_rows"], info1["chunk_planes"]],
+            "launch": {"variant": info1["variant"], "chunk_planes": info1["chunk_planes"], "grid": [info1["grid_x"], info1["grid_y"]], "block": info1["block"]},
             "sample_block": args.sample_block,
             "l2": "working set (~2.5 GB of fields, psi, ADE state, monitor buffers) far larger than the 126 MB L2; no flush needed",
             "parallelism": f"replicas x{world}",

@@ -241,7 +241,7 @@ struct fdtd_engine {
   int NX = 0, NY = 0, NZ = 0, P = 0, SZ = 0;
   int64_t plane = 0, vol = 0;
   int TY = 0, CX = 0;
-  int variant = 1;  // fused kernel register budget: 1 = up to 128/thread, 2 = 64/thread
+  int variant = 2;  // fused kernel register budget: 1 = up to 128/thread, 3 = 85/thread, 2 = 64/thread
   int cur = 0;  // index of the buffer holding the current state
   float* E[2][3] = {};
   float* H[2][3] = {};
@@ -405,10 +405,13 @@ void default_tiles(fdtd_engine* h) {
   h->TY = 1;
   int CX = h->desc.chunk_planes;
   if (CX <= 0) {
-    // about four resident warps per scheduler over the whole grid
-    const int64_t cols = static_cast<int64_t>((h->NY + kWarpRows - 1) / kWarpRows) * ((h->NZ + 29) / 30);
-    const int64_t want_chunks = std::max<int64_t>(1, (148 * 8 + cols - 1) / cols);
-    CX = static_cast<int>(std::max<int64_t>(16, (h->NX + want_chunks - 1) / want_chunks));
+    // Split x into chunks until the grid holds about ten waves of the
+    // 64-register variant (four 256-thread CTAs per SM on 148 SMs).  Shorter
+    // chunks recompute one halo plane each, which stays cheaper than idle SMs
+    // down to four planes.
+    const int64_t cols = static_cast<int64_t>((h->NY + kWarpRows - 1) / kWarpRows) * ((h->NZ + kWarpOut - 1) / kWarpOut);
+    const int64_t want_chunks = std::max<int64_t>(1, (148 * 4 * 10 + cols - 1) / cols);
+    CX = static_cast<int>(std::max<int64_t>(4, (h->NX + want_chunks - 1) / want_chunks));
   }
   h->CX = CX;
 }
@@ -1190,7 +1193,7 @@ int fdtd_engine_autotune(fdtd_engine* h, int* tile_rows, int* chunk_planes) {
   const int slot = static_cast<int>(h->checkpoints.size());
   rc = fdtd_engine_checkpoint_save(h, slot);
   if (rc) return rc;
-  const int cxs[] = {8, 16, 32, 64, 128};
+  const int cxs[] = {4, 6, 8, 12, 16, 24, 32};
   float best = 1e30f;
   int best_ty = 1, best_cx = h->CX, best_var = h->variant;
   for (int var = 1; var <= 3; ++var) {
