@@ -221,6 +221,36 @@ int fdtd_op_aux_magnetic(int n_e, float* h, const float* e, const float* h_decay
                          void* stream);
 int fdtd_op_aux_electric(int n_e, float* e, const float* h, const float* e_decay, const float* e_curl,
                          int source_index, float source_value, void* stream);
+
+/* Whole incident-line history in one call, allocating no device memory.  No
+ * counterpart in the reference: it is a variant of the history kernel behind
+ * fdtd_engine_add_aux_line whose running line state lives in a fixed device
+ * array instead of allocated scratch.
+ *
+ * For callers that cannot allocate: a process whose free device memory is all
+ * reserved by its own caching pool (cudaMalloc would fail or make the pool
+ * release cached blocks), and a caller on a latency-critical stream, where
+ * cudaFree's device-wide synchronisation would stall every other stream.
+ *
+ * Every pointer is device memory owned by the caller: the coefficient arrays
+ * (e_decay, e_curl: n_e; h_decay, h_curl: n_e - 1), source (n_steps values for
+ * the source cell), and the outputs e_hist and h_hist (n_steps x n_e, row n =
+ * the line before E/after H of step n; the last entry of each H row is zero).
+ * Same recurrence as fdtd_op_aux_magnetic followed by fdtd_op_aux_electric,
+ * stepped n_steps times from a zero line.
+ *
+ * Limit: n_e <= FDTD_AUX_STATIC_MAX_CELLS; larger lines return
+ * FDTD_ERR_INVALID_ARG.  The line state starts at zero on every call (the
+ * kernel clears it); nothing else needs clearing.  The first call on each
+ * device looks up the array's device address (which may load the module); make
+ * it once per device, with that device current, before any stream capture.
+ * The array is shared by every call on a device: calls that can overlap
+ * (different streams, or unordered host threads) race on it and both results
+ * are undefined, so order them on one stream. */
+#define FDTD_AUX_STATIC_MAX_CELLS 16384
+int fdtd_op_aux_line_history_static(int n_e, const float* e_decay, const float* e_curl, const float* h_decay,
+                                    const float* h_curl, int source_index, const float* source, int n_steps,
+                                    float* e_hist, float* h_hist, void* stream);
 /* Observers (observers.cu:7-78) and the batched full-field DFT (spectral.cu:9-146). */
 int fdtd_op_point_observers(const float* field, const int* fshape, int n_points, const int* pi, const int* pj,
                             const int* pk, float* re, float* im, float wcos, float wsin, void* stream);

@@ -83,6 +83,7 @@ _SIGNATURES = {
     "fdtd_op_add_line_patch": ([_vp, _c_int_p, _vp, _c_int_p, _c_int_p, _vp, _vp, _i, _f, _vp], _i),
     "fdtd_op_aux_magnetic": ([_i, _vp, _vp, _vp, _vp, _vp], _i),
     "fdtd_op_aux_electric": ([_i, _vp, _vp, _vp, _vp, _i, _f, _vp], _i),
+    "fdtd_op_aux_line_history_static": ([_i, _vp, _vp, _vp, _vp, _i, _vp, _i, _vp, _vp, _vp], _i),
     "fdtd_op_point_observers": ([_vp, _c_int_p, _i, _vp, _vp, _vp, _vp, _vp, _f, _f, _vp], _i),
     "fdtd_op_plane_observer": ([_vp, _c_int_p, _i, _i, _vp, _vp, _f, _f, _vp], _i),
     "fdtd_op_dft_volume": ([_i64, _i, _vp, _vp, _vp, _vp, _vp, _vp], _i),
