@@ -143,9 +143,10 @@ def test_engine_dispersive_tfsf_against_fp64_oracle():
     solver.close()
 
 
-@pytest.mark.parametrize("tiles", [(1, 1, 8), (3, 1, 5), (2, 1, 64), (2, 1, 13)])
+@pytest.mark.parametrize("tiles", [(1, 1, 8), (3, 1, 5), (2, 1, 64), (2, 1, 13), (4, 1, 8), (4, 1, 3), (4, 1, 41)])
 def test_tile_shape_does_not_change_results(tiles):
-    """Every (register budget, chunk_planes) launch gives bit-identical fields."""
+    """Every launch variant (register-prefetch budgets 1-3, TMA-fed 4) and
+    chunk length gives bit-identical fields."""
     wm = load_package()
     steps = 50
     cs = wm.compile_scene(_c1_scene(wm, cells=40, pml=6), steps)

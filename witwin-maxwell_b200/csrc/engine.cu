@@ -16,6 +16,7 @@
 
 #include "../../include/fdtd_b200.h"
 #include "engine.cuh"
+#include "tma_step.cuh"
 
 namespace fdtdb200 {
 template <bool kCpml, bool kCoef, bool kUniform, int kMinBlocks>
@@ -241,7 +242,9 @@ struct fdtd_engine {
   int NX = 0, NY = 0, NZ = 0, P = 0, SZ = 0;
   int64_t plane = 0, vol = 0;
   int TY = 0, CX = 0;
-  int variant = 2;  // fused kernel register budget: 1 = up to 128/thread, 3 = 85/thread, 2 = 64/thread
+  // Fused kernel: 1..3 = register-prefetch warp kernel with a register budget
+  // of up to 128 / 64 / 85 per thread; 4 = TMA-fed kernel.
+  int variant = 2;
   int cur = 0;  // index of the buffer holding the current state
   float* E[2][3] = {};
   float* H[2][3] = {};
@@ -278,6 +281,11 @@ struct fdtd_engine {
   int* d_pole_ptr = nullptr;
   int* d_pole_ids = nullptr;
   const int* d_plane_bits = nullptr;
+  unsigned char* d_warp_class = nullptr;  // sized for chunk length 1 (the largest table)
+  TmaMaps maps[2] = {};                    // tensor maps of E[cur], H[cur] for cur = 0, 1
+  bool tma_ready = false;
+  int* d_status = nullptr;                 // timeout flag written by bounded waits
+  int class_cx = 0;                       // chunk length the table was built for (0 = stale)
   std::vector<int*> index_bufs;
   RegionFlush* d_flush = nullptr;
   int n_flush = 0;
@@ -335,6 +343,51 @@ bool box_ok(const fdtd_engine* h, int comp, const int* box) {
   return true;
 }
 
+// Values of n pseudo-randomly chosen in-extent cells of a padded array.
+__global__ void coef_sample_kernel(const float* a, int NY, int P, int e0, int e1, int e2, int n, float* out) {
+  const int x = blockIdx.x * blockDim.x + threadIdx.x;
+  if (x >= n) return;
+  uint64_t z = 0x9E3779B97F4A7C15ull * (static_cast<uint64_t>(x) + 1);
+  z ^= z >> 31;
+  z *= 0xBF58476D1CE4E5B9ull;
+  z ^= z >> 27;
+  const uint64_t cells = static_cast<uint64_t>(e0) * e1 * e2;
+  const uint64_t c = z % cells;
+  const int k = static_cast<int>(c % e2);
+  const int j = static_cast<int>((c / e2) % e1);
+  const int i = static_cast<int>(c / (static_cast<uint64_t>(e2) * e1));
+  out[x] = a[(static_cast<int64_t>(i) * NY + j) * P + k];
+}
+
+int background_value(fdtd_engine* h, int comp, const float* arr, float* out) {
+  constexpr int kSamples = 4096;
+  int ext[3];
+  comp_extent(comp, h->NX, h->NY, h->NZ, ext);
+  float* d = nullptr;
+  CUDA_TRY(cudaMalloc(&d, sizeof(float) * kSamples));
+  coef_sample_kernel<<<kSamples / 256, 256, 0, h->stream>>>(arr, h->NY, h->P, ext[0], ext[1], ext[2], kSamples, d);
+  std::vector<float> v(kSamples);
+  cudaError_t err = cudaGetLastError();
+  if (err == cudaSuccess) err = cudaMemcpyAsync(v.data(), d, sizeof(float) * kSamples, cudaMemcpyDeviceToHost, h->stream);
+  if (err == cudaSuccess) err = cudaStreamSynchronize(h->stream);
+  cudaFree(d);
+  if (err != cudaSuccess) return cuda_fail(err, "coefficient background sample");
+  std::sort(v.begin(), v.end());
+  float best = v[0];
+  int best_n = 0;
+  for (int a = 0; a < kSamples;) {
+    int b = a;
+    while (b < kSamples && v[b] == v[a]) ++b;
+    if (b - a > best_n) {
+      best_n = b - a;
+      best = v[a];
+    }
+    a = b;
+  }
+  *out = best;
+  return 0;
+}
+
 void fill_params(const fdtd_engine* h, StepParams& p) {
   std::memset(&p, 0, sizeof(p));
   p.NX = h->NX;
@@ -387,6 +440,8 @@ void fill_params(const fdtd_engine* h, StepParams& p) {
   p.n_poles = static_cast<int>(h->poles.size());
   p.regions = h->d_regions;
   p.plane_bits = reinterpret_cast<const unsigned*>(h->d_plane_bits);
+  p.warp_class = h->d_warp_class;
+  p.status = h->d_status;
   for (int ph = 0; ph < 2; ++ph) {
     p.term_index[ph] = h->term_ix[ph];
     p.n_terms[ph] = h->n_terms_ph[ph];
@@ -420,6 +475,18 @@ dim3 step_grid(const fdtd_engine* h) {
   return dim3((h->NY + kWarpRows - 1) / kWarpRows, (h->NZ + kWarpOut - 1) / kWarpOut, (h->NX + h->CX - 1) / h->CX);
 }
 
+// Read (and clear) the device status word after the stream has drained.
+int check_status(fdtd_engine* h) {
+  int st = 0;
+  CUDA_TRY(cudaMemcpyAsync(&st, h->d_status, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
+  CUDA_TRY(cudaStreamSynchronize(h->stream));
+  if (st != 0) {
+    CUDA_TRY(cudaMemsetAsync(h->d_status, 0, sizeof(int), h->stream));
+    return fail(FDTD_ERR_TIMEOUT, "a bounded wait in the step kernel ran out");
+  }
+  return 0;
+}
+
 int launch_step(fdtd_engine* h, int n, int slot) {
   StepParams p;
   fill_params(h, p);
@@ -427,9 +494,18 @@ int launch_step(fdtd_engine* h, int n, int slot) {
   bool coef = false;
   for (int c = 0; c < 6; ++c) coef = coef || h->ecoef[c][0] || h->ecoef[c][1];
   const int block = kWarpRows * 32;
+  if (h->variant == 4 && !h->tma_ready)
+    return fail(FDTD_ERR_UNSUPPORTED, "TMA step kernel unavailable (no tensor-map driver entry point)");
+  if ((h->cpml || coef) && h->class_cx != h->CX) {
+    const int err = launch_classify(p, static_cast<int>(grid.y), static_cast<int>(grid.z), h->d_warp_class, h->stream);
+    if (err != 0) return cuda_fail(static_cast<cudaError_t>(err), "classify_kernel launch");
+    h->class_cx = h->CX;
+  }
 #define FDTD_LAUNCH(CPML, COEF, UNI)                                                                  \
   do {                                                                                           \
-    if (h->variant == 2) warp_step_kernel<CPML, COEF, UNI, 4><<<grid, block, 0, h->stream>>>(p, n, slot); \
+    if (h->variant == 4)                                                                          \
+      tma_step_kernel<CPML, COEF, UNI><<<grid, kTmaThreads, tma_smem_bytes(), h->stream>>>(p, h->maps[h->cur], n); \
+    else if (h->variant == 2) warp_step_kernel<CPML, COEF, UNI, 4><<<grid, block, 0, h->stream>>>(p, n, slot); \
     else if (h->variant == 3) warp_step_kernel<CPML, COEF, UNI, 3><<<grid, block, 0, h->stream>>>(p, n, slot); \
     else warp_step_kernel<CPML, COEF, UNI, 1><<<grid, block, 0, h->stream>>>(p, n, slot);            \
   } while (0)
@@ -659,6 +735,8 @@ int fdtd_engine_destroy(fdtd_engine* h) {
   cudaFree(h->d_regions);
   for (int* p : h->index_bufs) cudaFree(p);
   cudaFree(h->d_flush);
+  cudaFree(h->d_warp_class);
+  cudaFree(h->d_status);
   cudaFree(h->samples);
   cudaFree(h->w_e);
   cudaFree(h->w_h);
@@ -1075,6 +1153,35 @@ int fdtd_engine_finalize(fdtd_engine* h) {
   // The flush stages cnt x n_freq float2 weights (at most 64 x 256 x 8 B).
   CUDA_TRY(cudaFuncSetAttribute(dft_flush_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 static_cast<int>(sizeof(float2) * 64 * 256)));
+  // Background value of each coefficient array (the most frequent of a
+  // sample of its cells): warps whose footprint holds only background values
+  // use it as a scalar instead of reading the array.
+  for (int c = 0; c < 6; ++c) {
+    for (int w = 0; w < 2; ++w) {
+      if (!h->ecoef[c][w]) continue;
+      rc = background_value(h, c, h->ecoef[c][w], &h->ucoef[c][w]);
+      if (rc) return rc;
+    }
+  }
+  {
+    const int64_t kblocks = (h->NZ + kWarpOut - 1) / kWarpOut;
+    CUDA_TRY(cudaMalloc(&h->d_warp_class, static_cast<size_t>(h->NX) * kblocks * h->NY));
+    h->class_cx = 0;
+    CUDA_TRY(cudaMalloc(&h->d_status, sizeof(int)));
+    CUDA_TRY(cudaMemsetAsync(h->d_status, 0, sizeof(int), h->stream));
+  }
+  {
+    // TMA maps of both ping-pong buffers; without the driver entry point the
+    // TMA variant stays unavailable and the warp kernel runs.
+    bool ok = true;
+    for (int b = 0; b < 2 && ok; ++b) {
+      for (int c = 0; c < 3 && ok; ++c) {
+        ok = encode_field_map(&h->maps[b].e[c], h->E[b][c], h->NX, h->NY, h->P, tma_rows_e()) == 0 &&
+             encode_field_map(&h->maps[b].h[c], h->H[b][c], h->NX, h->NY, h->P, tma_rows_h()) == 0;
+      }
+    }
+    h->tma_ready = ok;
+  }
   CUDA_TRY(cudaStreamSynchronize(h->stream));
   h->finalized = true;
   return 0;
@@ -1113,7 +1220,7 @@ int fdtd_engine_step_range(fdtd_engine* h, int n0, int n1) {
   CUDA_TRY(cudaEventRecord(h->ev1, h->stream));
   CUDA_TRY(cudaEventSynchronize(h->ev1));
   CUDA_TRY(cudaEventElapsedTime(&h->last_ms, h->ev0, h->ev1));
-  return 0;
+  return check_status(h);
 }
 
 int fdtd_engine_flush(fdtd_engine* h) {
@@ -1196,7 +1303,8 @@ int fdtd_engine_autotune(fdtd_engine* h, int* tile_rows, int* chunk_planes) {
   const int cxs[] = {4, 6, 8, 12, 16, 24, 32};
   float best = 1e30f;
   int best_ty = 1, best_cx = h->CX, best_var = h->variant;
-  for (int var = 1; var <= 3; ++var) {
+  const int last_var = h->tma_ready ? 4 : 3;
+  for (int var = 1; var <= last_var; ++var) {
     for (int cx : cxs) {
       if (cx > 2 * h->NX) continue;
       h->variant = var;
@@ -1255,7 +1363,7 @@ int fdtd_engine_time_kernel(fdtd_engine* h, int n, int reps, float* ms) {
 }
 
 int fdtd_engine_set_launch(fdtd_engine* h, int variant, int tile_rows, int chunk_planes) {
-  if (!h || variant < 1 || variant > 3 || tile_rows < 0 || chunk_planes < 0)
+  if (!h || variant < 1 || variant > 4 || tile_rows < 0 || chunk_planes < 0)
     return fail(FDTD_ERR_INVALID_ARG, "bad launch configuration");
   (void)tile_rows;  // the warp-granular kernel has no tile height
   h->variant = variant;

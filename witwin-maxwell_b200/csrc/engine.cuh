@@ -99,7 +99,23 @@ struct StepParams {
   // Per-plane activity bits (kPlane* flags): which x-indexed lists hold items
   // for plane i.  Lets a warp skip every lookup on planes that have none.
   const unsigned* plane_bits;
+  // Per-warp feature class (kClass* bits) of each warp task, indexed
+  // [(chunk * kblocks + kblock) * NY + j]; built by launch_classify for the
+  // current chunk length.
+  const unsigned char* warp_class;
+  // Device status word: a kernel whose bounded wait ran out stores
+  // FDTD_ERR_TIMEOUT here (read back by the host after stepping).
+  int* status;
 };
+
+// A warp task needs the CPML code (some cell of its footprint lies in a slab)
+// or the coefficient arrays (some coefficient of its footprint differs from
+// the component's background value).
+constexpr unsigned kClassCpml = 1u;
+constexpr unsigned kClassCoef = 2u;
+
+// Fill p.warp_class (out) for chunk length p.CX: one warp per task.
+int launch_classify(const StepParams& p, int n_kblocks, int n_chunks, unsigned char* out, cudaStream_t stream);
 
 constexpr unsigned kPlaneHTerms = 1u;
 constexpr unsigned kPlaneETerms = 2u;

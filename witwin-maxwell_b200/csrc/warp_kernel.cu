@@ -20,152 +20,18 @@
 // Arithmetic restated from witwin/maxwell/fdtd/cuda/kernels/magnetic.cu:62-212,
 // electric.cu:242-311 and 462-941, dispersive.cu:18-83, sources.cu:135-154 and
 // 485-545, observers.cu:7-78.
-#include "engine.cuh"
+#include "step_device.cuh"
 
 namespace fdtdb200 {
 
-namespace {
-
-constexpr int kOut = 30;  // output z cells per warp
-constexpr unsigned kFull = 0xffffffffu;
-
-__device__ __forceinline__ float ldz(const float* base, int64_t off, bool ok) { return ok ? __ldg(base + off) : 0.0f; }
-
-__device__ __forceinline__ int slab_coord(const StepParams& p, int axis, int coord, int extent) {
-  const int lo = p.slab_lo[axis], hi = p.slab_hi[axis];
-  if (coord < 0) return -1;
-  if (coord < lo) return coord;
-  const int hs = extent - hi;
-  if (coord >= hs && coord < extent) return lo + coord - hs;
-  return -1;
-}
-
-// psi = b psi + c d; returns d / kappa + psi (magnetic.cu:105-111)
-__device__ __forceinline__ float psi_step(float d, float b, float c, float ik, const float* psi_in, float* psi_out,
-                                          int off, bool write) {
-  const float v = b * psi_in[off] + c * d;
-  if (write) psi_out[off] = v;
-  return d * ik + v;
-}
-
-// Slab element offsets (32-bit: every engine array holds fewer than 2^31 elements).
-__device__ __forceinline__ int xslab_off(const StepParams& p, int lx, int j, int k) { return (lx * p.NY + j) * p.P + k; }
-__device__ __forceinline__ int yslab_off(const StepParams& p, int i, int ly, int k) {
-  return (i * (p.slab_lo[1] + p.slab_hi[1]) + ly) * p.P + k;
-}
-__device__ __forceinline__ int zslab_off(const StepParams& p, int i, int j, int lz) { return (i * p.NY + j) * p.SZ + lz; }
-
-// True when the CSR list of `key` along `axis` holds at least one item.
-__device__ __forceinline__ bool list_nonempty(const BoxIndex& ix, int axis, int key) {
-  return __ldg(ix.ptr[axis] + key) < __ldg(ix.ptr[axis] + key + 1);
-}
-
-// Injection terms of one phase covering (i, j, k), scanning only the lists
-// flagged non-empty; value added to component (comp - base).
-__device__ __forceinline__ void add_terms(const StepParams& p, int phase, int base, int n, int i, int j, int k,
-                                          bool sx, bool sy, bool sz, float& v0, float& v1, float& v2) {
-  const BoxIndex& ix = p.term_index[phase];
-  const int key[3] = {i, j, k};
-  const bool scan[3] = {sx, sy, sz};
-#pragma unroll
-  for (int a = 0; a < 3; ++a) {
-    if (!scan[a]) continue;
-    const int b = __ldg(ix.ptr[a] + key[a]), e = __ldg(ix.ptr[a] + key[a] + 1);
-    for (int x = b; x < e; ++x) {
-      const InjectionTerm& t = p.terms[__ldg(ix.ids[a] + x)];
-      if (i < t.i0 || i >= t.i1 || j < t.j0 || j >= t.j1 || k < t.k0 || k >= t.k1) continue;
-      const int li = i - t.i0, lj = j - t.j0, lk = k - t.k0;
-      float s;
-      if (t.signal != nullptr) {
-        s = __ldg(t.signal + n);
-      } else {
-        const int la = t.sample_axis == 0 ? li : (t.sample_axis == 1 ? lj : lk);
-        s = __ldg(t.aux_hist + static_cast<int64_t>(n) * t.aux_len + __ldg(t.sample_index + la));
-      }
-      const float val = __ldg(t.coeff + (static_cast<int64_t>(li) * (t.j1 - t.j0) + lj) * (t.k1 - t.k0) + lk) * s * t.scale;
-      const int c = t.comp - base;
-      if (c == 0) v0 += val;
-      else if (c == 1) v1 += val;
-      else v2 += val;
-    }
-  }
-}
-
-// Advance the ADE poles covering (i, j, k) from E^n and subtract dt J / eps.
-// `lane_poles` has bit b set when pole b (b < 32) covers this lane's (j, k);
-// the plane list already restricts i.
-__device__ __forceinline__ void ade(const StepParams& p, unsigned lane_poles, int i, int j, int k, float e0, float e1,
-                                    float e2, float& v0, float& v1, float& v2) {
-  const int b = __ldg(p.pole_plane_ptr + i), e = __ldg(p.pole_plane_ptr + i + 1);
-  for (int x = b; x < e; ++x) {
-    const int id = __ldg(p.pole_plane_ids + x);
-    if (id < 32 && !((lane_poles >> id) & 1u)) continue;
-    const PoleTerm& pt = p.poles[id];
-    if (id >= 32 && (j < pt.j0 || j >= pt.j1 || k < pt.k0 || k >= pt.k1)) continue;
-    const int64_t o = (static_cast<int64_t>(i - pt.i0) * (pt.j1 - pt.j0) + (j - pt.j0)) * (pt.k1 - pt.k0) + (k - pt.k0);
-    const int c = pt.comp;
-    const float eo = c == 0 ? e0 : (c == 1 ? e1 : e2);
-    const float drive = __ldg(pt.drive + o);
-    float jn;
-    if (pt.kind == 0) {
-      const float prev = pt.pol[o];
-      const float next = pt.decay * prev + drive * eo;
-      pt.pol[o] = next;
-      jn = (next - prev) * pt.inv_dt;
-      pt.cur[o] = jn;
-    } else if (pt.kind == 1) {
-      jn = pt.decay * pt.cur[o] + drive * eo;
-      pt.cur[o] = jn;
-    } else {
-      const float pol = pt.pol[o];
-      jn = pt.decay * pt.cur[o] - pt.restoring * pol + drive * eo;
-      pt.cur[o] = jn;
-      pt.pol[o] = pol + pt.dt * jn;
-    }
-    const float sub = pt.dt * jn * __ldg(pt.inv_eps + o);
-    if (c == 0) v0 -= sub;
-    else if (c == 1) v1 -= sub;
-    else v2 -= sub;
-  }
-}
-
-// E edge status (electric.cu:242-268): 0 update, 1 keep (NONE/PML edge),
-// 2 PEC zero, 3 outside the Yee extent (stays zero).
-__device__ __forceinline__ int edge_mode(bool in_extent, bool alo, bool ahi, bool blo, bool bhi, int ma_lo, int ma_hi,
-                                         int mb_lo, int mb_hi) {
-  if (!in_extent) return 3;
-  if ((alo && ma_lo == BND_PEC) || (ahi && ma_hi == BND_PEC) || (blo && mb_lo == BND_PEC) || (bhi && mb_hi == BND_PEC))
-    return 2;
-  return (alo || ahi || blo || bhi) ? 1 : 0;
-}
-
-__device__ __forceinline__ float pick(int mode, float updated, float old) {
-  return mode == 0 ? updated : (mode == 1 ? old : 0.f);
-}
-
-// CPML profile values of one coordinate (b, c, 1/kappa).
-struct Prof {
-  float b, c, ik;
-};
-__device__ __forceinline__ Prof prof(const float* b, const float* c, const float* ik, int idx) {
-  return {__ldg(b + idx), __ldg(c + idx), __ldg(ik + idx)};
-}
-
-// Lookup flags that do not change along the x march (bits of `lf`).
-constexpr unsigned kLfHTermYm = 1u, kLfHTermYc = 2u, kLfHTermZ = 4u, kLfETermY = 8u, kLfETermZ = 16u;
-
-}  // namespace
-
-// kCpml: the scene has CPML slabs.  kCoef: some decay/curl coefficient is a
-// per-cell array.  kMinBlocks trades registers for occupancy.
-// kUniform: every axis has constant spacing, so the inverse spacings are the
-// scalars p.inv_e_u / p.inv_h_u.
-template <bool kCpml, bool kCoef, bool kUniform, int kMinBlocks>
-__global__ void __launch_bounds__(256, kMinBlocks) warp_step_kernel(const StepParams p, int n, int slot) {
-  const int lane = threadIdx.x & 31;
-  const int j = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+// The march of one warp task (row j, z block blockIdx.y, x chunk blockIdx.z).
+// kCpml: run the CPML psi code (the task's footprint touches a slab).  kCoef:
+// read the per-cell decay/curl arrays (some coefficient of the footprint
+// differs from the background scalars p.*_u).  kUniform: every axis has
+// constant spacing, so the inverse spacings are the scalars p.inv_e_u/inv_h_u.
+template <bool kCpml, bool kCoef, bool kUniform>
+__device__ __forceinline__ void march(const StepParams& p, int n, int lane, int j) {
   const int NX = p.NX, NY = p.NY, NZ = p.NZ, P = p.P;
-  if (j >= NY) return;  // whole warp; this kernel has no block-level barrier
   const int k = blockIdx.y * kOut - 1 + lane;
   const bool kok = k >= 0 && k < P;
   const bool out_lane = lane >= 1 && lane <= kOut && k < P;
@@ -189,19 +55,20 @@ __global__ void __launch_bounds__(256, kMinBlocks) warp_step_kernel(const StepPa
   const float iey = kUniform ? p.inv_e_u[1] : __ldg(p.inv_e[1] + j);
   const bool ylo = j == 0, yhi = j == NY - 1, zlo = k == 0, zhi = k == NZ - 1;
   const bool lane_edge = ylo || yhi || k <= 0 || k >= NZ - 1;
+  // CPML slab coordinates; the profile values are re-read (L1 hits) inside the
+  // slab branches rather than held in registers across the march.  y_slab is
+  // uniform over the warp; z_slab is made uniform with a vote, so a warp
+  // outside every z slab skips the z psi code entirely.
   int szh = -1, sze = -1, syh_m = -1, syh_c = -1, sye = -1;
-  Prof pzh{0.f, 0.f, 1.f}, pze{0.f, 0.f, 1.f}, pym{0.f, 0.f, 1.f}, pyc{0.f, 0.f, 1.f}, pye{0.f, 0.f, 1.f};
+  bool y_slab = false, z_slab = false;
   if (kCpml) {
     szh = slab_coord(p, 2, k, NZ - 1);
     sze = slab_coord(p, 2, k, NZ);
     syh_m = jm_ok ? slab_coord(p, 1, jm, NY - 1) : -1;
     syh_c = slab_coord(p, 1, j, NY - 1);
     sye = slab_coord(p, 1, j, NY);
-    if (szh >= 0) pzh = prof(p.hb[2], p.hc[2], p.hik[2], k);
-    if (sze >= 0) pze = prof(p.eb[2], p.ec[2], p.eik[2], k);
-    if (syh_m >= 0) pym = prof(p.hb[1], p.hc[1], p.hik[1], jm);
-    if (syh_c >= 0) pyc = prof(p.hb[1], p.hc[1], p.hik[1], j);
-    if (sye >= 0) pye = prof(p.eb[1], p.ec[1], p.eik[1], j);
+    y_slab = syh_m >= 0 || syh_c >= 0 || sye >= 0;
+    z_slab = __any_sync(kFull, szh >= 0 || sze >= 0);
   }
   unsigned lf = 0;
   if (p.n_terms[1]) {
@@ -259,6 +126,38 @@ __global__ void __launch_bounds__(256, kMinBlocks) warp_step_kernel(const StepPa
     const float hc0 = ldz(p.Hin[0], o + rc, kok);
     const float hc1 = ldz(p.Hin[1], o + rc, kok);
     const float hc2 = ldz(p.Hin[2], o + rc, kok);
+    const bool ix_ok = i < NX - 1;
+    const bool mx_ok = jm_ok && hz_kok, mz_ok = jm_ok && ix_ok && ez_kok;
+    const bool cx_ok = yc_ok && hz_kok, cy_ok = ix_ok && hz_kok, cz_ok = ix_ok && yc_ok && ez_kok;
+    // Old H psi values of this plane, loaded before the curl math so their
+    // latency overlaps it: x slab (Hz row j-1, Hy, Hz), y slab (Hx, Hz of rows
+    // j-1 and j), z slab (Hx row j-1, Hx, Hy).
+    int sxh = -1, sxe = -1;
+    float qx0 = 0.f, qx1 = 0.f, qx2 = 0.f, qy0 = 0.f, qy1 = 0.f, qy2 = 0.f, qy3 = 0.f, qz0 = 0.f, qz1 = 0.f, qz2 = 0.f;
+    if (kCpml) {
+      sxh = slab_coord(p, 0, i, NX - 1);
+      sxe = slab_coord(p, 0, i, NX);
+      if (sxh >= 0) {
+        qx0 = ldz(p.psiHin[2][0], xslab_off(p, sxh, jm, k), mz_ok);
+        qx1 = ldz(p.psiHin[1][0], xslab_off(p, sxh, j, k), cy_ok);
+        qx2 = ldz(p.psiHin[2][0], xslab_off(p, sxh, j, k), cz_ok);
+      }
+      if (y_slab) {
+        if (syh_m >= 0) {
+          qy0 = ldz(p.psiHin[0][0], yslab_off(p, i, syh_m, k), mx_ok);
+          qy1 = ldz(p.psiHin[2][1], yslab_off(p, i, syh_m, k), mz_ok);
+        }
+        if (syh_c >= 0) {
+          qy2 = ldz(p.psiHin[0][0], yslab_off(p, i, syh_c, k), cx_ok);
+          qy3 = ldz(p.psiHin[2][1], yslab_off(p, i, syh_c, k), cz_ok);
+        }
+      }
+      if (z_slab && szh >= 0) {
+        qz0 = ldz(p.psiHin[0][1], zslab_off(p, i, jm, szh), mx_ok);
+        qz1 = ldz(p.psiHin[0][1], zslab_off(p, i, j, szh), cx_ok);
+        qz2 = ldz(p.psiHin[1][1], zslab_off(p, i, j, szh), cy_ok);
+      }
+    }
     // E coefficient arrays of this plane, issued early so their latency hides
     // behind the H update
     float g0 = p.edecay_u[0], g1 = p.edecay_u[1], g2 = p.edecay_u[2];
@@ -272,7 +171,6 @@ __global__ void __launch_bounds__(256, kMinBlocks) warp_step_kernel(const StepPa
       if (p.edecay[1]) g1 = ldz(p.edecay[1], o + rc, ld);
       if (p.edecay[2]) g2 = ldz(p.edecay[2], o + rc, ld);
     }
-    const bool ix_ok = i < NX - 1;
     const float ihx = kUniform ? p.inv_h_u[0] : __ldg(p.inv_h[0] + (ix_ok ? i : 0));
     // z+1 neighbours of rows j-1 and j (the halo row needs Ey only: its Hy is unused)
     const float em1k = __shfl_down_sync(kFull, em1, 1);
@@ -286,26 +184,31 @@ __global__ void __launch_bounds__(256, kMinBlocks) warp_step_kernel(const StepPa
     float cxa = (ep2 - ec2) * ihy_c, cxb = (ec1k - ec1) * ihz;
     float cya = (nc2 - ec2) * ihx, cyb = (ec0k - ec0) * ihz;
     float cza = (nc1 - ec1) * ihx, czb = (ep0 - ec0) * ihy_c;
-    const bool mx_ok = jm_ok && hz_kok, mz_ok = jm_ok && ix_ok && ez_kok;
-    const bool cx_ok = yc_ok && hz_kok, cy_ok = ix_ok && hz_kok, cz_ok = ix_ok && yc_ok && ez_kok;
-    int sxh = -1, sxe = -1;
     if (kCpml) {
-      sxh = slab_coord(p, 0, i, NX - 1);
-      sxe = slab_coord(p, 0, i, NX);
-      if (sxh >= 0 || szh >= 0 || syh_m >= 0 || syh_c >= 0) {
-        const bool wr = own && out_lane;
-        Prof pxh{0.f, 0.f, 1.f};
-        if (sxh >= 0) pxh = prof(p.hb[0], p.hc[0], p.hik[0], i);
-        if (syh_m >= 0 && mx_ok) mxa = psi_step(mxa, pym.b, pym.c, pym.ik, p.psiHin[0][0], p.psiHout[0][0], yslab_off(p, i, syh_m, k), false);
-        if (szh >= 0 && mx_ok) mxb = psi_step(mxb, pzh.b, pzh.c, pzh.ik, p.psiHin[0][1], p.psiHout[0][1], zslab_off(p, i, jm, szh), false);
-        if (sxh >= 0 && mz_ok) mza = psi_step(mza, pxh.b, pxh.c, pxh.ik, p.psiHin[2][0], p.psiHout[2][0], xslab_off(p, sxh, jm, k), false);
-        if (syh_m >= 0 && mz_ok) mzb = psi_step(mzb, pym.b, pym.c, pym.ik, p.psiHin[2][1], p.psiHout[2][1], yslab_off(p, i, syh_m, k), false);
-        if (syh_c >= 0 && cx_ok) cxa = psi_step(cxa, pyc.b, pyc.c, pyc.ik, p.psiHin[0][0], p.psiHout[0][0], yslab_off(p, i, syh_c, k), wr);
-        if (szh >= 0 && cx_ok) cxb = psi_step(cxb, pzh.b, pzh.c, pzh.ik, p.psiHin[0][1], p.psiHout[0][1], zslab_off(p, i, j, szh), wr);
-        if (sxh >= 0 && cy_ok) cya = psi_step(cya, pxh.b, pxh.c, pxh.ik, p.psiHin[1][0], p.psiHout[1][0], xslab_off(p, sxh, j, k), wr);
-        if (szh >= 0 && cy_ok) cyb = psi_step(cyb, pzh.b, pzh.c, pzh.ik, p.psiHin[1][1], p.psiHout[1][1], zslab_off(p, i, j, szh), wr);
-        if (sxh >= 0 && cz_ok) cza = psi_step(cza, pxh.b, pxh.c, pxh.ik, p.psiHin[2][0], p.psiHout[2][0], xslab_off(p, sxh, j, k), wr);
-        if (syh_c >= 0 && cz_ok) czb = psi_step(czb, pyc.b, pyc.c, pyc.ik, p.psiHin[2][1], p.psiHout[2][1], yslab_off(p, i, syh_c, k), wr);
+      const bool wr = own && out_lane;
+      if (sxh >= 0) {  // plane inside an x slab: uniform over the warp
+        const Prof px = prof(p.hb[0], p.hc[0], p.hik[0], i);
+        if (mz_ok) mza = psi_apply(mza, px.b, px.c, px.ik, qx0, p.psiHout[2][0], xslab_off(p, sxh, jm, k), false);
+        if (cy_ok) cya = psi_apply(cya, px.b, px.c, px.ik, qx1, p.psiHout[1][0], xslab_off(p, sxh, j, k), wr);
+        if (cz_ok) cza = psi_apply(cza, px.b, px.c, px.ik, qx2, p.psiHout[2][0], xslab_off(p, sxh, j, k), wr);
+      }
+      if (y_slab) {
+        if (syh_m >= 0) {
+          const Prof py = prof(p.hb[1], p.hc[1], p.hik[1], jm);
+          if (mx_ok) mxa = psi_apply(mxa, py.b, py.c, py.ik, qy0, p.psiHout[0][0], yslab_off(p, i, syh_m, k), false);
+          if (mz_ok) mzb = psi_apply(mzb, py.b, py.c, py.ik, qy1, p.psiHout[2][1], yslab_off(p, i, syh_m, k), false);
+        }
+        if (syh_c >= 0) {
+          const Prof py = prof(p.hb[1], p.hc[1], p.hik[1], j);
+          if (cx_ok) cxa = psi_apply(cxa, py.b, py.c, py.ik, qy2, p.psiHout[0][0], yslab_off(p, i, syh_c, k), wr);
+          if (cz_ok) czb = psi_apply(czb, py.b, py.c, py.ik, qy3, p.psiHout[2][1], yslab_off(p, i, syh_c, k), wr);
+        }
+      }
+      if (z_slab && szh >= 0) {
+        const Prof pz = prof(p.hb[2], p.hc[2], p.hik[2], k);
+        if (mx_ok) mxb = psi_apply(mxb, pz.b, pz.c, pz.ik, qz0, p.psiHout[0][1], zslab_off(p, i, jm, szh), false);
+        if (cx_ok) cxb = psi_apply(cxb, pz.b, pz.c, pz.ik, qz1, p.psiHout[0][1], zslab_off(p, i, j, szh), wr);
+        if (cy_ok) cyb = psi_apply(cyb, pz.b, pz.c, pz.ik, qz2, p.psiHout[1][1], zslab_off(p, i, j, szh), wr);
       }
     }
     float dHx = p.hdecay_u[0], cHx = p.hcurl_u[0], dHy = p.hdecay_u[1], cHy = p.hcurl_u[1], dHz = p.hdecay_u[2],
@@ -353,15 +256,22 @@ __global__ void __launch_bounds__(256, kMinBlocks) warp_step_kernel(const StepPa
         m1 = edge_mode(yc_ok && ez_kok, xlo, xhi, zlo, zhi, p.bnd[0], p.bnd[1], p.bnd[4], p.bnd[5]);
         m2 = edge_mode(hz_kok, xlo, xhi, ylo, yhi, p.bnd[0], p.bnd[1], p.bnd[2], p.bnd[3]);
       }
-      if (kCpml && (sxe >= 0 || sye >= 0 || sze >= 0)) {
-        Prof pxe{0.f, 0.f, 1.f};
-        if (sxe >= 0) pxe = prof(p.eb[0], p.ec[0], p.eik[0], i);
-        if (sye >= 0 && m0 == 0) d0a = psi_step(d0a, pye.b, pye.c, pye.ik, p.psiE[0][0], p.psiE[0][0], yslab_off(p, i, sye, k), true);
-        if (sze >= 0 && m0 == 0) d0b = psi_step(d0b, pze.b, pze.c, pze.ik, p.psiE[0][1], p.psiE[0][1], zslab_off(p, i, j, sze), true);
-        if (sxe >= 0 && m1 == 0) d1a = psi_step(d1a, pxe.b, pxe.c, pxe.ik, p.psiE[1][0], p.psiE[1][0], xslab_off(p, sxe, j, k), true);
-        if (sze >= 0 && m1 == 0) d1b = psi_step(d1b, pze.b, pze.c, pze.ik, p.psiE[1][1], p.psiE[1][1], zslab_off(p, i, j, sze), true);
-        if (sxe >= 0 && m2 == 0) d2a = psi_step(d2a, pxe.b, pxe.c, pxe.ik, p.psiE[2][0], p.psiE[2][0], xslab_off(p, sxe, j, k), true);
-        if (sye >= 0 && m2 == 0) d2b = psi_step(d2b, pye.b, pye.c, pye.ik, p.psiE[2][1], p.psiE[2][1], yslab_off(p, i, sye, k), true);
+      if (kCpml) {
+        if (sxe >= 0) {
+          const Prof px = prof(p.eb[0], p.ec[0], p.eik[0], i);
+          if (m1 == 0) d1a = psi_step(d1a, px.b, px.c, px.ik, p.psiE[1][0], p.psiE[1][0], xslab_off(p, sxe, j, k), true);
+          if (m2 == 0) d2a = psi_step(d2a, px.b, px.c, px.ik, p.psiE[2][0], p.psiE[2][0], xslab_off(p, sxe, j, k), true);
+        }
+        if (sye >= 0) {
+          const Prof py = prof(p.eb[1], p.ec[1], p.eik[1], j);
+          if (m0 == 0) d0a = psi_step(d0a, py.b, py.c, py.ik, p.psiE[0][0], p.psiE[0][0], yslab_off(p, i, sye, k), true);
+          if (m2 == 0) d2b = psi_step(d2b, py.b, py.c, py.ik, p.psiE[2][1], p.psiE[2][1], yslab_off(p, i, sye, k), true);
+        }
+        if (z_slab && sze >= 0) {
+          const Prof pz = prof(p.eb[2], p.ec[2], p.eik[2], k);
+          if (m0 == 0) d0b = psi_step(d0b, pz.b, pz.c, pz.ik, p.psiE[0][1], p.psiE[0][1], zslab_off(p, i, j, sze), true);
+          if (m1 == 0) d1b = psi_step(d1b, pz.b, pz.c, pz.ik, p.psiE[1][1], p.psiE[1][1], zslab_off(p, i, j, sze), true);
+        }
       }
       float v0 = pick(m0, ec0 * g0 + c0 * (d0a - d0b), ec0);
       float v1 = pick(m1, ec1 * g1 + c1 * (d1b - d1a), ec1);
@@ -386,6 +296,89 @@ __global__ void __launch_bounds__(256, kMinBlocks) warp_step_kernel(const StepPa
     ep0 = np0;
     ep2 = np2;
   }
+}
+
+// kAnyCpml / kAnyCoef: the scene has CPML slabs / some coefficient array.
+// Each warp reads its class and runs the cheapest march that is exact for its
+// footprint, so the CPML and coefficient code runs only where it changes the
+// result.  kMinBlocks trades registers for occupancy.
+template <bool kAnyCpml, bool kAnyCoef, bool kUniform, int kMinBlocks>
+__global__ void __launch_bounds__(256, kMinBlocks) warp_step_kernel(const StepParams p, int n, int slot) {
+  (void)slot;
+  const int lane = threadIdx.x & 31;
+  const int j = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  if (j >= p.NY) return;  // whole warp; this kernel has no block-level barrier
+  unsigned cls = 0;
+  if (kAnyCpml || kAnyCoef)
+    cls = __ldg(p.warp_class + (static_cast<int64_t>(blockIdx.z) * gridDim.y + blockIdx.y) * p.NY + j);
+  if (kAnyCpml && (cls & kClassCpml)) {
+    if (kAnyCoef && (cls & kClassCoef)) march<true, true, kUniform>(p, n, lane, j);
+    else march<true, false, kUniform>(p, n, lane, j);
+  } else {
+    if (kAnyCoef && (cls & kClassCoef)) march<false, true, kUniform>(p, n, lane, j);
+    else march<false, false, kUniform>(p, n, lane, j);
+  }
+}
+
+namespace {
+
+// Yee extent of component c (0..2 Ex..Ez, 3..5 Hx..Hz) along each axis.
+__device__ __forceinline__ void comp_ext(int c, int NX, int NY, int NZ, int& e0, int& e1, int& e2) {
+  e0 = (c == 0 || c == 4 || c == 5) ? NX - 1 : NX;
+  e1 = (c == 1 || c == 3 || c == 5) ? NY - 1 : NY;
+  e2 = (c == 2 || c == 3 || c == 4) ? NZ - 1 : NZ;
+}
+
+// One warp per task; the footprint is every (plane, row, lane) the march
+// touches: planes [istart, i1), rows j-1 and j, lanes k = 30 s - 1 .. 30 s + 30.
+__global__ void classify_kernel(const StepParams p, int n_kblocks, int n_chunks, unsigned char* out) {
+  const int lane = threadIdx.x & 31;
+  const int64_t task = static_cast<int64_t>(blockIdx.x) * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  const int NX = p.NX, NY = p.NY, NZ = p.NZ, P = p.P;
+  if (task >= static_cast<int64_t>(n_chunks) * n_kblocks * NY) return;
+  const int j = static_cast<int>(task % NY);
+  const int s = static_cast<int>((task / NY) % n_kblocks);
+  const int c = static_cast<int>(task / (static_cast<int64_t>(NY) * n_kblocks));
+  const int k = s * kOut - 1 + lane;
+  const bool kok = k >= 0 && k < P;
+  const int i0 = c * p.CX, i1 = min(i0 + p.CX, NX), istart = max(i0 - 1, 0);
+  const int jm = j >= 1 ? j - 1 : j;
+  bool cpml = false;
+  if (p.cpml) {
+    cpml = (kok && (slab_coord(p, 2, k, NZ - 1) >= 0 || slab_coord(p, 2, k, NZ) >= 0)) ||
+           slab_coord(p, 1, jm, NY - 1) >= 0 || slab_coord(p, 1, j, NY - 1) >= 0 || slab_coord(p, 1, j, NY) >= 0;
+    for (int i = istart; i < i1 && !cpml; ++i) cpml = slab_coord(p, 0, i, NX - 1) >= 0 || slab_coord(p, 0, i, NX) >= 0;
+  }
+  bool coef = false;
+  for (int comp = 0; comp < 6; ++comp) {
+    const float* dec = comp < 3 ? p.edecay[comp] : p.hdecay[comp - 3];
+    const float* cur = comp < 3 ? p.ecurl[comp] : p.hcurl[comp - 3];
+    if (!dec && !cur) continue;
+    const float dbg = comp < 3 ? p.edecay_u[comp] : p.hdecay_u[comp - 3];
+    const float cbg = comp < 3 ? p.ecurl_u[comp] : p.hcurl_u[comp - 3];
+    int e0, e1, e2;
+    comp_ext(comp, NX, NY, NZ, e0, e1, e2);
+    for (int i = istart; i < i1 && !coef; ++i) {
+      for (int r = 0; r < 2; ++r) {
+        const int jj = r ? j : jm;
+        if (!kok || i >= e0 || jj >= e1 || k >= e2) continue;
+        const int64_t o = (static_cast<int64_t>(i) * NY + jj) * P + k;
+        if (dec && __ldg(dec + o) != dbg) coef = true;
+        if (cur && __ldg(cur + o) != cbg) coef = true;
+      }
+    }
+  }
+  const unsigned any_cpml = __any_sync(kFull, cpml), any_coef = __any_sync(kFull, coef);
+  if (lane == 0) out[task] = static_cast<unsigned char>((any_cpml ? kClassCpml : 0u) | (any_coef ? kClassCoef : 0u));
+}
+
+}  // namespace
+
+int launch_classify(const StepParams& p, int n_kblocks, int n_chunks, unsigned char* out, cudaStream_t stream) {
+  const int64_t tasks = static_cast<int64_t>(n_chunks) * n_kblocks * p.NY;
+  const int64_t blocks = (tasks + 7) / 8;
+  classify_kernel<<<static_cast<unsigned>(blocks), 256, 0, stream>>>(p, n_kblocks, n_chunks, out);
+  return static_cast<int>(cudaGetLastError());
 }
 
 #define FDTD_INSTANTIATE(CPML, COEF, UNI)                                                  \
