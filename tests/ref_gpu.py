@@ -1,0 +1,241 @@
+"""The reference's own CUDA FDTD ops, stepped in the reference's order (test checker).
+
+Loads the library that ``oracle/build_ref.py`` compiles from the reference's
+sources into ``oracle/_ref/`` and drives its torch ops
+(``torch.ops.witwin_maxwell_fdtd_cuda.*``, schemas at
+witwin/maxwell/fdtd/cuda/extension.cpp:2059-2196) over the tensors of one
+compiled scene, one op per launch, in the order of
+witwin/maxwell/fdtd/runtime/stepping.py:1740-1815 and :2295-2330: H update,
+TFSF magnetic corrections, aux H, ADE advance, E update, TFSF electric
+corrections, aux E, soft sources, ADE subtraction, PEC clamp.  The monitor
+DFT is accumulated here in float64 from the stepped fields (phase recurrence
+as observers.py:577-659).  Only tests import this module.
+"""
+from __future__ import annotations
+
+from pathlib import Path
+
+import numpy as np
+import torch
+
+ROOT = Path(__file__).resolve().parents[1]
+REF_LIB = ROOT / "oracle" / "_ref" / "witwin_maxwell_fdtd_cuda.so"
+COMPONENTS = ("Ex", "Ey", "Ez", "Hx", "Hy", "Hz")
+_H_SPEC = {"Hx": (1, 2, "Ey", "Ez"), "Hy": (0, 2, "Ex", "Ez"), "Hz": (0, 1, "Ex", "Ey")}
+_E_SPEC = {"Ex": (1, 2, "Hy", "Hz"), "Ey": (0, 2, "Hx", "Hz"), "Ez": (0, 1, "Hx", "Hy")}
+_loaded = False
+
+
+def available() -> bool:
+    return REF_LIB.exists()
+
+
+def ops():
+    global _loaded
+    if not _loaded:
+        torch.ops.load_library(str(REF_LIB))
+        _loaded = True
+    return torch.ops.witwin_maxwell_fdtd_cuda
+
+
+def _shape(name, nodes):
+    nx, ny, nz = nodes
+    return {
+        "Ex": (nx - 1, ny, nz), "Ey": (nx, ny - 1, nz), "Ez": (nx, ny, nz - 1),
+        "Hx": (nx, ny - 1, nz - 1), "Hy": (nx - 1, ny, nz - 1), "Hz": (nx - 1, ny - 1, nz),
+    }[name]
+
+
+class RefGpuSimulation:
+    def __init__(self, compiled, device: str = "cuda"):
+        self.cs = cs = compiled
+        self.op = ops()
+        dev = torch.device(device)
+        self.dev = dev
+
+        def t(a, dtype=torch.float32):
+            return torch.as_tensor(np.ascontiguousarray(a)).to(device=dev, dtype=dtype).contiguous()
+
+        nodes = cs.nodes
+        self.F = {n: torch.zeros(_shape(n, nodes), device=dev) for n in COMPONENTS}
+        self.decay, self.curl = {}, {}
+        for n in COMPONENTS:
+            du, cu = cs.uniform[n]
+            shape = _shape(n, nodes)
+            self.decay[n] = torch.full(shape, du, device=dev) if cs.decay[n] is None else t(cs.decay[n])
+            self.curl[n] = torch.full(shape, cu, device=dev) if cs.curl[n] is None else t(cs.curl[n])
+        self.inv_e = [t(a) for a in cs.inv_e]
+        self.inv_h = [t(a) for a in cs.inv_h]
+        self.cp = {k: [t(a) for a in v] for k, v in cs.cpml.items()}
+        self.cpml = any(cs.pml_lo) or any(cs.pml_hi)
+        self.psi, self.slab = {}, {}
+        for n in COMPONENTS:
+            spec = _H_SPEC.get(n) or _E_SPEC[n]
+            shape = _shape(n, nodes)
+            for which, axis in enumerate(spec[:2]):
+                size = shape[axis]
+                low = min(cs.pml_lo[axis], size)
+                high = min(cs.pml_hi[axis], max(size - low, 0))
+                cshape = list(shape)
+                cshape[axis] = low + high
+                self.psi[(n, which)] = torch.zeros(cshape, device=dev)
+                self.slab[(n, which)] = (low, size - high, high)
+        self.poles = []
+        for pole in cs.poles:
+            shape = _shape(pole.component, nodes)
+            b = pole.box
+            drive = np.zeros(shape, np.float32)
+            drive[b[0]:b[1], b[2]:b[3], b[4]:b[5]] = pole.drive
+            inv_eps = (1.0 / cs.eps[pole.component]).astype(np.float32)
+            inv_eps[b[0]:b[1], b[2]:b[3], b[4]:b[5]] = pole.inv_eps
+            self.poles.append({
+                "comp": pole.component, "kind": pole.kind, "decay": float(pole.decay),
+                "restoring": float(pole.restoring), "drive": t(drive), "inv_eps": t(inv_eps),
+                "P": torch.zeros(shape, device=dev), "J": torch.zeros(shape, device=dev),
+            })
+        self.patches = [(p.component, p.box, t(p.coeff), np.asarray(p.signal, np.float32)) for p in cs.patches]
+        self.aux = None
+        if cs.aux_line is not None:
+            a = cs.aux_line
+            ne = a.e_decay.size
+            self.aux = {
+                "e": torch.zeros(ne, device=dev), "h": torch.zeros(ne - 1, device=dev),
+                "ed": t(a.e_decay), "ec": t(a.e_curl), "hd": t(a.h_decay), "hc": t(a.h_curl),
+                "src": int(a.source_index), "signal": np.asarray(a.source, np.float32),
+            }
+        self.lines = [(lp.component, lp.box, t(lp.coeff), lp.sample_kind, int(lp.sample_axis),
+                       t(lp.sample_index, torch.int32), float(lp.scale)) for lp in cs.line_patches]
+        self.freqs = np.asarray(cs.frequencies, dtype=np.float64)
+        nf = self.freqs.size
+        self.acc = []
+        for reg in cs.regions:
+            b = reg.box
+            shape = (nf, b[1] - b[0], b[3] - b[2], b[5] - b[4])
+            self.acc.append([torch.zeros(shape, dtype=torch.float64, device=dev),
+                             torch.zeros(shape, dtype=torch.float64, device=dev)])
+        omega = 2.0 * np.pi * self.freqs
+        self.step_c, self.step_s = np.cos(omega * cs.dt), np.sin(omega * cs.dt)
+        self.hoff_c, self.hoff_s = np.cos(-0.5 * omega * cs.dt), np.sin(-0.5 * omega * cs.dt)
+        self.pc, self.ps = np.ones(nf), np.zeros(nf)
+        self.window_sum = 0.0
+        self.step = 0
+        self.monitors = True
+
+    # ------------------------------------------------------------------ ops
+    def _update_h(self):
+        F, cp = self.F, self.cp
+        for n, (A, B, first, second) in _H_SPEC.items():
+            fn = f"update_magnetic_h{n[1]}"
+            if self.cpml:
+                sa, sb = self.slab[(n, 0)], self.slab[(n, 1)]
+                getattr(self.op, fn + "_cpml_compressed")(
+                    F[n], F[first], F[second], self.decay[n], self.curl[n], self.psi[(n, 0)], self.psi[(n, 1)],
+                    cp["ik_h"][A], cp["b_h"][A], cp["c_h"][A], cp["ik_h"][B], cp["b_h"][B], cp["c_h"][B],
+                    self.inv_h[A], self.inv_h[B], sa[0], sa[1], sa[2], sb[0], sb[1], sb[2], None, None)
+            else:
+                getattr(self.op, fn + "_standard")(F[n], F[first], F[second], self.decay[n], self.curl[n],
+                                                   self.inv_h[A], self.inv_h[B], None, None)
+
+    def _update_e(self):
+        F, cp, bnd = self.F, self.cp, self.cs.boundary
+        for n, (A, B, first, second) in _E_SPEC.items():
+            fn = f"update_electric_e{n[1]}"
+            modes = (bnd[2 * A], bnd[2 * A + 1], bnd[2 * B], bnd[2 * B + 1])
+            if self.cpml:
+                sa, sb = self.slab[(n, 0)], self.slab[(n, 1)]
+                getattr(self.op, fn + "_cpml_compressed")(
+                    F[n], F[first], F[second], self.decay[n], self.curl[n], self.psi[(n, 0)], self.psi[(n, 1)],
+                    cp["ik_e"][A], cp["b_e"][A], cp["c_e"][A], cp["ik_e"][B], cp["b_e"][B], cp["c_e"][B],
+                    self.inv_e[A], self.inv_e[B], *modes, sa[0], sa[1], sa[2], sb[0], sb[1], sb[2], None, None)
+            else:
+                getattr(self.op, fn + "_standard")(F[n], F[first], F[second], self.decay[n], self.curl[n],
+                                                   self.inv_e[A], self.inv_e[B], *modes, None, None)
+
+    def _advance_ade(self):
+        dt = float(self.cs.dt)
+        for p in self.poles:
+            e = self.F[p["comp"]]
+            if p["kind"] == 0:
+                self.op.update_debye_current(e, p["P"], p["J"], p["drive"], p["decay"], dt)
+            elif p["kind"] == 1:
+                self.op.update_drude_current(e, p["J"], p["drive"], p["decay"])
+            else:
+                self.op.update_lorentz_current(e, p["P"], p["J"], p["drive"], p["decay"], p["restoring"], dt)
+
+    def _apply_ade(self):
+        dt = float(self.cs.dt)
+        for p in self.poles:
+            self.op.apply_polarization_current(self.F[p["comp"]], p["J"], p["inv_eps"], dt)
+
+    def _line_corrections(self, magnetic: bool):
+        incident = self.aux["e"] if magnetic else self.aux["h"]
+        for comp, box, coeff, _kind, axis, idx, scale in self.lines:
+            if (comp[0] == "H") != magnetic:
+                continue
+            self.op.add_scaled_line_source_patch(self.F[comp], coeff, incident, idx, axis, box[0], box[2], box[4],
+                                                 scale)
+
+    def _clamp_pec(self):
+        bnd = self.cs.boundary
+        for n, (A, B, _, _) in _E_SPEC.items():
+            for axis in (A, B):
+                for side in (0, 1):
+                    if bnd[2 * axis + side] == 4:
+                        self.op.clamp_field_face(self.F[n], axis, side)
+
+    def _accumulate(self, n):
+        cs = self.cs
+        if self.freqs.size == 0 or not cs.regions:
+            return
+        w = float(cs.window[n])
+        wc, ws = w * self.pc, w * self.ps
+        hc = wc * self.hoff_c - ws * self.hoff_s
+        hs = ws * self.hoff_c + wc * self.hoff_s
+        for reg, (re, im) in zip(cs.regions, self.acc):
+            b = reg.box
+            v = self.F[reg.component][b[0]:b[1], b[2]:b[3], b[4]:b[5]].double()
+            cc, ss = (wc, ws) if reg.component[0] == "E" else (hc, hs)
+            re += torch.as_tensor(cc, device=self.dev).view(-1, 1, 1, 1) * v
+            im += torch.as_tensor(ss, device=self.dev).view(-1, 1, 1, 1) * v
+        self.window_sum += w
+        self.pc, self.ps = (self.pc * self.step_c - self.ps * self.step_s,
+                            self.ps * self.step_c + self.pc * self.step_s)
+
+    def step_once(self):
+        n = self.step
+        self._update_h()
+        if self.aux is not None:
+            self._line_corrections(True)
+            self.op.update_auxiliary_magnetic(self.aux["h"], self.aux["e"], self.aux["hd"], self.aux["hc"])
+        self._advance_ade()
+        self._update_e()
+        if self.aux is not None:
+            self._line_corrections(False)
+            self.op.update_auxiliary_electric(self.aux["e"], self.aux["h"], self.aux["ed"], self.aux["ec"],
+                                              self.aux["src"], float(self.aux["signal"][n]))
+        for comp, box, coeff, signal in self.patches:
+            self.op.add_source_patch(self.F[comp], coeff, box[0], box[2], box[4], float(signal[n]))
+        self._apply_ade()
+        if self.aux is None:
+            self._clamp_pec()
+        if self.monitors:
+            self._accumulate(n)
+        self.step += 1
+
+    def run(self, steps: int):
+        for _ in range(int(steps)):
+            self.step_once()
+        return self
+
+    def fields(self) -> dict:
+        return {n: v.cpu().numpy() for n, v in self.F.items()}
+
+    def monitor_results(self) -> dict:
+        cs = self.cs
+        scale = 2.0 / self.window_sum if self.window_sum > 0 else 0.0
+        out: dict = {}
+        for reg, (re, im) in zip(cs.regions, self.acc):
+            fidx = [cs.frequencies.index(f) for f in cs.monitor_frequencies[reg.monitor]]
+            data = (re[fidx].cpu().numpy() + 1j * im[fidx].cpu().numpy()) * scale
+            out.setdefault(reg.monitor, {})[reg.component] = data
+        return out
