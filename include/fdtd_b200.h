@@ -171,6 +171,37 @@ int fdtd_engine_time_kernel(fdtd_engine* h, int n, int reps, float* ms);
 /* Device time of the last step_range in milliseconds (CUDA events). */
 int fdtd_engine_last_ms(fdtd_engine* h, float* ms);
 
+/* Reverse-time adjoint: the exact discrete transpose of the fused step (H and
+ * E updates, CPML psi, E edge modes), monitor seeds and dL/deps of design
+ * boxes.  Replaces the reference's native reverse runners
+ * (witwin/maxwell/fdtd/adjoint/native.py:48-725, kernels/adjoint.cu:295-411 and
+ * 1224-1690) and its segment replay (adjoint/core.py:3527-3565).
+ *
+ * fdtd_engine_adjoint_init: allocate and zero the adjoint state.
+ * design_boxes holds 6 ints per E component ([i0,i1,j0,j1,k0,k1] in that
+ * component's Yee index space; an empty box means none) or is NULL.  Boxes
+ * must stay clear of CPML slabs and domain edges.  max_segment is
+ * the longest replay (steps).  Scenes with ADE poles return FDTD_ERR_UNSUPPORTED. */
+int fdtd_engine_adjoint_init(fdtd_engine* h, const int* design_boxes, int max_segment);
+/* Monitor gradients dL/d(unscaled DFT accumulator), [n_freq][n_samples]
+ * (host or device pointers); NULL clears the seeds. */
+int fdtd_engine_adjoint_set_seed(fdtd_engine* h, const float* g_re, const float* g_im);
+/* Forward replay of steps [n0, n1) from the current state (restore a
+ * checkpoint first) without monitor sampling, recording the design-box E
+ * history E^{n0} .. E^{n1}. */
+int fdtd_engine_replay_range(fdtd_engine* h, int n0, int n1);
+/* Reverse steps n1-1 down to n0; with design boxes the last replay must cover
+ * [n0, n1). */
+int fdtd_engine_adjoint_range(fdtd_engine* h, int n1, int n0);
+/* Accumulated dL/deps (absolute permittivity) of the design box of E
+ * component comp (0..2), box-dense [i][j][k]. */
+int fdtd_engine_adjoint_grad(fdtd_engine* h, int comp, float* out);
+/* Adjoint state in the reference's shapes: kind 0 = field component comp
+ * (0..5, which ignored), kind 1 = CPML psi (comp 0..5, which 0/1 as
+ * fdtd_engine_pack_psi). */
+int fdtd_engine_adjoint_pack(fdtd_engine* h, int kind, int comp, int which, const float* src);
+int fdtd_engine_adjoint_unpack(fdtd_engine* h, int kind, int comp, int which, float* dst);
+
 /* ------------------------------------------------------------------------ */
 /* 2. Per-op entry points (reference op semantics)                           */
 /* ------------------------------------------------------------------------ */

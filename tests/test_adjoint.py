@@ -1,0 +1,178 @@
+"""Reverse-time adjoint (GPU): exact transpose of the fused step and
+permittivity gradients against central finite differences.
+
+- Dot-product test: for random states x (E, H, CPML psi) and y (their
+  adjoints), <F x, y> = <x, F^T y> where F is one source-free forward step and
+  F^T one adjoint step; relative tolerance 1e-5 (FP32 sums of ~1e5 terms).
+- dL/deps_r of a design region for L = sum |X|^2 over a point monitor's
+  spectrum, against central differences (h = 1e-2 on eps_r, FP32 fields);
+  relative tolerance 1e-2 per checked cell, and the adjoint must be the same
+  through torch.autograd.
+"""
+from __future__ import annotations
+
+import ctypes
+
+import numpy as np
+import pytest
+import torch
+
+from conftest import load_package
+
+pytestmark = pytest.mark.gpu
+FIELDS = ("Ex", "Ey", "Ez", "Hx", "Hy", "Hz")
+
+
+def _psi_shapes(cs):
+    shapes = {}
+    axes = {0: (1, 2), 1: (0, 2), 2: (0, 1)}
+    for comp, name in enumerate(FIELDS):
+        c = comp % 3
+        nx, ny, nz = cs.nodes
+        ext = {
+            "Ex": (nx - 1, ny, nz), "Ey": (nx, ny - 1, nz), "Ez": (nx, ny, nz - 1),
+            "Hx": (nx, ny - 1, nz - 1), "Hy": (nx - 1, ny, nz - 1), "Hz": (nx - 1, ny - 1, nz),
+        }[name]
+        for which, axis in enumerate(axes[c]):
+            L = cs.pml_lo[axis] + cs.pml_hi[axis]
+            if L == 0:
+                continue
+            shape = list(ext)
+            shape[axis] = L
+            shapes[(comp, which)] = tuple(shape)
+    return shapes
+
+
+def _scene(wm, boundary=None):
+    sc = wm.Scene(cells=(20, 18, 16), spacing=25e-9, pml_cells=4)
+    if boundary is not None:
+        sc.boundary = boundary
+        sc.pml_cells = 0 if all(b != wm.BOUNDARY_PML for b in boundary) else 4
+    sc.structures.append(wm.Structure(wm.Box((6, 5, 5), (12, 11, 10)), wm.Medium(eps_r=3.0)))
+    return sc
+
+
+@pytest.mark.parametrize("kind", ["cpml", "pec", "mixed"])
+def test_adjoint_step_is_the_exact_transpose(kind):
+    wm = load_package()
+    lib = wm._lib.load()
+    P, E, N = wm.BOUNDARY_PML, wm.BOUNDARY_PEC, wm.BOUNDARY_NONE
+    boundary = {"cpml": None, "pec": (E,) * 6, "mixed": (P, E, N, P, P, E)}[kind]
+    cs = wm.compile_scene(_scene(wm, boundary), 4)
+    solver = wm.solver.B200FDTD(cs).init_field()
+    h = solver.handle
+    wm._lib.check(lib.fdtd_engine_adjoint_init(h, None, 1), "adjoint_init")
+    rng = np.random.default_rng(7)
+    dev = solver.device
+    psi = _psi_shapes(cs)
+    x, y = {}, {}
+    for comp, name in enumerate(FIELDS):
+        shape = tuple(solver.field(name).shape)
+        x[("f", comp, 0)] = torch.tensor(rng.standard_normal(shape), dtype=torch.float32, device=dev)
+        y[("f", comp, 0)] = torch.tensor(rng.standard_normal(shape), dtype=torch.float32, device=dev)
+    for (comp, which), shape in psi.items():
+        x[("p", comp, which)] = torch.tensor(rng.standard_normal(shape), dtype=torch.float32, device=dev)
+        y[("p", comp, which)] = torch.tensor(rng.standard_normal(shape), dtype=torch.float32, device=dev)
+    # forward: F x
+    for (kd, comp, which), t in x.items():
+        if kd == "f":
+            wm._lib.check(lib.fdtd_engine_pack_field(h, comp, wm._lib.ptr(t)), "pack")
+        else:
+            wm._lib.check(lib.fdtd_engine_pack_psi(h, comp, which, wm._lib.ptr(t)), "pack_psi")
+    solver.step_range(0, 1)
+    fx = {}
+    for key, t in x.items():
+        out = torch.empty_like(t)
+        kd, comp, which = key
+        if kd == "f":
+            wm._lib.check(lib.fdtd_engine_unpack_field(h, comp, wm._lib.ptr(out)), "unpack")
+        else:
+            wm._lib.check(lib.fdtd_engine_unpack_psi(h, comp, which, wm._lib.ptr(out)), "unpack_psi")
+        fx[key] = out
+    # adjoint: F^T y
+    for (kd, comp, which), t in y.items():
+        wm._lib.check(lib.fdtd_engine_adjoint_pack(h, 0 if kd == "f" else 1, comp, which, wm._lib.ptr(t)), "adj_pack")
+    wm._lib.check(lib.fdtd_engine_adjoint_range(h, 1, 0), "adjoint_range")
+    fty = {}
+    for key, t in y.items():
+        out = torch.empty_like(t)
+        kd, comp, which = key
+        wm._lib.check(lib.fdtd_engine_adjoint_unpack(h, 0 if kd == "f" else 1, comp, which, wm._lib.ptr(out)), "adj_unpack")
+        fty[key] = out
+    torch.cuda.synchronize()
+    lhs = sum(float((fx[k].double() * y[k].double()).sum()) for k in x)
+    rhs = sum(float((x[k].double() * fty[k].double()).sum()) for k in x)
+    scale = sum(float(fx[k].double().abs().mul(y[k].double().abs()).sum()) for k in x)
+    solver.close()
+    assert abs(lhs - rhs) <= 1e-5 * scale, (lhs, rhs, scale)
+
+
+def _design_scene(wm, eps_r):
+    sc = wm.Scene(cells=(28, 24, 24), spacing=25e-9, pml_cells=5)
+    sc.sources.append(wm.PointDipole((9, 12, 12), "Ez", wm.GaussianPulse(300e12, 100e12), width=25e-9))
+    sc.material_regions.append(wm.MaterialRegion((12, 10, 10), (16, 14, 13), eps_r))
+    sc.monitors.append(wm.PointMonitor("probe", (20, 12, 12), frequencies=(300e12,)))
+    return sc
+
+
+def _loss(mons):
+    return sum(float(np.sum(np.abs(np.asarray(v.cpu().numpy())) ** 2)) for v in mons["probe"].values())
+
+
+def test_design_gradient_matches_finite_differences():
+    wm = load_package()
+    adj = wm.adjoint
+    steps = 320
+    rng = np.random.default_rng(3)
+    eps_r = 2.0 + 2.0 * rng.random((4, 4, 3))
+    problem = adj.DesignProblem(_design_scene(wm, eps_r), steps, stride=64)
+    mons = problem.forward(eps_r)
+    grad_out = {"probe": {c: 2.0 * v for c, v in mons["probe"].items()}}  # d sum|X|^2 / dX* convention
+    g = problem.backward(grad_out)
+    problem.close()
+    assert np.isfinite(g).all() and np.abs(g).max() > 0
+    order = np.argsort(-np.abs(g).ravel())[:4]
+    h = 1e-2
+    for flat in order:
+        idx = np.unravel_index(flat, eps_r.shape)
+        vals = []
+        for sgn in (1.0, -1.0):
+            e = eps_r.copy()
+            e[idx] += sgn * h
+            p = adj.DesignProblem(_design_scene(wm, e), steps, stride=steps)
+            vals.append(_loss(p.forward(e)))
+            p.close()
+        fd = (vals[0] - vals[1]) / (2 * h)
+        assert abs(g[idx] - fd) <= 1e-2 * abs(fd), (idx, g[idx], fd)
+
+
+def test_design_gradient_through_autograd():
+    wm = load_package()
+    adj = wm.adjoint
+    steps = 200
+    eps_r = np.full((4, 4, 3), 3.0)
+    problem = adj.DesignProblem(_design_scene(wm, eps_r), steps, stride=50)
+    t = torch.tensor(eps_r, dtype=torch.float32, requires_grad=True)
+    mons = adj.design_monitors(t, problem, [("probe", c) for c in ("Ex", "Ey", "Ez", "Hx", "Hy", "Hz")])
+    loss = sum((v.abs() ** 2).sum() for v in mons["probe"].values())
+    loss.backward()
+    direct = adj.DesignProblem(_design_scene(wm, eps_r), steps, stride=steps)
+    m2 = direct.forward(eps_r)
+    g2 = direct.backward({"probe": {c: 2.0 * v for c, v in m2["probe"].items()}})
+    direct.close()
+    problem.close()
+    np.testing.assert_allclose(t.grad.numpy(), g2, rtol=1e-4, atol=1e-6 * np.abs(g2).max())
+
+
+def test_adjoint_rejects_dispersive_scenes_and_edge_designs():
+    wm = load_package()
+    lib = wm._lib.load()
+    sc = _design_scene(wm, np.full((4, 4, 3), 2.0))
+    sc.structures.append(wm.Structure(wm.Box((2, 2, 2), (5, 5, 5)), wm.Medium.drude(2e15 / (2 * np.pi), 1e14 / (2 * np.pi))))
+    solver = wm.solver.B200FDTD(wm.compile_scene(sc, 10)).init_field()
+    assert lib.fdtd_engine_adjoint_init(solver.handle, None, 4) == -3
+    solver.close()
+    solver = wm.solver.B200FDTD(wm.compile_scene(_design_scene(wm, np.full((4, 4, 3), 2.0)), 10)).init_field()
+    bad = (ctypes.c_int * 18)(*([1, 5, 3, 6, 3, 6] + [0] * 12))  # reaches into the CPML slab
+    assert lib.fdtd_engine_adjoint_init(solver.handle, bad, 4) == -1
+    solver.close()

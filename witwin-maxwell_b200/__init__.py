@@ -5,6 +5,7 @@ Modules:
     solver      B200FDTD: the fused sm_100a step engine behind the FDTD solve contract
     backend     NativeFDTDModule-compatible per-op surface (camelCase kernel names)
     simulation  Simulation.fdtd(...).run() -> Result facade
+    adjoint     reverse-time adjoint: dL/deps_r of a design region (torch.autograd.Function)
     _lib        ctypes binding of libfdtd_b200.so (C ABI in include/fdtd_b200.h)
 """
 from . import scene, workloads
@@ -39,7 +40,7 @@ __version__ = "0.1.0"
 def __getattr__(name):
     # Lazily import the CUDA-backed modules so that scene compilation and the
     # library's symbol table can be used on machines without a GPU.
-    if name in ("solver", "backend", "simulation", "_lib"):
+    if name in ("solver", "backend", "simulation", "adjoint", "_lib"):
         import importlib
 
         return importlib.import_module(f".{name}", __name__)

@@ -1,0 +1,193 @@
+"""Reverse-time adjoint gradients of monitor objectives with respect to a
+design region's permittivity, on the fused engine.
+
+Restates the reference's differentiable run for this path
+(witwin/maxwell/fdtd/adjoint/bridge.py:957-1409 loop, core.py:379-383 stride,
+core.py:3527-3565 segment replay, checkpoint.py:365-568 checkpoints,
+material_pullback.py:266 pullback):
+
+1. forward: ``B200FDTD`` steps the scene and saves a full-state checkpoint
+   (E, H, CPML psi) at the start of every ``stride``-step segment;
+2. seeds: dL/d(monitor spectra) becomes dL/d(unscaled DFT accumulator);
+3. reverse: segments from last to first: restore the checkpoint, replay the
+   segment recording the design-box E history, run the adjoint steps
+   backward (``fdtd_engine_adjoint_range``), which accumulates dL/deps of the
+   Yee E components in the design boxes;
+4. pullback: dL/deps(Yee) -> dL/deps_r of the design cells (the scene
+   compiler averages node permittivities onto the components, eps = eps0 *
+   (node_a + node_b) / 2).
+
+``design_monitors`` wraps it as a ``torch.autograd.Function``: monitor
+spectra are differentiable functions of the design permittivity.
+"""
+from __future__ import annotations
+
+import ctypes
+import dataclasses
+
+import numpy as np
+import torch
+
+from . import _lib
+from .scene import EPSILON_0, MaterialRegion, Scene, compile_scene
+from .solver import B200FDTD
+
+
+def design_boxes(region: MaterialRegion, nodes) -> list[tuple[int, int, int, int, int, int] | None]:
+    """Yee-index boxes of Ex, Ey, Ez whose permittivity depends on the design
+    nodes [lo, hi): along a component's own axis a cell averages nodes i and
+    i + 1, so the box starts one cell lower."""
+    out = []
+    for c in range(3):
+        ext = [n - 1 if a == c else n for a, n in enumerate(nodes)]
+        box = []
+        for a in range(3):
+            lo = region.lo[a] - (1 if a == c else 0)
+            hi = region.hi[a]
+            box += [max(lo, 0), min(hi, ext[a])]
+        out.append(tuple(box))
+    return out
+
+
+def pullback(region: MaterialRegion, boxes, grads) -> np.ndarray:
+    """dL/deps_r of the design cells from dL/deps of the Yee components."""
+    shape = tuple(h - l for l, h in zip(region.lo, region.hi))
+    out = np.zeros(shape, dtype=np.float64)
+    for c, (box, g) in enumerate(zip(boxes, grads)):
+        g = np.asarray(g, dtype=np.float64) * (0.5 * EPSILON_0)
+        # node n of the design contributes to the cells n - e_c and n along axis c
+        for shift in (0, 1):
+            lo = [box[2 * a] for a in range(3)]
+            # cell index = node index - shift (along axis c only)
+            src = [slice(None)] * 3
+            dst = [slice(None)] * 3
+            for a in range(3):
+                node_lo = lo[a] + (shift if a == c else 0)
+                node_hi = box[2 * a + 1] + (shift if a == c else 0)
+                a0 = max(node_lo, region.lo[a])
+                a1 = min(node_hi, region.hi[a])
+                if a1 <= a0:
+                    break
+                src[a] = slice(a0 - node_lo, a1 - node_lo)
+                dst[a] = slice(a0 - region.lo[a], a1 - region.lo[a])
+            else:
+                out[tuple(dst)] += g[tuple(src)]
+    return out
+
+
+class DesignProblem:
+    """One scene with a design region; ``forward(eps_r)`` solves it and keeps
+    the checkpoints, ``backward(grad)`` returns dL/deps_r for the spectra
+    gradients ``grad`` ({monitor: {component: complex array like forward's}})."""
+
+    def __init__(self, scene: Scene, steps: int, stride: int = 100, device: str = "cuda"):
+        if not scene.material_regions:
+            raise ValueError("the scene has no MaterialRegion to differentiate")
+        self.scene = scene
+        self.steps = int(steps)
+        self.stride = max(1, min(int(stride), self.steps))
+        self.device = device
+        self.solver: B200FDTD | None = None
+        self.boxes = None
+        self.region = None
+
+    def _scene_with(self, eps_r: np.ndarray) -> Scene:
+        region = self.scene.material_regions[0]
+        new_region = MaterialRegion(region.lo, region.hi, np.asarray(eps_r, dtype=np.float64))
+        return dataclasses.replace(self.scene, material_regions=[new_region] + list(self.scene.material_regions[1:]))
+
+    def forward(self, eps_r: np.ndarray) -> dict:
+        if self.solver is not None:
+            self.solver.close()
+        scene = self._scene_with(eps_r)
+        cs = compile_scene(scene, self.steps)
+        self.region = cs.design
+        solver = B200FDTD(cs, device=self.device).init_field()
+        self.boxes = design_boxes(self.region, cs.nodes)
+        flat = [v for box in self.boxes for v in box]
+        _lib.check(solver.lib.fdtd_engine_adjoint_init(solver.handle, _lib.int_array(flat), self.stride),
+                   "adjoint_init")
+        for s0 in range(0, self.steps, self.stride):
+            solver.checkpoint_save(s0 // self.stride)
+            solver.step_range(s0, min(s0 + self.stride, self.steps))
+        self.solver = solver
+        return solver.monitor_results()
+
+    def _seeds(self, grad: dict) -> tuple[torch.Tensor, torch.Tensor]:
+        solver = self.solver
+        cs = solver.compiled
+        nf = len(cs.frequencies)
+        g_re = torch.zeros((nf, solver.n_samples), device=solver.device)
+        g_im = torch.zeros((nf, solver.n_samples), device=solver.device)
+        norm = float(np.sum(cs.window[: solver.steps_done]))
+        scale = 2.0 / norm if norm > 0 else 0.0
+        for reg, base in zip(cs.regions, solver.region_base):
+            g = grad.get(reg.monitor, {}).get(reg.component)
+            if g is None:
+                continue
+            g = torch.as_tensor(g).to(device=solver.device, dtype=torch.complex64)
+            b = reg.box
+            count = (b[1] - b[0]) * (b[3] - b[2]) * (b[5] - b[4])
+            fidx = [cs.frequencies.index(f) for f in cs.monitor_frequencies[reg.monitor]]
+            flat = g.reshape(len(fidx), count)
+            g_re[fidx, base:base + count] += scale * flat.real
+            g_im[fidx, base:base + count] += scale * flat.imag
+        return g_re, g_im
+
+    def backward(self, grad: dict) -> np.ndarray:
+        solver = self.solver
+        if solver is None:
+            raise RuntimeError("backward before forward")
+        lib, h = solver.lib, solver.handle
+        g_re, g_im = self._seeds(grad)
+        _lib.check(lib.fdtd_engine_adjoint_set_seed(h, _lib.ptr(g_re), _lib.ptr(g_im)), "adjoint_set_seed")
+        for s0 in reversed(range(0, self.steps, self.stride)):
+            s1 = min(s0 + self.stride, self.steps)
+            solver.checkpoint_load(s0 // self.stride)
+            _lib.check(lib.fdtd_engine_replay_range(h, s0, s1), "replay_range")
+            _lib.check(lib.fdtd_engine_adjoint_range(h, s1, s0), "adjoint_range")
+        grads = []
+        for c, box in enumerate(self.boxes):
+            shape = (box[1] - box[0], box[3] - box[2], box[5] - box[4])
+            out = torch.empty(shape, device=solver.device)
+            _lib.check(lib.fdtd_engine_adjoint_grad(h, c, _lib.ptr(out)), "adjoint_grad")
+            grads.append(out.cpu().numpy())
+        return pullback(self.region, self.boxes, grads)
+
+    def close(self):
+        if self.solver is not None:
+            self.solver.close()
+            self.solver = None
+
+
+class _DesignFunction(torch.autograd.Function):
+    @staticmethod
+    def forward(ctx, eps_r, problem, keys):
+        mons = problem.forward(eps_r.detach().cpu().numpy())
+        ctx.problem = problem
+        ctx.keys = keys
+        ctx.eps_shape = eps_r.shape
+        ctx.eps_device = eps_r.device
+        return tuple(mons[m][c].detach().clone() for m, c in keys)
+
+    @staticmethod
+    def backward(ctx, *grads):
+        grad: dict = {}
+        for (m, c), g in zip(ctx.keys, grads):
+            if g is not None:
+                grad.setdefault(m, {})[c] = g
+        g_eps = ctx.problem.backward(grad)
+        return torch.as_tensor(g_eps, dtype=torch.float32, device=ctx.eps_device).reshape(ctx.eps_shape), None, None
+
+
+def design_monitors(eps_r: torch.Tensor, problem: DesignProblem, keys) -> dict:
+    """Monitor spectra as differentiable functions of the design permittivity.
+
+    ``keys`` lists the (monitor, component) pairs to return; the result maps
+    monitor -> component -> complex tensor, as ``B200FDTD.monitor_results``."""
+    keys = tuple((str(m), str(c)) for m, c in keys)
+    outs = _DesignFunction.apply(eps_r, problem, keys)
+    result: dict = {}
+    for (m, c), t in zip(keys, outs):
+        result.setdefault(m, {})[c] = t
+    return result

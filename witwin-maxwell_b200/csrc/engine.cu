@@ -17,6 +17,7 @@
 #include "../../include/fdtd_b200.h"
 #include "engine.cuh"
 #include "tma_step.cuh"
+#include "adjoint.cuh"
 
 namespace fdtdb200 {
 template <bool kCpml, bool kCoef, bool kUniform, int kMinBlocks>
@@ -139,14 +140,6 @@ __global__ void dft_weight_kernel(int n_freq, int n_steps, const double* omega, 
   }
 }
 
-struct RegionFlush {
-  int64_t base;
-  int64_t count;
-  int is_h;
-  int comp;
-  int i0, j0, k0, nj, nk;
-};
-
 // Copy the monitor cells of every sample region from the current fields into
 // sample slot `slot` (one CTA column per region; observers.cu:7-78 sample the
 // same values: E^{n+1} and H^{n+1/2} after all corrections of the step).
@@ -236,6 +229,16 @@ struct Checkpoint {
   bool valid = false;
 };
 
+// Adjoint state (reverse-time pass): adjoint fields and CPML psi in the
+// forward layouts, monitor seeds, design boxes with their replayed E history.
+struct AdjointHost {
+  bool ready = false;
+  AdjParams q{};
+  std::vector<float*> bufs;  // everything allocated for the adjoint
+  int max_segment = 0;
+  int replay_n0 = -1, replay_n1 = -1;
+};
+
 struct fdtd_engine {
   fdtd_grid_desc desc{};
   cudaStream_t stream = nullptr;
@@ -304,6 +307,7 @@ struct fdtd_engine {
   float last_ms = 0.0f;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   std::vector<Checkpoint> checkpoints;
+  AdjointHost adj;
 };
 
 namespace {
@@ -736,6 +740,7 @@ int fdtd_engine_destroy(fdtd_engine* h) {
   for (int* p : h->index_bufs) cudaFree(p);
   cudaFree(h->d_flush);
   cudaFree(h->d_warp_class);
+  for (float* p : h->adj.bufs) cudaFree(p);
   cudaFree(h->d_status);
   cudaFree(h->samples);
   cudaFree(h->w_e);
@@ -1368,6 +1373,190 @@ int fdtd_engine_set_launch(fdtd_engine* h, int variant, int tile_rows, int chunk
   (void)tile_rows;  // the warp-granular kernel has no tile height
   h->variant = variant;
   if (chunk_planes > 0) h->CX = chunk_planes;
+  return 0;
+}
+
+// ---------------------------------------------------------------------------
+// Reverse-time adjoint (witwin/maxwell/fdtd/adjoint/native.py:48-725,
+// core.py:3527-3565 segment replay, checkpoint.py:365-568)
+// ---------------------------------------------------------------------------
+static int adj_alloc(fdtd_engine* h, float** out, size_t n) {
+  *out = nullptr;
+  if (n == 0) return 0;
+  CUDA_TRY(cudaMalloc(out, n * sizeof(float)));
+  CUDA_TRY(cudaMemsetAsync(*out, 0, n * sizeof(float), h->stream));
+  h->adj.bufs.push_back(*out);
+  return 0;
+}
+
+int fdtd_engine_adjoint_init(fdtd_engine* h, const int* design_boxes, int max_segment) {
+  if (!h || max_segment < 1) return fail(FDTD_ERR_INVALID_ARG, "bad adjoint arguments");
+  if (!h->finalized) return fail(FDTD_ERR_STATE, "engine not finalized");
+  if (!h->poles.empty()) return fail(FDTD_ERR_UNSUPPORTED, "the adjoint of dispersive (ADE) media is not supported");
+  if (h->adj.ready) return fail(FDTD_ERR_STATE, "adjoint already initialised");
+  AdjointHost& a = h->adj;
+  a.q = AdjParams{};
+  for (int c = 0; c < 3; ++c) {
+    int rc = adj_alloc(h, &a.q.gE[c], h->vol);
+    if (!rc) rc = adj_alloc(h, &a.q.gH[c], h->vol);
+    if (rc) return rc;
+    const int ax[2] = {axis_a(c), axis_b(c)};
+    for (int w = 0; w < 2; ++w) {
+      const size_t n = static_cast<size_t>(slab_elems(h, ax[w]));
+      rc = adj_alloc(h, &a.q.gpsiE[c][w], n);
+      if (!rc) rc = adj_alloc(h, &a.q.gpsiH[c][w], n);
+      if (rc) return rc;
+    }
+  }
+  a.q.n_samples = h->n_samples;
+  a.q.inv_dt = static_cast<float>(1.0 / static_cast<double>(static_cast<float>(h->desc.dt)));
+  a.max_segment = max_segment;
+  for (int c = 0; c < 3; ++c) {
+    DesignBox& d = a.q.design[c];
+    d = DesignBox{};
+    if (!design_boxes) continue;
+    const int* b = design_boxes + 6 * c;
+    if (b[0] >= b[1] || b[2] >= b[3] || b[4] >= b[5]) continue;
+    if (!box_ok(h, c, b)) return fail(FDTD_ERR_INVALID_ARG, "design box outside the component extent");
+    // The gradient formula needs plain interior updates: no CPML slab or edge.
+    for (int ax = 0; ax < 3; ++ax) {
+      const int n_ax = ax == 0 ? h->NX : (ax == 1 ? h->NY : h->NZ);
+      if (b[2 * ax] < h->desc.pml_lo[ax] || b[2 * ax + 1] > n_ax - 1 - h->desc.pml_hi[ax])
+        return fail(FDTD_ERR_INVALID_ARG, "design box reaches into a CPML slab or the domain edge");
+    }
+    for (int ax = 0; ax < 3; ++ax) {
+      d.lo[ax] = b[2 * ax];
+      d.hi[ax] = b[2 * ax + 1];
+    }
+    d.cells = static_cast<int64_t>(b[1] - b[0]) * (b[3] - b[2]) * (b[5] - b[4]);
+    int rc = adj_alloc(h, &d.hist, static_cast<size_t>(d.cells) * (max_segment + 1));
+    if (!rc) rc = adj_alloc(h, &d.grad, static_cast<size_t>(d.cells));
+    if (rc) return rc;
+  }
+  CUDA_TRY(cudaStreamSynchronize(h->stream));
+  a.ready = true;
+  return 0;
+}
+
+int fdtd_engine_adjoint_set_seed(fdtd_engine* h, const float* g_re, const float* g_im) {
+  if (!h || !h->adj.ready) return fail(FDTD_ERR_STATE, "adjoint not initialised");
+  AdjointHost& a = h->adj;
+  if (!g_re || !g_im) {
+    a.q.seed_re = nullptr;
+    a.q.seed_im = nullptr;
+    return 0;
+  }
+  if (h->n_samples == 0 || h->n_freq == 0) return fail(FDTD_ERR_STATE, "no monitor samples to seed");
+  const size_t n = static_cast<size_t>(h->n_freq) * h->n_samples;
+  if (!a.q.seed_re) {
+    float *re = nullptr, *im = nullptr;
+    int rc = adj_alloc(h, &re, n);
+    if (!rc) rc = adj_alloc(h, &im, n);
+    if (rc) return rc;
+    a.q.seed_re = re;
+    a.q.seed_im = im;
+  }
+  CUDA_TRY(cudaMemcpyAsync(const_cast<float*>(a.q.seed_re), g_re, n * sizeof(float), cudaMemcpyDefault, h->stream));
+  CUDA_TRY(cudaMemcpyAsync(const_cast<float*>(a.q.seed_im), g_im, n * sizeof(float), cudaMemcpyDefault, h->stream));
+  return 0;
+}
+
+int fdtd_engine_replay_range(fdtd_engine* h, int n0, int n1) {
+  if (!h || !h->adj.ready) return fail(FDTD_ERR_STATE, "adjoint not initialised");
+  if (n0 < 0 || n1 < n0 || n1 - n0 > h->adj.max_segment) return fail(FDTD_ERR_INVALID_ARG, "bad replay range");
+  for (const auto& t : h->terms)
+    if (t.signal && n1 > t.aux_len) return fail(FDTD_ERR_INVALID_ARG, "source signal table shorter than the range");
+  for (const auto& l : h->lines)
+    if (n1 > l.n_steps) return fail(FDTD_ERR_INVALID_ARG, "incident line history shorter than the range");
+  int rc = flush_samples(h);  // buffered forward samples belong to the forward run
+  if (rc) return rc;
+  StepParams p;
+  fill_params(h, p);
+  int err = launch_design_record(p, h->adj.q, 0, h->stream);
+  if (err) return cuda_fail(static_cast<cudaError_t>(err), "design record");
+  for (int n = n0; n < n1; ++n) {
+    rc = launch_step(h, n, -1);
+    if (rc) return rc;
+    fill_params(h, p);
+    err = launch_design_record(p, h->adj.q, n + 1 - n0, h->stream);
+    if (err) return cuda_fail(static_cast<cudaError_t>(err), "design record");
+  }
+  h->adj.replay_n0 = n0;
+  h->adj.replay_n1 = n1;
+  return check_status(h);
+}
+
+int fdtd_engine_adjoint_range(fdtd_engine* h, int n1, int n0) {
+  if (!h || !h->adj.ready) return fail(FDTD_ERR_STATE, "adjoint not initialised");
+  if (n0 < 0 || n1 < n0) return fail(FDTD_ERR_INVALID_ARG, "bad adjoint range");
+  AdjointHost& a = h->adj;
+  bool design = false;
+  for (int c = 0; c < 3; ++c) design = design || a.q.design[c].grad;
+  if (design && (n0 < a.replay_n0 || n1 > a.replay_n1))
+    return fail(FDTD_ERR_STATE, "adjoint range not covered by the last replay");
+  if (a.q.seed_re && n1 > h->dft_steps) return fail(FDTD_ERR_INVALID_ARG, "DFT weight table shorter than the range");
+  StepParams p;
+  fill_params(h, p);
+  for (int n = n1 - 1; n >= n0; --n) {
+    AdjParams q = a.q;
+    q.hist_slot = design ? n - a.replay_n0 : 0;
+    const int err = launch_adjoint_step(p, q, h->d_flush, q.seed_re ? h->n_flush : 0, h->w_e, h->w_h, h->n_freq, n,
+                                        h->stream);
+    if (err) return cuda_fail(static_cast<cudaError_t>(err), "adjoint step");
+  }
+  CUDA_TRY(cudaStreamSynchronize(h->stream));
+  return 0;
+}
+
+int fdtd_engine_adjoint_grad(fdtd_engine* h, int comp, float* out) {
+  if (!h || !h->adj.ready || comp < 0 || comp > 2 || !out) return fail(FDTD_ERR_INVALID_ARG, "bad gradient read");
+  const DesignBox& d = h->adj.q.design[comp];
+  if (!d.grad) return fail(FDTD_ERR_STATE, "no design box for this component");
+  CUDA_TRY(cudaMemcpyAsync(out, d.grad, sizeof(float) * d.cells, cudaMemcpyDefault, h->stream));
+  CUDA_TRY(cudaStreamSynchronize(h->stream));
+  return 0;
+}
+
+static int adj_geometry(fdtd_engine* h, int kind, int comp, int which, float** buf, int shape[3], int* py, int* pz) {
+  int ext[3];
+  comp_extent(comp, h->NX, h->NY, h->NZ, ext);
+  const int c = comp % 3;
+  if (kind == 0) {
+    *buf = comp < 3 ? h->adj.q.gE[c] : h->adj.q.gH[c];
+    for (int ax = 0; ax < 3; ++ax) shape[ax] = ext[ax];
+    *py = h->NY;
+    *pz = h->P;
+    return 1;
+  }
+  const int axis = which == 0 ? axis_a(c) : axis_b(c);
+  const int L = h->desc.pml_lo[axis] + h->desc.pml_hi[axis];
+  for (int ax = 0; ax < 3; ++ax) shape[ax] = ext[ax];
+  shape[axis] = L;
+  *buf = comp < 3 ? h->adj.q.gpsiE[c][which] : h->adj.q.gpsiH[c][which];
+  *py = axis == 1 ? L : h->NY;
+  *pz = axis == 2 ? L : h->P;
+  return L;
+}
+
+int fdtd_engine_adjoint_pack(fdtd_engine* h, int kind, int comp, int which, const float* src) {
+  if (!h || !h->adj.ready || kind < 0 || kind > 1 || comp < 0 || comp > 5 || which < 0 || which > 1 || !src)
+    return fail(FDTD_ERR_INVALID_ARG, "bad adjoint pack arguments");
+  float* buf;
+  int shape[3], py, pz;
+  if (adj_geometry(h, kind, comp, which, &buf, shape, &py, &pz) == 0) return 0;
+  pack_kernel<<<1024, 256, 0, h->stream>>>(buf, src, shape[0], shape[1], shape[2], py, pz);
+  CUDA_TRY(cudaGetLastError());
+  return 0;
+}
+
+int fdtd_engine_adjoint_unpack(fdtd_engine* h, int kind, int comp, int which, float* dst) {
+  if (!h || !h->adj.ready || kind < 0 || kind > 1 || comp < 0 || comp > 5 || which < 0 || which > 1 || !dst)
+    return fail(FDTD_ERR_INVALID_ARG, "bad adjoint unpack arguments");
+  float* buf;
+  int shape[3], py, pz;
+  if (adj_geometry(h, kind, comp, which, &buf, shape, &py, &pz) == 0) return 0;
+  unpack_kernel<<<1024, 256, 0, h->stream>>>(dst, buf, shape[0], shape[1], shape[2], py, pz);
+  CUDA_TRY(cudaGetLastError());
   return 0;
 }
 

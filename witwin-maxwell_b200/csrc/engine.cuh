@@ -38,6 +38,16 @@ struct PoleTerm {
   float* cur;            // box-dense current
 };
 
+// One monitor region in flush order: slots [base, base + count) of component
+// comp (0..5) over the box starting at (i0, j0, k0) with nj x nk cells per plane.
+struct RegionFlush {
+  int64_t base;
+  int64_t count;
+  int is_h;
+  int comp;
+  int i0, j0, k0, nj, nk;
+};
+
 // A box of one component whose values are written into the per-step sample
 // ring buffer that feeds the batched monitor DFT.
 struct SampleRegion {
