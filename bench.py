@@ -309,6 +309,8 @@ def run_b200_arm(args, wm, world, rank, local):
     # ---------------- end to end through the public API, host buffers ----------------
     if args.e2e:
         result["e2e"] = run_e2e(args, wm, cs, device, world)
+    if args.adjoint:
+        result["adjoint"] = run_adjoint_bench(wm, device)
     if rank == 0 and args.cpu_baseline:
         try:
             threads = os.cpu_count() or 1
@@ -322,6 +324,50 @@ def run_b200_arm(args, wm, world, rank, local):
             result["cpu_baseline"] = {"value": None, "unit": METRIC, "cores": os.cpu_count(), "kind": "port",
                                       "sample": f"failed: {exc}"}
     return result
+
+
+def run_adjoint_bench(wm, device):
+    """Forward + adjoint gradient of the 160x160x96 design workload (3000 steps)
+    against a plain forward solve of the same scene, device time on the engine's
+    stream.  Two history modes: "store" keeps the design-box E history of every
+    step in HBM (2.4 GB here, no replay); "replay" keeps a full-state checkpoint
+    every 100 steps and re-runs each segment during the backward pass."""
+    import torch
+
+    steps, stride = 3000, 100
+    scene = wm.workloads.adjoint_160(steps)
+    eps_r = scene.material_regions[0].eps_r
+    out = {
+        "workload": "adjoint_160: 160x160x96 cells, 10-cell CPML, 64x64x16 design block eps_r~U[1,12), "
+                    "300 THz ramped CW, |E|^2 over a 16x16 patch",
+        "steps": steps,
+        "design_cells": int(np.prod(eps_r.shape)),
+        "gradient_check": "tests/test_adjoint.py: exact transpose (dot-product test) and central finite differences",
+    }
+    cs = None
+    grads = {}
+    for mode in ("store", "replay"):
+        problem = wm.adjoint.DesignProblem(scene, steps, stride=stride, device=str(device), history=mode)
+        mons = problem.forward(eps_r)
+        g = problem.backward({"patch": {c: 2.0 * v for c, v in mons["patch"].items()}})
+        grads[mode] = g
+        out[mode] = {"forward_ms": problem.timings["forward_ms"], "backward_ms": problem.timings["backward_ms"]}
+        if mode == "replay":
+            out[mode]["checkpoint_stride"] = stride
+        cs = problem.solver.compiled
+        problem.close()
+        torch.cuda.empty_cache()
+    plain = wm.solver.B200FDTD(cs, device=device).init_field()
+    plain_ms = plain.step_range(0, steps)
+    plain.close()
+    torch.cuda.empty_cache()
+    out["forward_plain_ms"] = plain_ms
+    for mode in ("store", "replay"):
+        out[mode]["fwd_adj_over_fwd"] = (out[mode]["forward_ms"] + out[mode]["backward_ms"]) / plain_ms
+    out["fwd_adj_over_fwd"] = out["store"]["fwd_adj_over_fwd"]
+    den = float(np.abs(grads["replay"]).max())
+    out["store_vs_replay_max_rel_diff"] = float(np.abs(grads["store"] - grads["replay"]).max() / den) if den else 0.0
+    return out
 
 
 def run_e2e(args, wm, cs, device, world):
@@ -384,6 +430,8 @@ def main():
     ap.add_argument("--autotune", action="store_true")
     ap.add_argument("--no-cpu-baseline", dest="cpu_baseline", action="store_false")
     ap.add_argument("--no-e2e", dest="e2e", action="store_false")
+    ap.add_argument("--no-adjoint", dest="adjoint", action="store_false",
+                    help="skip the forward+adjoint timing of the 160x160x96 design workload")
     ap.add_argument("--cells", type=int, default=256,
                     help="cells per axis of the (scaled) workload; 256 is the benchmark, smaller sizes are for profiling")
     args = ap.parse_args()

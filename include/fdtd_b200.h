@@ -149,6 +149,9 @@ int fdtd_engine_flush(fdtd_engine* h);
 /* Checkpoints of the full time-stepping state (fields, psi, ADE state),
  * witwin/maxwell/fdtd/checkpoint.py:365-568. */
 int fdtd_engine_checkpoint_save(fdtd_engine* h, int slot);
+/* Allocate checkpoint slots [0, n_slots) now (one allocation per slot), so
+ * that later saves allocate nothing. */
+int fdtd_engine_checkpoint_reserve(fdtd_engine* h, int n_slots);
 int fdtd_engine_checkpoint_load(fdtd_engine* h, int slot);
 
 /* Tile shape selection: time the candidate (tile_rows, chunk_planes) pairs on
@@ -190,6 +193,10 @@ int fdtd_engine_adjoint_set_seed(fdtd_engine* h, const float* g_re, const float*
  * checkpoint first) without monitor sampling, recording the design-box E
  * history E^{n0} .. E^{n1}. */
 int fdtd_engine_replay_range(fdtd_engine* h, int n0, int n1);
+/* fdtd_engine_step_range with monitor sampling that also records the
+ * design-box E history E^{n0} .. E^{n1} (n1 - n0 <= max_segment), so that the
+ * reverse pass over [n0, n1) needs no replay: the whole history stays in HBM. */
+int fdtd_engine_step_range_recorded(fdtd_engine* h, int n0, int n1);
 /* Reverse steps n1-1 down to n0; with design boxes the last replay must cover
  * [n0, n1). */
 int fdtd_engine_adjoint_range(fdtd_engine* h, int n1, int n0);

@@ -125,7 +125,7 @@ def test_design_gradient_matches_finite_differences():
     steps = 320
     rng = np.random.default_rng(3)
     eps_r = 2.0 + 2.0 * rng.random((4, 4, 3))
-    problem = adj.DesignProblem(_design_scene(wm, eps_r), steps, stride=64)
+    problem = adj.DesignProblem(_design_scene(wm, eps_r), steps, stride=64, history="replay")
     mons = problem.forward(eps_r)
     grad_out = {"probe": {c: 2.0 * v for c, v in mons["probe"].items()}}  # d sum|X|^2 / dX* convention
     g = problem.backward(grad_out)
@@ -147,16 +147,17 @@ def test_design_gradient_matches_finite_differences():
 
 
 def test_design_gradient_through_autograd():
+    """torch.autograd over the stored-history path equals the checkpoint-replay path."""
     wm = load_package()
     adj = wm.adjoint
     steps = 200
     eps_r = np.full((4, 4, 3), 3.0)
-    problem = adj.DesignProblem(_design_scene(wm, eps_r), steps, stride=50)
+    problem = adj.DesignProblem(_design_scene(wm, eps_r), steps, history="store")
     t = torch.tensor(eps_r, dtype=torch.float32, requires_grad=True)
     mons = adj.design_monitors(t, problem, [("probe", c) for c in ("Ex", "Ey", "Ez", "Hx", "Hy", "Hz")])
     loss = sum((v.abs() ** 2).sum() for v in mons["probe"].values())
     loss.backward()
-    direct = adj.DesignProblem(_design_scene(wm, eps_r), steps, stride=steps)
+    direct = adj.DesignProblem(_design_scene(wm, eps_r), steps, stride=50, history="replay")
     m2 = direct.forward(eps_r)
     g2 = direct.backward({"probe": {c: 2.0 * v for c, v in m2["probe"].items()}})
     direct.close()

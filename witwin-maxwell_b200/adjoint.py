@@ -76,20 +76,34 @@ def pullback(region: MaterialRegion, boxes, grads) -> np.ndarray:
 
 
 class DesignProblem:
-    """One scene with a design region; ``forward(eps_r)`` solves it and keeps
-    the checkpoints, ``backward(grad)`` returns dL/deps_r for the spectra
-    gradients ``grad`` ({monitor: {component: complex array like forward's}})."""
+    """One scene with a design region; ``forward(eps_r)`` solves it,
+    ``backward(grad)`` returns dL/deps_r for the spectra gradients ``grad``
+    ({monitor: {component: complex array like forward's}}).
 
-    def __init__(self, scene: Scene, steps: int, stride: int = 100, device: str = "cuda"):
+    ``history`` chooses how the reverse pass gets the design-box E history:
+    "store" records all of it during the forward run (steps x design cells x 4
+    bytes of HBM, no replay), "replay" keeps a full-state checkpoint every
+    ``stride`` steps and re-runs each segment during the backward pass (the
+    reference's scheme, for histories too large to keep), "auto" stores when
+    the history fits in ``history_budget`` bytes."""
+
+    def __init__(self, scene: Scene, steps: int, stride: int = 100, device: str = "cuda", history: str = "auto",
+                 history_budget: int = 16 << 30):
         if not scene.material_regions:
             raise ValueError("the scene has no MaterialRegion to differentiate")
+        if history not in ("auto", "store", "replay"):
+            raise ValueError(f"history must be auto, store or replay, not {history!r}")
         self.scene = scene
         self.steps = int(steps)
         self.stride = max(1, min(int(stride), self.steps))
         self.device = device
+        self.history = history
+        self.history_budget = int(history_budget)
+        self.stored = False
         self.solver: B200FDTD | None = None
         self.boxes = None
         self.region = None
+        self.timings: dict = {}  # device ms of the last forward (with checkpoints) and backward
 
     def _scene_with(self, eps_r: np.ndarray) -> Scene:
         region = self.scene.material_regions[0]
@@ -105,11 +119,27 @@ class DesignProblem:
         solver = B200FDTD(cs, device=self.device).init_field()
         self.boxes = design_boxes(self.region, cs.nodes)
         flat = [v for box in self.boxes for v in box]
-        _lib.check(solver.lib.fdtd_engine_adjoint_init(solver.handle, _lib.int_array(flat), self.stride),
-                   "adjoint_init")
-        for s0 in range(0, self.steps, self.stride):
-            solver.checkpoint_save(s0 // self.stride)
-            solver.step_range(s0, min(s0 + self.stride, self.steps))
+        cells = sum((b[1] - b[0]) * (b[3] - b[2]) * (b[5] - b[4]) for b in self.boxes)
+        hist_bytes = 4 * cells * (self.steps + 1)
+        self.stored = self.history == "store" or (self.history == "auto" and hist_bytes <= self.history_budget)
+        lib, h = solver.lib, solver.handle
+        segment = self.steps if self.stored else self.stride
+        _lib.check(lib.fdtd_engine_adjoint_init(h, _lib.int_array(flat), segment), "adjoint_init")
+        if not self.stored:
+            n_slots = (self.steps + self.stride - 1) // self.stride
+            _lib.check(lib.fdtd_engine_checkpoint_reserve(h, n_slots), "checkpoint_reserve")
+        ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+        ev[0].record(solver.stream)
+        if self.stored:
+            _lib.check(lib.fdtd_engine_step_range_recorded(h, 0, self.steps), "step_range_recorded")
+            solver.steps_done = self.steps
+        else:
+            for s0 in range(0, self.steps, self.stride):
+                solver.checkpoint_save(s0 // self.stride)
+                solver.step_range(s0, min(s0 + self.stride, self.steps))
+        ev[1].record(solver.stream)
+        ev[1].synchronize()
+        self.timings = {"forward_ms": ev[0].elapsed_time(ev[1])}
         self.solver = solver
         return solver.monitor_results()
 
@@ -141,11 +171,19 @@ class DesignProblem:
         lib, h = solver.lib, solver.handle
         g_re, g_im = self._seeds(grad)
         _lib.check(lib.fdtd_engine_adjoint_set_seed(h, _lib.ptr(g_re), _lib.ptr(g_im)), "adjoint_set_seed")
-        for s0 in reversed(range(0, self.steps, self.stride)):
-            s1 = min(s0 + self.stride, self.steps)
-            solver.checkpoint_load(s0 // self.stride)
-            _lib.check(lib.fdtd_engine_replay_range(h, s0, s1), "replay_range")
-            _lib.check(lib.fdtd_engine_adjoint_range(h, s1, s0), "adjoint_range")
+        ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+        ev[0].record(solver.stream)
+        if self.stored:
+            _lib.check(lib.fdtd_engine_adjoint_range(h, self.steps, 0), "adjoint_range")
+        else:
+            for s0 in reversed(range(0, self.steps, self.stride)):
+                s1 = min(s0 + self.stride, self.steps)
+                solver.checkpoint_load(s0 // self.stride)
+                _lib.check(lib.fdtd_engine_replay_range(h, s0, s1), "replay_range")
+                _lib.check(lib.fdtd_engine_adjoint_range(h, s1, s0), "adjoint_range")
+        ev[1].record(solver.stream)
+        ev[1].synchronize()
+        self.timings["backward_ms"] = ev[0].elapsed_time(ev[1])
         grads = []
         for c, box in enumerate(self.boxes):
             shape = (box[1] - box[0], box[3] - box[2], box[5] - box[4])

@@ -224,8 +224,10 @@ struct AuxLine {
   float* h_hist = nullptr;
 };
 
+// A checkpoint slot: one allocation holding every state array back to back.
 struct Checkpoint {
-  std::vector<float*> bufs;
+  float* store = nullptr;
+  std::vector<float*> bufs;  // views into store, in state_buffers order
   bool valid = false;
 };
 
@@ -732,8 +734,7 @@ int fdtd_engine_destroy(fdtd_engine* h) {
     cudaFree(l.e_hist);
     cudaFree(l.h_hist);
   }
-  for (auto& ck : h->checkpoints)
-    for (float* p : ck.bufs) cudaFree(p);
+  for (auto& ck : h->checkpoints) cudaFree(ck.store);
   cudaFree(h->d_terms);
   cudaFree(h->d_poles);
   cudaFree(h->d_regions);
@@ -1192,7 +1193,17 @@ int fdtd_engine_finalize(fdtd_engine* h) {
   return 0;
 }
 
-int fdtd_engine_step_range(fdtd_engine* h, int n0, int n1) {
+static int step_range_impl(fdtd_engine* h, int n0, int n1, bool record);
+
+int fdtd_engine_step_range(fdtd_engine* h, int n0, int n1) { return step_range_impl(h, n0, n1, false); }
+
+int fdtd_engine_step_range_recorded(fdtd_engine* h, int n0, int n1) {
+  if (!h || !h->adj.ready) return fail(FDTD_ERR_STATE, "adjoint not initialised");
+  if (n0 < 0 || n1 < n0 || n1 - n0 > h->adj.max_segment) return fail(FDTD_ERR_INVALID_ARG, "bad recorded range");
+  return step_range_impl(h, n0, n1, true);
+}
+
+static int step_range_impl(fdtd_engine* h, int n0, int n1, bool record) {
   if (!h) return fail(FDTD_ERR_INVALID_ARG, "null engine");
   if (!h->finalized) return fail(FDTD_ERR_STATE, "engine not finalized");
   if (n1 < n0 || n0 < 0) return fail(FDTD_ERR_INVALID_ARG, "bad step range");
@@ -1205,6 +1216,12 @@ int fdtd_engine_step_range(fdtd_engine* h, int n0, int n1) {
   if (h->n_samples > 0 && h->n_freq > 0 && n1 > h->dft_steps)
     return fail(FDTD_ERR_INVALID_ARG, "DFT weight table shorter than the range");
   CUDA_TRY(cudaEventRecord(h->ev0, h->stream));
+  if (record) {
+    StepParams p;
+    fill_params(h, p);
+    const int err = launch_design_record(p, h->adj.q, 0, h->stream);
+    if (err) return cuda_fail(static_cast<cudaError_t>(err), "design record");
+  }
   for (int n = n0; n < n1; ++n) {
     if (h->pending == 0) h->pending_base = n;
     if (h->pending_base + h->pending != n) {
@@ -1214,6 +1231,12 @@ int fdtd_engine_step_range(fdtd_engine* h, int n0, int n1) {
     }
     int rc = launch_step(h, n, h->pending);
     if (rc) return rc;
+    if (record) {
+      StepParams p;
+      fill_params(h, p);
+      const int err = launch_design_record(p, h->adj.q, n + 1 - n0, h->stream);
+      if (err) return cuda_fail(static_cast<cudaError_t>(err), "design record");
+    }
     if (h->n_samples > 0) {
       ++h->pending;
       if (h->pending == h->M) {
@@ -1225,6 +1248,10 @@ int fdtd_engine_step_range(fdtd_engine* h, int n0, int n1) {
   CUDA_TRY(cudaEventRecord(h->ev1, h->stream));
   CUDA_TRY(cudaEventSynchronize(h->ev1));
   CUDA_TRY(cudaEventElapsedTime(&h->last_ms, h->ev0, h->ev1));
+  if (record) {
+    h->adj.replay_n0 = n0;
+    h->adj.replay_n1 = n1;
+  }
   return check_status(h);
 }
 
@@ -1265,17 +1292,42 @@ static void state_buffers(fdtd_engine* h, std::vector<std::pair<float*, size_t>>
   }
 }
 
+static int checkpoint_alloc(Checkpoint& ck, const std::vector<std::pair<float*, size_t>>& bufs) {
+  if (ck.store && ck.bufs.size() == bufs.size()) return 0;
+  cudaFree(ck.store);
+  ck.store = nullptr;
+  size_t total = 0;
+  for (const auto& b : bufs) total += (b.second + 63) / 64 * 64;  // 256-byte aligned views
+  CUDA_TRY(cudaMalloc(&ck.store, std::max<size_t>(total, 1) * sizeof(float)));
+  ck.bufs.clear();
+  size_t off = 0;
+  for (const auto& b : bufs) {
+    ck.bufs.push_back(ck.store + off);
+    off += (b.second + 63) / 64 * 64;
+  }
+  return 0;
+}
+
+int fdtd_engine_checkpoint_reserve(fdtd_engine* h, int n_slots) {
+  if (!h || n_slots < 0 || n_slots > 1 << 20) return fail(FDTD_ERR_INVALID_ARG, "bad checkpoint count");
+  if (static_cast<int>(h->checkpoints.size()) < n_slots) h->checkpoints.resize(n_slots);
+  std::vector<std::pair<float*, size_t>> bufs;
+  state_buffers(h, bufs);
+  for (int s = 0; s < n_slots; ++s) {
+    int rc = checkpoint_alloc(h->checkpoints[s], bufs);
+    if (rc) return rc;
+  }
+  return 0;
+}
+
 int fdtd_engine_checkpoint_save(fdtd_engine* h, int slot) {
   if (!h || slot < 0 || slot > 1 << 20) return fail(FDTD_ERR_INVALID_ARG, "bad checkpoint slot");
   if (static_cast<int>(h->checkpoints.size()) <= slot) h->checkpoints.resize(slot + 1);
   std::vector<std::pair<float*, size_t>> bufs;
   state_buffers(h, bufs);
   Checkpoint& ck = h->checkpoints[slot];
-  if (ck.bufs.size() != bufs.size()) {
-    for (float* p : ck.bufs) cudaFree(p);
-    ck.bufs.assign(bufs.size(), nullptr);
-    for (size_t x = 0; x < bufs.size(); ++x) CUDA_TRY(cudaMalloc(&ck.bufs[x], bufs[x].second * sizeof(float)));
-  }
+  int rc = checkpoint_alloc(ck, bufs);
+  if (rc) return rc;
   for (size_t x = 0; x < bufs.size(); ++x)
     CUDA_TRY(cudaMemcpyAsync(ck.bufs[x], bufs[x].first, bufs[x].second * sizeof(float), cudaMemcpyDeviceToDevice,
                              h->stream));
@@ -1338,7 +1390,7 @@ int fdtd_engine_autotune(fdtd_engine* h, int* tile_rows, int* chunk_planes) {
   h->variant = best_var;
   rc = fdtd_engine_checkpoint_load(h, slot);
   if (rc) return rc;
-  for (float* p : h->checkpoints[slot].bufs) cudaFree(p);
+  cudaFree(h->checkpoints[slot].store);
   h->checkpoints.pop_back();
   h->pending = 0;
   h->pending_base = next_step;
