@@ -42,26 +42,33 @@ def needs_rebuild() -> bool:
 
 
 def build(force: bool = False, verbose: bool = False, extra_flags: list[str] | None = None) -> Path:
+    """Compile every ``csrc/*.cu`` to an object (in parallel, one nvcc per
+    source) and link them into ``libfdtd_b200.so``."""
     if not force and not needs_rebuild():
         return LIB_PATH
-    cmd = [
-        _nvcc(),
-        *GENCODE,
-        "-O3",
-        "-lineinfo",
-        "-std=c++17",
-        "-Xcompiler",
-        "-fPIC",
-        "-shared",
-        "-o",
-        str(LIB_PATH) + ".tmp",
-        *[str(s) for s in sources()],
-    ]
-    if extra_flags:
-        cmd[1:1] = list(extra_flags)
-    if verbose:
-        print(" ".join(cmd), file=sys.stderr)
-    subprocess.run(cmd, check=True, cwd=str(PACKAGE_DIR))
+    import tempfile
+    from concurrent.futures import ThreadPoolExecutor
+
+    flags = [*GENCODE, "-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", *(extra_flags or [])]
+    with tempfile.TemporaryDirectory(prefix="fdtd_b200_build_") as tmp:
+        objs = []
+        cmds = []
+        for src in sources():
+            obj = Path(tmp) / (src.stem + ".o")
+            objs.append(obj)
+            cmds.append([_nvcc(), *flags, "-c", str(src), "-o", str(obj)])
+
+        def run(cmd: list[str]) -> None:
+            if verbose:
+                print(" ".join(cmd), file=sys.stderr)
+            subprocess.run(cmd, check=True, cwd=str(PACKAGE_DIR))
+
+        workers = max(1, min(len(cmds), os.cpu_count() or 1))
+        with ThreadPoolExecutor(max_workers=workers) as pool:
+            for fut in [pool.submit(run, c) for c in cmds]:
+                fut.result()
+        link = [_nvcc(), *GENCODE, "-shared", "-o", str(LIB_PATH) + ".tmp", *[str(o) for o in objs]]
+        run(link)
     os.replace(str(LIB_PATH) + ".tmp", LIB_PATH)
     return LIB_PATH
 

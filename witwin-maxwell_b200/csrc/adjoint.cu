@@ -59,7 +59,7 @@ __device__ __forceinline__ int64_t cell(const StepParams& p, int i, int j, int k
 
 // Slab offset of the psi element of axis `axis` at (i, j, k) with slab coordinate s.
 __device__ __forceinline__ int slab_off(const StepParams& p, int axis, int s, int i, int j, int k) {
-  return axis == 0 ? xslab_off(p, s, j, k) : (axis == 1 ? yslab_off(p, i, s, k) : zslab_off(p, i, j, s));
+  return axis == 0 ? xslab_off(p, s, j, k) : (axis == 1 ? yslab_off(p, i, s, k) : zslab_off(p, i, j, k));
 }
 
 __device__ __forceinline__ int coord(int axis, int i, int j, int k) { return axis == 0 ? i : (axis == 1 ? j : k); }

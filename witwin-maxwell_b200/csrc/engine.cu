@@ -22,6 +22,14 @@
 namespace fdtdb200 {
 template <bool kCpml, bool kCoef, bool kUniform, int kMinBlocks>
 __global__ void warp_step_kernel(const StepParams p, int n, int slot);
+int launch_classify_vec(const StepParams& p, int V, int n_kblocks, int n_chunks, unsigned char* out,
+                        cudaStream_t stream);
+using VecLauncher = int (*)(const StepParams&, int, dim3, bool, bool, bool, cudaStream_t);
+int launch_vec_v4(const StepParams&, int, dim3, bool, bool, bool, cudaStream_t);
+int launch_vec_v2(const StepParams&, int, dim3, bool, bool, bool, cudaStream_t);
+int launch_vec_r2d4(const StepParams&, int, dim3, bool, bool, bool, cudaStream_t);
+int launch_vec_r2d3(const StepParams&, int, dim3, bool, bool, bool, cudaStream_t);
+int launch_vec_r4d3(const StepParams&, int, dim3, bool, bool, bool, cudaStream_t);
 }
 
 using namespace fdtdb200;
@@ -67,7 +75,11 @@ void comp_extent(int comp, int NX, int NY, int NZ, int ext[3]) {
   }
 }
 
-__global__ void pack_kernel(float* dst, const float* src, int sx, int sy, int sz, int NY, int P) {
+// Dense [sx][sy][sz] <-> internal [.][NY][P] copies.  Inner coordinates
+// k >= zlo move by zshift (the high segment of a z-slab psi row); every other
+// array passes zlo = INT_MAX.
+__global__ void pack_kernel(float* dst, const float* src, int sx, int sy, int sz, int NY, int P, int zlo,
+                            int zshift) {
   const int64_t total = static_cast<int64_t>(sx) * sy * sz;
   for (int64_t x = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; x < total;
        x += static_cast<int64_t>(gridDim.x) * blockDim.x) {
@@ -75,11 +87,12 @@ __global__ void pack_kernel(float* dst, const float* src, int sx, int sy, int sz
     const int64_t r = x / sz;
     const int j = static_cast<int>(r % sy);
     const int i = static_cast<int>(r / sy);
-    dst[(static_cast<int64_t>(i) * NY + j) * P + k] = src[x];
+    dst[(static_cast<int64_t>(i) * NY + j) * P + (k < zlo ? k : k + zshift)] = src[x];
   }
 }
 
-__global__ void unpack_kernel(float* dst, const float* src, int sx, int sy, int sz, int NY, int P) {
+__global__ void unpack_kernel(float* dst, const float* src, int sx, int sy, int sz, int NY, int P, int zlo,
+                              int zshift) {
   const int64_t total = static_cast<int64_t>(sx) * sy * sz;
   for (int64_t x = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; x < total;
        x += static_cast<int64_t>(gridDim.x) * blockDim.x) {
@@ -87,9 +100,11 @@ __global__ void unpack_kernel(float* dst, const float* src, int sx, int sy, int 
     const int64_t r = x / sz;
     const int j = static_cast<int>(r % sy);
     const int i = static_cast<int>(r / sy);
-    dst[x] = src[(static_cast<int64_t>(i) * NY + j) * P + k];
+    dst[x] = src[(static_cast<int64_t>(i) * NY + j) * P + (k < zlo ? k : k + zshift)];
   }
 }
+
+constexpr int kNoRemap = 0x7fffffff;
 
 // Precompute the history of a 1-D incident line (one block, sequential in time).
 // Restates AuxiliaryGrid1D.advance_magnetic / advance_electric,
@@ -212,10 +227,39 @@ struct DevBuf {
   size_t n = 0;
 };
 
+constexpr int kDefaultVariant = 2;
+
+constexpr int kMaxVariant = 9;
+
+// z cells per lane of a launch variant (1 for the scalar kernels 1-4).
+int variant_v(int variant) {
+  switch (variant) {
+    case 5: case 9: return 4;
+    case 6: case 7: case 8: return 2;
+    default: return 1;
+  }
+}
+
+// Launcher of a z-vectorised variant (5: 4 cells per lane, direct loads;
+// 6: 2 cells, direct; 7 / 8: 2 cells, 4- / 3-plane cp.async ring; 9: 4 cells,
+// 3-plane ring).
+VecLauncher vec_launcher(int variant) {
+  switch (variant) {
+    case 5: return launch_vec_v4;
+    case 6: return launch_vec_v2;
+    case 7: return launch_vec_r2d4;
+    case 8: return launch_vec_r2d3;
+    case 9: return launch_vec_r4d3;
+    default: return nullptr;
+  }
+}
+
 struct PoleHost {
   PoleTerm t;
   float *drive = nullptr, *inv_eps = nullptr, *pol = nullptr, *cur = nullptr;
-  int64_t count = 0;
+  int64_t count = 0;  // cells of the box
+  int64_t rows = 0;   // (i, j) rows of the box
+  int nk = 0, nkk = 0, koff = 0;  // z cells, padded z pitch, offset of k0 in a padded row
 };
 
 struct AuxLine {
@@ -245,11 +289,13 @@ struct fdtd_engine {
   fdtd_grid_desc desc{};
   cudaStream_t stream = nullptr;
   int NX = 0, NY = 0, NZ = 0, P = 0, SZ = 0;
+  int zlo4 = 0, zhs4 = 0;  // z-slab psi row segments (StepParams::zlo4 / zhs4)
   int64_t plane = 0, vol = 0;
   int TY = 0, CX = 0;
   // Fused kernel: 1..3 = register-prefetch warp kernel with a register budget
-  // of up to 128 / 64 / 85 per thread; 4 = TMA-fed kernel.
-  int variant = 2;
+  // of up to 128 / 64 / 85 per thread; 4 = TMA-fed kernel; 5..9 = z-vectorised
+  // warp kernels (vec_launcher).
+  int variant = kDefaultVariant;
   int cur = 0;  // index of the buffer holding the current state
   float* E[2][3] = {};
   float* H[2][3] = {};
@@ -290,7 +336,7 @@ struct fdtd_engine {
   TmaMaps maps[2] = {};                    // tensor maps of E[cur], H[cur] for cur = 0, 1
   bool tma_ready = false;
   int* d_status = nullptr;                 // timeout flag written by bounded waits
-  int class_cx = 0;                       // chunk length the table was built for (0 = stale)
+  int class_key = 0;                      // (chunk length, lane width) the table was built for (0 = stale)
   std::vector<int*> index_bufs;
   RegionFlush* d_flush = nullptr;
   int n_flush = 0;
@@ -337,7 +383,7 @@ int64_t slab_elems(const fdtd_engine* h, int axis) {
   if (L == 0) return 0;
   if (axis == 0) return static_cast<int64_t>(L) * h->NY * h->P;
   if (axis == 1) return static_cast<int64_t>(h->NX) * L * h->P;
-  return static_cast<int64_t>(h->NX) * h->NY * L;
+  return static_cast<int64_t>(h->NX) * h->NY * h->SZ;
 }
 
 bool box_ok(const fdtd_engine* h, int comp, const int* box) {
@@ -401,6 +447,8 @@ void fill_params(const fdtd_engine* h, StepParams& p) {
   p.NZ = h->NZ;
   p.P = h->P;
   p.SZ = h->SZ;
+  p.zlo4 = h->zlo4;
+  p.zhs4 = h->zhs4;
   p.TY = h->TY;
   p.CX = h->CX;
   p.Q = h->P / 4;
@@ -462,9 +510,23 @@ void fill_params(const fdtd_engine* h, StepParams& p) {
 constexpr int kWarpRows = 8;   // warps (y rows) per CTA of the step kernel
 constexpr int kWarpOut = 30;   // z cells produced per warp
 
+int z_blocks(const fdtd_engine* h) {
+  const int V = variant_v(h->variant);
+  const int span = V == 1 ? kWarpOut : 31 * V;
+  return (h->NZ + span - 1) / span;
+}
+
 void default_tiles(fdtd_engine* h) {
   h->TY = 1;
   int CX = h->desc.chunk_planes;
+  if (CX <= 0 && variant_v(h->variant) > 1) {
+    // Vectorised kernel (one or two 256-thread CTAs per SM): about six waves
+    // of warps, chunks of at least eight planes.
+    const int64_t cols = static_cast<int64_t>((h->NY + kWarpRows - 1) / kWarpRows) * z_blocks(h);
+    const int per_sm = variant_v(h->variant) == 4 ? 1 : 2;  // CTAs per SM (registers / ring)
+    const int64_t want_chunks = std::max<int64_t>(1, (148 * per_sm * 6 + cols - 1) / cols);
+    CX = static_cast<int>(std::max<int64_t>(8, (h->NX + want_chunks - 1) / want_chunks));
+  }
   if (CX <= 0) {
     // Split x into chunks until the grid holds about ten waves of the
     // 64-register variant (four 256-thread CTAs per SM on 148 SMs).  Shorter
@@ -478,7 +540,7 @@ void default_tiles(fdtd_engine* h) {
 }
 
 dim3 step_grid(const fdtd_engine* h) {
-  return dim3((h->NY + kWarpRows - 1) / kWarpRows, (h->NZ + kWarpOut - 1) / kWarpOut, (h->NX + h->CX - 1) / h->CX);
+  return dim3((h->NY + kWarpRows - 1) / kWarpRows, z_blocks(h), (h->NX + h->CX - 1) / h->CX);
 }
 
 // Read (and clear) the device status word after the stream has drained.
@@ -502,11 +564,19 @@ int launch_step(fdtd_engine* h, int n, int slot) {
   const int block = kWarpRows * 32;
   if (h->variant == 4 && !h->tma_ready)
     return fail(FDTD_ERR_UNSUPPORTED, "TMA step kernel unavailable (no tensor-map driver entry point)");
-  if ((h->cpml || coef) && h->class_cx != h->CX) {
-    const int err = launch_classify(p, static_cast<int>(grid.y), static_cast<int>(grid.z), h->d_warp_class, h->stream);
+  const int V = variant_v(h->variant);
+  const int key = h->CX * 8 + V;
+  if ((h->cpml || coef) && h->class_key != key) {
+    const int err = V == 1 ? launch_classify(p, static_cast<int>(grid.y), static_cast<int>(grid.z), h->d_warp_class, h->stream)
+                           : launch_classify_vec(p, V, static_cast<int>(grid.y), static_cast<int>(grid.z), h->d_warp_class,
+                                                 h->stream);
     if (err != 0) return cuda_fail(static_cast<cudaError_t>(err), "classify_kernel launch");
-    h->class_cx = h->CX;
+    h->class_key = key;
   }
+  if (VecLauncher vl = vec_launcher(h->variant)) {
+    const int err = vl(p, n, grid, h->cpml, coef, h->uniform_grid, h->stream);
+    if (err != 0) return cuda_fail(static_cast<cudaError_t>(err), "vec_step_kernel launch");
+  } else {
 #define FDTD_LAUNCH(CPML, COEF, UNI)                                                                  \
   do {                                                                                           \
     if (h->variant == 4)                                                                          \
@@ -533,6 +603,7 @@ int launch_step(fdtd_engine* h, int n, int slot) {
     }
   }
 #undef FDTD_LAUNCH
+  }
   cudaError_t err = cudaGetLastError();
   if (err != cudaSuccess) return cuda_fail(err, "warp_step_kernel launch");
   ++h->launches;
@@ -680,7 +751,17 @@ int fdtd_engine_create(const fdtd_grid_desc* desc, void* stream, fdtd_engine** o
   h->NY = desc->ny;
   h->NZ = desc->nz;
   h->P = (desc->nz + 3) / 4 * 4;
-  h->SZ = desc->pml_lo[2] + desc->pml_hi[2];
+  {
+    // z-slab psi rows: low slab at [0, zlo4), high slab cells k >= zhs4 at
+    // zlo4 + k - zhs4, with zlo4 = lo rounded up and zhs4 = the first high-slab
+    // cell of any component rounded down to multiples of four.  When the two
+    // segments would overlap the rows are kept whole (zlo4 = zhs4 = P).
+    const int lo = desc->pml_lo[2], hi = desc->pml_hi[2];
+    h->zlo4 = (lo + 3) / 4 * 4;
+    h->zhs4 = (desc->nz - 1 - hi) / 4 * 4;
+    if (h->zhs4 < h->zlo4) h->zlo4 = h->zhs4 = h->P;
+    h->SZ = (lo + hi > 0) ? h->zlo4 + (h->P - h->zhs4) : 0;
+  }
   h->plane = static_cast<int64_t>(h->NY) * h->P;
   h->vol = h->plane * h->NX;
   h->M = desc->sample_block > 0 ? std::min(desc->sample_block, 64) : 32;
@@ -794,7 +875,7 @@ int fdtd_engine_set_coefficients(fdtd_engine* h, int comp, const float* decay, f
     }
     int rc = dev_alloc(h, &h->ecoef[comp][w], h->vol);
     if (rc) return rc;
-    pack_kernel<<<1024, 256, 0, h->stream>>>(h->ecoef[comp][w], src[w], ext[0], ext[1], ext[2], h->NY, h->P);
+    pack_kernel<<<1024, 256, 0, h->stream>>>(h->ecoef[comp][w], src[w], ext[0], ext[1], ext[2], h->NY, h->P, kNoRemap, 0);
     CUDA_TRY(cudaGetLastError());
   }
   return 0;
@@ -805,7 +886,7 @@ int fdtd_engine_pack_field(fdtd_engine* h, int comp, const float* src) {
   int ext[3];
   comp_extent(comp, h->NX, h->NY, h->NZ, ext);
   float* dst = comp < 3 ? h->E[h->cur][comp] : h->H[h->cur][comp - 3];
-  pack_kernel<<<1024, 256, 0, h->stream>>>(dst, src, ext[0], ext[1], ext[2], h->NY, h->P);
+  pack_kernel<<<1024, 256, 0, h->stream>>>(dst, src, ext[0], ext[1], ext[2], h->NY, h->P, kNoRemap, 0);
   CUDA_TRY(cudaGetLastError());
   return 0;
 }
@@ -815,13 +896,21 @@ int fdtd_engine_unpack_field(fdtd_engine* h, int comp, float* dst) {
   int ext[3];
   comp_extent(comp, h->NX, h->NY, h->NZ, ext);
   const float* src = comp < 3 ? h->E[h->cur][comp] : h->H[h->cur][comp - 3];
-  unpack_kernel<<<1024, 256, 0, h->stream>>>(dst, src, ext[0], ext[1], ext[2], h->NY, h->P);
+  unpack_kernel<<<1024, 256, 0, h->stream>>>(dst, src, ext[0], ext[1], ext[2], h->NY, h->P, kNoRemap, 0);
   CUDA_TRY(cudaGetLastError());
   return 0;
 }
 
+// Inner-coordinate remap of a z-slab psi array of a component with z extent
+// `ext_z`: slab coordinate s >= zlo (the high slab) sits at s + zshift.
+static void zslab_remap(const fdtd_engine* h, int ext_z, int* zlo, int* zshift) {
+  const int lo = h->desc.pml_lo[2], hi = h->desc.pml_hi[2];
+  *zlo = lo;
+  *zshift = h->zlo4 - lo + (ext_z - hi) - h->zhs4;
+}
+
 static int psi_geometry(fdtd_engine* h, int comp, int which, float** buf, int shape[3], int* pitch_y,
-                        int* pitch_z) {
+                        int* pitch_z, int* zlo, int* zshift) {
   const int c = comp % 3;
   const int axis = which == 0 ? axis_a(c) : axis_b(c);
   int ext[3];
@@ -832,9 +921,12 @@ static int psi_geometry(fdtd_engine* h, int comp, int which, float** buf, int sh
   shape[2] = ext[2];
   shape[axis] = L;
   *buf = comp < 3 ? h->psiE[c][which] : h->psiH[h->cur][c][which];
-  // internal pitches: x slab [L][NY][P], y slab [NX][L][P], z slab [NX][NY][L]
+  // internal pitches: x slab [L][NY][P], y slab [NX][L][P], z slab [NX][NY][SZ]
   *pitch_y = axis == 1 ? L : h->NY;
-  *pitch_z = axis == 2 ? L : h->P;
+  *pitch_z = axis == 2 ? h->SZ : h->P;
+  *zlo = kNoRemap;
+  *zshift = 0;
+  if (axis == 2) zslab_remap(h, ext[2], zlo, zshift);
   return L;
 }
 
@@ -842,9 +934,9 @@ int fdtd_engine_pack_psi(fdtd_engine* h, int comp, int which, const float* src) 
   if (!h || comp < 0 || comp > 5 || which < 0 || which > 1 || !src)
     return fail(FDTD_ERR_INVALID_ARG, "bad psi pack arguments");
   float* buf;
-  int shape[3], py, pz;
-  if (psi_geometry(h, comp, which, &buf, shape, &py, &pz) == 0) return 0;
-  pack_kernel<<<1024, 256, 0, h->stream>>>(buf, src, shape[0], shape[1], shape[2], py, pz);
+  int shape[3], py, pz, zlo, zshift;
+  if (psi_geometry(h, comp, which, &buf, shape, &py, &pz, &zlo, &zshift) == 0) return 0;
+  pack_kernel<<<1024, 256, 0, h->stream>>>(buf, src, shape[0], shape[1], shape[2], py, pz, zlo, zshift);
   CUDA_TRY(cudaGetLastError());
   return 0;
 }
@@ -853,9 +945,9 @@ int fdtd_engine_unpack_psi(fdtd_engine* h, int comp, int which, float* dst) {
   if (!h || comp < 0 || comp > 5 || which < 0 || which > 1 || !dst)
     return fail(FDTD_ERR_INVALID_ARG, "bad psi unpack arguments");
   float* buf;
-  int shape[3], py, pz;
-  if (psi_geometry(h, comp, which, &buf, shape, &py, &pz) == 0) return 0;
-  unpack_kernel<<<1024, 256, 0, h->stream>>>(dst, buf, shape[0], shape[1], shape[2], py, pz);
+  int shape[3], py, pz, zlo, zshift;
+  if (psi_geometry(h, comp, which, &buf, shape, &py, &pz, &zlo, &zshift) == 0) return 0;
+  unpack_kernel<<<1024, 256, 0, h->stream>>>(dst, buf, shape[0], shape[1], shape[2], py, pz, zlo, zshift);
   CUDA_TRY(cudaGetLastError());
   return 0;
 }
@@ -867,15 +959,30 @@ int fdtd_engine_add_pole(fdtd_engine* h, int comp, int kind, const int* box, con
   if (h->finalized) return fail(FDTD_ERR_STATE, "engine already finalized");
   if (!box_ok(h, comp, box)) return fail(FDTD_ERR_INVALID_ARG, "pole box outside the component extent");
   PoleHost ph;
-  ph.count = static_cast<int64_t>(box[1] - box[0]) * (box[3] - box[2]) * (box[5] - box[4]);
-  CUDA_TRY(cudaMalloc(&ph.drive, ph.count * sizeof(float)));
-  CUDA_TRY(cudaMalloc(&ph.inv_eps, ph.count * sizeof(float)));
-  CUDA_TRY(cudaMalloc(&ph.pol, ph.count * sizeof(float)));
-  CUDA_TRY(cudaMalloc(&ph.cur, ph.count * sizeof(float)));
-  CUDA_TRY(cudaMemcpyAsync(ph.drive, drive, ph.count * sizeof(float), cudaMemcpyDefault, h->stream));
-  CUDA_TRY(cudaMemcpyAsync(ph.inv_eps, inv_eps, ph.count * sizeof(float), cudaMemcpyDefault, h->stream));
-  CUDA_TRY(cudaMemsetAsync(ph.pol, 0, ph.count * sizeof(float), h->stream));
-  CUDA_TRY(cudaMemsetAsync(ph.cur, 0, ph.count * sizeof(float), h->stream));
+  // Stored with the z range padded to multiples of four (zero drive and 1/eps
+  // in the padding) so the vectorised step kernel reads whole lane groups.
+  const int nk = box[5] - box[4];
+  const int kk0 = box[4] & ~3, kk1 = (box[5] + 3) & ~3;
+  const int nkk = kk1 - kk0;
+  const int64_t rows = static_cast<int64_t>(box[1] - box[0]) * (box[3] - box[2]);
+  ph.count = rows * nk;
+  ph.rows = rows;
+  ph.nk = nk;
+  ph.nkk = nkk;
+  ph.koff = box[4] - kk0;
+  const size_t bytes = static_cast<size_t>(rows) * nkk * sizeof(float);
+  CUDA_TRY(cudaMalloc(&ph.drive, bytes));
+  CUDA_TRY(cudaMalloc(&ph.inv_eps, bytes));
+  CUDA_TRY(cudaMalloc(&ph.pol, bytes));
+  CUDA_TRY(cudaMalloc(&ph.cur, bytes));
+  CUDA_TRY(cudaMemsetAsync(ph.drive, 0, bytes, h->stream));
+  CUDA_TRY(cudaMemsetAsync(ph.inv_eps, 0, bytes, h->stream));
+  CUDA_TRY(cudaMemsetAsync(ph.pol, 0, bytes, h->stream));
+  CUDA_TRY(cudaMemsetAsync(ph.cur, 0, bytes, h->stream));
+  CUDA_TRY(cudaMemcpy2DAsync(ph.drive + ph.koff, nkk * sizeof(float), drive, nk * sizeof(float), nk * sizeof(float),
+                             rows, cudaMemcpyDefault, h->stream));
+  CUDA_TRY(cudaMemcpy2DAsync(ph.inv_eps + ph.koff, nkk * sizeof(float), inv_eps, nk * sizeof(float),
+                             nk * sizeof(float), rows, cudaMemcpyDefault, h->stream));
   PoleTerm& t = ph.t;
   t.comp = comp;
   t.kind = kind;
@@ -885,6 +992,8 @@ int fdtd_engine_add_pole(fdtd_engine* h, int comp, int kind, const int* box, con
   t.j1 = box[3];
   t.k0 = box[4];
   t.k1 = box[5];
+  t.kk0 = kk0;
+  t.nkk = nkk;
   t.decay = decay;
   t.restoring = restoring;
   t.dt = static_cast<float>(h->desc.dt);
@@ -902,8 +1011,11 @@ int fdtd_engine_pole_state(fdtd_engine* h, int pole_id, float* pol_out, float* c
   if (!h || pole_id < 0 || pole_id >= static_cast<int>(h->poles.size()))
     return fail(FDTD_ERR_INVALID_ARG, "bad pole id");
   const PoleHost& ph = h->poles[pole_id];
-  if (pol_out) CUDA_TRY(cudaMemcpyAsync(pol_out, ph.pol, ph.count * sizeof(float), cudaMemcpyDefault, h->stream));
-  if (cur_out) CUDA_TRY(cudaMemcpyAsync(cur_out, ph.cur, ph.count * sizeof(float), cudaMemcpyDefault, h->stream));
+  const size_t w = ph.nk * sizeof(float), pitch = ph.nkk * sizeof(float);
+  if (pol_out)
+    CUDA_TRY(cudaMemcpy2DAsync(pol_out, w, ph.pol + ph.koff, pitch, w, ph.rows, cudaMemcpyDefault, h->stream));
+  if (cur_out)
+    CUDA_TRY(cudaMemcpy2DAsync(cur_out, w, ph.cur + ph.koff, pitch, w, ph.rows, cudaMemcpyDefault, h->stream));
   return 0;
 }
 
@@ -1172,7 +1284,7 @@ int fdtd_engine_finalize(fdtd_engine* h) {
   {
     const int64_t kblocks = (h->NZ + kWarpOut - 1) / kWarpOut;
     CUDA_TRY(cudaMalloc(&h->d_warp_class, static_cast<size_t>(h->NX) * kblocks * h->NY));
-    h->class_cx = 0;
+    h->class_key = 0;
     CUDA_TRY(cudaMalloc(&h->d_status, sizeof(int)));
     CUDA_TRY(cudaMemsetAsync(h->d_status, 0, sizeof(int), h->stream));
   }
@@ -1287,8 +1399,8 @@ static void state_buffers(fdtd_engine* h, std::vector<std::pair<float*, size_t>>
     }
   }
   for (auto& ph : h->poles) {
-    out.push_back({ph.pol, static_cast<size_t>(ph.count)});
-    out.push_back({ph.cur, static_cast<size_t>(ph.count)});
+    out.push_back({ph.pol, static_cast<size_t>(ph.rows * ph.nkk)});
+    out.push_back({ph.cur, static_cast<size_t>(ph.rows * ph.nkk)});
   }
 }
 
@@ -1357,11 +1469,11 @@ int fdtd_engine_autotune(fdtd_engine* h, int* tile_rows, int* chunk_planes) {
   const int slot = static_cast<int>(h->checkpoints.size());
   rc = fdtd_engine_checkpoint_save(h, slot);
   if (rc) return rc;
-  const int cxs[] = {4, 6, 8, 12, 16, 24, 32};
+  const int cxs[] = {4, 6, 8, 12, 16, 24, 32, 48};
   float best = 1e30f;
   int best_ty = 1, best_cx = h->CX, best_var = h->variant;
-  const int last_var = h->tma_ready ? 4 : 3;
-  for (int var = 1; var <= last_var; ++var) {
+  for (int var = 1; var <= kMaxVariant; ++var) {
+    if (var == 4 && !h->tma_ready) continue;
     for (int cx : cxs) {
       if (cx > 2 * h->NX) continue;
       h->variant = var;
@@ -1420,11 +1532,12 @@ int fdtd_engine_time_kernel(fdtd_engine* h, int n, int reps, float* ms) {
 }
 
 int fdtd_engine_set_launch(fdtd_engine* h, int variant, int tile_rows, int chunk_planes) {
-  if (!h || variant < 1 || variant > 4 || tile_rows < 0 || chunk_planes < 0)
+  if (!h || variant < 1 || variant > kMaxVariant || tile_rows < 0 || chunk_planes < 0)
     return fail(FDTD_ERR_INVALID_ARG, "bad launch configuration");
-  (void)tile_rows;  // the warp-granular kernel has no tile height
+  (void)tile_rows;  // the warp-granular kernels have no tile height
   h->variant = variant;
   if (chunk_planes > 0) h->CX = chunk_planes;
+  else default_tiles(h);
   return 0;
 }
 
@@ -1569,10 +1682,13 @@ int fdtd_engine_adjoint_grad(fdtd_engine* h, int comp, float* out) {
   return 0;
 }
 
-static int adj_geometry(fdtd_engine* h, int kind, int comp, int which, float** buf, int shape[3], int* py, int* pz) {
+static int adj_geometry(fdtd_engine* h, int kind, int comp, int which, float** buf, int shape[3], int* py, int* pz,
+                        int* zlo, int* zshift) {
   int ext[3];
   comp_extent(comp, h->NX, h->NY, h->NZ, ext);
   const int c = comp % 3;
+  *zlo = kNoRemap;
+  *zshift = 0;
   if (kind == 0) {
     *buf = comp < 3 ? h->adj.q.gE[c] : h->adj.q.gH[c];
     for (int ax = 0; ax < 3; ++ax) shape[ax] = ext[ax];
@@ -1586,7 +1702,8 @@ static int adj_geometry(fdtd_engine* h, int kind, int comp, int which, float** b
   shape[axis] = L;
   *buf = comp < 3 ? h->adj.q.gpsiE[c][which] : h->adj.q.gpsiH[c][which];
   *py = axis == 1 ? L : h->NY;
-  *pz = axis == 2 ? L : h->P;
+  *pz = axis == 2 ? h->SZ : h->P;
+  if (axis == 2) zslab_remap(h, ext[2], zlo, zshift);
   return L;
 }
 
@@ -1595,8 +1712,9 @@ int fdtd_engine_adjoint_pack(fdtd_engine* h, int kind, int comp, int which, cons
     return fail(FDTD_ERR_INVALID_ARG, "bad adjoint pack arguments");
   float* buf;
   int shape[3], py, pz;
-  if (adj_geometry(h, kind, comp, which, &buf, shape, &py, &pz) == 0) return 0;
-  pack_kernel<<<1024, 256, 0, h->stream>>>(buf, src, shape[0], shape[1], shape[2], py, pz);
+  int zlo, zshift;
+  if (adj_geometry(h, kind, comp, which, &buf, shape, &py, &pz, &zlo, &zshift) == 0) return 0;
+  pack_kernel<<<1024, 256, 0, h->stream>>>(buf, src, shape[0], shape[1], shape[2], py, pz, zlo, zshift);
   CUDA_TRY(cudaGetLastError());
   return 0;
 }
@@ -1606,8 +1724,9 @@ int fdtd_engine_adjoint_unpack(fdtd_engine* h, int kind, int comp, int which, fl
     return fail(FDTD_ERR_INVALID_ARG, "bad adjoint unpack arguments");
   float* buf;
   int shape[3], py, pz;
-  if (adj_geometry(h, kind, comp, which, &buf, shape, &py, &pz) == 0) return 0;
-  unpack_kernel<<<1024, 256, 0, h->stream>>>(dst, buf, shape[0], shape[1], shape[2], py, pz);
+  int zlo, zshift;
+  if (adj_geometry(h, kind, comp, which, &buf, shape, &py, &pz, &zlo, &zshift) == 0) return 0;
+  unpack_kernel<<<1024, 256, 0, h->stream>>>(dst, buf, shape[0], shape[1], shape[2], py, pz, zlo, zshift);
   CUDA_TRY(cudaGetLastError());
   return 0;
 }

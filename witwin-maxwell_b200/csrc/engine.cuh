@@ -31,11 +31,15 @@ struct PoleTerm {
   int comp;  // 0..2
   int kind;  // 0 Debye, 1 Drude, 2 Lorentz
   int i0, i1, j0, j1, k0, k1;
+  // z range of the stored arrays: [kk0, kk0 + nkk) with kk0 = k0 rounded down
+  // and kk0 + nkk = k1 rounded up to multiples of four; the padding cells have
+  // zero drive and zero 1/eps, so their state stays zero.
+  int kk0, nkk;
   float decay, restoring, dt, inv_dt;
-  const float* drive;    // box-dense
-  const float* inv_eps;  // box-dense (1/eps of the component, absolute)
-  float* pol;            // box-dense polarisation (Debye, Lorentz)
-  float* cur;            // box-dense current
+  const float* drive;    // [i1-i0][j1-j0][nkk]
+  const float* inv_eps;  // same layout (1/eps of the component, absolute)
+  float* pol;            // same layout: polarisation (Debye, Lorentz)
+  float* cur;            // same layout: current
 };
 
 // One monitor region in flush order: slots [base, base + count) of component
@@ -87,6 +91,10 @@ struct StepParams {
   const float* hc[3];
   const float* hik[3];
   int slab_lo[3], slab_hi[3];
+  // z-slab psi rows hold the low slab at [0, zlo4) and the high slab cells
+  // k >= zhs4 at zlo4 + k - zhs4 (both segment starts multiples of four, so a
+  // vector lane group maps to contiguous aligned storage); row length SZ.
+  int zlo4, zhs4;
   float* psiE[3][2];
   const float* psiHin[3][2];
   float* psiHout[3][2];

@@ -46,7 +46,10 @@ __device__ __forceinline__ int xslab_off(const StepParams& p, int lx, int j, int
 __device__ __forceinline__ int yslab_off(const StepParams& p, int i, int ly, int k) {
   return (i * (p.slab_lo[1] + p.slab_hi[1]) + ly) * p.P + k;
 }
-__device__ __forceinline__ int zslab_off(const StepParams& p, int i, int j, int lz) { return (i * p.NY + j) * p.SZ + lz; }
+// z slab: cell k (inside the low or high slab of its component) of row (i, j).
+__device__ __forceinline__ int zslab_off(const StepParams& p, int i, int j, int k) {
+  return (i * p.NY + j) * p.SZ + (k < p.zlo4 ? k : p.zlo4 + k - p.zhs4);
+}
 
 // True when the CSR list of `key` along `axis` holds at least one item.
 __device__ __forceinline__ bool list_nonempty(const BoxIndex& ix, int axis, int key) {
@@ -86,39 +89,69 @@ __device__ __forceinline__ void add_terms(const StepParams& p, int phase, int ba
 
 // Advance the ADE poles covering (i, j, k) from E^n and subtract dt J / eps.
 // `lane_poles` has bit b set when pole b (b < 32) covers this lane's (j, k);
-// the plane list already restricts i.
+// the plane list already restricts i.  Poles are taken three at a time with
+// every state load issued before the first update, so the load latencies of a
+// multi-component material overlap; the subtractions keep the list order.
 __device__ __forceinline__ void ade(const StepParams& p, unsigned lane_poles, int i, int j, int k, float e0, float e1,
                                     float e2, float& v0, float& v1, float& v2) {
+  constexpr int kB = 3;
   const int b = __ldg(p.pole_plane_ptr + i), e = __ldg(p.pole_plane_ptr + i + 1);
-  for (int x = b; x < e; ++x) {
-    const int id = __ldg(p.pole_plane_ids + x);
-    if (id < 32 && !((lane_poles >> id) & 1u)) continue;
-    const PoleTerm& pt = p.poles[id];
-    if (id >= 32 && (j < pt.j0 || j >= pt.j1 || k < pt.k0 || k >= pt.k1)) continue;
-    const int64_t o = (static_cast<int64_t>(i - pt.i0) * (pt.j1 - pt.j0) + (j - pt.j0)) * (pt.k1 - pt.k0) + (k - pt.k0);
-    const int c = pt.comp;
-    const float eo = c == 0 ? e0 : (c == 1 ? e1 : e2);
-    const float drive = __ldg(pt.drive + o);
-    float jn;
-    if (pt.kind == 0) {
-      const float prev = pt.pol[o];
-      const float next = pt.decay * prev + drive * eo;
-      pt.pol[o] = next;
-      jn = (next - prev) * pt.inv_dt;
-      pt.cur[o] = jn;
-    } else if (pt.kind == 1) {
-      jn = pt.decay * pt.cur[o] + drive * eo;
-      pt.cur[o] = jn;
-    } else {
-      const float pol = pt.pol[o];
-      jn = pt.decay * pt.cur[o] - pt.restoring * pol + drive * eo;
-      pt.cur[o] = jn;
-      pt.pol[o] = pol + pt.dt * jn;
+  for (int x0 = b; x0 < e; x0 += kB) {
+    const PoleTerm* pts[kB];
+    int64_t offs[kB];
+    bool act[kB];
+    float drive[kB], ie[kB], pol[kB], cur[kB];
+#pragma unroll
+    for (int u = 0; u < kB; ++u) {
+      act[u] = false;
+      pts[u] = p.poles;
+      offs[u] = 0;
+      drive[u] = ie[u] = pol[u] = cur[u] = 0.f;
+      if (x0 + u < e) {
+        const int id = __ldg(p.pole_plane_ids + x0 + u);
+        const PoleTerm* pt = p.poles + id;
+        act[u] = id < 32 ? ((lane_poles >> id) & 1u) != 0 : (j >= pt->j0 && j < pt->j1 && k >= pt->k0 && k < pt->k1);
+        pts[u] = pt;
+      }
+      if (act[u]) {
+        const PoleTerm& pt = *pts[u];
+        const int64_t o =
+            (static_cast<int64_t>(i - pt.i0) * (pt.j1 - pt.j0) + (j - pt.j0)) * pt.nkk + (k - pt.kk0);
+        offs[u] = o;
+        drive[u] = __ldg(pt.drive + o);
+        ie[u] = __ldg(pt.inv_eps + o);
+        if (pt.kind != 1) pol[u] = pt.pol[o];
+        if (pt.kind != 0) cur[u] = pt.cur[o];
+      }
     }
-    const float sub = pt.dt * jn * __ldg(pt.inv_eps + o);
-    if (c == 0) v0 -= sub;
-    else if (c == 1) v1 -= sub;
-    else v2 -= sub;
+#pragma unroll
+    for (int u = 0; u < kB; ++u) {
+      if (!act[u]) continue;
+      const PoleTerm& pt = *pts[u];
+      const int64_t o = offs[u];
+      const int c = pt.comp;
+      const float eo = c == 0 ? e0 : (c == 1 ? e1 : e2);
+      float jn;
+      if (pt.kind == 0) {
+        const float prev = pol[u];
+        const float next = pt.decay * prev + drive[u] * eo;
+        pt.pol[o] = next;
+        jn = (next - prev) * pt.inv_dt;
+        pt.cur[o] = jn;
+      } else if (pt.kind == 1) {
+        jn = pt.decay * cur[u] + drive[u] * eo;
+        pt.cur[o] = jn;
+      } else {
+        const float pl = pol[u];
+        jn = pt.decay * cur[u] - pt.restoring * pl + drive[u] * eo;
+        pt.cur[o] = jn;
+        pt.pol[o] = pl + pt.dt * jn;
+      }
+      const float sub = pt.dt * jn * ie[u];
+      if (c == 0) v0 -= sub;
+      else if (c == 1) v1 -= sub;
+      else v2 -= sub;
+    }
   }
 }
 

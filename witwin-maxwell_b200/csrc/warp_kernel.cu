@@ -153,9 +153,9 @@ __device__ __forceinline__ void march(const StepParams& p, int n, int lane, int 
         }
       }
       if (z_slab && szh >= 0) {
-        qz0 = ldz(p.psiHin[0][1], zslab_off(p, i, jm, szh), mx_ok);
-        qz1 = ldz(p.psiHin[0][1], zslab_off(p, i, j, szh), cx_ok);
-        qz2 = ldz(p.psiHin[1][1], zslab_off(p, i, j, szh), cy_ok);
+        qz0 = ldz(p.psiHin[0][1], zslab_off(p, i, jm, k), mx_ok);
+        qz1 = ldz(p.psiHin[0][1], zslab_off(p, i, j, k), cx_ok);
+        qz2 = ldz(p.psiHin[1][1], zslab_off(p, i, j, k), cy_ok);
       }
     }
     // E coefficient arrays of this plane, issued early so their latency hides
@@ -206,9 +206,9 @@ __device__ __forceinline__ void march(const StepParams& p, int n, int lane, int 
       }
       if (z_slab && szh >= 0) {
         const Prof pz = prof(p.hb[2], p.hc[2], p.hik[2], k);
-        if (mx_ok) mxb = psi_apply(mxb, pz.b, pz.c, pz.ik, qz0, p.psiHout[0][1], zslab_off(p, i, jm, szh), false);
-        if (cx_ok) cxb = psi_apply(cxb, pz.b, pz.c, pz.ik, qz1, p.psiHout[0][1], zslab_off(p, i, j, szh), wr);
-        if (cy_ok) cyb = psi_apply(cyb, pz.b, pz.c, pz.ik, qz2, p.psiHout[1][1], zslab_off(p, i, j, szh), wr);
+        if (mx_ok) mxb = psi_apply(mxb, pz.b, pz.c, pz.ik, qz0, p.psiHout[0][1], zslab_off(p, i, jm, k), false);
+        if (cx_ok) cxb = psi_apply(cxb, pz.b, pz.c, pz.ik, qz1, p.psiHout[0][1], zslab_off(p, i, j, k), wr);
+        if (cy_ok) cyb = psi_apply(cyb, pz.b, pz.c, pz.ik, qz2, p.psiHout[1][1], zslab_off(p, i, j, k), wr);
       }
     }
     float dHx = p.hdecay_u[0], cHx = p.hcurl_u[0], dHy = p.hdecay_u[1], cHy = p.hcurl_u[1], dHz = p.hdecay_u[2],
@@ -269,8 +269,8 @@ __device__ __forceinline__ void march(const StepParams& p, int n, int lane, int 
         }
         if (z_slab && sze >= 0) {
           const Prof pz = prof(p.eb[2], p.ec[2], p.eik[2], k);
-          if (m0 == 0) d0b = psi_step(d0b, pz.b, pz.c, pz.ik, p.psiE[0][1], p.psiE[0][1], zslab_off(p, i, j, sze), true);
-          if (m1 == 0) d1b = psi_step(d1b, pz.b, pz.c, pz.ik, p.psiE[1][1], p.psiE[1][1], zslab_off(p, i, j, sze), true);
+          if (m0 == 0) d0b = psi_step(d0b, pz.b, pz.c, pz.ik, p.psiE[0][1], p.psiE[0][1], zslab_off(p, i, j, k), true);
+          if (m1 == 0) d1b = psi_step(d1b, pz.b, pz.c, pz.ik, p.psiE[1][1], p.psiE[1][1], zslab_off(p, i, j, k), true);
         }
       }
       float v0 = pick(m0, ec0 * g0 + c0 * (d0a - d0b), ec0);
