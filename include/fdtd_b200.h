@@ -72,6 +72,24 @@ typedef struct {
 int fdtd_engine_create(const fdtd_grid_desc* desc, void* stream, fdtd_engine** out);
 int fdtd_engine_destroy(fdtd_engine* h);
 
+/* Field storage of the engine's state: FDTD_STORE_F32 (default, exact FP32
+ * path), FDTD_STORE_F16 or FDTD_STORE_BF16 (E and H stored in 16 bits, all
+ * arithmetic in FP32; ADE pole state FP32 with FP16 fields, BF16 with BF16
+ * fields).  A stored value x of
+ * component c (0..2 Ex..Ez, 3..5 Hx..Hz) represents x * scales[c]; scales
+ * must be powers of two, or NULL: FP16 then estimates them at finalize from the
+ * source tables and the TFSF incident line (peak mapped to [32, 64)), BF16
+ * uses 1.  No counterpart in the reference (its fields are FP32 only,
+ * stepping.py:1625-1630).  Call right after fdtd_engine_create (the field
+ * buffers are re-allocated and zeroed).  Reduced storage runs launch variant 2
+ * only, and the adjoint needs FP32.  FP16 values above 65504 * scale overflow
+ * to infinity: give explicit scales when the sources do not bound the field. */
+#define FDTD_STORE_F32 0
+#define FDTD_STORE_F16 1
+#define FDTD_STORE_BF16 2
+int fdtd_engine_set_storage(fdtd_engine* h, int kind, const float* scales);
+int fdtd_engine_get_storage(fdtd_engine* h, int* kind, float* scales);
+
 /* Per-axis inverse spacings: inv_e has N entries (dual), inv_h N-1 (primal),
  * witwin/maxwell/fdtd/runtime/initialization.py:131-139. */
 int fdtd_engine_set_spacing(fdtd_engine* h, int axis, const float* inv_e, const float* inv_h);
@@ -157,11 +175,15 @@ int fdtd_engine_checkpoint_load(fdtd_engine* h, int slot);
 /* Tile shape selection: time the candidate (tile_rows, chunk_planes) pairs on
  * the bound scene (state is saved and restored) and keep the fastest. */
 int fdtd_engine_autotune(fdtd_engine* h, int* tile_rows, int* chunk_planes);
-/* Launch configuration of the fused step kernel: the register budget variant
- * (1: unconstrained, about 100 registers per thread; 3: at most 85, three
- * 256-thread CTAs per SM; 2: at most 64, four CTAs per SM) and the number of x
- * planes each warp marches through (chunk_planes, 0 keeps the current value).
- * tile_rows is accepted for compatibility and ignored. */
+/* Launch configuration of the fused step kernel.  Variants 1-3: the scalar
+ * warp kernel (one z cell per lane) with a register budget of about 100 (1),
+ * 64 (2, the default: four 256-thread CTAs per SM) or 85 (3) per thread;
+ * 4: the same warp decomposition fed by TMA plane tiles; 5-9: the z-vectorised
+ * warp kernel (5: four cells per lane, 6: two cells per lane, direct loads;
+ * 7 / 8: two cells per lane fed by a 4- / 3-plane cp.async ring; 9: four cells
+ * per lane, 3-plane ring).  chunk_planes is the number of x planes each warp
+ * marches through (0 picks the variant's default).  tile_rows is accepted
+ * for compatibility and ignored. */
 int fdtd_engine_set_launch(fdtd_engine* h, int variant, int tile_rows, int chunk_planes);
 int fdtd_engine_get_launch(fdtd_engine* h, int* variant, int* tile_rows, int* chunk_planes);
 /* Launch configuration and launch count bookkeeping. */

@@ -41,6 +41,8 @@ _SIGNATURES = {
     "fdtd_version": ([], ctypes.c_char_p),
     "fdtd_engine_create": ([ctypes.POINTER(FdtdGridDesc), _vp, ctypes.POINTER(_vp)], _i),
     "fdtd_engine_destroy": ([_vp], _i),
+    "fdtd_engine_set_storage": ([_vp, _i, _vp], _i),
+    "fdtd_engine_get_storage": ([_vp, _c_int_p, _vp], _i),
     "fdtd_engine_set_spacing": ([_vp, _i, _vp, _vp], _i),
     "fdtd_engine_set_cpml": ([_vp, _i, _vp, _vp, _vp, _vp, _vp, _vp], _i),
     "fdtd_engine_set_coefficients": ([_vp, _i, _vp, _f, _vp, _f], _i),

@@ -5,9 +5,12 @@
 // 4 so each z row starts on a 16-byte boundary and can be read as float4),
 // cells outside a component's Yee extent are held at zero.  CPML psi arrays
 // are kept only on their slabs; ADE state only on the pole boxes.
+#include <cuda_bf16.h>
+#include <cuda_fp16.h>
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <type_traits>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -24,6 +27,7 @@ template <bool kCpml, bool kCoef, bool kUniform, int kMinBlocks>
 __global__ void warp_step_kernel(const StepParams p, int n, int slot);
 int launch_classify_vec(const StepParams& p, int V, int n_kblocks, int n_chunks, unsigned char* out,
                         cudaStream_t stream);
+int launch_step_reduced(const StepParams& p, int n, dim3 grid, bool cpml, bool coef, bool uni, cudaStream_t stream);
 using VecLauncher = int (*)(const StepParams&, int, dim3, bool, bool, bool, cudaStream_t);
 int launch_vec_v4(const StepParams&, int, dim3, bool, bool, bool, cudaStream_t);
 int launch_vec_v2(const StepParams&, int, dim3, bool, bool, bool, cudaStream_t);
@@ -106,6 +110,53 @@ __global__ void unpack_kernel(float* dst, const float* src, int sx, int sy, int 
 
 constexpr int kNoRemap = 0x7fffffff;
 
+// Dense FP32 [sx][sy][sz] <-> internal reduced-storage [.][NY][P] field
+// (value = stored * scale).
+template <typename TS>
+__global__ void pack_field_rs_kernel(TS* dst, const float* src, int sx, int sy, int sz, int NY, int P, float inv) {
+  const int64_t total = static_cast<int64_t>(sx) * sy * sz;
+  for (int64_t x = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; x < total;
+       x += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    const int k = static_cast<int>(x % sz);
+    const int64_t r = x / sz;
+    const int j = static_cast<int>(r % sy);
+    const int i = static_cast<int>(r / sy);
+    const float v = src[x] * inv;
+    TS out;
+    if constexpr (sizeof(TS) == 2 && std::is_same<TS, __half>::value) out = __float2half_rn(v);
+    else out = __float2bfloat16_rn(v);
+    dst[(static_cast<int64_t>(i) * NY + j) * P + k] = out;
+  }
+}
+
+template <typename TS>
+__global__ void unpack_field_rs_kernel(float* dst, const TS* src, int sx, int sy, int sz, int NY, int P, float scale) {
+  const int64_t total = static_cast<int64_t>(sx) * sy * sz;
+  for (int64_t x = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; x < total;
+       x += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    const int k = static_cast<int>(x % sz);
+    const int64_t r = x / sz;
+    const int j = static_cast<int>(r % sy);
+    const int i = static_cast<int>(r / sy);
+    const TS v = src[(static_cast<int64_t>(i) * NY + j) * P + k];
+    float f;
+    if constexpr (std::is_same<TS, __half>::value) f = __half2float(v);
+    else f = __bfloat162float(v);
+    dst[x] = f * scale;
+  }
+}
+
+// BF16 pole state [rows][nkk] (cells [koff, koff + nk) of each row) -> dense FP32 [rows][nk].
+__global__ void unpack_pole_bf16_kernel(float* dst, const __nv_bfloat16* src, int64_t rows, int nk, int nkk, int koff) {
+  const int64_t total = rows * nk;
+  for (int64_t x = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; x < total;
+       x += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    const int64_t r = x / nk;
+    const int k = static_cast<int>(x % nk);
+    dst[x] = __bfloat162float(src[r * nkk + koff + k]);
+  }
+}
+
 // Precompute the history of a 1-D incident line (one block, sequential in time).
 // Restates AuxiliaryGrid1D.advance_magnetic / advance_electric,
 // witwin/maxwell/fdtd/excitation/spatial.py:443-462 and sources.cu:803-839.
@@ -160,12 +211,20 @@ __global__ void dft_weight_kernel(int n_freq, int n_steps, const double* omega, 
 // same values: E^{n+1} and H^{n+1/2} after all corrections of the step).
 struct FieldPtrs {
   const float* f[6];
+  int storage;       // kStoreF32 / kStoreF16 / kStoreBF16
+  float scale[6];    // stored value * scale = field value (reduced storage)
 };
+
+__device__ __forceinline__ float load_field(const FieldPtrs& fp, int comp, int64_t off) {
+  if (fp.storage == kStoreF16) return __half2float(reinterpret_cast<const __half*>(fp.f[comp])[off]) * fp.scale[comp];
+  if (fp.storage == kStoreBF16)
+    return __bfloat162float(reinterpret_cast<const __nv_bfloat16*>(fp.f[comp])[off]) * fp.scale[comp];
+  return __ldg(fp.f[comp] + off);
+}
 
 __global__ void sample_gather_kernel(const RegionFlush* regions, const FieldPtrs fields, int NY, int P,
                                      float* samples, int64_t n_samples, int slot) {
   const RegionFlush rg = regions[blockIdx.y];
-  const float* f = fields.f[rg.comp];
   float* out = samples + static_cast<int64_t>(slot) * n_samples + rg.base;
   for (int64_t x = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; x < rg.count;
        x += static_cast<int64_t>(gridDim.x) * blockDim.x) {
@@ -173,7 +232,7 @@ __global__ void sample_gather_kernel(const RegionFlush* regions, const FieldPtrs
     const int64_t r = x / rg.nk;
     const int lj = static_cast<int>(r % rg.nj);
     const int li = static_cast<int>(r / rg.nj);
-    out[x] = __ldg(f + (static_cast<int64_t>(rg.i0 + li) * NY + rg.j0 + lj) * P + rg.k0 + lk);
+    out[x] = load_field(fields, rg.comp, (static_cast<int64_t>(rg.i0 + li) * NY + rg.j0 + lj) * P + rg.k0 + lk);
   }
 }
 
@@ -260,6 +319,7 @@ struct PoleHost {
   int64_t count = 0;  // cells of the box
   int64_t rows = 0;   // (i, j) rows of the box
   int nk = 0, nkk = 0, koff = 0;  // z cells, padded z pitch, offset of k0 in a padded row
+  int64_t state_floats = 0;       // size of pol / cur in 4-byte words
 };
 
 struct AuxLine {
@@ -290,6 +350,11 @@ struct fdtd_engine {
   cudaStream_t stream = nullptr;
   int NX = 0, NY = 0, NZ = 0, P = 0, SZ = 0;
   int zlo4 = 0, zhs4 = 0;  // z-slab psi row segments (StepParams::zlo4 / zhs4)
+  // Field storage (kStore*) and per-component scales (stored * scale = value);
+  // scales_set: the caller fixed the scales (else finalize estimates them).
+  int storage = 0;
+  float fscale[6] = {1, 1, 1, 1, 1, 1};
+  bool scales_set = false;
   int64_t plane = 0, vol = 0;
   int TY = 0, CX = 0;
   // Fused kernel: 1..3 = register-prefetch warp kernel with a register budget
@@ -378,6 +443,9 @@ int dev_copy(fdtd_engine* h, float** out, const float* src, size_t n) {
   return 0;
 }
 
+// Size of one field array in 4-byte words (two reduced values per word).
+int64_t field_floats(const fdtd_engine* h) { return h->storage == kStoreF32 ? h->vol : (h->vol + 1) / 2; }
+
 int64_t slab_elems(const fdtd_engine* h, int axis) {
   const int L = h->desc.pml_lo[axis] + h->desc.pml_hi[axis];
   if (L == 0) return 0;
@@ -447,6 +515,11 @@ void fill_params(const fdtd_engine* h, StepParams& p) {
   p.NZ = h->NZ;
   p.P = h->P;
   p.SZ = h->SZ;
+  p.storage = h->storage;
+  for (int c = 0; c < 6; ++c) {
+    p.fscale[c] = h->fscale[c];
+    p.finv[c] = 1.0f / h->fscale[c];
+  }
   p.zlo4 = h->zlo4;
   p.zhs4 = h->zhs4;
   p.TY = h->TY;
@@ -573,7 +646,10 @@ int launch_step(fdtd_engine* h, int n, int slot) {
     if (err != 0) return cuda_fail(static_cast<cudaError_t>(err), "classify_kernel launch");
     h->class_key = key;
   }
-  if (VecLauncher vl = vec_launcher(h->variant)) {
+  if (h->storage != kStoreF32) {
+    const int err = launch_step_reduced(p, n, grid, h->cpml, coef, h->uniform_grid, h->stream);
+    if (err != 0) return cuda_fail(static_cast<cudaError_t>(err), "warp_step_kernel_rs launch");
+  } else if (VecLauncher vl = vec_launcher(h->variant)) {
     const int err = vl(p, n, grid, h->cpml, coef, h->uniform_grid, h->stream);
     if (err != 0) return cuda_fail(static_cast<cudaError_t>(err), "vec_step_kernel launch");
   } else {
@@ -614,6 +690,8 @@ int launch_step(fdtd_engine* h, int n, int slot) {
       fields.f[c] = h->E[h->cur][c];
       fields.f[3 + c] = h->H[h->cur][c];
     }
+    fields.storage = h->storage;
+    for (int c = 0; c < 6; ++c) fields.scale[c] = h->fscale[c];
     const int gx = static_cast<int>(std::min<int64_t>((h->max_region + 255) / 256, 2048));
     sample_gather_kernel<<<dim3(std::max(gx, 1), h->n_flush), 256, 0, h->stream>>>(
         h->d_flush, fields, h->NY, h->P, h->samples, h->n_samples, slot);
@@ -837,6 +915,51 @@ int fdtd_engine_destroy(fdtd_engine* h) {
   return 0;
 }
 
+int fdtd_engine_set_storage(fdtd_engine* h, int kind, const float* scales) {
+  if (!h || kind < kStoreF32 || kind > kStoreBF16) return fail(FDTD_ERR_INVALID_ARG, "bad storage kind");
+  if (h->finalized || !h->poles.empty() || !h->checkpoints.empty())
+    return fail(FDTD_ERR_STATE, "storage must be chosen right after fdtd_engine_create");
+  if (scales) {
+    for (int c = 0; c < 6; ++c) {
+      int e = 0;
+      if (!(scales[c] > 0.0f) || !std::isfinite(scales[c]) || std::frexp(scales[c], &e) != 0.5f)
+        return fail(FDTD_ERR_INVALID_ARG, "storage scales must be positive powers of two");
+    }
+  }
+  if (kind != h->storage) {
+    // Re-allocate the four field buffer sets in the new element size (zeroed).
+    CUDA_TRY(cudaStreamSynchronize(h->stream));
+    for (int b = 0; b < 2; ++b)
+      for (int c = 0; c < 3; ++c)
+        for (float** buf : {&h->E[b][c], &h->H[b][c]}) {
+          auto it = std::find(h->owned.begin(), h->owned.end(), *buf);
+          if (it != h->owned.end()) h->owned.erase(it);
+          cudaFree(*buf);
+          *buf = nullptr;
+        }
+    h->storage = kind;
+    for (int b = 0; b < 2; ++b)
+      for (int c = 0; c < 3; ++c) {
+        int rc = dev_alloc(h, &h->E[b][c], static_cast<size_t>(field_floats(h)));
+        if (!rc) rc = dev_alloc(h, &h->H[b][c], static_cast<size_t>(field_floats(h)));
+        if (rc) return rc;
+      }
+    h->cur = 0;
+  }
+  for (int c = 0; c < 6; ++c) h->fscale[c] = scales ? scales[c] : 1.0f;
+  h->scales_set = scales != nullptr;
+  if (kind != kStoreF32) h->variant = 2;
+  return 0;
+}
+
+int fdtd_engine_get_storage(fdtd_engine* h, int* kind, float* scales) {
+  if (!h) return fail(FDTD_ERR_INVALID_ARG, "null engine");
+  if (kind) *kind = h->storage;
+  if (scales)
+    for (int c = 0; c < 6; ++c) scales[c] = h->fscale[c];
+  return 0;
+}
+
 int fdtd_engine_set_spacing(fdtd_engine* h, int axis, const float* inv_e, const float* inv_h) {
   if (!h || axis < 0 || axis > 2 || !inv_e || !inv_h) return fail(FDTD_ERR_INVALID_ARG, "bad spacing arguments");
   const int n[3] = {h->NX, h->NY, h->NZ};
@@ -886,7 +1009,15 @@ int fdtd_engine_pack_field(fdtd_engine* h, int comp, const float* src) {
   int ext[3];
   comp_extent(comp, h->NX, h->NY, h->NZ, ext);
   float* dst = comp < 3 ? h->E[h->cur][comp] : h->H[h->cur][comp - 3];
-  pack_kernel<<<1024, 256, 0, h->stream>>>(dst, src, ext[0], ext[1], ext[2], h->NY, h->P, kNoRemap, 0);
+  const float inv = 1.0f / h->fscale[comp];
+  if (h->storage == kStoreF16)
+    pack_field_rs_kernel<__half><<<1024, 256, 0, h->stream>>>(reinterpret_cast<__half*>(dst), src, ext[0], ext[1],
+                                                              ext[2], h->NY, h->P, inv);
+  else if (h->storage == kStoreBF16)
+    pack_field_rs_kernel<__nv_bfloat16><<<1024, 256, 0, h->stream>>>(reinterpret_cast<__nv_bfloat16*>(dst), src,
+                                                                     ext[0], ext[1], ext[2], h->NY, h->P, inv);
+  else
+    pack_kernel<<<1024, 256, 0, h->stream>>>(dst, src, ext[0], ext[1], ext[2], h->NY, h->P, kNoRemap, 0);
   CUDA_TRY(cudaGetLastError());
   return 0;
 }
@@ -896,7 +1027,14 @@ int fdtd_engine_unpack_field(fdtd_engine* h, int comp, float* dst) {
   int ext[3];
   comp_extent(comp, h->NX, h->NY, h->NZ, ext);
   const float* src = comp < 3 ? h->E[h->cur][comp] : h->H[h->cur][comp - 3];
-  unpack_kernel<<<1024, 256, 0, h->stream>>>(dst, src, ext[0], ext[1], ext[2], h->NY, h->P, kNoRemap, 0);
+  if (h->storage == kStoreF16)
+    unpack_field_rs_kernel<__half><<<1024, 256, 0, h->stream>>>(dst, reinterpret_cast<const __half*>(src), ext[0],
+                                                                ext[1], ext[2], h->NY, h->P, h->fscale[comp]);
+  else if (h->storage == kStoreBF16)
+    unpack_field_rs_kernel<__nv_bfloat16><<<1024, 256, 0, h->stream>>>(
+        dst, reinterpret_cast<const __nv_bfloat16*>(src), ext[0], ext[1], ext[2], h->NY, h->P, h->fscale[comp]);
+  else
+    unpack_kernel<<<1024, 256, 0, h->stream>>>(dst, src, ext[0], ext[1], ext[2], h->NY, h->P, kNoRemap, 0);
   CUDA_TRY(cudaGetLastError());
   return 0;
 }
@@ -971,14 +1109,18 @@ int fdtd_engine_add_pole(fdtd_engine* h, int comp, int kind, const int* box, con
   ph.nkk = nkk;
   ph.koff = box[4] - kk0;
   const size_t bytes = static_cast<size_t>(rows) * nkk * sizeof(float);
+  // state arrays: BF16 with BF16 field storage, FP32 otherwise
+  ph.state_floats =
+      static_cast<int64_t>((static_cast<size_t>(rows) * nkk * (h->storage == kStoreBF16 ? 2 : 4) + 3) / 4);
+  const size_t sbytes = static_cast<size_t>(ph.state_floats) * sizeof(float);
   CUDA_TRY(cudaMalloc(&ph.drive, bytes));
   CUDA_TRY(cudaMalloc(&ph.inv_eps, bytes));
-  CUDA_TRY(cudaMalloc(&ph.pol, bytes));
-  CUDA_TRY(cudaMalloc(&ph.cur, bytes));
+  CUDA_TRY(cudaMalloc(&ph.pol, sbytes));
+  CUDA_TRY(cudaMalloc(&ph.cur, sbytes));
   CUDA_TRY(cudaMemsetAsync(ph.drive, 0, bytes, h->stream));
   CUDA_TRY(cudaMemsetAsync(ph.inv_eps, 0, bytes, h->stream));
-  CUDA_TRY(cudaMemsetAsync(ph.pol, 0, bytes, h->stream));
-  CUDA_TRY(cudaMemsetAsync(ph.cur, 0, bytes, h->stream));
+  CUDA_TRY(cudaMemsetAsync(ph.pol, 0, sbytes, h->stream));
+  CUDA_TRY(cudaMemsetAsync(ph.cur, 0, sbytes, h->stream));
   CUDA_TRY(cudaMemcpy2DAsync(ph.drive + ph.koff, nkk * sizeof(float), drive, nk * sizeof(float), nk * sizeof(float),
                              rows, cudaMemcpyDefault, h->stream));
   CUDA_TRY(cudaMemcpy2DAsync(ph.inv_eps + ph.koff, nkk * sizeof(float), inv_eps, nk * sizeof(float),
@@ -1011,6 +1153,16 @@ int fdtd_engine_pole_state(fdtd_engine* h, int pole_id, float* pol_out, float* c
   if (!h || pole_id < 0 || pole_id >= static_cast<int>(h->poles.size()))
     return fail(FDTD_ERR_INVALID_ARG, "bad pole id");
   const PoleHost& ph = h->poles[pole_id];
+  if (h->storage == kStoreBF16) {
+    if (pol_out)
+      unpack_pole_bf16_kernel<<<256, 256, 0, h->stream>>>(pol_out, reinterpret_cast<const __nv_bfloat16*>(ph.pol),
+                                                          ph.rows, ph.nk, ph.nkk, ph.koff);
+    if (cur_out)
+      unpack_pole_bf16_kernel<<<256, 256, 0, h->stream>>>(cur_out, reinterpret_cast<const __nv_bfloat16*>(ph.cur),
+                                                          ph.rows, ph.nk, ph.nkk, ph.koff);
+    CUDA_TRY(cudaGetLastError());
+    return 0;
+  }
   const size_t w = ph.nk * sizeof(float), pitch = ph.nkk * sizeof(float);
   if (pol_out)
     CUDA_TRY(cudaMemcpy2DAsync(pol_out, w, ph.pol + ph.koff, pitch, w, ph.rows, cudaMemcpyDefault, h->stream));
@@ -1159,9 +1311,68 @@ int fdtd_engine_set_dft(fdtd_engine* h, int n_freq, const double* omega, int n_s
   return 0;
 }
 
+namespace {
+
+float host_absmax(const std::vector<float>& v) {
+  float m = 0.0f;
+  for (float x : v) m = std::max(m, std::fabs(x));
+  return m;
+}
+
+// FP16 storage scales from the sources: the E peak is bounded by the incident
+// line's E history (TFSF) and, for soft sources, by max|coeff| times the sum of
+// |signal| over the table; the H peak by the line's H history and E / eta0.
+// Each scale maps its estimate to [32, 64), leaving three decades of headroom
+// below the FP16 maximum 65504 and keeping six decades of values above the
+// FP16 normal range.
+int estimate_scales(fdtd_engine* h) {
+  double e_peak = 0.0, h_peak = 0.0;
+  for (const auto& t : h->terms) {
+    const int64_t cells = static_cast<int64_t>(t.i1 - t.i0) * (t.j1 - t.j0) * (t.k1 - t.k0);
+    std::vector<float> coeff(static_cast<size_t>(cells));
+    CUDA_TRY(cudaMemcpy(coeff.data(), t.coeff, sizeof(float) * cells, cudaMemcpyDeviceToHost));
+    const double cmax = host_absmax(coeff) * std::fabs(t.scale);
+    if (t.signal) {
+      std::vector<float> sig(static_cast<size_t>(t.aux_len));
+      CUDA_TRY(cudaMemcpy(sig.data(), t.signal, sizeof(float) * t.aux_len, cudaMemcpyDeviceToHost));
+      double sum = 0.0;
+      for (float x : sig) sum += std::fabs(x);
+      if (t.comp < 3) e_peak = std::max(e_peak, cmax * sum);
+      else h_peak = std::max(h_peak, cmax * sum);
+    }
+  }
+  for (const auto& l : h->lines) {
+    const size_t n = static_cast<size_t>(l.n_steps) * l.ne;
+    std::vector<float> v(n);
+    CUDA_TRY(cudaMemcpy(v.data(), l.e_hist, sizeof(float) * n, cudaMemcpyDeviceToHost));
+    e_peak = std::max(e_peak, static_cast<double>(host_absmax(v)));
+    CUDA_TRY(cudaMemcpy(v.data(), l.h_hist, sizeof(float) * n, cudaMemcpyDeviceToHost));
+    h_peak = std::max(h_peak, static_cast<double>(host_absmax(v)));
+  }
+  constexpr double kEta0 = 376.730313668;
+  h_peak = std::max(h_peak, e_peak / kEta0);
+  auto pick = [](double peak) {
+    if (!(peak > 0.0) || !std::isfinite(peak)) return 1.0f;
+    int e = 0;
+    std::frexp(peak, &e);  // peak in [2^(e-1), 2^e)
+    return static_cast<float>(std::ldexp(1.0, e - 6));
+  };
+  for (int c = 0; c < 3; ++c) {
+    h->fscale[c] = pick(e_peak);
+    h->fscale[3 + c] = pick(h_peak);
+  }
+  return 0;
+}
+
+}  // namespace
+
 int fdtd_engine_finalize(fdtd_engine* h) {
   if (!h) return fail(FDTD_ERR_INVALID_ARG, "null engine");
   if (h->finalized) return 0;
+  if (h->storage == kStoreF16 && !h->scales_set) {
+    const int rc = estimate_scales(h);
+    if (rc) return rc;
+  }
   for (int a = 0; a < 3; ++a) {
     if (!h->inv_e[a] || !h->inv_h[a]) return fail(FDTD_ERR_STATE, "spacing not set on every axis");
     if (h->cpml && (!h->eb[a] || !h->hb[a])) return fail(FDTD_ERR_STATE, "CPML profile not set on every axis");
@@ -1291,7 +1502,7 @@ int fdtd_engine_finalize(fdtd_engine* h) {
   {
     // TMA maps of both ping-pong buffers; without the driver entry point the
     // TMA variant stays unavailable and the warp kernel runs.
-    bool ok = true;
+    bool ok = h->storage == kStoreF32;
     for (int b = 0; b < 2 && ok; ++b) {
       for (int c = 0; c < 3 && ok; ++c) {
         ok = encode_field_map(&h->maps[b].e[c], h->E[b][c], h->NX, h->NY, h->P, tma_rows_e()) == 0 &&
@@ -1386,8 +1597,8 @@ int fdtd_engine_read_dft(fdtd_engine* h, float* re, float* im) {
 static void state_buffers(fdtd_engine* h, std::vector<std::pair<float*, size_t>>& out) {
   const int c0 = h->cur;
   for (int c = 0; c < 3; ++c) {
-    out.push_back({h->E[c0][c], static_cast<size_t>(h->vol)});
-    out.push_back({h->H[c0][c], static_cast<size_t>(h->vol)});
+    out.push_back({h->E[c0][c], static_cast<size_t>(field_floats(h))});
+    out.push_back({h->H[c0][c], static_cast<size_t>(field_floats(h))});
   }
   for (int c = 0; c < 3; ++c) {
     const int ax[2] = {axis_a(c), axis_b(c)};
@@ -1399,8 +1610,8 @@ static void state_buffers(fdtd_engine* h, std::vector<std::pair<float*, size_t>>
     }
   }
   for (auto& ph : h->poles) {
-    out.push_back({ph.pol, static_cast<size_t>(ph.rows * ph.nkk)});
-    out.push_back({ph.cur, static_cast<size_t>(ph.rows * ph.nkk)});
+    out.push_back({ph.pol, static_cast<size_t>(ph.state_floats)});
+    out.push_back({ph.cur, static_cast<size_t>(ph.state_floats)});
   }
 }
 
@@ -1474,6 +1685,7 @@ int fdtd_engine_autotune(fdtd_engine* h, int* tile_rows, int* chunk_planes) {
   int best_ty = 1, best_cx = h->CX, best_var = h->variant;
   for (int var = 1; var <= kMaxVariant; ++var) {
     if (var == 4 && !h->tma_ready) continue;
+    if (h->storage != kStoreF32 && var != 2) continue;  // reduced storage: the 64-register kernel only
     for (int cx : cxs) {
       if (cx > 2 * h->NX) continue;
       h->variant = var;
@@ -1535,6 +1747,8 @@ int fdtd_engine_set_launch(fdtd_engine* h, int variant, int tile_rows, int chunk
   if (!h || variant < 1 || variant > kMaxVariant || tile_rows < 0 || chunk_planes < 0)
     return fail(FDTD_ERR_INVALID_ARG, "bad launch configuration");
   (void)tile_rows;  // the warp-granular kernels have no tile height
+  if (h->storage != kStoreF32 && variant != 2)
+    return fail(FDTD_ERR_UNSUPPORTED, "reduced field storage runs launch variant 2 only");
   h->variant = variant;
   if (chunk_planes > 0) h->CX = chunk_planes;
   else default_tiles(h);
@@ -1558,6 +1772,7 @@ int fdtd_engine_adjoint_init(fdtd_engine* h, const int* design_boxes, int max_se
   if (!h || max_segment < 1) return fail(FDTD_ERR_INVALID_ARG, "bad adjoint arguments");
   if (!h->finalized) return fail(FDTD_ERR_STATE, "engine not finalized");
   if (!h->poles.empty()) return fail(FDTD_ERR_UNSUPPORTED, "the adjoint of dispersive (ADE) media is not supported");
+  if (h->storage != kStoreF32) return fail(FDTD_ERR_UNSUPPORTED, "the adjoint runs on FP32 field storage only");
   if (h->adj.ready) return fail(FDTD_ERR_STATE, "adjoint already initialised");
   AdjointHost& a = h->adj;
   a.q = AdjParams{};

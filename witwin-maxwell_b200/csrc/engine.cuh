@@ -121,6 +121,13 @@ struct StepParams {
   // [(chunk * kblocks + kblock) * NY + j]; built by launch_classify for the
   // current chunk length.
   const unsigned char* warp_class;
+  // Field storage: kStoreF32, kStoreF16 or kStoreBF16 (E, H arrays hold that
+  // type; ADE pole state is BF16 with BF16 fields, FP32 otherwise).  A stored field
+  // value x of component c (0..2 Ex..Ez, 3..5 Hx..Hz) means x * fscale[c];
+  // finv[c] = 1 / fscale[c].  Scales are powers of two, so the FP32 path and the
+  // round trip through storage lose nothing beyond the storage rounding.
+  int storage;
+  float fscale[6], finv[6];
   // Device status word: a kernel whose bounded wait ran out stores
   // FDTD_ERR_TIMEOUT here (read back by the host after stepping).
   int* status;
@@ -134,6 +141,10 @@ constexpr unsigned kClassCoef = 2u;
 
 // Fill p.warp_class (out) for chunk length p.CX: one warp per task.
 int launch_classify(const StepParams& p, int n_kblocks, int n_chunks, unsigned char* out, cudaStream_t stream);
+
+constexpr int kStoreF32 = 0;
+constexpr int kStoreF16 = 1;
+constexpr int kStoreBF16 = 2;
 
 constexpr unsigned kPlaneHTerms = 1u;
 constexpr unsigned kPlaneETerms = 2u;

@@ -5,6 +5,9 @@
 // 462-941, dispersive.cu:18-83, sources.cu:135-154 and 485-545.
 #pragma once
 
+#include <cuda_bf16.h>
+#include <cuda_fp16.h>
+
 #include "engine.cuh"
 
 namespace fdtdb200 {
@@ -15,6 +18,53 @@ constexpr int kOut = 30;  // output z cells per warp
 constexpr unsigned kFull = 0xffffffffu;
 
 __device__ __forceinline__ float ldz(const float* base, int64_t off, bool ok) { return ok ? __ldg(base + off) : 0.0f; }
+
+// Stored element types: FP32 (the exact path), FP16 and BF16 (reduced storage,
+// FP32 arithmetic).
+__device__ __forceinline__ float to_f32(float x) { return x; }
+__device__ __forceinline__ float to_f32(__half x) { return __half2float(x); }
+__device__ __forceinline__ float to_f32(__nv_bfloat16 x) { return __bfloat162float(x); }
+template <typename T>
+__device__ __forceinline__ T from_f32(float v);
+template <>
+__device__ __forceinline__ float from_f32<float>(float v) { return v; }
+template <>
+__device__ __forceinline__ __half from_f32<__half>(float v) { return __float2half_rn(v); }
+template <>
+__device__ __forceinline__ __nv_bfloat16 from_f32<__nv_bfloat16>(float v) { return __float2bfloat16_rn(v); }
+
+// Field load of stored type TS (scaled by `scale` unless FP32), zero when !ok.
+template <typename TS>
+__device__ __forceinline__ float ldf(const float* base, int64_t off, bool ok, float scale) {
+  if constexpr (sizeof(TS) == 4) {
+    (void)scale;
+    return ok ? __ldg(base + off) : 0.0f;
+  } else {
+    return ok ? to_f32(__ldg(reinterpret_cast<const TS*>(base) + off)) * scale : 0.0f;
+  }
+}
+
+// Streaming field store of type TS (value multiplied by `inv` unless FP32).
+template <typename TS>
+__device__ __forceinline__ void stf(float* base, int64_t off, float v, float inv) {
+  if constexpr (sizeof(TS) == 4) {
+    (void)inv;
+    __stcg(base + off, v);
+  } else {
+    TS* q = reinterpret_cast<TS*>(base) + off;
+    *q = from_f32<TS>(v * inv);
+  }
+}
+
+// ADE state element of type TA (FP32 or BF16, unscaled).
+template <typename TA>
+__device__ __forceinline__ float lda(const float* base, int64_t off) {
+  return to_f32(reinterpret_cast<const TA*>(base)[off]);
+}
+template <typename TA>
+__device__ __forceinline__ void sta(float* base, int64_t off, float v) {
+  reinterpret_cast<TA*>(base)[off] = from_f32<TA>(v);
+}
 
 __device__ __forceinline__ int slab_coord(const StepParams& p, int axis, int coord, int extent) {
   const int lo = p.slab_lo[axis], hi = p.slab_hi[axis];
@@ -92,9 +142,15 @@ __device__ __forceinline__ void add_terms(const StepParams& p, int phase, int ba
 // the plane list already restricts i.  Poles are taken three at a time with
 // every state load issued before the first update, so the load latencies of a
 // multi-component material overlap; the subtractions keep the list order.
+#ifndef FDTD_ADE_BATCH
+// Poles whose state loads are issued together.  1 in the 64-register kernel:
+// a batch of three spills registers there and costs more than it hides.
+#define FDTD_ADE_BATCH 1
+#endif
+template <typename TA = float>
 __device__ __forceinline__ void ade(const StepParams& p, unsigned lane_poles, int i, int j, int k, float e0, float e1,
                                     float e2, float& v0, float& v1, float& v2) {
-  constexpr int kB = 3;
+  constexpr int kB = FDTD_ADE_BATCH;
   const int b = __ldg(p.pole_plane_ptr + i), e = __ldg(p.pole_plane_ptr + i + 1);
   for (int x0 = b; x0 < e; x0 += kB) {
     const PoleTerm* pts[kB];
@@ -120,8 +176,8 @@ __device__ __forceinline__ void ade(const StepParams& p, unsigned lane_poles, in
         offs[u] = o;
         drive[u] = __ldg(pt.drive + o);
         ie[u] = __ldg(pt.inv_eps + o);
-        if (pt.kind != 1) pol[u] = pt.pol[o];
-        if (pt.kind != 0) cur[u] = pt.cur[o];
+        if (pt.kind != 1) pol[u] = lda<TA>(pt.pol, o);
+        if (pt.kind != 0) cur[u] = lda<TA>(pt.cur, o);
       }
     }
 #pragma unroll
@@ -135,17 +191,17 @@ __device__ __forceinline__ void ade(const StepParams& p, unsigned lane_poles, in
       if (pt.kind == 0) {
         const float prev = pol[u];
         const float next = pt.decay * prev + drive[u] * eo;
-        pt.pol[o] = next;
+        sta<TA>(pt.pol, o, next);
         jn = (next - prev) * pt.inv_dt;
-        pt.cur[o] = jn;
+        sta<TA>(pt.cur, o, jn);
       } else if (pt.kind == 1) {
         jn = pt.decay * cur[u] + drive[u] * eo;
-        pt.cur[o] = jn;
+        sta<TA>(pt.cur, o, jn);
       } else {
         const float pl = pol[u];
         jn = pt.decay * cur[u] - pt.restoring * pl + drive[u] * eo;
-        pt.cur[o] = jn;
-        pt.pol[o] = pl + pt.dt * jn;
+        sta<TA>(pt.cur, o, jn);
+        sta<TA>(pt.pol, o, pl + pt.dt * jn);
       }
       const float sub = pt.dt * jn * ie[u];
       if (c == 0) v0 -= sub;

@@ -20,6 +20,8 @@
 // Arithmetic restated from witwin/maxwell/fdtd/cuda/kernels/magnetic.cu:62-212,
 // electric.cu:242-311 and 462-941, dispersive.cu:18-83, sources.cu:135-154 and
 // 485-545, observers.cu:7-78.
+#include <type_traits>
+
 #include "step_device.cuh"
 
 namespace fdtdb200 {
@@ -29,8 +31,13 @@ namespace fdtdb200 {
 // read the per-cell decay/curl arrays (some coefficient of the footprint
 // differs from the background scalars p.*_u).  kUniform: every axis has
 // constant spacing, so the inverse spacings are the scalars p.inv_e_u/inv_h_u.
-template <bool kCpml, bool kCoef, bool kUniform>
+// TS: stored field type (float = the exact FP32 path; __half / __nv_bfloat16 =
+// reduced storage with per-component scales).  ADE pole state is BF16 with
+// BF16 fields and FP32 otherwise (FP16 would need per-pole scales that the
+// source tables do not bound).
+template <typename TS, bool kCpml, bool kCoef, bool kUniform>
 __device__ __forceinline__ void march(const StepParams& p, int n, int lane, int j) {
+  using TA = typename std::conditional<std::is_same<TS, __nv_bfloat16>::value, __nv_bfloat16, float>::type;
   const int NX = p.NX, NY = p.NY, NZ = p.NZ, P = p.P;
   const int k = blockIdx.y * kOut - 1 + lane;
   const bool kok = k >= 0 && k < P;
@@ -94,14 +101,14 @@ __device__ __forceinline__ void march(const StepParams& p, int n, int lane, int 
   float em0, em1, em2, ec0, ec1, ec2, ep0, ep2;
   {
     const int o = istart * ps;
-    em0 = ldz(p.Ein[0], o + rm, kok && jm_ok);
-    em1 = ldz(p.Ein[1], o + rm, kok && jm_ok);
-    em2 = ldz(p.Ein[2], o + rm, kok && jm_ok);
-    ec0 = ldz(p.Ein[0], o + rc, kok);
-    ec1 = ldz(p.Ein[1], o + rc, kok);
-    ec2 = ldz(p.Ein[2], o + rc, kok);
-    ep0 = ldz(p.Ein[0], o + rp, kok && jp_ok);
-    ep2 = ldz(p.Ein[2], o + rp, kok && jp_ok);
+    em0 = ldf<TS>(p.Ein[0], o + rm, kok && jm_ok, p.fscale[0]);
+    em1 = ldf<TS>(p.Ein[1], o + rm, kok && jm_ok, p.fscale[1]);
+    em2 = ldf<TS>(p.Ein[2], o + rm, kok && jm_ok, p.fscale[2]);
+    ec0 = ldf<TS>(p.Ein[0], o + rc, kok, p.fscale[0]);
+    ec1 = ldf<TS>(p.Ein[1], o + rc, kok, p.fscale[1]);
+    ec2 = ldf<TS>(p.Ein[2], o + rc, kok, p.fscale[2]);
+    ep0 = ldf<TS>(p.Ein[0], o + rp, kok && jp_ok, p.fscale[0]);
+    ep2 = ldf<TS>(p.Ein[2], o + rp, kok && jp_ok, p.fscale[2]);
   }
   float hpz = 0.f, hpy = 0.f;  // Hz, Hy of row j at plane i-1
 
@@ -112,20 +119,20 @@ __device__ __forceinline__ void march(const StepParams& p, int n, int lane, int 
     const int on = o + ps;
     const unsigned pb = __ldg(p.plane_bits + i);
     // E^n(i+1) of rows j-1, j, j+1 (the next plane's E^n(i))
-    const float nm0 = ldz(p.Ein[0], on + rm, kok && jm_ok && inext);
-    const float nm1 = ldz(p.Ein[1], on + rm, kok && jm_ok && inext);
-    const float nm2 = ldz(p.Ein[2], on + rm, kok && jm_ok && inext);
-    const float nc0 = ldz(p.Ein[0], on + rc, kok && inext);
-    const float nc1 = ldz(p.Ein[1], on + rc, kok && inext);
-    const float nc2 = ldz(p.Ein[2], on + rc, kok && inext);
-    const float np0 = ldz(p.Ein[0], on + rp, kok && jp_ok && inext);
-    const float np2 = ldz(p.Ein[2], on + rp, kok && jp_ok && inext);
+    const float nm0 = ldf<TS>(p.Ein[0], on + rm, kok && jm_ok && inext, p.fscale[0]);
+    const float nm1 = ldf<TS>(p.Ein[1], on + rm, kok && jm_ok && inext, p.fscale[1]);
+    const float nm2 = ldf<TS>(p.Ein[2], on + rm, kok && jm_ok && inext, p.fscale[2]);
+    const float nc0 = ldf<TS>(p.Ein[0], on + rc, kok && inext, p.fscale[0]);
+    const float nc1 = ldf<TS>(p.Ein[1], on + rc, kok && inext, p.fscale[1]);
+    const float nc2 = ldf<TS>(p.Ein[2], on + rc, kok && inext, p.fscale[2]);
+    const float np0 = ldf<TS>(p.Ein[0], on + rp, kok && jp_ok && inext, p.fscale[0]);
+    const float np2 = ldf<TS>(p.Ein[2], on + rp, kok && jp_ok && inext, p.fscale[2]);
     // H^{n-1/2}(i) of rows j-1 and j
-    const float hm0 = ldz(p.Hin[0], o + rm, kok && jm_ok);
-    const float hm2 = ldz(p.Hin[2], o + rm, kok && jm_ok);
-    const float hc0 = ldz(p.Hin[0], o + rc, kok);
-    const float hc1 = ldz(p.Hin[1], o + rc, kok);
-    const float hc2 = ldz(p.Hin[2], o + rc, kok);
+    const float hm0 = ldf<TS>(p.Hin[0], o + rm, kok && jm_ok, p.fscale[3]);
+    const float hm2 = ldf<TS>(p.Hin[2], o + rm, kok && jm_ok, p.fscale[5]);
+    const float hc0 = ldf<TS>(p.Hin[0], o + rc, kok, p.fscale[3]);
+    const float hc1 = ldf<TS>(p.Hin[1], o + rc, kok, p.fscale[4]);
+    const float hc2 = ldf<TS>(p.Hin[2], o + rc, kok, p.fscale[5]);
     const bool ix_ok = i < NX - 1;
     const bool mx_ok = jm_ok && hz_kok, mz_ok = jm_ok && ix_ok && ez_kok;
     const bool cx_ok = yc_ok && hz_kok, cy_ok = ix_ok && hz_kok, cz_ok = ix_ok && yc_ok && ez_kok;
@@ -235,9 +242,9 @@ __device__ __forceinline__ void march(const StepParams& p, int n, int lane, int 
       add_terms(p, 1, 3, n, i, j, k, pb & kPlaneHTerms, lf & kLfHTermYc, lf & kLfHTermZ, hcx, hcy, hcz);
     }
     if (own && out_lane) {
-      __stcg(p.Hout[0] + o + rc, hcx);
-      __stcg(p.Hout[1] + o + rc, hcy);
-      __stcg(p.Hout[2] + o + rc, hcz);
+      stf<TS>(p.Hout[0], o + rc, hcx, p.finv[3]);
+      stf<TS>(p.Hout[1], o + rc, hcy, p.finv[4]);
+      stf<TS>(p.Hout[2], o + rc, hcz, p.finv[5]);
     }
 
     // ---------------- E^{n+1}(i), row j ----------------
@@ -278,12 +285,12 @@ __device__ __forceinline__ void march(const StepParams& p, int n, int lane, int 
       float v2 = pick(m2, ec2 * g2 + c2 * (d2a - d2b), ec2);
       // ADE subtraction, TFSF electric corrections and soft sources: the
       // additive terms of witwin/maxwell/fdtd/runtime/stepping.py:2295-2320.
-      if (pb & kPlanePoles) ade(p, lane_poles, i, j, k, ec0, ec1, ec2, v0, v1, v2);
+      if (pb & kPlanePoles) ade<TA>(p, lane_poles, i, j, k, ec0, ec1, ec2, v0, v1, v2);
       if ((pb & kPlaneETerms) || (lf & (kLfETermY | kLfETermZ)))
         add_terms(p, 0, 0, n, i, j, k, pb & kPlaneETerms, lf & kLfETermY, lf & kLfETermZ, v0, v1, v2);
-      __stcg(p.Eout[0] + o + rc, v0);
-      __stcg(p.Eout[1] + o + rc, v1);
-      __stcg(p.Eout[2] + o + rc, v2);
+      stf<TS>(p.Eout[0], o + rc, v0, p.finv[0]);
+      stf<TS>(p.Eout[1], o + rc, v1, p.finv[1]);
+      stf<TS>(p.Eout[2], o + rc, v2, p.finv[2]);
     }
     hpz = hcz;
     hpy = hcy;
@@ -312,12 +319,58 @@ __global__ void __launch_bounds__(256, kMinBlocks) warp_step_kernel(const StepPa
   if (kAnyCpml || kAnyCoef)
     cls = __ldg(p.warp_class + (static_cast<int64_t>(blockIdx.z) * gridDim.y + blockIdx.y) * p.NY + j);
   if (kAnyCpml && (cls & kClassCpml)) {
-    if (kAnyCoef && (cls & kClassCoef)) march<true, true, kUniform>(p, n, lane, j);
-    else march<true, false, kUniform>(p, n, lane, j);
+    if (kAnyCoef && (cls & kClassCoef)) march<float, true, true, kUniform>(p, n, lane, j);
+    else march<float, true, false, kUniform>(p, n, lane, j);
   } else {
-    if (kAnyCoef && (cls & kClassCoef)) march<false, true, kUniform>(p, n, lane, j);
-    else march<false, false, kUniform>(p, n, lane, j);
+    if (kAnyCoef && (cls & kClassCoef)) march<float, false, true, kUniform>(p, n, lane, j);
+    else march<float, false, false, kUniform>(p, n, lane, j);
   }
+}
+
+// Reduced-storage step kernel (TS = __half or __nv_bfloat16): the 64-register
+// launch of warp_step_kernel with fields in TS and ADE state in BF16.
+template <typename TS, bool kAnyCpml, bool kAnyCoef, bool kUniform>
+__global__ void __launch_bounds__(256, 4) warp_step_kernel_rs(const StepParams p, int n) {
+  const int lane = threadIdx.x & 31;
+  const int j = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  if (j >= p.NY) return;
+  unsigned cls = 0;
+  if (kAnyCpml || kAnyCoef)
+    cls = __ldg(p.warp_class + (static_cast<int64_t>(blockIdx.z) * gridDim.y + blockIdx.y) * p.NY + j);
+  if (kAnyCpml && (cls & kClassCpml)) {
+    if (kAnyCoef && (cls & kClassCoef)) march<TS, true, true, kUniform>(p, n, lane, j);
+    else march<TS, true, false, kUniform>(p, n, lane, j);
+  } else {
+    if (kAnyCoef && (cls & kClassCoef)) march<TS, false, true, kUniform>(p, n, lane, j);
+    else march<TS, false, false, kUniform>(p, n, lane, j);
+  }
+}
+
+int launch_step_reduced(const StepParams& p, int n, dim3 grid, bool cpml, bool coef, bool uni, cudaStream_t stream) {
+#define FDTD_RS_PICK(TS)                                                                   \
+  do {                                                                                     \
+    if (uni) {                                                                             \
+      if (cpml) {                                                                          \
+        if (coef) warp_step_kernel_rs<TS, true, true, true><<<grid, 256, 0, stream>>>(p, n);   \
+        else warp_step_kernel_rs<TS, true, false, true><<<grid, 256, 0, stream>>>(p, n);       \
+      } else {                                                                             \
+        if (coef) warp_step_kernel_rs<TS, false, true, true><<<grid, 256, 0, stream>>>(p, n);  \
+        else warp_step_kernel_rs<TS, false, false, true><<<grid, 256, 0, stream>>>(p, n);      \
+      }                                                                                    \
+    } else {                                                                               \
+      if (cpml) {                                                                          \
+        if (coef) warp_step_kernel_rs<TS, true, true, false><<<grid, 256, 0, stream>>>(p, n);  \
+        else warp_step_kernel_rs<TS, true, false, false><<<grid, 256, 0, stream>>>(p, n);      \
+      } else {                                                                             \
+        if (coef) warp_step_kernel_rs<TS, false, true, false><<<grid, 256, 0, stream>>>(p, n); \
+        else warp_step_kernel_rs<TS, false, false, false><<<grid, 256, 0, stream>>>(p, n);     \
+      }                                                                                    \
+    }                                                                                      \
+  } while (0)
+  if (p.storage == kStoreF16) FDTD_RS_PICK(__half);
+  else FDTD_RS_PICK(__nv_bfloat16);
+#undef FDTD_RS_PICK
+  return static_cast<int>(cudaGetLastError());
 }
 
 namespace {

@@ -27,6 +27,13 @@ def _require_cuda(device: torch.device) -> None:
         raise RuntimeError("B200FDTD requires a CUDA device; there is no CPU path")
 
 
+# Field storage kinds of the engine (fdtd_engine_set_storage): FP32 is the exact
+# path; FP16 / BF16 store E and H in 16 bits with per-component power-of-two
+# scales (arithmetic stays FP32; ADE pole state is FP32 with FP16 fields and
+# BF16 with BF16 fields).
+STORAGE_KINDS = {"fp32": 0, "fp16": 1, "bf16": 2}
+
+
 class B200FDTD:
     def __init__(
         self,
@@ -36,7 +43,13 @@ class B200FDTD:
         sample_block: int = 32,
         tile_rows: int = 0,
         chunk_planes: int = 0,
+        storage: str = "fp32",
+        storage_scales=None,
     ):
+        if storage not in STORAGE_KINDS:
+            raise ValueError(f"storage must be one of {sorted(STORAGE_KINDS)}")
+        self.storage = storage
+        self.storage_scales_arg = None if storage_scales is None else [float(x) for x in storage_scales]
         self.compiled = compiled
         self.device = torch.device(device if device is not None else "cuda")
         _require_cuda(self.device)
@@ -79,6 +92,13 @@ class B200FDTD:
                        "fdtd_engine_create")
             self.handle = handle
             h = handle
+            if self.storage != "fp32" or self.storage_scales_arg is not None:
+                sc = None
+                if self.storage_scales_arg is not None:
+                    if len(self.storage_scales_arg) != 6:
+                        raise ValueError("storage_scales needs six values (Ex, Ey, Ez, Hx, Hy, Hz)")
+                    sc = (ctypes.c_float * 6)(*self.storage_scales_arg)
+                _lib.check(lib.fdtd_engine_set_storage(h, STORAGE_KINDS[self.storage], sc), "set_storage")
             for a in range(3):
                 _lib.check(lib.fdtd_engine_set_spacing(h, a, _lib.ptr(self._dev(cs.inv_e[a])), _lib.ptr(self._dev(cs.inv_h[a]))),
                            "set_spacing")
@@ -189,6 +209,14 @@ class B200FDTD:
 
     def set_launch(self, variant: int, tile_rows: int = 0, chunk_planes: int = 0) -> None:
         _lib.check(self.lib.fdtd_engine_set_launch(self.handle, int(variant), int(tile_rows), int(chunk_planes)), "set_launch")
+
+    def storage_scales(self) -> tuple[str, list[float]]:
+        """The engine's field storage kind and per-component scales (Ex..Hz)."""
+        kind = ctypes.c_int()
+        sc = (ctypes.c_float * 6)()
+        _lib.check(self.lib.fdtd_engine_get_storage(self.handle, ctypes.byref(kind), sc), "get_storage")
+        name = {v: k for k, v in STORAGE_KINDS.items()}[kind.value]
+        return name, [float(x) for x in sc]
 
     def get_launch(self) -> tuple[int, int, int]:
         v, ty, cx = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
