@@ -196,6 +196,26 @@ int fdtd_engine_time_kernel(fdtd_engine* h, int n, int reps, float* ms);
 /* Device time of the last step_range in milliseconds (CUDA events). */
 int fdtd_engine_last_ms(fdtd_engine* h, float* ms);
 
+/* Batched scenes: independent engines (finalized, created on `stream`, with
+ * one common even sample block M) stepped together.  Each block of M steps of
+ * every engine is captured once into a CUDA graph in which every engine runs
+ * on its own stream forked from `stream`, so the small scenes of a design
+ * batch fill the GPU together; the graph is replayed for every block (the
+ * block's base step is written to each engine's device-side base before the
+ * replay) and the remaining steps run as direct launches.  Results equal the
+ * engines stepped one by one.  No counterpart in the reference, which steps
+ * one scene per Simulation (witwin/maxwell/fdtd/runtime/stepping.py:2289-2345).
+ * While a batch exists its engines are stepped only through it. */
+typedef struct fdtd_batch fdtd_batch;
+int fdtd_batch_create(fdtd_engine* const* engines, int n, void* stream, fdtd_batch** out);
+int fdtd_batch_destroy(fdtd_batch* b);
+/* Launch-shape autotune per size class (node counts rounded to 32): the first
+ * engine of each class runs fdtd_engine_autotune, the others take its pick. */
+int fdtd_batch_autotune(fdtd_batch* b);
+int fdtd_batch_step_range(fdtd_batch* b, int n0, int n1);
+int fdtd_batch_last_ms(fdtd_batch* b, float* ms);
+int fdtd_batch_info(fdtd_batch* b, int* n_engines, int* block_steps, int64_t* graph_launches);
+
 /* Reverse-time adjoint: the exact discrete transpose of the fused step (H and
  * E updates, CPML psi, E edge modes), monitor seeds and dL/deps of design
  * boxes.  Replaces the reference's native reverse runners

@@ -83,7 +83,7 @@ def test_reduced_storage_state_round_trip_and_limits():
     estimated from the sources; launch variants other than 2 and the adjoint
     are refused."""
     wm = load_package()
-    cs = wm.compile_scene(wm.workloads.plain_small(cells=24, pml=4), 10)
+    cs = wm.compile_scene(wm.workloads.plain_small(cells=32, pml=4), 10)
     solver = wm.solver.B200FDTD(cs, storage="fp16").init_field()
     kind, scales = solver.storage_scales()
     assert kind == "fp16"
@@ -110,7 +110,7 @@ def test_reduced_storage_state_round_trip_and_limits():
 
 def test_explicit_scales_must_be_powers_of_two():
     wm = load_package()
-    cs = wm.compile_scene(wm.workloads.plain_small(cells=24, pml=4), 10)
+    cs = wm.compile_scene(wm.workloads.plain_small(cells=32, pml=4), 10)
     with pytest.raises(wm._lib.FdtdError):
         wm.solver.B200FDTD(cs, storage="fp16", storage_scales=[0.3] * 6).init_field()
     solver = wm.solver.B200FDTD(cs, storage="fp16", storage_scales=[0.25] * 3 + [2.0 ** -10] * 3).init_field()

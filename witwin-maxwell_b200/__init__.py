@@ -2,7 +2,8 @@
 
 Modules:
     scene       scene description and compilation into solver-scene tensors
-    solver      B200FDTD: the fused sm_100a step engine behind the FDTD solve contract
+    solver      B200FDTD: the fused sm_100a step engine behind the FDTD solve contract;
+                B200Batch: independent scenes stepped together (graph-captured blocks)
     backend     NativeFDTDModule-compatible per-op surface (camelCase kernel names)
     simulation  Simulation.fdtd(...).run() -> Result facade
     adjoint     reverse-time adjoint: dL/deps_r of a design region (torch.autograd.Function)
@@ -48,6 +49,10 @@ def __getattr__(name):
         from .solver import B200FDTD
 
         return B200FDTD
+    if name == "B200Batch":
+        from .solver import B200Batch
+
+        return B200Batch
     if name == "Simulation":
         from .simulation import Simulation
 

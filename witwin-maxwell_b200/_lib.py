@@ -41,6 +41,12 @@ _SIGNATURES = {
     "fdtd_version": ([], ctypes.c_char_p),
     "fdtd_engine_create": ([ctypes.POINTER(FdtdGridDesc), _vp, ctypes.POINTER(_vp)], _i),
     "fdtd_engine_destroy": ([_vp], _i),
+    "fdtd_batch_create": ([_vp, _i, _vp, ctypes.POINTER(_vp)], _i),
+    "fdtd_batch_destroy": ([_vp], _i),
+    "fdtd_batch_autotune": ([_vp], _i),
+    "fdtd_batch_step_range": ([_vp, _i, _i], _i),
+    "fdtd_batch_last_ms": ([_vp, ctypes.POINTER(_f)], _i),
+    "fdtd_batch_info": ([_vp, _c_int_p, _c_int_p, _c_i64_p], _i),
     "fdtd_engine_set_storage": ([_vp, _i, _vp], _i),
     "fdtd_engine_get_storage": ([_vp, _c_int_p, _vp], _i),
     "fdtd_engine_set_spacing": ([_vp, _i, _vp, _vp], _i),

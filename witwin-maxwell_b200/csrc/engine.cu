@@ -240,8 +240,9 @@ __global__ void sample_gather_kernel(const RegionFlush* regions, const FieldPtrs
 // compensation of the accumulator update.
 __global__ void dft_flush_kernel(const float* samples, int64_t n_samples, int cnt, int n_base, int n_freq,
                                  const float2* w_e, const float2* w_h, const RegionFlush* regions,
-                                 float* acc_re, float* acc_im, float* cmp_re, float* cmp_im) {
+                                 float* acc_re, float* acc_im, float* cmp_re, float* cmp_im, const int* base_dev) {
   extern __shared__ float2 sw[];  // [cnt][n_freq]
+  if (base_dev) n_base += __ldg(base_dev);
   const RegionFlush rg = regions[blockIdx.y];
   const float2* w = rg.is_h ? w_h : w_e;
   for (int x = threadIdx.x; x < cnt * n_freq; x += blockDim.x) {
@@ -355,6 +356,12 @@ struct fdtd_engine {
   int storage = 0;
   float fscale[6] = {1, 1, 1, 1, 1, 1};
   bool scales_set = false;
+  // Graph-captured step blocks (fdtd_batch_*): while graph_base is set the
+  // launches carry step indices relative to graph_n0 and read the block's base
+  // step from d_base.
+  int* d_base = nullptr;
+  bool graph_base = false;
+  int graph_n0 = 0;
   int64_t plane = 0, vol = 0;
   int TY = 0, CX = 0;
   // Fused kernel: 1..3 = register-prefetch warp kernel with a register budget
@@ -516,6 +523,7 @@ void fill_params(const fdtd_engine* h, StepParams& p) {
   p.P = h->P;
   p.SZ = h->SZ;
   p.storage = h->storage;
+  p.step_base = h->graph_base ? h->d_base : nullptr;
   for (int c = 0; c < 6; ++c) {
     p.fscale[c] = h->fscale[c];
     p.finv[c] = 1.0f / h->fscale[c];
@@ -628,6 +636,27 @@ int check_status(fdtd_engine* h) {
   return 0;
 }
 
+bool has_coef(const fdtd_engine* h) {
+  for (int c = 0; c < 6; ++c)
+    if (h->ecoef[c][0] || h->ecoef[c][1]) return true;
+  return false;
+}
+
+// Build the per-warp class table for the current launch shape if it is stale.
+int ensure_classified(fdtd_engine* h, const StepParams& p) {
+  const dim3 grid = step_grid(h);
+  const int V = variant_v(h->variant);
+  const int key = h->CX * 8 + V;
+  if ((h->cpml || has_coef(h)) && h->class_key != key) {
+    const int err = V == 1 ? launch_classify(p, static_cast<int>(grid.y), static_cast<int>(grid.z), h->d_warp_class, h->stream)
+                           : launch_classify_vec(p, V, static_cast<int>(grid.y), static_cast<int>(grid.z), h->d_warp_class,
+                                                 h->stream);
+    if (err != 0) return cuda_fail(static_cast<cudaError_t>(err), "classify_kernel launch");
+    h->class_key = key;
+  }
+  return 0;
+}
+
 int launch_step(fdtd_engine* h, int n, int slot) {
   StepParams p;
   fill_params(h, p);
@@ -637,14 +666,9 @@ int launch_step(fdtd_engine* h, int n, int slot) {
   const int block = kWarpRows * 32;
   if (h->variant == 4 && !h->tma_ready)
     return fail(FDTD_ERR_UNSUPPORTED, "TMA step kernel unavailable (no tensor-map driver entry point)");
-  const int V = variant_v(h->variant);
-  const int key = h->CX * 8 + V;
-  if ((h->cpml || coef) && h->class_key != key) {
-    const int err = V == 1 ? launch_classify(p, static_cast<int>(grid.y), static_cast<int>(grid.z), h->d_warp_class, h->stream)
-                           : launch_classify_vec(p, V, static_cast<int>(grid.y), static_cast<int>(grid.z), h->d_warp_class,
-                                                 h->stream);
-    if (err != 0) return cuda_fail(static_cast<cudaError_t>(err), "classify_kernel launch");
-    h->class_key = key;
+  {
+    const int rc = ensure_classified(h, p);
+    if (rc) return rc;
   }
   if (h->storage != kStoreF32) {
     const int err = launch_step_reduced(p, n, grid, h->cpml, coef, h->uniform_grid, h->stream);
@@ -711,9 +735,11 @@ int flush_samples(fdtd_engine* h) {
     const int gx = static_cast<int>(std::min<int64_t>((h->max_region + threads - 1) / threads, 4096));
     const dim3 grid(std::max(gx, 1), h->n_flush);
     const size_t smem = sizeof(float2) * static_cast<size_t>(h->pending) * h->n_freq;
-    dft_flush_kernel<<<grid, threads, smem, h->stream>>>(h->samples, h->n_samples, h->pending, h->pending_base,
-                                                           h->n_freq, h->w_e, h->w_h, h->d_flush, h->acc_re,
-                                                           h->acc_im, h->cmp_re, h->cmp_im);
+    // In a captured step block the weights start at the block's device-side base step.
+    const int n_base = h->graph_base ? h->pending_base - h->graph_n0 : h->pending_base;
+    dft_flush_kernel<<<grid, threads, smem, h->stream>>>(h->samples, h->n_samples, h->pending, n_base, h->n_freq,
+                                                           h->w_e, h->w_h, h->d_flush, h->acc_re, h->acc_im,
+                                                           h->cmp_re, h->cmp_im, h->graph_base ? h->d_base : nullptr);
     cudaError_t err = cudaGetLastError();
     if (err != cudaSuccess) return cuda_fail(err, "dft_flush_kernel launch");
     ++h->launches;
@@ -902,6 +928,7 @@ int fdtd_engine_destroy(fdtd_engine* h) {
   cudaFree(h->d_warp_class);
   for (float* p : h->adj.bufs) cudaFree(p);
   cudaFree(h->d_status);
+  cudaFree(h->d_base);
   cudaFree(h->samples);
   cudaFree(h->w_e);
   cudaFree(h->w_h);
@@ -1498,6 +1525,8 @@ int fdtd_engine_finalize(fdtd_engine* h) {
     h->class_key = 0;
     CUDA_TRY(cudaMalloc(&h->d_status, sizeof(int)));
     CUDA_TRY(cudaMemsetAsync(h->d_status, 0, sizeof(int), h->stream));
+    CUDA_TRY(cudaMalloc(&h->d_base, sizeof(int)));
+    CUDA_TRY(cudaMemsetAsync(h->d_base, 0, sizeof(int), h->stream));
   }
   {
     // TMA maps of both ping-pong buffers; without the driver entry point the
@@ -1970,6 +1999,285 @@ int fdtd_engine_info(fdtd_engine* h, int* tile_rows, int* chunk_planes, int* gri
 int fdtd_engine_last_ms(fdtd_engine* h, float* ms) {
   if (!h || !ms) return fail(FDTD_ERR_INVALID_ARG, "bad arguments");
   *ms = h->last_ms;
+  return 0;
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Batched scenes: independent engines stepped together.  A block of M steps
+// (M = the engines' common monitor sample block) of every engine is captured
+// once into one CUDA graph: each engine's launches go to its own stream forked
+// from the batch stream, so the kernels of all scenes run concurrently and
+// small scenes fill the GPU together.  The graph holds step indices relative
+// to the block start; the block's base step is written to every engine's
+// device-side base before each replay, so one graph serves the whole range.
+// ---------------------------------------------------------------------------
+namespace {
+__global__ void set_bases_kernel(int* const* bases, int n, int value) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) *bases[i] = value;
+}
+}  // namespace
+
+struct fdtd_batch {
+  std::vector<fdtd_engine*> eng;
+  cudaStream_t stream = nullptr;
+  std::vector<cudaStream_t> streams;
+  std::vector<cudaEvent_t> join;
+  cudaEvent_t fork = nullptr, ev0 = nullptr, ev1 = nullptr;
+  // capture origin: the batch stream may be the legacy default stream, on
+  // which capture is not permitted
+  cudaStream_t cap = nullptr;
+  int** d_bases = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  int M = 0;
+  float last_ms = 0.0f;
+  int64_t graph_launches = 0;
+};
+
+static void batch_release_graph(fdtd_batch* b) {
+  if (b->exec) cudaGraphExecDestroy(b->exec);
+  b->exec = nullptr;
+}
+
+// Capture one M-step block of every engine into b->exec.
+static int batch_capture(fdtd_batch* b) {
+  for (fdtd_engine* h : b->eng) {
+    StepParams p;
+    fill_params(h, p);
+    const int rc = ensure_classified(h, p);
+    if (rc) return rc;
+  }
+  CUDA_TRY(cudaStreamSynchronize(b->stream));
+  CUDA_TRY(cudaStreamBeginCapture(b->cap, cudaStreamCaptureModeRelaxed));
+  int rc = 0;
+  cudaError_t err = cudaEventRecord(b->fork, b->cap);
+  for (size_t i = 0; i < b->eng.size() && err == cudaSuccess && rc == 0; ++i) {
+    fdtd_engine* h = b->eng[i];
+    err = cudaStreamWaitEvent(b->streams[i], b->fork, 0);
+    if (err != cudaSuccess) break;
+    const int64_t launches0 = h->launches;
+    const int cur0 = h->cur, pending0 = h->pending, base0 = h->pending_base;
+    h->stream = b->streams[i];
+    h->graph_base = true;
+    h->graph_n0 = 0;
+    h->pending = 0;
+    h->pending_base = 0;
+    for (int s = 0; s < b->M && rc == 0; ++s) {
+      rc = launch_step(h, s, h->n_samples > 0 ? h->pending : -1);
+      if (h->n_samples > 0) ++h->pending;
+    }
+    if (rc == 0) rc = flush_samples(h);
+    h->stream = b->stream;
+    h->graph_base = false;
+    h->launches = launches0;
+    h->cur = cur0;  // M is even: the captured block returns the ping-pong to its start
+    h->pending = pending0;
+    h->pending_base = base0;
+    if (rc == 0) err = cudaEventRecord(b->join[i], b->streams[i]);
+    if (rc == 0 && err == cudaSuccess) err = cudaStreamWaitEvent(b->cap, b->join[i], 0);
+  }
+  cudaGraph_t graph = nullptr;
+  const cudaError_t end = cudaStreamEndCapture(b->cap, &graph);
+  if (rc || err != cudaSuccess || end != cudaSuccess) {
+    if (graph) cudaGraphDestroy(graph);
+    if (rc) return rc;
+    return cuda_fail(err != cudaSuccess ? err : end, "batch capture");
+  }
+  const cudaError_t inst = cudaGraphInstantiate(&b->exec, graph, 0);
+  cudaGraphDestroy(graph);
+  if (inst != cudaSuccess) {
+    b->exec = nullptr;
+    return cuda_fail(inst, "cudaGraphInstantiate");
+  }
+  return 0;
+}
+
+extern "C" {
+
+int fdtd_batch_create(fdtd_engine* const* engines, int n, void* stream, fdtd_batch** out) {
+  if (!engines || n < 1 || !out) return fail(FDTD_ERR_INVALID_ARG, "bad batch arguments");
+  *out = nullptr;
+  const cudaStream_t st = static_cast<cudaStream_t>(stream);
+  int M = -1;
+  for (int i = 0; i < n; ++i) {
+    fdtd_engine* h = engines[i];
+    if (!h || !h->finalized) return fail(FDTD_ERR_STATE, "every batch engine must be finalized");
+    if (h->stream != st) return fail(FDTD_ERR_INVALID_ARG, "batch engines must be created on the batch stream");
+    if (M < 0) M = h->M;
+    if (h->M != M) return fail(FDTD_ERR_INVALID_ARG, "batch engines need the same sample block");
+    for (int k = 0; k < i; ++k)
+      if (engines[k] == h) return fail(FDTD_ERR_INVALID_ARG, "an engine appears twice in the batch");
+  }
+  if (M % 2 != 0) return fail(FDTD_ERR_INVALID_ARG, "the batch step block (sample block) must be even");
+  fdtd_batch* b = new fdtd_batch();
+  b->eng.assign(engines, engines + n);
+  b->stream = st;
+  b->M = M;
+  b->streams.resize(n, nullptr);
+  b->join.resize(n, nullptr);
+  cudaError_t err = cudaEventCreateWithFlags(&b->fork, cudaEventDisableTiming);
+  if (err == cudaSuccess) err = cudaEventCreate(&b->ev0);
+  if (err == cudaSuccess) err = cudaEventCreate(&b->ev1);
+  if (err == cudaSuccess) err = cudaStreamCreateWithFlags(&b->cap, cudaStreamNonBlocking);
+  for (int i = 0; i < n && err == cudaSuccess; ++i) {
+    err = cudaStreamCreateWithFlags(&b->streams[i], cudaStreamNonBlocking);
+    if (err == cudaSuccess) err = cudaEventCreateWithFlags(&b->join[i], cudaEventDisableTiming);
+  }
+  if (err == cudaSuccess) err = cudaMalloc(&b->d_bases, sizeof(int*) * n);
+  if (err == cudaSuccess) {
+    std::vector<int*> bases(n);
+    for (int i = 0; i < n; ++i) bases[i] = engines[i]->d_base;
+    err = cudaMemcpy(b->d_bases, bases.data(), sizeof(int*) * n, cudaMemcpyHostToDevice);
+  }
+  if (err != cudaSuccess) {
+    const int rc = cuda_fail(err, "batch create");
+    fdtd_batch_destroy(b);
+    return rc;
+  }
+  *out = b;
+  return 0;
+}
+
+int fdtd_batch_destroy(fdtd_batch* b) {
+  if (!b) return 0;
+  if (b->stream) cudaStreamSynchronize(b->stream);
+  batch_release_graph(b);
+  for (cudaStream_t s : b->streams)
+    if (s) cudaStreamDestroy(s);
+  for (cudaEvent_t e : b->join)
+    if (e) cudaEventDestroy(e);
+  if (b->cap) cudaStreamDestroy(b->cap);
+  if (b->fork) cudaEventDestroy(b->fork);
+  if (b->ev0) cudaEventDestroy(b->ev0);
+  if (b->ev1) cudaEventDestroy(b->ev1);
+  cudaFree(b->d_bases);
+  delete b;
+  return 0;
+}
+
+int fdtd_batch_autotune(fdtd_batch* b) {
+  if (!b) return fail(FDTD_ERR_INVALID_ARG, "null batch");
+  // One autotune per size class (node counts rounded to 32, CPML or not): the
+  // class's first engine times the launch variants and chunk lengths, the
+  // others take its pick.
+  std::vector<std::pair<std::vector<int>, fdtd_engine*>> classes;
+  for (fdtd_engine* h : b->eng) {
+    const std::vector<int> key = {(h->NX + 16) / 32, (h->NY + 16) / 32, (h->NZ + 16) / 32, h->cpml ? 1 : 0};
+    fdtd_engine* rep = nullptr;
+    for (auto& c : classes)
+      if (c.first == key) rep = c.second;
+    if (!rep) {
+      int ty = 0, cx = 0;
+      const int rc = fdtd_engine_autotune(h, &ty, &cx);
+      if (rc) return rc;
+      classes.push_back({key, h});
+    } else {
+      const int rc = fdtd_engine_set_launch(h, rep->variant, 1, rep->CX);
+      if (rc) return rc;
+    }
+  }
+  batch_release_graph(b);
+  return 0;
+}
+
+int fdtd_batch_step_range(fdtd_batch* b, int n0, int n1) {
+  if (!b) return fail(FDTD_ERR_INVALID_ARG, "null batch");
+  if (n1 < n0 || n0 < 0) return fail(FDTD_ERR_INVALID_ARG, "bad step range");
+  for (fdtd_engine* h : b->eng) {
+    for (const auto& t : h->terms)
+      if (t.signal && n1 > t.aux_len) return fail(FDTD_ERR_INVALID_ARG, "source signal table shorter than the range");
+    for (const auto& l : h->lines)
+      if (n1 > l.n_steps) return fail(FDTD_ERR_INVALID_ARG, "incident line history shorter than the range");
+    if (h->n_samples > 0 && h->n_freq > 0 && n1 > h->dft_steps)
+      return fail(FDTD_ERR_INVALID_ARG, "DFT weight table shorter than the range");
+    if (h->stream != b->stream) return fail(FDTD_ERR_STATE, "a batch engine moved to another stream");
+  }
+  CUDA_TRY(cudaEventRecord(b->ev0, b->stream));
+  // Monitor samples are flushed into the DFT sums in the same groups as
+  // fdtd_engine_step_range would (a partial block stays pending across calls),
+  // so a batch gives the spectra of the engines stepped one by one.  Samples
+  // that do not continue at n0, or engines whose pending counts differ, are
+  // flushed first.
+  bool aligned = true;
+  for (fdtd_engine* h : b->eng) {
+    if (h->pending > 0 && h->pending_base + h->pending != n0) {
+      const int rc = flush_samples(h);
+      if (rc) return rc;
+    }
+    aligned = aligned && h->pending == b->eng[0]->pending;
+  }
+  if (!aligned) {
+    for (fdtd_engine* h : b->eng) {
+      const int rc = flush_samples(h);
+      if (rc) return rc;
+    }
+  }
+  // direct launches of [from, to) for every engine, as in fdtd_engine_step_range
+  auto direct = [&](int from, int to) -> int {
+    for (fdtd_engine* h : b->eng) {
+      for (int t = from; t < to; ++t) {
+        if (h->pending == 0) h->pending_base = t;
+        int rc = launch_step(h, t, h->pending);
+        if (rc) return rc;
+        if (h->n_samples > 0 && ++h->pending == h->M) {
+          rc = flush_samples(h);
+          if (rc) return rc;
+        }
+      }
+    }
+    return 0;
+  };
+  int n = n0;
+  // complete a pending partial block first, so graph blocks start with no samples pending
+  const int lead = b->eng[0]->pending > 0 ? std::min(n1 - n0, b->M - b->eng[0]->pending) : 0;
+  if (lead > 0) {
+    const int rc = direct(n, n + lead);
+    if (rc) return rc;
+    n += lead;
+  }
+  const int N = static_cast<int>(b->eng.size());
+  bool empty = true;
+  for (fdtd_engine* h : b->eng) empty = empty && h->pending == 0;
+  while (empty && n + b->M <= n1) {
+    if (!b->exec) {
+      const int rc = batch_capture(b);
+      if (rc) return rc;
+    }
+    set_bases_kernel<<<(N + 127) / 128, 128, 0, b->stream>>>(b->d_bases, N, n);
+    CUDA_TRY(cudaGetLastError());
+    CUDA_TRY(cudaGraphLaunch(b->exec, b->stream));
+    ++b->graph_launches;
+    n += b->M;
+    for (fdtd_engine* h : b->eng) h->pending_base = n;
+  }
+  {
+    // tail steps (fewer than a block) run as direct launches; their samples stay pending
+    const int rc = direct(n, n1);
+    if (rc) return rc;
+  }
+  CUDA_TRY(cudaEventRecord(b->ev1, b->stream));
+  CUDA_TRY(cudaEventSynchronize(b->ev1));
+  CUDA_TRY(cudaEventElapsedTime(&b->last_ms, b->ev0, b->ev1));
+  for (fdtd_engine* h : b->eng) {
+    const int rc = check_status(h);
+    if (rc) return rc;
+  }
+  return 0;
+}
+
+int fdtd_batch_last_ms(fdtd_batch* b, float* ms) {
+  if (!b || !ms) return fail(FDTD_ERR_INVALID_ARG, "bad arguments");
+  *ms = b->last_ms;
+  return 0;
+}
+
+int fdtd_batch_info(fdtd_batch* b, int* n_engines, int* block_steps, int64_t* graph_launches) {
+  if (!b) return fail(FDTD_ERR_INVALID_ARG, "null batch");
+  if (n_engines) *n_engines = static_cast<int>(b->eng.size());
+  if (block_steps) *block_steps = b->M;
+  if (graph_launches) *graph_launches = b->graph_launches;
   return 0;
 }
 

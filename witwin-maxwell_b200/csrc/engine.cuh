@@ -128,6 +128,9 @@ struct StepParams {
   // round trip through storage lose nothing beyond the storage rounding.
   int storage;
   float fscale[6], finv[6];
+  // When set, the step index of a launch is *step_base + n (graph-captured
+  // step blocks whose base step is written before each replay); else n.
+  const int* step_base;
   // Device status word: a kernel whose bounded wait ran out stores
   // FDTD_ERR_TIMEOUT here (read back by the host after stepping).
   int* status;

@@ -387,6 +387,7 @@ __device__ __forceinline__ void tma_march(const StepParams& p, const Ring& ring,
 // warps + 1 producer warp; dynamic shared memory = tma_smem_bytes().
 template <bool kAnyCpml, bool kAnyCoef, bool kUniform>
 __global__ void __launch_bounds__(kTmaThreads, 3) tma_step_kernel(const StepParams p, const __grid_constant__ TmaMaps maps, int n) {
+  if (p.step_base) n += __ldg(p.step_base);
   extern __shared__ unsigned char smem_raw[];
   float* stages = reinterpret_cast<float*>((reinterpret_cast<uintptr_t>(smem_raw) + 127) & ~uintptr_t(127));
   uint64_t* bars = reinterpret_cast<uint64_t*>(stages + kStages * kStageFloats);

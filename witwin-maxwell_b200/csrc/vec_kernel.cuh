@@ -878,6 +878,7 @@ __global__ void classify_vec_kernel(const StepParams p, int n_kblocks, int n_chu
 // warp runs the cheapest march that is exact for its footprint class.
 template <int V, int D, bool kAnyCpml, bool kAnyCoef, bool kUniform, int kMinBlocks>
 __global__ void __launch_bounds__(256, kMinBlocks) vec_step_kernel(const StepParams p, int n) {
+  if (p.step_base) n += __ldg(p.step_base);
   const int lane = threadIdx.x & 31;
   const int j = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
   if (j >= p.NY) return;  // whole warp; this kernel has no block-level barrier

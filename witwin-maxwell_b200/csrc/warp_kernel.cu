@@ -312,6 +312,7 @@ __device__ __forceinline__ void march(const StepParams& p, int n, int lane, int 
 template <bool kAnyCpml, bool kAnyCoef, bool kUniform, int kMinBlocks>
 __global__ void __launch_bounds__(256, kMinBlocks) warp_step_kernel(const StepParams p, int n, int slot) {
   (void)slot;
+  if (p.step_base) n += __ldg(p.step_base);
   const int lane = threadIdx.x & 31;
   const int j = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
   if (j >= p.NY) return;  // whole warp; this kernel has no block-level barrier
@@ -331,6 +332,7 @@ __global__ void __launch_bounds__(256, kMinBlocks) warp_step_kernel(const StepPa
 // launch of warp_step_kernel with fields in TS and ADE state in BF16.
 template <typename TS, bool kAnyCpml, bool kAnyCoef, bool kUniform>
 __global__ void __launch_bounds__(256, 4) warp_step_kernel_rs(const StepParams p, int n) {
+  if (p.step_base) n += __ldg(p.step_base);
   const int lane = threadIdx.x & 31;
   const int j = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
   if (j >= p.NY) return;

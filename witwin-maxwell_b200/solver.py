@@ -302,3 +302,57 @@ class B200FDTD:
             self.close()
         except Exception:
             pass
+
+
+class B200Batch:
+    """Independent scenes stepped together (fdtd_batch_*): each block of
+    ``sample_block`` steps of every scene is one CUDA graph replay in which the
+    scenes' kernels run concurrently on their own streams.  Results equal the
+    solvers stepped one by one.  The solvers must share the device and the
+    stream they were initialised on; while the batch exists, step them through it."""
+
+    def __init__(self, solvers):
+        self.solvers = list(solvers)
+        if not self.solvers:
+            raise ValueError("empty batch")
+        for s in self.solvers:
+            if s.handle is None:
+                s.init_field()
+        self.lib = _lib.load()
+        self.handle = None
+        handles = (ctypes.c_void_p * len(self.solvers))(*[s.handle.value for s in self.solvers])
+        stream = self.solvers[0].stream
+        out = ctypes.c_void_p()
+        _lib.check(self.lib.fdtd_batch_create(handles, len(self.solvers), ctypes.c_void_p(stream.cuda_stream), ctypes.byref(out)),
+                   "fdtd_batch_create")
+        self.handle = out
+        self.steps_done = 0
+
+    def autotune(self) -> None:
+        _lib.check(self.lib.fdtd_batch_autotune(self.handle), "fdtd_batch_autotune")
+
+    def step_range(self, n0: int, n1: int) -> float:
+        """Advance every scene over [n0, n1); returns the device time in ms."""
+        _lib.check(self.lib.fdtd_batch_step_range(self.handle, int(n0), int(n1)), "fdtd_batch_step_range")
+        self.steps_done = max(self.steps_done, int(n1))
+        for s in self.solvers:
+            s.steps_done = max(s.steps_done, int(n1))
+        ms = ctypes.c_float()
+        _lib.check(self.lib.fdtd_batch_last_ms(self.handle, ctypes.byref(ms)), "fdtd_batch_last_ms")
+        return float(ms.value)
+
+    def info(self) -> dict:
+        n, m, g = ctypes.c_int(), ctypes.c_int(), ctypes.c_int64()
+        _lib.check(self.lib.fdtd_batch_info(self.handle, ctypes.byref(n), ctypes.byref(m), ctypes.byref(g)), "fdtd_batch_info")
+        return {"scenes": n.value, "block_steps": m.value, "graph_launches": g.value}
+
+    def close(self) -> None:
+        if self.handle is not None:
+            self.lib.fdtd_batch_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -84,6 +84,35 @@ def adjoint_160(steps: int = 3000, seed: int = 0) -> Scene:
     return sc
 
 
+def batched_designs(n_scenes: int = 32, seed: int = 1, size_range: tuple[int, int] = (64, 192), pml: int = 8,
+                    n_freq: int = 8) -> list[Scene]:
+    """Batched design workload: ``n_scenes`` independent scenes whose cell counts per axis
+    are drawn uniformly from ``size_range`` (numpy.random.default_rng(seed)); 8-cell CPML;
+    4-8 boxes per scene (seeded positions and sizes) of diagonal anisotropic permittivity
+    with eps_xx, eps_yy, eps_zz ~ U[1, 6]; an Ez point dipole (300/100 THz pulse) at the
+    centre; an 8-frequency (250-350 THz) point monitor of all six components."""
+    rng = np.random.default_rng(seed)
+    lo_n, hi_n = size_range
+    freqs = tuple(np.linspace(250e12, 350e12, n_freq))
+    scenes = []
+    for _ in range(n_scenes):
+        cells = tuple(int(v) for v in rng.integers(lo_n, hi_n + 1, size=3))
+        sc = Scene(cells=cells, spacing=SPACING, pml_cells=pml)
+        for _ in range(int(rng.integers(4, 9))):
+            size = [int(rng.integers(4, max(5, (c - 2 * pml) // 3))) for c in cells]
+            lo = [int(rng.integers(pml + 1, max(pml + 2, c - pml - s_ - 1))) for c, s_ in zip(cells, size)]
+            eps = tuple(float(v) for v in rng.uniform(1.0, 6.0, size=3))
+            sc.structures.append(
+                Structure(Box(tuple(lo), tuple(l + s_ for l, s_ in zip(lo, size))), Medium(eps_r=1.0, eps_diag=eps))
+            )
+        centre = tuple(c // 2 for c in cells)
+        sc.sources.append(PointDipole(centre, "Ez", GaussianPulse(300e12, 100e12), width=SPACING))
+        probe = (centre[0] + cells[0] // 4, centre[1], centre[2])
+        sc.monitors.append(PointMonitor("probe", probe, frequencies=freqs))
+        scenes.append(sc)
+    return scenes
+
+
 def algorithmic_bytes(compiled, *, kahan: bool = True, storage_bytes: int = 4) -> dict:
     """Compulsory HBM bytes per cell-update of one leapfrog step (every state array read
     once and written once), split into the fused step kernel's share and the whole step.
