@@ -309,6 +309,10 @@ def run_b200_arm(args, wm, world, rank, local):
     # ---------------- end to end through the public API, host buffers ----------------
     if args.e2e:
         result["e2e"] = run_e2e(args, wm, cs, device, world)
+    if args.reduced:
+        result["reduced_storage"] = run_reduced_bench(args, wm, cs, device, kernel_ms, elapsed_s * 1e3 / args.steps)
+    if args.batched:
+        result["batched"] = run_batched_bench(wm, device)
     if args.adjoint:
         result["adjoint"] = run_adjoint_bench(wm, device)
     if rank == 0 and args.cpu_baseline:
@@ -324,6 +328,95 @@ def run_b200_arm(args, wm, world, rank, local):
             result["cpu_baseline"] = {"value": None, "unit": METRIC, "cores": os.cpu_count(), "kind": "port",
                                       "sample": f"failed: {exc}"}
     return result
+
+
+def _joint_rel_l2(got: dict, ref: dict) -> float:
+    num = sum(float(np.linalg.norm(np.asarray(got[k], np.complex128).ravel() - np.asarray(ref[k], np.complex128).ravel())) ** 2 for k in ref)
+    den = sum(float(np.linalg.norm(np.asarray(ref[k], np.complex128).ravel())) ** 2 for k in ref)
+    return (num / den) ** 0.5 if den > 0 else 0.0
+
+
+def run_reduced_bench(args, wm, cs, device, fp32_kernel_ms, fp32_step_ms):
+    """FP16 / BF16 field storage (FP32 arithmetic) on the same workload: step-kernel
+    and whole-step time against FP32, and each monitor's relative L2 against the
+    FP32 engine after 400 steps (the FP32 engine itself is within 2e-6 of the FP64
+    oracle on this workload scaled to 96^3: tests/test_reference_gpu.py,
+    tests/test_precision.py hold the FP64-oracle bars)."""
+    import torch
+
+    steps = 400
+    out = {"steps_compared": steps, "reference": "FP32 engine, same scene and steps"}
+    runs = {}
+    for st in ("fp32", "fp16", "bf16"):
+        solver = wm.solver.B200FDTD(cs, device=device, sample_block=args.sample_block, storage=st).init_field()
+        solver.step_range(0, 4)
+        k_ms = solver.time_kernel(4, 8) if st != "fp32" else fp32_kernel_ms
+        solver.close()
+        solver = wm.solver.B200FDTD(cs, device=device, sample_block=args.sample_block, storage=st).init_field()
+        ms = solver.step_range(0, steps)
+        runs[st] = {k: {c: v.cpu().numpy() for c, v in d.items()} for k, d in solver.monitor_results().items()}
+        if st != "fp32":
+            out[st] = {
+                "kernel_ms": k_ms,
+                "kernel_speedup_vs_fp32": fp32_kernel_ms / k_ms,
+                "step_ms": ms / steps,
+                "gcell_updates_per_s": cs.cells * steps / (ms * 1e-3) / 1e9,
+                "scales": solver.storage_scales()[1],
+            }
+        else:
+            out["fp32_step_ms"] = ms / steps
+        solver.close()
+        torch.cuda.empty_cache()
+    for st in ("fp16", "bf16"):
+        errs = {m: _joint_rel_l2(runs[st][m], runs["fp32"][m]) for m in runs["fp32"]}
+        out[st]["monitor_rel_l2_vs_fp32"] = {m: float(f"{e:.3e}") for m, e in errs.items()}
+        out[st]["max_monitor_rel_l2_vs_fp32"] = max(errs.values())
+        out[st]["algorithmic_bytes_per_cell_update"] = round(wm.workloads.algorithmic_bytes(cs, storage_bytes=2)["step_kernel"], 3)
+    return out
+
+
+def run_batched_bench(wm, device, steps: int = 256):
+    """32 independent anisotropic design scenes (cell counts per axis ~ U{64..192},
+    seeded): the batch (one CUDA graph replay per 32-step block, scenes on their
+    own streams, launch shapes from the per-size-class autotune) against the same
+    scenes stepped one after another, device time."""
+    import torch
+
+    scenes = wm.workloads.batched_designs()
+    compiled = [wm.compile_scene(sc, steps + 64) for sc in scenes]
+    cells = sum(c.cells for c in compiled)
+    solvers = [wm.solver.B200FDTD(c, device=device).init_field() for c in compiled]
+    for sv in solvers:
+        sv.step_range(0, 32)
+    seq_ms = sum(sv.step_range(32, 32 + steps) for sv in solvers)
+    for sv in solvers:
+        sv.close()
+    torch.cuda.empty_cache()
+    solvers = [wm.solver.B200FDTD(c, device=device).init_field() for c in compiled]
+    batch = wm.solver.B200Batch(solvers)
+    t0 = time.perf_counter()
+    batch.autotune()
+    tune_s = time.perf_counter() - t0
+    batch.step_range(0, 32)
+    ms = batch.step_range(32, 32 + steps)
+    info = batch.info()
+    batch.close()
+    for sv in solvers:
+        sv.close()
+    torch.cuda.empty_cache()
+    return {
+        "workload": "batched_designs: 32 scenes, cells per axis ~ U{64..192} (seed 1), 8-cell CPML, 4-8 diagonal "
+                    "anisotropic eps boxes, Ez dipole, 8-frequency point monitor",
+        "cells_total": int(cells),
+        "steps": steps,
+        "batched_ms": ms,
+        "batched_gcell_updates_per_s": cells * steps / (ms * 1e-3) / 1e9,
+        "sequential_ms": seq_ms,
+        "sequential_gcell_updates_per_s": cells * steps / (seq_ms * 1e-3) / 1e9,
+        "speedup": seq_ms / ms,
+        "autotune_s": tune_s,
+        "graph_launches": info["graph_launches"],
+    }
 
 
 def run_adjoint_bench(wm, device):
@@ -430,6 +523,10 @@ def main():
     ap.add_argument("--autotune", action="store_true")
     ap.add_argument("--no-cpu-baseline", dest="cpu_baseline", action="store_false")
     ap.add_argument("--no-e2e", dest="e2e", action="store_false")
+    ap.add_argument("--no-reduced", dest="reduced", action="store_false",
+                    help="skip the FP16 / BF16 field-storage timing and error")
+    ap.add_argument("--no-batched", dest="batched", action="store_false",
+                    help="skip the 32-scene batched design workload")
     ap.add_argument("--no-adjoint", dest="adjoint", action="store_false",
                     help="skip the forward+adjoint timing of the 160x160x96 design workload")
     ap.add_argument("--cells", type=int, default=256,

@@ -102,59 +102,62 @@ __device__ float h_term_adjoint(const StepParams& p, const AdjParams& q, int c, 
   return ik * g_eff + cc * (gq + g_eff);
 }
 
-__device__ __forceinline__ float inv_at(const float* arr, int idx, int n) { return (idx >= 0 && idx < n) ? __ldg(arr + idx) : 0.0f; }
-
-__device__ __forceinline__ void unflatten(const StepParams& p, int64_t x, int& i, int& j, int& k) {
-  k = static_cast<int>(x % p.P);
-  const int64_t r = x / p.P;
-  j = static_cast<int>(r % p.NY);
-  i = static_cast<int>(r / p.NY);
+// Inverse spacing of index idx (zero outside [0, n)); on a uniform grid the
+// axis value u, without a load.
+template <bool kUniform>
+__device__ __forceinline__ float inv_at(const float* arr, int idx, int n, float u) {
+  if (kUniform) return (idx >= 0 && idx < n) ? u : 0.0f;
+  return (idx >= 0 && idx < n) ? __ldg(arr + idx) : 0.0f;
 }
 
 // ---- pass A: gH_mid = gH + C_H^T g(d_E) (in place in q.gH) ----
+template <bool kUniform>
 __global__ void adj_pass_a_kernel(const StepParams p, const AdjParams q) {
-  const int64_t vol = static_cast<int64_t>(p.NX) * p.NY * p.P;
-  for (int64_t x = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; x < vol;
-       x += static_cast<int64_t>(gridDim.x) * blockDim.x) {
-    int i, j, k;
-    unflatten(p, x, i, j, k);
+  {
+    // one thread per cell: k from the x-dimension, rows and planes from y and z
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    const int j = blockIdx.y, i = blockIdx.z;
+    if (k >= p.P) return;
+    const int64_t x = (static_cast<int64_t>(i) * p.NY + j) * p.P + k;
     const float* iex = p.inv_e[0];
     const float* iey = p.inv_e[1];
     const float* iez = p.inv_e[2];
     if (h_in_extent(p, 0, i, j, k)) {  // Hx: Ey d1b (z), Ez d2b (y)
       float g = q.gH[0][x];
-      g += inv_at(iez, k, p.NZ) * e_term_adjoint(p, q, 1, 1, i, j, k) -
-           inv_at(iez, k + 1, p.NZ) * e_term_adjoint(p, q, 1, 1, i, j, k + 1);
-      g += inv_at(iey, j, p.NY) * e_term_adjoint(p, q, 2, 1, i, j, k) -
-           inv_at(iey, j + 1, p.NY) * e_term_adjoint(p, q, 2, 1, i, j + 1, k);
+      g += inv_at<kUniform>(iez, k, p.NZ, p.inv_e_u[2]) * e_term_adjoint(p, q, 1, 1, i, j, k) -
+           inv_at<kUniform>(iez, k + 1, p.NZ, p.inv_e_u[2]) * e_term_adjoint(p, q, 1, 1, i, j, k + 1);
+      g += inv_at<kUniform>(iey, j, p.NY, p.inv_e_u[1]) * e_term_adjoint(p, q, 2, 1, i, j, k) -
+           inv_at<kUniform>(iey, j + 1, p.NY, p.inv_e_u[1]) * e_term_adjoint(p, q, 2, 1, i, j + 1, k);
       q.gH[0][x] = g;
     }
     if (h_in_extent(p, 1, i, j, k)) {  // Hy: Ex d0b (z), Ez d2a (x)
       float g = q.gH[1][x];
-      g += inv_at(iez, k, p.NZ) * e_term_adjoint(p, q, 0, 1, i, j, k) -
-           inv_at(iez, k + 1, p.NZ) * e_term_adjoint(p, q, 0, 1, i, j, k + 1);
-      g += inv_at(iex, i, p.NX) * e_term_adjoint(p, q, 2, 0, i, j, k) -
-           inv_at(iex, i + 1, p.NX) * e_term_adjoint(p, q, 2, 0, i + 1, j, k);
+      g += inv_at<kUniform>(iez, k, p.NZ, p.inv_e_u[2]) * e_term_adjoint(p, q, 0, 1, i, j, k) -
+           inv_at<kUniform>(iez, k + 1, p.NZ, p.inv_e_u[2]) * e_term_adjoint(p, q, 0, 1, i, j, k + 1);
+      g += inv_at<kUniform>(iex, i, p.NX, p.inv_e_u[0]) * e_term_adjoint(p, q, 2, 0, i, j, k) -
+           inv_at<kUniform>(iex, i + 1, p.NX, p.inv_e_u[0]) * e_term_adjoint(p, q, 2, 0, i + 1, j, k);
       q.gH[1][x] = g;
     }
     if (h_in_extent(p, 2, i, j, k)) {  // Hz: Ex d0a (y), Ey d1a (x)
       float g = q.gH[2][x];
-      g += inv_at(iey, j, p.NY) * e_term_adjoint(p, q, 0, 0, i, j, k) -
-           inv_at(iey, j + 1, p.NY) * e_term_adjoint(p, q, 0, 0, i, j + 1, k);
-      g += inv_at(iex, i, p.NX) * e_term_adjoint(p, q, 1, 0, i, j, k) -
-           inv_at(iex, i + 1, p.NX) * e_term_adjoint(p, q, 1, 0, i + 1, j, k);
+      g += inv_at<kUniform>(iey, j, p.NY, p.inv_e_u[1]) * e_term_adjoint(p, q, 0, 0, i, j, k) -
+           inv_at<kUniform>(iey, j + 1, p.NY, p.inv_e_u[1]) * e_term_adjoint(p, q, 0, 0, i, j + 1, k);
+      g += inv_at<kUniform>(iex, i, p.NX, p.inv_e_u[0]) * e_term_adjoint(p, q, 1, 0, i, j, k) -
+           inv_at<kUniform>(iex, i + 1, p.NX, p.inv_e_u[0]) * e_term_adjoint(p, q, 1, 0, i + 1, j, k);
       q.gH[2][x] = g;
     }
   }
 }
 
 // ---- pass B: gE = de gE' - C_E^T g(d_H); adjoint E psi; design gradient ----
+template <bool kUniform>
 __global__ void adj_pass_b_kernel(const StepParams p, const AdjParams q) {
-  const int64_t vol = static_cast<int64_t>(p.NX) * p.NY * p.P;
-  for (int64_t x = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; x < vol;
-       x += static_cast<int64_t>(gridDim.x) * blockDim.x) {
-    int i, j, k;
-    unflatten(p, x, i, j, k);
+  {
+    // one thread per cell: k from the x-dimension, rows and planes from y and z
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    const int j = blockIdx.y, i = blockIdx.z;
+    if (k >= p.P) return;
+    const int64_t x = (static_cast<int64_t>(i) * p.NY + j) * p.P + k;
     const float* ihx = p.inv_h[0];
     const float* ihy = p.inv_h[1];
     const float* ihz = p.inv_h[2];
@@ -165,20 +168,20 @@ __global__ void adj_pass_b_kernel(const StepParams p, const AdjParams q) {
       float g = m == 0 ? coef(p.edecay[c], p.edecay_u[c], x) * gp : (m == 1 ? gp : 0.0f);
       // H-update terms reading this E cell (forward differences of E)
       if (c == 0) {  // Hy cyb (z), Hz czb (y)
-        g += -inv_at(ihz, k, p.NZ - 1) * h_term_adjoint(p, q, 1, 1, i, j, k) +
-             inv_at(ihz, k - 1, p.NZ - 1) * h_term_adjoint(p, q, 1, 1, i, j, k - 1);
-        g += -inv_at(ihy, j, p.NY - 1) * h_term_adjoint(p, q, 2, 1, i, j, k) +
-             inv_at(ihy, j - 1, p.NY - 1) * h_term_adjoint(p, q, 2, 1, i, j - 1, k);
+        g += -inv_at<kUniform>(ihz, k, p.NZ - 1, p.inv_h_u[2]) * h_term_adjoint(p, q, 1, 1, i, j, k) +
+             inv_at<kUniform>(ihz, k - 1, p.NZ - 1, p.inv_h_u[2]) * h_term_adjoint(p, q, 1, 1, i, j, k - 1);
+        g += -inv_at<kUniform>(ihy, j, p.NY - 1, p.inv_h_u[1]) * h_term_adjoint(p, q, 2, 1, i, j, k) +
+             inv_at<kUniform>(ihy, j - 1, p.NY - 1, p.inv_h_u[1]) * h_term_adjoint(p, q, 2, 1, i, j - 1, k);
       } else if (c == 1) {  // Hx cxb (z), Hz cza (x)
-        g += -inv_at(ihz, k, p.NZ - 1) * h_term_adjoint(p, q, 0, 1, i, j, k) +
-             inv_at(ihz, k - 1, p.NZ - 1) * h_term_adjoint(p, q, 0, 1, i, j, k - 1);
-        g += -inv_at(ihx, i, p.NX - 1) * h_term_adjoint(p, q, 2, 0, i, j, k) +
-             inv_at(ihx, i - 1, p.NX - 1) * h_term_adjoint(p, q, 2, 0, i - 1, j, k);
+        g += -inv_at<kUniform>(ihz, k, p.NZ - 1, p.inv_h_u[2]) * h_term_adjoint(p, q, 0, 1, i, j, k) +
+             inv_at<kUniform>(ihz, k - 1, p.NZ - 1, p.inv_h_u[2]) * h_term_adjoint(p, q, 0, 1, i, j, k - 1);
+        g += -inv_at<kUniform>(ihx, i, p.NX - 1, p.inv_h_u[0]) * h_term_adjoint(p, q, 2, 0, i, j, k) +
+             inv_at<kUniform>(ihx, i - 1, p.NX - 1, p.inv_h_u[0]) * h_term_adjoint(p, q, 2, 0, i - 1, j, k);
       } else {  // Hx cxa (y), Hy cya (x)
-        g += -inv_at(ihy, j, p.NY - 1) * h_term_adjoint(p, q, 0, 0, i, j, k) +
-             inv_at(ihy, j - 1, p.NY - 1) * h_term_adjoint(p, q, 0, 0, i, j - 1, k);
-        g += -inv_at(ihx, i, p.NX - 1) * h_term_adjoint(p, q, 1, 0, i, j, k) +
-             inv_at(ihx, i - 1, p.NX - 1) * h_term_adjoint(p, q, 1, 0, i - 1, j, k);
+        g += -inv_at<kUniform>(ihy, j, p.NY - 1, p.inv_h_u[1]) * h_term_adjoint(p, q, 0, 0, i, j, k) +
+             inv_at<kUniform>(ihy, j - 1, p.NY - 1, p.inv_h_u[1]) * h_term_adjoint(p, q, 0, 0, i, j - 1, k);
+        g += -inv_at<kUniform>(ihx, i, p.NX - 1, p.inv_h_u[0]) * h_term_adjoint(p, q, 1, 0, i, j, k) +
+             inv_at<kUniform>(ihx, i - 1, p.NX - 1, p.inv_h_u[0]) * h_term_adjoint(p, q, 1, 0, i - 1, j, k);
       }
       if (m == 0) {
         const float ce = coef(p.ecurl[c], p.ecurl_u[c], x);
@@ -212,13 +215,27 @@ __global__ void adj_pass_b_kernel(const StepParams p, const AdjParams q) {
 
 // ---- pass C: adjoint H psi; gH = dh gH_mid ----
 __global__ void adj_pass_c_kernel(const StepParams p, const AdjParams q) {
-  const int64_t vol = static_cast<int64_t>(p.NX) * p.NY * p.P;
-  for (int64_t x = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; x < vol;
-       x += static_cast<int64_t>(gridDim.x) * blockDim.x) {
-    int i, j, k;
-    unflatten(p, x, i, j, k);
+  {
+    // one thread per cell: k from the x-dimension, rows and planes from y and z
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    const int j = blockIdx.y, i = blockIdx.z;
+    if (k >= p.P) return;
+    const int64_t x = (static_cast<int64_t>(i) * p.NY + j) * p.P + k;
     for (int c = 0; c < 3; ++c) {
       if (!h_in_extent(p, c, i, j, k)) continue;
+      // With unit magnetic decay (no magnetic loss) gH = gH_mid already: only
+      // CPML slab cells have work (their adjoint psi).
+      if (!p.hdecay[c] && p.hdecay_u[c] == 1.0f) {
+        bool slab = false;
+        if (p.cpml) {
+          for (int w = 0; w < 2; ++w) {
+            const int axis = w == 0 ? (c == 0 ? 1 : 0) : (c == 2 ? 1 : 2);
+            const int extent = axis == 0 ? p.NX - 1 : (axis == 1 ? p.NY - 1 : p.NZ - 1);
+            slab = slab || slab_coord(p, axis, coord(axis, i, j, k), extent) >= 0;
+          }
+        }
+        if (!slab) continue;
+      }
       const float gm = q.gH[c][x];
       if (p.cpml) {
         const float v = coef(p.hcurl[c], p.hcurl_u[c], x) * gm;
@@ -291,14 +308,19 @@ unsigned grid_for(int64_t n) {
 
 int launch_adjoint_step(const StepParams& p, const AdjParams& q, const RegionFlush* regions, int n_regions,
                         const float2* w_e, const float2* w_h, int n_freq, int n, cudaStream_t stream) {
-  const int64_t vol = static_cast<int64_t>(p.NX) * p.NY * p.P;
   if (n_regions > 0 && q.seed_re) {
     dim3 grid(64, n_regions);
     adj_seed_kernel<<<grid, 256, 0, stream>>>(p, q, regions, n_regions, w_e, w_h, n_freq, n);
   }
-  adj_pass_a_kernel<<<grid_for(vol), 256, 0, stream>>>(p, q);
-  adj_pass_b_kernel<<<grid_for(vol), 256, 0, stream>>>(p, q);
-  adj_pass_c_kernel<<<grid_for(vol), 256, 0, stream>>>(p, q);
+  const dim3 cells((p.P + 127) / 128, p.NY, p.NX);
+  if (p.uniform_grid) {
+    adj_pass_a_kernel<true><<<cells, 128, 0, stream>>>(p, q);
+    adj_pass_b_kernel<true><<<cells, 128, 0, stream>>>(p, q);
+  } else {
+    adj_pass_a_kernel<false><<<cells, 128, 0, stream>>>(p, q);
+    adj_pass_b_kernel<false><<<cells, 128, 0, stream>>>(p, q);
+  }
+  adj_pass_c_kernel<<<cells, 128, 0, stream>>>(p, q);
   return static_cast<int>(cudaGetLastError());
 }
 

@@ -523,6 +523,7 @@ void fill_params(const fdtd_engine* h, StepParams& p) {
   p.P = h->P;
   p.SZ = h->SZ;
   p.storage = h->storage;
+  p.uniform_grid = h->uniform_grid ? 1 : 0;
   p.step_base = h->graph_base ? h->d_base : nullptr;
   for (int c = 0; c < 6; ++c) {
     p.fscale[c] = h->fscale[c];

@@ -84,6 +84,7 @@ struct StepParams {
   const float* inv_e[3];
   const float* inv_h[3];
   float inv_e_u[3], inv_h_u[3];  // uniform-grid values (used when every entry of an axis is equal)
+  int uniform_grid;              // every axis has constant spacing (inv_*_u hold the values)
   const float* eb[3];
   const float* ec[3];
   const float* eik[3];
