@@ -216,6 +216,24 @@ int fdtd_batch_step_range(fdtd_batch* b, int n0, int n1);
 int fdtd_batch_last_ms(fdtd_batch* b, float* ms);
 int fdtd_batch_info(fdtd_batch* b, int* n_engines, int* block_steps, int64_t* graph_launches);
 
+/* Periodic and Bloch-periodic faces (x and y axes, both faces of an axis
+ * alike, no CPML on that axis).  The step kernel defers the E cells whose
+ * backward difference wraps around the grid; a wrap kernel updates them once
+ * the whole new H is in memory, reading the far face with the phase e^{-ikL} /
+ * e^{+ikL} (witwin/maxwell/fdtd/cuda/kernels/electric.cu:124-168, 356-453,
+ * 1164-1229).  A periodic engine steps with fdtd_engine_step_range.  A Bloch
+ * field is complex: create two engines on the same scene (the real and the
+ * imaginary part, each with the sources of its part) and step them as one pair;
+ * phase_cos / phase_sin hold cos(k L) and sin(k L) per axis (x, y, z; entries of
+ * axes without Bloch faces are ignored).  Periodic and Bloch engines run launch
+ * variants 1-3 with FP32 storage, and have no adjoint. */
+typedef struct fdtd_bloch fdtd_bloch;
+int fdtd_bloch_create(fdtd_engine* re, fdtd_engine* im, const float* phase_cos, const float* phase_sin,
+                      fdtd_bloch** out);
+int fdtd_bloch_destroy(fdtd_bloch* p);
+int fdtd_bloch_step_range(fdtd_bloch* p, int n0, int n1);
+int fdtd_bloch_last_ms(fdtd_bloch* p, float* ms);
+
 /* Reverse-time adjoint: the exact discrete transpose of the fused step (H and
  * E updates, CPML psi, E edge modes), monitor seeds and dL/deps of design
  * boxes.  Replaces the reference's native reverse runners

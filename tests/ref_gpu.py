@@ -47,7 +47,7 @@ def _shape(name, nodes):
 
 
 class RefGpuSimulation:
-    def __init__(self, compiled, device: str = "cuda"):
+    def __init__(self, compiled, device: str = "cuda", channel: int = 0):
         self.cs = cs = compiled
         self.op = ops()
         dev = torch.device(device)
@@ -93,7 +93,8 @@ class RefGpuSimulation:
                 "restoring": float(pole.restoring), "drive": t(drive), "inv_eps": t(inv_eps),
                 "P": torch.zeros(shape, device=dev), "J": torch.zeros(shape, device=dev),
             })
-        self.patches = [(p.component, p.box, t(p.coeff), np.asarray(p.signal, np.float32)) for p in cs.patches]
+        self.patches = [(p.component, p.box, t(p.coeff), np.asarray(p.signal, np.float32)) for p in cs.patches
+                        if getattr(p, "channel", 0) == channel]
         self.aux = None
         if cs.aux_line is not None:
             a = cs.aux_line
@@ -239,3 +240,65 @@ class RefGpuSimulation:
             data = (re[fidx].cpu().numpy() + 1j * im[fidx].cpu().numpy()) * scale
             out.setdefault(reg.monitor, {})[reg.component] = data
         return out
+
+
+class RefGpuBloch:
+    """A complex field on x / y Bloch faces with PEC (or NONE) z faces, stepped
+    with the reference's own ops: per channel the standard H updates, ADE,
+    source patches and PEC clamps of RefGpuSimulation, and for E the
+    reference's complex Bloch kernels update_electric_ex_bloch_y_standard_z,
+    update_electric_ey_bloch_x_standard_z and update_electric_ez_bloch
+    (electric.cu:356-453, 1164-1229), as stepping.py:1118-1173 and 1790 order
+    them.  Monitors are the complex DFT A + iB of the two channels' spectra."""
+
+    def __init__(self, compiled, device: str = "cuda"):
+        cs = compiled
+        if cs.cpml and (any(cs.pml_lo) or any(cs.pml_hi)):
+            raise ValueError("the Bloch checker covers scenes without CPML")
+        self.cs = cs
+        self.re = RefGpuSimulation(cs, device, channel=0)
+        self.im = RefGpuSimulation(cs, device, channel=1)
+        self.op = self.re.op
+
+    def _update_e(self):
+        cs, R, I = self.cs, self.re.F, self.im.F
+        c, s = cs.bloch_cos, cs.bloch_sin
+        inv = self.re.inv_e
+        zl, zh = cs.boundary[4], cs.boundary[5]
+        self.op.update_electric_ex_bloch_y_standard_z(
+            R["Ex"], I["Ex"], R["Hy"], I["Hy"], R["Hz"], I["Hz"], self.re.decay["Ex"], self.re.curl["Ex"],
+            float(c[1]), float(s[1]), inv[1], inv[2], zl, zh)
+        self.op.update_electric_ey_bloch_x_standard_z(
+            R["Ey"], I["Ey"], R["Hx"], I["Hx"], R["Hz"], I["Hz"], self.re.decay["Ey"], self.re.curl["Ey"],
+            float(c[0]), float(s[0]), inv[0], inv[2], zl, zh)
+        self.op.update_electric_ez_bloch(
+            R["Ez"], I["Ez"], R["Hx"], I["Hx"], R["Hy"], I["Hy"], self.re.decay["Ez"], self.re.curl["Ez"],
+            float(c[0]), float(s[0]), float(c[1]), float(s[1]), inv[0], inv[1])
+
+    def step_once(self):
+        re, im = self.re, self.im
+        n = re.step
+        re._update_h()
+        im._update_h()
+        re._advance_ade()
+        im._advance_ade()
+        self._update_e()
+        for sim in (re, im):
+            for comp, box, coeff, signal in sim.patches:
+                self.op.add_source_patch(sim.F[comp], coeff, box[0], box[2], box[4], float(signal[n]))
+            sim._apply_ade()
+            sim._clamp_pec()
+            sim._accumulate(n)
+            sim.step += 1
+
+    def run(self, steps: int):
+        for _ in range(int(steps)):
+            self.step_once()
+        return self
+
+    def fields(self) -> tuple[dict, dict]:
+        return self.re.fields(), self.im.fields()
+
+    def monitor_results(self) -> dict:
+        a, b = self.re.monitor_results(), self.im.monitor_results()
+        return {m: {c: a[m][c] + 1j * b[m][c] for c in a[m]} for m in a}

@@ -241,10 +241,17 @@ def test_engine_rejects_bad_inputs():
     rc = lib.fdtd_engine_create(ctypes.byref(desc), None, ctypes.byref(handle))
     assert rc == -1 and b"at least 3" in lib.fdtd_last_error()
     desc.nx = desc.ny = desc.nz = 10
-    desc.boundary[0] = 3  # Bloch face: not supported by the fused engine
+    desc.boundary[0] = 5  # PMC face: the per-op path only
+    rc = lib.fdtd_engine_create(ctypes.byref(desc), None, ctypes.byref(handle))
+    assert rc == -3
+    desc.boundary[0] = 3  # a Bloch low face needs a Bloch high face
+    rc = lib.fdtd_engine_create(ctypes.byref(desc), None, ctypes.byref(handle))
+    assert rc == -1 and b"must match" in lib.fdtd_last_error()
+    desc.boundary[4] = desc.boundary[5] = 2  # periodic z: not supported
     rc = lib.fdtd_engine_create(ctypes.byref(desc), None, ctypes.byref(handle))
     assert rc == -3
     desc.boundary[0] = 1
+    desc.boundary[4] = desc.boundary[5] = 0
     rc = lib.fdtd_engine_create(ctypes.byref(desc), None, ctypes.byref(handle))
     assert rc == 0
     # stepping before finalize is a state error, not a crash

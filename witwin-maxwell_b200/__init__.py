@@ -24,6 +24,7 @@ from .scene import (
     MaterialRegion,
     Medium,
     PlaneMonitor,
+    PlaneSource,
     PlaneWaveTFSF,
     PointDipole,
     PointMonitor,

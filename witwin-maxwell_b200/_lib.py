@@ -41,6 +41,10 @@ _SIGNATURES = {
     "fdtd_version": ([], ctypes.c_char_p),
     "fdtd_engine_create": ([ctypes.POINTER(FdtdGridDesc), _vp, ctypes.POINTER(_vp)], _i),
     "fdtd_engine_destroy": ([_vp], _i),
+    "fdtd_bloch_create": ([_vp, _vp, ctypes.POINTER(_f), ctypes.POINTER(_f), ctypes.POINTER(_vp)], _i),
+    "fdtd_bloch_destroy": ([_vp], _i),
+    "fdtd_bloch_step_range": ([_vp, _i, _i], _i),
+    "fdtd_bloch_last_ms": ([_vp, ctypes.POINTER(_f)], _i),
     "fdtd_batch_create": ([_vp, _i, _vp, ctypes.POINTER(_vp)], _i),
     "fdtd_batch_destroy": ([_vp], _i),
     "fdtd_batch_autotune": ([_vp], _i),

@@ -362,6 +362,13 @@ struct fdtd_engine {
   int* d_base = nullptr;
   bool graph_base = false;
   int graph_n0 = 0;
+  // Periodic / Bloch faces (x, y): the step kernel defers the E cells on them
+  // to the wrap kernel.  bloch: some face is Bloch (complex field, stepped as
+  // the real channel or imaginary channel of an fdtd_bloch pair); in_pair: the
+  // pair runs the wrap kernel and the monitor gather of this engine.
+  bool wrap = false;
+  bool bloch = false;
+  bool in_pair = false;
   int64_t plane = 0, vol = 0;
   int TY = 0, CX = 0;
   // Fused kernel: 1..3 = register-prefetch warp kernel with a register budget
@@ -637,6 +644,9 @@ int check_status(fdtd_engine* h) {
   return 0;
 }
 
+int launch_wrap_single(fdtd_engine* h, int n);
+int launch_gather(fdtd_engine* h, int slot);
+
 bool has_coef(const fdtd_engine* h) {
   for (int c = 0; c < 6; ++c)
     if (h->ecoef[c][0] || h->ecoef[c][1]) return true;
@@ -709,6 +719,34 @@ int launch_step(fdtd_engine* h, int n, int slot) {
   if (err != cudaSuccess) return cuda_fail(err, "warp_step_kernel launch");
   ++h->launches;
   h->cur = 1 - h->cur;
+  if (h->in_pair) return 0;  // the Bloch pair runs the wrap kernel and the gather
+  if (h->wrap) {
+    const int rc = launch_wrap_single(h, n);
+    if (rc) return rc;
+  }
+  return launch_gather(h, slot);
+}
+
+// Wrap kernel of a real periodic engine after its step (phase 1 on every axis).
+int launch_wrap_single(fdtd_engine* h, int n) {
+  StepParams p;
+  fill_params(h, p);
+  WrapFields f;
+  for (int c = 0; c < 3; ++c) {
+    f.eold[c] = h->E[1 - h->cur][c];
+    f.enew[c] = h->E[h->cur][c];
+    f.hnew[c] = h->H[h->cur][c];
+  }
+  const float pc[3] = {1.0f, 1.0f, 1.0f}, ps[3] = {0.0f, 0.0f, 0.0f};
+  const int err = launch_wrap_fixup(p, nullptr, f, nullptr, pc, ps, n, h->stream);
+  if (err != 0) return cuda_fail(static_cast<cudaError_t>(err), "wrap_fixup_kernel launch");
+  ++h->launches;
+  return 0;
+}
+
+// Copy the monitor cells of the current state into sample slot `slot` (no-op for slot < 0).
+int launch_gather(fdtd_engine* h, int slot) {
+  cudaError_t err = cudaSuccess;
   if (h->n_flush > 0 && h->samples && slot >= 0) {
     FieldPtrs fields;
     for (int c = 0; c < 3; ++c) {
@@ -840,9 +878,17 @@ int fdtd_engine_create(const fdtd_grid_desc* desc, void* stream, fdtd_engine** o
   if (!(desc->dt > 0.0)) return fail(FDTD_ERR_INVALID_ARG, "dt must be positive");
   for (int f = 0; f < 6; ++f) {
     const int b = desc->boundary[f];
-    if (b != FDTD_BND_NONE && b != FDTD_BND_PML && b != FDTD_BND_PEC)
-      return fail(FDTD_ERR_UNSUPPORTED,
-                  "fused engine supports NONE, PML and PEC faces; periodic, Bloch and PMC faces use the per-op path");
+    const bool wrap = b == FDTD_BND_PERIODIC || b == FDTD_BND_BLOCH;
+    if (b != FDTD_BND_NONE && b != FDTD_BND_PML && b != FDTD_BND_PEC && !wrap)
+      return fail(FDTD_ERR_UNSUPPORTED, "fused engine supports NONE, PML, PEC, periodic and Bloch faces; PMC faces use the per-op path");
+    if (wrap && f >= 4) return fail(FDTD_ERR_UNSUPPORTED, "periodic and Bloch faces are supported on x and y");
+  }
+  for (int a = 0; a < 2; ++a) {
+    const int lo = desc->boundary[2 * a], hi = desc->boundary[2 * a + 1];
+    const bool wlo = lo == FDTD_BND_PERIODIC || lo == FDTD_BND_BLOCH, whi = hi == FDTD_BND_PERIODIC || hi == FDTD_BND_BLOCH;
+    if ((wlo || whi) && lo != hi) return fail(FDTD_ERR_INVALID_ARG, "both faces of a periodic or Bloch axis must match");
+    if (wlo && desc->pml_lo[a] + desc->pml_hi[a] != 0)
+      return fail(FDTD_ERR_INVALID_ARG, "a periodic or Bloch axis has no CPML slabs");
   }
   const int n[3] = {desc->nx, desc->ny, desc->nz};
   for (int a = 0; a < 3; ++a) {
@@ -851,6 +897,10 @@ int fdtd_engine_create(const fdtd_grid_desc* desc, void* stream, fdtd_engine** o
   }
   fdtd_engine* h = new fdtd_engine();
   h->desc = *desc;
+  for (int f = 0; f < 4; ++f) {
+    if (desc->boundary[f] == FDTD_BND_PERIODIC || desc->boundary[f] == FDTD_BND_BLOCH) h->wrap = true;
+    if (desc->boundary[f] == FDTD_BND_BLOCH) h->bloch = true;
+  }
   h->stream = static_cast<cudaStream_t>(stream);
   h->NX = desc->nx;
   h->NY = desc->ny;
@@ -947,6 +997,7 @@ int fdtd_engine_set_storage(fdtd_engine* h, int kind, const float* scales) {
   if (!h || kind < kStoreF32 || kind > kStoreBF16) return fail(FDTD_ERR_INVALID_ARG, "bad storage kind");
   if (h->finalized || !h->poles.empty() || !h->checkpoints.empty())
     return fail(FDTD_ERR_STATE, "storage must be chosen right after fdtd_engine_create");
+  if (h->wrap && kind != kStoreF32) return fail(FDTD_ERR_UNSUPPORTED, "periodic and Bloch faces need FP32 storage");
   if (scales) {
     for (int c = 0; c < 6; ++c) {
       int e = 0;
@@ -1559,6 +1610,8 @@ int fdtd_engine_step_range_recorded(fdtd_engine* h, int n0, int n1) {
 static int step_range_impl(fdtd_engine* h, int n0, int n1, bool record) {
   if (!h) return fail(FDTD_ERR_INVALID_ARG, "null engine");
   if (!h->finalized) return fail(FDTD_ERR_STATE, "engine not finalized");
+  if (h->bloch || h->in_pair)
+    return fail(FDTD_ERR_STATE, "Bloch faces carry a complex field: step the engines with fdtd_bloch_step_range");
   if (n1 < n0 || n0 < 0) return fail(FDTD_ERR_INVALID_ARG, "bad step range");
   for (const auto& t : h->terms) {
     if (t.signal && n1 > t.aux_len) return fail(FDTD_ERR_INVALID_ARG, "source signal table shorter than the range");
@@ -1716,6 +1769,7 @@ int fdtd_engine_autotune(fdtd_engine* h, int* tile_rows, int* chunk_planes) {
   for (int var = 1; var <= kMaxVariant; ++var) {
     if (var == 4 && !h->tma_ready) continue;
     if (h->storage != kStoreF32 && var != 2) continue;  // reduced storage: the 64-register kernel only
+    if (h->wrap && var > 3) continue;                    // wrap faces: the scalar warp kernels only
     for (int cx : cxs) {
       if (cx > 2 * h->NX) continue;
       h->variant = var;
@@ -1779,6 +1833,8 @@ int fdtd_engine_set_launch(fdtd_engine* h, int variant, int tile_rows, int chunk
   (void)tile_rows;  // the warp-granular kernels have no tile height
   if (h->storage != kStoreF32 && variant != 2)
     return fail(FDTD_ERR_UNSUPPORTED, "reduced field storage runs launch variant 2 only");
+  if (h->wrap && variant > 3)
+    return fail(FDTD_ERR_UNSUPPORTED, "periodic and Bloch faces run launch variants 1-3 only");
   h->variant = variant;
   if (chunk_planes > 0) h->CX = chunk_planes;
   else default_tiles(h);
@@ -1803,6 +1859,7 @@ int fdtd_engine_adjoint_init(fdtd_engine* h, const int* design_boxes, int max_se
   if (!h->finalized) return fail(FDTD_ERR_STATE, "engine not finalized");
   if (!h->poles.empty()) return fail(FDTD_ERR_UNSUPPORTED, "the adjoint of dispersive (ADE) media is not supported");
   if (h->storage != kStoreF32) return fail(FDTD_ERR_UNSUPPORTED, "the adjoint runs on FP32 field storage only");
+  if (h->wrap) return fail(FDTD_ERR_UNSUPPORTED, "the adjoint of periodic and Bloch faces is not supported");
   if (h->adj.ready) return fail(FDTD_ERR_STATE, "adjoint already initialised");
   AdjointHost& a = h->adj;
   a.q = AdjParams{};
@@ -2279,6 +2336,132 @@ int fdtd_batch_info(fdtd_batch* b, int* n_engines, int* block_steps, int64_t* gr
   if (n_engines) *n_engines = static_cast<int>(b->eng.size());
   if (block_steps) *block_steps = b->M;
   if (graph_launches) *graph_launches = b->graph_launches;
+  return 0;
+}
+
+
+// ---------------------------------------------------------------------------
+// Bloch pairs: a Bloch-periodic scene carries a complex field.  Its real and
+// imaginary parts are two engines (same grid, coefficients and monitors; each
+// holds the sources of its part); they evolve independently except on the
+// Bloch faces, where the wrap kernel couples them through the phase e^{ikL}.
+// ---------------------------------------------------------------------------
+}  // extern "C"
+
+struct fdtd_bloch {
+  fdtd_engine* re = nullptr;
+  fdtd_engine* im = nullptr;
+  float pc[3] = {1, 1, 1}, ps[3] = {0, 0, 0};
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  float last_ms = 0.0f;
+};
+
+extern "C" {
+
+int fdtd_bloch_create(fdtd_engine* re, fdtd_engine* im, const float* phase_cos, const float* phase_sin,
+                      fdtd_bloch** out) {
+  if (!re || !im || re == im || !phase_cos || !phase_sin || !out) return fail(FDTD_ERR_INVALID_ARG, "bad Bloch pair arguments");
+  *out = nullptr;
+  if (!re->finalized || !im->finalized) return fail(FDTD_ERR_STATE, "both engines must be finalized");
+  if (re->in_pair || im->in_pair) return fail(FDTD_ERR_STATE, "an engine is already in a Bloch pair");
+  if (!re->wrap) return fail(FDTD_ERR_INVALID_ARG, "the engines have no periodic or Bloch face");
+  const fdtd_grid_desc &a = re->desc, &b = im->desc;
+  bool same = a.nx == b.nx && a.ny == b.ny && a.nz == b.nz && a.dt == b.dt && re->stream == im->stream && re->M == im->M;
+  for (int f = 0; f < 6; ++f) same = same && a.boundary[f] == b.boundary[f];
+  for (int x = 0; x < 3; ++x) same = same && a.pml_lo[x] == b.pml_lo[x] && a.pml_hi[x] == b.pml_hi[x];
+  if (!same) return fail(FDTD_ERR_INVALID_ARG, "the two channels need the same grid, boundaries, stream and sample block");
+  if (re->variant > 3 || im->variant > 3) return fail(FDTD_ERR_UNSUPPORTED, "Bloch pairs run launch variants 1-3");
+  fdtd_bloch* p = new fdtd_bloch();
+  p->re = re;
+  p->im = im;
+  for (int x = 0; x < 3; ++x) {
+    const bool bl = x < 2 && a.boundary[2 * x] == FDTD_BND_BLOCH;
+    p->pc[x] = bl ? phase_cos[x] : 1.0f;
+    p->ps[x] = bl ? phase_sin[x] : 0.0f;
+  }
+  cudaError_t err = cudaEventCreate(&p->ev0);
+  if (err == cudaSuccess) err = cudaEventCreate(&p->ev1);
+  if (err != cudaSuccess) {
+    const int rc = cuda_fail(err, "Bloch pair events");
+    fdtd_bloch_destroy(p);
+    return rc;
+  }
+  re->in_pair = im->in_pair = true;
+  *out = p;
+  return 0;
+}
+
+int fdtd_bloch_destroy(fdtd_bloch* p) {
+  if (!p) return 0;
+  if (p->re) p->re->in_pair = false;
+  if (p->im) p->im->in_pair = false;
+  if (p->ev0) cudaEventDestroy(p->ev0);
+  if (p->ev1) cudaEventDestroy(p->ev1);
+  delete p;
+  return 0;
+}
+
+int fdtd_bloch_step_range(fdtd_bloch* p, int n0, int n1) {
+  if (!p) return fail(FDTD_ERR_INVALID_ARG, "null Bloch pair");
+  if (n1 < n0 || n0 < 0) return fail(FDTD_ERR_INVALID_ARG, "bad step range");
+  fdtd_engine* hs[2] = {p->re, p->im};
+  for (fdtd_engine* h : hs) {
+    for (const auto& t : h->terms)
+      if (t.signal && n1 > t.aux_len) return fail(FDTD_ERR_INVALID_ARG, "source signal table shorter than the range");
+    for (const auto& l : h->lines)
+      if (n1 > l.n_steps) return fail(FDTD_ERR_INVALID_ARG, "incident line history shorter than the range");
+    if (h->n_samples > 0 && h->n_freq > 0 && n1 > h->dft_steps)
+      return fail(FDTD_ERR_INVALID_ARG, "DFT weight table shorter than the range");
+  }
+  const cudaStream_t st = p->re->stream;
+  CUDA_TRY(cudaEventRecord(p->ev0, st));
+  for (int n = n0; n < n1; ++n) {
+    for (fdtd_engine* h : hs) {
+      if (h->pending == 0) h->pending_base = n;
+      if (h->pending_base + h->pending != n) {
+        const int rc = flush_samples(h);
+        if (rc) return rc;
+        h->pending_base = n;
+      }
+      const int rc = launch_step(h, n, -1);  // step kernel only: the pair runs the wrap kernel
+      if (rc) return rc;
+    }
+    StepParams pr, pim;
+    fill_params(p->re, pr);
+    fill_params(p->im, pim);
+    WrapFields fr, fi;
+    for (int c = 0; c < 3; ++c) {
+      fr.eold[c] = p->re->E[1 - p->re->cur][c];
+      fr.enew[c] = p->re->E[p->re->cur][c];
+      fr.hnew[c] = p->re->H[p->re->cur][c];
+      fi.eold[c] = p->im->E[1 - p->im->cur][c];
+      fi.enew[c] = p->im->E[p->im->cur][c];
+      fi.hnew[c] = p->im->H[p->im->cur][c];
+    }
+    const int err = launch_wrap_fixup(pr, &pim, fr, &fi, p->pc, p->ps, n, st);
+    if (err != 0) return cuda_fail(static_cast<cudaError_t>(err), "wrap_fixup_kernel launch");
+    for (fdtd_engine* h : hs) {
+      int rc = launch_gather(h, h->n_samples > 0 ? h->pending : -1);
+      if (rc) return rc;
+      if (h->n_samples > 0 && ++h->pending == h->M) {
+        rc = flush_samples(h);
+        if (rc) return rc;
+      }
+    }
+  }
+  CUDA_TRY(cudaEventRecord(p->ev1, st));
+  CUDA_TRY(cudaEventSynchronize(p->ev1));
+  CUDA_TRY(cudaEventElapsedTime(&p->last_ms, p->ev0, p->ev1));
+  for (fdtd_engine* h : hs) {
+    const int rc = check_status(h);
+    if (rc) return rc;
+  }
+  return 0;
+}
+
+int fdtd_bloch_last_ms(fdtd_bloch* p, float* ms) {
+  if (!p || !ms) return fail(FDTD_ERR_INVALID_ARG, "bad arguments");
+  *ms = p->last_ms;
   return 0;
 }
 

@@ -146,6 +146,19 @@ constexpr unsigned kClassCoef = 2u;
 // Fill p.warp_class (out) for chunk length p.CX: one warp per task.
 int launch_classify(const StepParams& p, int n_kblocks, int n_chunks, unsigned char* out, cudaStream_t stream);
 
+// Wrap faces (periodic / Bloch axes): the new-E output, old-E and new-H
+// inputs of one field channel after its step kernel, for the wrap kernel
+// (bloch.cu) that updates the E cells the step kernel defers.
+struct WrapFields {
+  const float* eold[3];
+  float* enew[3];
+  const float* hnew[3];
+};
+int64_t wrap_cell_count(const StepParams& p);
+// pim / fi: the imaginary channel of a Bloch pair, or nullptr (real periodic).
+int launch_wrap_fixup(const StepParams& pr, const StepParams* pim, const WrapFields& fr, const WrapFields* fi,
+                      const float* phase_cos, const float* phase_sin, int n, cudaStream_t stream);
+
 constexpr int kStoreF32 = 0;
 constexpr int kStoreF16 = 1;
 constexpr int kStoreBF16 = 2;

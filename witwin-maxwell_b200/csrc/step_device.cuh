@@ -147,9 +147,11 @@ __device__ __forceinline__ void add_terms(const StepParams& p, int phase, int ba
 // a batch of three spills registers there and costs more than it hides.
 #define FDTD_ADE_BATCH 1
 #endif
+// comp_mask: bit c set when component c is updated here (deferred wrap-face
+// components are advanced by the wrap kernel instead).
 template <typename TA = float>
 __device__ __forceinline__ void ade(const StepParams& p, unsigned lane_poles, int i, int j, int k, float e0, float e1,
-                                    float e2, float& v0, float& v1, float& v2) {
+                                    float e2, float& v0, float& v1, float& v2, unsigned comp_mask = 7u) {
   constexpr int kB = FDTD_ADE_BATCH;
   const int b = __ldg(p.pole_plane_ptr + i), e = __ldg(p.pole_plane_ptr + i + 1);
   for (int x0 = b; x0 < e; x0 += kB) {
@@ -167,6 +169,7 @@ __device__ __forceinline__ void ade(const StepParams& p, unsigned lane_poles, in
         const int id = __ldg(p.pole_plane_ids + x0 + u);
         const PoleTerm* pt = p.poles + id;
         act[u] = id < 32 ? ((lane_poles >> id) & 1u) != 0 : (j >= pt->j0 && j < pt->j1 && k >= pt->k0 && k < pt->k1);
+        act[u] = act[u] && ((comp_mask >> pt->comp) & 1u);
         pts[u] = pt;
       }
       if (act[u]) {
@@ -212,12 +215,20 @@ __device__ __forceinline__ void ade(const StepParams& p, unsigned lane_poles, in
 }
 
 // E edge status (electric.cu:242-268): 0 update, 1 keep (NONE/PML edge),
-// 2 PEC zero, 3 outside the Yee extent (stays zero).
+// 2 PEC zero, 3 outside the Yee extent (stays zero), 4 deferred: a cell on a
+// periodic or Bloch face, whose backward difference wraps to the far side of
+// the grid; the step kernel leaves it (and its ADE state) alone and the wrap
+// kernel (bloch.cu) updates it once the whole new H is in memory
+// (electric.cu:133-168 bloch_backward_diff_axis, :23-40 boundary_diff_*).
+constexpr int kModeDeferred = 4;
+__host__ __device__ __forceinline__ bool wraps(int mode) { return mode == BND_PERIODIC || mode == BND_BLOCH; }
 __device__ __forceinline__ int edge_mode(bool in_extent, bool alo, bool ahi, bool blo, bool bhi, int ma_lo, int ma_hi,
                                          int mb_lo, int mb_hi) {
   if (!in_extent) return 3;
   if ((alo && ma_lo == BND_PEC) || (ahi && ma_hi == BND_PEC) || (blo && mb_lo == BND_PEC) || (bhi && mb_hi == BND_PEC))
     return 2;
+  if ((alo && wraps(ma_lo)) || (ahi && wraps(ma_hi)) || (blo && wraps(mb_lo)) || (bhi && wraps(mb_hi)))
+    return kModeDeferred;
   return (alo || ahi || blo || bhi) ? 1 : 0;
 }
 

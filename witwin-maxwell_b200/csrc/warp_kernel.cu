@@ -285,12 +285,17 @@ __device__ __forceinline__ void march(const StepParams& p, int n, int lane, int 
       float v2 = pick(m2, ec2 * g2 + c2 * (d2a - d2b), ec2);
       // ADE subtraction, TFSF electric corrections and soft sources: the
       // additive terms of witwin/maxwell/fdtd/runtime/stepping.py:2295-2320.
-      if (pb & kPlanePoles) ade<TA>(p, lane_poles, i, j, k, ec0, ec1, ec2, v0, v1, v2);
+      if (pb & kPlanePoles) {
+        const unsigned upd = (m0 != kModeDeferred ? 1u : 0u) | (m1 != kModeDeferred ? 2u : 0u) |
+                             (m2 != kModeDeferred ? 4u : 0u);
+        ade<TA>(p, lane_poles, i, j, k, ec0, ec1, ec2, v0, v1, v2, upd);
+      }
       if ((pb & kPlaneETerms) || (lf & (kLfETermY | kLfETermZ)))
         add_terms(p, 0, 0, n, i, j, k, pb & kPlaneETerms, lf & kLfETermY, lf & kLfETermZ, v0, v1, v2);
-      stf<TS>(p.Eout[0], o + rc, v0, p.finv[0]);
-      stf<TS>(p.Eout[1], o + rc, v1, p.finv[1]);
-      stf<TS>(p.Eout[2], o + rc, v2, p.finv[2]);
+      // deferred (wrap-face) cells are written by the wrap kernel
+      if (m0 != kModeDeferred) stf<TS>(p.Eout[0], o + rc, v0, p.finv[0]);
+      if (m1 != kModeDeferred) stf<TS>(p.Eout[1], o + rc, v1, p.finv[1]);
+      if (m2 != kModeDeferred) stf<TS>(p.Eout[2], o + rc, v2, p.finv[2]);
     }
     hpz = hcz;
     hpy = hcy;

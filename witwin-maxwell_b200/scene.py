@@ -239,6 +239,22 @@ class PointDipole:
 
 
 @dataclass(frozen=True)
+class PlaneSource:
+    """Soft current sheet on the plane ``index`` normal to ``axis`` driving the
+    tangential component ``polarization`` over the whole plane, with the
+    transverse phase profile e^{i (k_x x + k_y y)} of the scene's Bloch
+    wavevector (a uniform sheet when it is zero).  The coefficient is the
+    component's -dt/eps times the inverse spacing along ``axis`` (a surface
+    current J_s adds -dt J_s / (eps d) to E, as injection.py:807-970 does for
+    soft surface sources)."""
+
+    axis: int
+    index: int
+    polarization: str
+    source_time: object
+
+
+@dataclass(frozen=True)
 class PlaneWaveTFSF:
     """Axis-aligned plane wave injected through a TFSF box (or slab along the propagation axis)."""
 
@@ -304,6 +320,10 @@ class Scene:
     monitors: list = field(default_factory=list)
     courant: float = 0.99
     dt: float | None = None
+    # Bloch wavevector (rad/m) of the x / y Bloch faces: the field on the high
+    # face is e^{i k L} times the field on the low face
+    # (witwin/maxwell/fdtd/boundary/bloch.py:79-90).
+    bloch_k: tuple[float, float, float] = (0.0, 0.0, 0.0)
 
     @property
     def nodes(self) -> tuple[int, int, int]:
@@ -342,6 +362,7 @@ class CompiledPatch:
     box: tuple[int, int, int, int, int, int]
     coeff: np.ndarray  # box-dense float32
     signal: np.ndarray  # float32 per step
+    channel: int = 0  # 0: the (real part of the) field, 1: the imaginary part of a Bloch field
 
 
 @dataclass
@@ -397,6 +418,11 @@ class CompiledScene:
     monitor_frequencies: dict
     window: np.ndarray  # float64 per step
     design: MaterialRegion | None = None
+    # Bloch faces: the field is complex (real and imaginary channels) and the
+    # wrap phase of axis a is bloch_cos[a] + i bloch_sin[a] = e^{i k_a L_a}.
+    complex_fields: bool = False
+    bloch_cos: tuple[float, float, float] = (1.0, 1.0, 1.0)
+    bloch_sin: tuple[float, float, float] = (0.0, 0.0, 0.0)
 
     @property
     def cells(self) -> int:
@@ -734,7 +760,11 @@ def compile_scene(scene: Scene, time_steps: int) -> CompiledScene:
         if isinstance(src, PointDipole):
             box, coeff = _dipole_patch(scene, src, eps, dt)
             patches.append(CompiledPatch(src.polarization, box, coeff, _source_signal(src.source_time, dt, time_steps)))
+        elif isinstance(src, PlaneSource):
+            patches.extend(_plane_source_patches(scene, src, eps, dt, time_steps))
         elif isinstance(src, PlaneWaveTFSF):
+            if any(b == BOUNDARY_BLOCH for b in scene.boundary):
+                raise ValueError("TFSF sources with Bloch faces are not supported; use PlaneSource")
             if aux_line is not None:
                 raise ValueError("one TFSF source per scene")
             curl_full = {}
@@ -769,9 +799,45 @@ def compile_scene(scene: Scene, time_steps: int) -> CompiledScene:
                 box = tuple(box)
             regions.append(CompiledRegion(mon.name, comp, box))
     window = np.ones(time_steps, dtype=np.float64)  # pulses force window "none" (spectral.py:244-267)
+    complex_fields = any(b == BOUNDARY_BLOCH for b in scene.boundary)
+    bcos, bsin = [1.0, 1.0, 1.0], [0.0, 0.0, 0.0]
+    for a in range(3):
+        if scene.boundary[2 * a] == BOUNDARY_BLOCH:
+            angle = float(scene.bloch_k[a]) * float(scene.cells[a]) * d
+            bcos[a], bsin[a] = math.cos(angle), math.sin(angle)
     return CompiledScene(
         nodes=nodes, spacing=d, dt=dt, time_steps=time_steps, boundary=tuple(scene.boundary), pml_lo=pml_lo,
         pml_hi=pml_hi, inv_e=inv_e, inv_h=inv_h, cpml=cp, eps=eps, decay=decay, curl=curl, uniform=uniform,
         poles=poles, patches=patches, aux_line=aux_line, line_patches=line_patches, regions=regions,
         frequencies=tuple(freq_list), monitor_frequencies=mon_freqs, window=window, design=design,
+        complex_fields=complex_fields, bloch_cos=tuple(bcos), bloch_sin=tuple(bsin),
     )
+
+
+def _plane_source_patches(scene: Scene, src: PlaneSource, eps: dict, dt: float, steps: int) -> list:
+    """Patches of a PlaneSource: the real part (channel 0) and, on a Bloch
+    scene, the imaginary part (channel 1) of coeff * e^{i k.r} over the plane."""
+    name = src.polarization
+    if "xyz".index(name[1]) == src.axis:
+        raise ValueError("a plane source drives a component tangential to its plane")
+    d = float(scene.spacing)
+    shape = component_shape(name, scene.nodes)
+    box = [0, shape[0], 0, shape[1], 0, shape[2]]
+    box[2 * src.axis], box[2 * src.axis + 1] = int(src.index), int(src.index) + 1
+    if not 0 <= src.index < shape[src.axis]:
+        raise ValueError("plane source index outside the component")
+    own = "xyz".index(name[1])
+    coords = []
+    for a in range(3):
+        c = np.arange(box[2 * a], box[2 * a + 1], dtype=np.float64) * d
+        coords.append(c + (0.5 * d if a == own else 0.0))
+    phase = (float(scene.bloch_k[0]) * coords[0][:, None, None] + float(scene.bloch_k[1]) * coords[1][None, :, None]
+             + 0.0 * coords[2][None, None, :])
+    sl = tuple(slice(box[2 * a], box[2 * a + 1]) for a in range(3))
+    base = (np.float64(-dt) / eps[name][sl].astype(np.float64)) / d
+    signal = _source_signal(src.source_time, dt, steps)
+    out = [CompiledPatch(name, tuple(box), np.ascontiguousarray((base * np.cos(phase)).astype(np.float32)), signal, 0)]
+    if any(b == BOUNDARY_BLOCH for b in scene.boundary):
+        out.append(CompiledPatch(name, tuple(box), np.ascontiguousarray((base * np.sin(phase)).astype(np.float32)),
+                                 signal, 1))
+    return out

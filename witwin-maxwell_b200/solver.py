@@ -58,6 +58,8 @@ class B200FDTD:
         self.tile_rows = int(tile_rows)
         self.chunk_planes = int(chunk_planes)
         self.handle = None
+        self.handle_imag = None  # imaginary-part engine of a Bloch scene
+        self.pair = None  # fdtd_bloch pair coupling the two on the Bloch faces
         self.region_base: list[int] = []
         self.n_samples = 0
         self.pole_ids: list[int] = []
@@ -72,10 +74,30 @@ class B200FDTD:
 
     def init_field(self) -> "B200FDTD":
         cs = self.compiled
+        with torch.cuda.device(self.device):
+            self.stream = torch.cuda.current_stream(self.device)
+        self.handle = self._build_engine(0)
+        self.handle_imag = None
+        self.pair = None
+        if cs.complex_fields:
+            # Bloch faces: the imaginary part is a second engine, coupled to the
+            # first on the wrap faces by fdtd_bloch_step_range
+            self.handle_imag = self._build_engine(1)
+            pc = (ctypes.c_float * 3)(*cs.bloch_cos)
+            ps = (ctypes.c_float * 3)(*cs.bloch_sin)
+            pair = ctypes.c_void_p()
+            _lib.check(self.lib.fdtd_bloch_create(self.handle, self.handle_imag, pc, ps, ctypes.byref(pair)),
+                       "fdtd_bloch_create")
+            self.pair = pair
+        return self
+
+    def _build_engine(self, channel: int):
+        """Create and finalize one engine for this scene: channel 0 holds the
+        field (the real part on a Bloch scene), channel 1 the imaginary part."""
+        cs = self.compiled
         lib = self.lib
         with torch.cuda.device(self.device):
-            stream = torch.cuda.current_stream(self.device)
-            self.stream = stream
+            stream = self.stream
             desc = _lib.FdtdGridDesc()
             desc.nx, desc.ny, desc.nz = (int(n) for n in cs.nodes)
             desc.dt = float(cs.dt)
@@ -90,7 +112,6 @@ class B200FDTD:
             handle = ctypes.c_void_p()
             _lib.check(lib.fdtd_engine_create(ctypes.byref(desc), ctypes.c_void_p(stream.cuda_stream), ctypes.byref(handle)),
                        "fdtd_engine_create")
-            self.handle = handle
             h = handle
             if self.storage != "fp32" or self.storage_scales_arg is not None:
                 sc = None
@@ -132,6 +153,8 @@ class B200FDTD:
                 )
                 self.pole_ids.append(pid.value)
             for patch in cs.patches:
+                if getattr(patch, "channel", 0) != channel:
+                    continue
                 sig = self._dev(patch.signal)
                 _lib.check(
                     lib.fdtd_engine_add_patch(
@@ -140,7 +163,7 @@ class B200FDTD:
                     ),
                     "add_patch",
                 )
-            if cs.aux_line is not None:
+            if cs.aux_line is not None and channel == 0:
                 aux = cs.aux_line
                 line = ctypes.c_int()
                 src = self._dev(aux.source)
@@ -185,15 +208,19 @@ class B200FDTD:
             _lib.check(lib.fdtd_engine_finalize(h), "finalize")
             torch.cuda.synchronize(self.device)
             self._keep.clear()
-        return self
+        return h
 
     # --------------------------------------------------------------- stepping
     def step_range(self, n0: int, n1: int) -> float:
         """Advance steps [n0, n1); returns the device time in ms (CUDA events)."""
-        _lib.check(self.lib.fdtd_engine_step_range(self.handle, int(n0), int(n1)), "step_range")
-        self.steps_done = max(self.steps_done, int(n1))
         ms = ctypes.c_float()
-        _lib.check(self.lib.fdtd_engine_last_ms(self.handle, ctypes.byref(ms)), "last_ms")
+        if getattr(self, "pair", None) is not None:
+            _lib.check(self.lib.fdtd_bloch_step_range(self.pair, int(n0), int(n1)), "fdtd_bloch_step_range")
+            _lib.check(self.lib.fdtd_bloch_last_ms(self.pair, ctypes.byref(ms)), "fdtd_bloch_last_ms")
+        else:
+            _lib.check(self.lib.fdtd_engine_step_range(self.handle, int(n0), int(n1)), "step_range")
+            _lib.check(self.lib.fdtd_engine_last_ms(self.handle, ctypes.byref(ms)), "last_ms")
+        self.steps_done = max(self.steps_done, int(n1))
         return float(ms.value)
 
     def time_kernel(self, n: int, reps: int) -> float:
@@ -247,10 +274,14 @@ class B200FDTD:
         _lib.check(self.lib.fdtd_engine_checkpoint_load(self.handle, int(slot)), "checkpoint_load")
 
     # ---------------------------------------------------------------- outputs
-    def field(self, name: str) -> torch.Tensor:
+    def field(self, name: str, imag: bool = False) -> torch.Tensor:
+        """A field component in its Yee shape (the imaginary part of a Bloch field with imag=True)."""
         shape = component_shape(name, self.compiled.nodes)
         out = torch.empty(shape, device=self.device, dtype=torch.float32)
-        _lib.check(self.lib.fdtd_engine_unpack_field(self.handle, COMP_INDEX[name], _lib.ptr(out)), "unpack_field")
+        h = self.handle_imag if imag else self.handle
+        if h is None:
+            raise ValueError("the scene has no imaginary field channel")
+        _lib.check(self.lib.fdtd_engine_unpack_field(h, COMP_INDEX[name], _lib.ptr(out)), "unpack_field")
         return out
 
     def set_field(self, name: str, value: torch.Tensor) -> None:
@@ -267,11 +298,13 @@ class B200FDTD:
         _lib.check(self.lib.fdtd_engine_pole_state(self.handle, self.pole_ids[index], _lib.ptr(pol), _lib.ptr(cur)), "pole_state")
         return pol, cur
 
-    def raw_dft(self) -> tuple[torch.Tensor, torch.Tensor]:
+    def raw_dft(self, imag: bool = False) -> tuple[torch.Tensor, torch.Tensor]:
+        """Unscaled DFT accumulators of one field channel, [freq][slot]."""
         nf = len(self.compiled.frequencies)
         re = torch.empty((nf, self.n_samples), device=self.device)
         im = torch.empty((nf, self.n_samples), device=self.device)
-        _lib.check(self.lib.fdtd_engine_read_dft(self.handle, _lib.ptr(re), _lib.ptr(im)), "read_dft")
+        h = self.handle_imag if imag else self.handle
+        _lib.check(self.lib.fdtd_engine_read_dft(h, _lib.ptr(re), _lib.ptr(im)), "read_dft")
         return re, im
 
     def monitor_results(self) -> dict:
@@ -280,6 +313,10 @@ class B200FDTD:
         if not cs.regions or not cs.frequencies:
             return {}
         re, im = self.raw_dft()
+        if getattr(self, "handle_imag", None) is not None:
+            # complex field F = A + iB: DFT(F) = DFT(A) + i DFT(B)
+            re_b, im_b = self.raw_dft(imag=True)
+            re, im = re - im_b, im + re_b
         norm = float(np.sum(cs.window[: self.steps_done]))
         scale = 2.0 / norm if norm > 0 else 0.0
         out: dict = {}
@@ -293,6 +330,12 @@ class B200FDTD:
         return out
 
     def close(self) -> None:
+        if getattr(self, "pair", None) is not None:
+            self.lib.fdtd_bloch_destroy(self.pair)
+            self.pair = None
+        if getattr(self, "handle_imag", None) is not None:
+            self.lib.fdtd_engine_destroy(self.handle_imag)
+            self.handle_imag = None
         if self.handle is not None:
             self.lib.fdtd_engine_destroy(self.handle)
             self.handle = None
