@@ -66,6 +66,20 @@ def test_small_scene_matches_reference_kernels():
     _compare(cs, 200)
 
 
+def test_full_field_dft_matches_reference_kernels():
+    """Full-field running DFT (VolumeMonitor over every cell of Ex, Ey, Ez and Hz)
+    of a 32^3 CPML scene with a dielectric box and a Drude slab, 200 steps, 4
+    frequencies: the engine's sample ring and batched flush against the
+    reference's fields accumulated in float64."""
+    wm = load_package()
+    sc = _c1_scene(wm, cells=32, pml=6)
+    sc.structures.append(wm.Structure(wm.Box((8, 0, 0), (12, 32, 32)), wm.Medium.drude(2e15 / (2 * np.pi), 1e14 / (2 * np.pi))))
+    sc.monitors = [wm.VolumeMonitor("volume", ("Ex", "Ey", "Ez", "Hz"), (250e12, 280e12, 310e12, 350e12))]
+    cs = wm.compile_scene(sc, 200)
+    assert len(cs.regions) == 4 and cs.regions[0].box == (0, 32, 0, 33, 0, 33)
+    _compare(cs, 200)
+
+
 def test_engine_beats_reference_kernel_sequence():
     wm = load_package()
     steps = 10

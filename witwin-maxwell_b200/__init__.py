@@ -28,6 +28,7 @@ from .scene import (
     PlaneWaveTFSF,
     PointDipole,
     PointMonitor,
+    VolumeMonitor,
     Scene,
     Sphere,
     Structure,

@@ -226,12 +226,13 @@ __global__ void sample_gather_kernel(const RegionFlush* regions, const FieldPtrs
                                      float* samples, int64_t n_samples, int slot) {
   const RegionFlush rg = regions[blockIdx.y];
   float* out = samples + static_cast<int64_t>(slot) * n_samples + rg.base;
-  for (int64_t x = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; x < rg.count;
-       x += static_cast<int64_t>(gridDim.x) * blockDim.x) {
-    const int lk = static_cast<int>(x % rg.nk);
-    const int64_t r = x / rg.nk;
-    const int lj = static_cast<int>(r % rg.nj);
-    const int li = static_cast<int>(r / rg.nj);
+  // 32-bit cell arithmetic: a region holds fewer than 2^31 cells (checked at set-up)
+  const int count = static_cast<int>(rg.count), nk = rg.nk, nj = rg.nj;
+  for (int x = blockIdx.x * blockDim.x + threadIdx.x; x < count; x += gridDim.x * blockDim.x) {
+    const int r = x / nk;
+    const int lk = x - r * nk;
+    const int li = r / nj;
+    const int lj = r - li * nj;
     out[x] = load_field(fields, rg.comp, (static_cast<int64_t>(rg.i0 + li) * NY + rg.j0 + lj) * P + rg.k0 + lk);
   }
 }
@@ -1353,6 +1354,8 @@ int fdtd_engine_add_sample_region(fdtd_engine* h, int comp, const int* box, int6
   if (!h || comp < 0 || comp > 5 || !box) return fail(FDTD_ERR_INVALID_ARG, "bad sample region arguments");
   if (h->finalized) return fail(FDTD_ERR_STATE, "engine already finalized");
   if (!box_ok(h, comp, box)) return fail(FDTD_ERR_INVALID_ARG, "sample region outside the component extent");
+  if (static_cast<int64_t>(box[1] - box[0]) * (box[3] - box[2]) * (box[5] - box[4]) >= (int64_t(1) << 31))
+    return fail(FDTD_ERR_INVALID_ARG, "a sample region holds at most 2^31 - 1 cells");
   SampleRegion r{};
   r.comp = comp;
   r.i0 = box[0];

@@ -285,6 +285,20 @@ class PointMonitor:
     frequencies: tuple[float, ...] = ()
 
 
+@dataclass(frozen=True)
+class VolumeMonitor:
+    """Running DFT of whole field components over a box of cells (the full grid
+    by default): the reference's full-field DFT (runtime/spectral.py:309-652,
+    kernels/spectral.cu:9-146, E components by default), accumulated through
+    the engine's monitor sample ring and batched flush like every monitor."""
+
+    name: str
+    components: tuple[str, ...] = ("Ex", "Ey", "Ez")
+    frequencies: tuple[float, ...] = ()
+    lo: tuple[int, int, int] | None = None
+    hi: tuple[int, int, int] | None = None
+
+
 def tangential_components(axis: int) -> tuple[str, ...]:
     """Tangential field components of a monitor plane (witwin/maxwell/monitors.py:71-77)."""
     return {0: ("Ey", "Ez", "Hy", "Hz"), 1: ("Ex", "Ez", "Hx", "Hz"), 2: ("Ex", "Ey", "Hx", "Hy")}[axis]
@@ -787,6 +801,10 @@ def compile_scene(scene: Scene, time_steps: int) -> CompiledScene:
             if isinstance(mon, PointMonitor):
                 i, j, k = mon.index
                 box = (i, i + 1, j, j + 1, k, k + 1)
+            elif isinstance(mon, VolumeMonitor):
+                lo = mon.lo if mon.lo is not None else (0, 0, 0)
+                hi = mon.hi if mon.hi is not None else shape
+                box = tuple(v for a in range(3) for v in (int(lo[a]), min(int(hi[a]), shape[a])))
             else:
                 box = [0, shape[0], 0, shape[1], 0, shape[2]]
                 box[2 * mon.axis] = mon.index
