@@ -505,15 +505,8 @@ def run_adjoint_bench(wm, device):
 
 def run_e2e(args, wm, cs, device, world):
     """Gcell-updates/s of Simulation-style solve from host buffers: upload the compiled
-    scene tensors (pinned), run the steps, read the monitor spectra back."""
+    scene tensors from host memory, run the steps, read the monitor spectra back."""
     import torch
-
-    pinned = {}
-
-    def pin(a):
-        t = torch.as_tensor(np.ascontiguousarray(a)).pin_memory()
-        pinned[id(a)] = t
-        return t
 
     h2d = 0
     for arr in [*cs.inv_e, *cs.inv_h, *[x for v in cs.cpml.values() for x in v]]:
@@ -548,7 +541,6 @@ def run_e2e(args, wm, cs, device, world):
     elapsed = max_over_ranks(elapsed, world, device)
     d2h = sum(v.numel() * v.element_size() for d in host.values() for v in d.values())
     solver.close()
-    del pinned
     return {
         "value": cs.cells * args.steps * world / elapsed / 1e9,
         "unit": METRIC,
@@ -556,7 +548,7 @@ def run_e2e(args, wm, cs, device, world):
         "d2h_bytes_per_step": int(round(d2h / args.steps)),
         "h2d_bytes_per_solve": int(h2d),
         "d2h_bytes_per_solve": int(d2h),
-        "what": f"one solve of {args.steps} steps through B200FDTD: scene upload from pinned host memory, engine build, "
+        "what": f"one solve of {args.steps} steps through B200FDTD: scene upload from host (numpy) arrays, engine build, "
                 "stepping, spectra read-back (after one untimed short solve); the per-step bytes are the solve's "
                 "bytes over its steps",
         "wall_s": elapsed,
