@@ -123,6 +123,8 @@ int fdtd_engine_unpack_psi(fdtd_engine* h, int comp, int which, float* dst);
 int fdtd_engine_add_pole(fdtd_engine* h, int comp, int kind, const int* box, const float* drive,
                          const float* inv_eps, float decay, float restoring, int* pole_id);
 int fdtd_engine_pole_state(fdtd_engine* h, int pole_id, float* pol_out, float* cur_out);
+/* Overwrite a pole's state (box-dense, either pointer may be NULL); FP32 or FP16 field storage. */
+int fdtd_engine_set_pole_state(fdtd_engine* h, int pole_id, const float* pol, const float* cur);
 
 /* Soft source patch: comp gets coeff[cell] * signal[n] added at step n
  * (witwin/maxwell/fdtd/cuda/kernels/sources.cu:135-154; the signal table
@@ -243,8 +245,11 @@ int fdtd_bloch_last_ms(fdtd_bloch* p, float* ms);
  * fdtd_engine_adjoint_init: allocate and zero the adjoint state.
  * design_boxes holds 6 ints per E component ([i0,i1,j0,j1,k0,k1] in that
  * component's Yee index space; an empty box means none) or is NULL.  Boxes
- * must stay clear of CPML slabs and domain edges.  max_segment is
- * the longest replay (steps).  Scenes with ADE poles return FDTD_ERR_UNSUPPORTED. */
+ * must stay clear of CPML slabs and domain edges, and of the boxes of ADE
+ * poles of their component.  max_segment is the longest replay (steps).
+ * Dispersive (ADE) media carry adjoint pole state through the exact transpose
+ * of the Debye / Drude / Lorentz recursions (the reference's dispersive reverse
+ * runner, witwin/maxwell/fdtd/adjoint/native.py:2104). */
 int fdtd_engine_adjoint_init(fdtd_engine* h, const int* design_boxes, int max_segment);
 /* Monitor gradients dL/d(unscaled DFT accumulator), [n_freq][n_samples]
  * (host or device pointers); NULL clears the seeds. */
@@ -265,7 +270,8 @@ int fdtd_engine_adjoint_range(fdtd_engine* h, int n1, int n0);
 int fdtd_engine_adjoint_grad(fdtd_engine* h, int comp, float* out);
 /* Adjoint state in the reference's shapes: kind 0 = field component comp
  * (0..5, which ignored), kind 1 = CPML psi (comp 0..5, which 0/1 as
- * fdtd_engine_pack_psi). */
+ * fdtd_engine_pack_psi), kind 2 = ADE pole state (comp = pole id, which 0 = the
+ * adjoint of P, 1 = the adjoint of J; box-dense). */
 int fdtd_engine_adjoint_pack(fdtd_engine* h, int kind, int comp, int which, const float* src);
 int fdtd_engine_adjoint_unpack(fdtd_engine* h, int kind, int comp, int which, float* dst);
 

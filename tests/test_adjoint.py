@@ -43,22 +43,32 @@ def _psi_shapes(cs):
     return shapes
 
 
-def _scene(wm, boundary=None):
+def _scene(wm, boundary=None, dispersive=False):
     sc = wm.Scene(cells=(20, 18, 16), spacing=25e-9, pml_cells=4)
     if boundary is not None:
         sc.boundary = boundary
         sc.pml_cells = 0 if all(b != wm.BOUNDARY_PML for b in boundary) else 4
     sc.structures.append(wm.Structure(wm.Box((6, 5, 5), (12, 11, 10)), wm.Medium(eps_r=3.0)))
+    if dispersive:
+        # one medium of each ADE kind, the Drude slab reaching into the CPML
+        sc.structures.append(wm.Structure(wm.Box((13, 2, 3), (15, 16, 13)), wm.Medium.drude(2e15 / (2 * np.pi), 1e14 / (2 * np.pi))))
+        sc.structures.append(wm.Structure(wm.Sphere((8, 8, 11), 2.5), wm.Medium.lorentz(2.0, 3.0, 250e12, 20e12)))
+        sc.structures.append(wm.Structure(wm.Box((4, 12, 4), (7, 15, 8)), wm.Medium.debye(2.5, 3.5, 1e-14)))
     return sc
 
 
-@pytest.mark.parametrize("kind", ["cpml", "pec", "mixed"])
+@pytest.mark.parametrize("kind", ["cpml", "pec", "mixed", "dispersive"])
 def test_adjoint_step_is_the_exact_transpose(kind):
+    """<F x, y> = <x, F^T y> over E, H, CPML psi and (dispersive) the ADE pole
+    state: P of Debye and Lorentz poles, J of Drude and Lorentz poles (the J a
+    Debye pole stores is an output of the step, not a state it reads)."""
     wm = load_package()
     lib = wm._lib.load()
     P, E, N = wm.BOUNDARY_PML, wm.BOUNDARY_PEC, wm.BOUNDARY_NONE
-    boundary = {"cpml": None, "pec": (E,) * 6, "mixed": (P, E, N, P, P, E)}[kind]
-    cs = wm.compile_scene(_scene(wm, boundary), 4)
+    boundary = {"cpml": None, "pec": (E,) * 6, "mixed": (P, E, N, P, P, E), "dispersive": None}[kind]
+    cs = wm.compile_scene(_scene(wm, boundary, dispersive=kind == "dispersive"), 4)
+    if kind == "dispersive":
+        assert {p.kind for p in cs.poles} == {0, 1, 2}
     solver = wm.solver.B200FDTD(cs).init_field()
     h = solver.handle
     wm._lib.check(lib.fdtd_engine_adjoint_init(h, None, 1), "adjoint_init")
@@ -73,12 +83,24 @@ def test_adjoint_step_is_the_exact_transpose(kind):
     for (comp, which), shape in psi.items():
         x[("p", comp, which)] = torch.tensor(rng.standard_normal(shape), dtype=torch.float32, device=dev)
         y[("p", comp, which)] = torch.tensor(rng.standard_normal(shape), dtype=torch.float32, device=dev)
+    for pid, pole in enumerate(cs.poles):
+        b = pole.box
+        shape = (b[1] - b[0], b[3] - b[2], b[5] - b[4])
+        for which in (0, 1):  # 0: P, 1: J
+            x[("a", pid, which)] = torch.tensor(rng.standard_normal(shape), dtype=torch.float32, device=dev)
+            state = (which == 0 and pole.kind in (0, 2)) or (which == 1 and pole.kind in (1, 2))
+            yv = rng.standard_normal(shape) if state else np.zeros(shape)
+            y[("a", pid, which)] = torch.tensor(yv, dtype=torch.float32, device=dev)
+    kind_code = {"f": 0, "p": 1, "a": 2}
     # forward: F x
     for (kd, comp, which), t in x.items():
         if kd == "f":
             wm._lib.check(lib.fdtd_engine_pack_field(h, comp, wm._lib.ptr(t)), "pack")
-        else:
+        elif kd == "p":
             wm._lib.check(lib.fdtd_engine_pack_psi(h, comp, which, wm._lib.ptr(t)), "pack_psi")
+        else:
+            args = (wm._lib.ptr(t), None) if which == 0 else (None, wm._lib.ptr(t))
+            wm._lib.check(lib.fdtd_engine_set_pole_state(h, solver.pole_ids[comp], *args), "set_pole_state")
     solver.step_range(0, 1)
     fx = {}
     for key, t in x.items():
@@ -86,18 +108,21 @@ def test_adjoint_step_is_the_exact_transpose(kind):
         kd, comp, which = key
         if kd == "f":
             wm._lib.check(lib.fdtd_engine_unpack_field(h, comp, wm._lib.ptr(out)), "unpack")
-        else:
+        elif kd == "p":
             wm._lib.check(lib.fdtd_engine_unpack_psi(h, comp, which, wm._lib.ptr(out)), "unpack_psi")
+        else:
+            args = (wm._lib.ptr(out), None) if which == 0 else (None, wm._lib.ptr(out))
+            wm._lib.check(lib.fdtd_engine_pole_state(h, solver.pole_ids[comp], *args), "pole_state")
         fx[key] = out
     # adjoint: F^T y
     for (kd, comp, which), t in y.items():
-        wm._lib.check(lib.fdtd_engine_adjoint_pack(h, 0 if kd == "f" else 1, comp, which, wm._lib.ptr(t)), "adj_pack")
+        wm._lib.check(lib.fdtd_engine_adjoint_pack(h, kind_code[kd], comp, which, wm._lib.ptr(t)), "adj_pack")
     wm._lib.check(lib.fdtd_engine_adjoint_range(h, 1, 0), "adjoint_range")
     fty = {}
     for key, t in y.items():
         out = torch.empty_like(t)
         kd, comp, which = key
-        wm._lib.check(lib.fdtd_engine_adjoint_unpack(h, 0 if kd == "f" else 1, comp, which, wm._lib.ptr(out)), "adj_unpack")
+        wm._lib.check(lib.fdtd_engine_adjoint_unpack(h, kind_code[kd], comp, which, wm._lib.ptr(out)), "adj_unpack")
         fty[key] = out
     torch.cuda.synchronize()
     lhs = sum(float((fx[k].double() * y[k].double()).sum()) for k in x)
@@ -107,8 +132,12 @@ def test_adjoint_step_is_the_exact_transpose(kind):
     assert abs(lhs - rhs) <= 1e-5 * scale, (lhs, rhs, scale)
 
 
-def _design_scene(wm, eps_r):
+def _design_scene(wm, eps_r, dispersive=False):
     sc = wm.Scene(cells=(28, 24, 24), spacing=25e-9, pml_cells=5)
+    if dispersive:
+        # a Lorentz block between the design region and the probe, a Drude block behind the source
+        sc.structures.append(wm.Structure(wm.Box((17, 9, 9), (19, 15, 15)), wm.Medium.lorentz(2.0, 3.0, 250e12, 20e12)))
+        sc.structures.append(wm.Structure(wm.Box((6, 8, 8), (7, 16, 16)), wm.Medium.drude(2e15 / (2 * np.pi), 1e14 / (2 * np.pi))))
     sc.sources.append(wm.PointDipole((9, 12, 12), "Ez", wm.GaussianPulse(300e12, 100e12), width=25e-9))
     sc.material_regions.append(wm.MaterialRegion((12, 10, 10), (16, 14, 13), eps_r))
     sc.monitors.append(wm.PointMonitor("probe", (20, 12, 12), frequencies=(300e12,)))
@@ -119,13 +148,14 @@ def _loss(mons):
     return sum(float(np.sum(np.abs(np.asarray(v.cpu().numpy())) ** 2)) for v in mons["probe"].values())
 
 
-def test_design_gradient_matches_finite_differences():
+@pytest.mark.parametrize("dispersive", [False, True])
+def test_design_gradient_matches_finite_differences(dispersive):
     wm = load_package()
     adj = wm.adjoint
     steps = 320
     rng = np.random.default_rng(3)
     eps_r = 2.0 + 2.0 * rng.random((4, 4, 3))
-    problem = adj.DesignProblem(_design_scene(wm, eps_r), steps, stride=64, history="replay")
+    problem = adj.DesignProblem(_design_scene(wm, eps_r, dispersive), steps, stride=64, history="replay")
     mons = problem.forward(eps_r)
     grad_out = {"probe": {c: 2.0 * v for c, v in mons["probe"].items()}}  # d sum|X|^2 / dX* convention
     g = problem.backward(grad_out)
@@ -139,7 +169,7 @@ def test_design_gradient_matches_finite_differences():
         for sgn in (1.0, -1.0):
             e = eps_r.copy()
             e[idx] += sgn * h
-            p = adj.DesignProblem(_design_scene(wm, e), steps, stride=steps)
+            p = adj.DesignProblem(_design_scene(wm, e, dispersive), steps, stride=steps)
             vals.append(_loss(p.forward(e)))
             p.close()
         fd = (vals[0] - vals[1]) / (2 * h)
@@ -165,13 +195,17 @@ def test_design_gradient_through_autograd():
     np.testing.assert_allclose(t.grad.numpy(), g2, rtol=1e-4, atol=1e-6 * np.abs(g2).max())
 
 
-def test_adjoint_rejects_dispersive_scenes_and_edge_designs():
+def test_adjoint_rejects_designs_on_ade_cells_and_edges():
     wm = load_package()
     lib = wm._lib.load()
     sc = _design_scene(wm, np.full((4, 4, 3), 2.0))
-    sc.structures.append(wm.Structure(wm.Box((2, 2, 2), (5, 5, 5)), wm.Medium.drude(2e15 / (2 * np.pi), 1e14 / (2 * np.pi))))
-    solver = wm.solver.B200FDTD(wm.compile_scene(sc, 10)).init_field()
-    assert lib.fdtd_engine_adjoint_init(solver.handle, None, 4) == -3
+    sc.structures.append(wm.Structure(wm.Box((10, 9, 9), (14, 13, 12)), wm.Medium.drude(2e15 / (2 * np.pi), 1e14 / (2 * np.pi))))
+    cs = wm.compile_scene(sc, 10)
+    solver = wm.solver.B200FDTD(cs).init_field()
+    ez = next(p.box for p in cs.poles if p.component == "Ex")
+    box = (ctypes.c_int * 18)(*(list(ez) + [0] * 12))  # the Ex design box on the Drude cells
+    assert lib.fdtd_engine_adjoint_init(solver.handle, box, 4) == -1
+    assert b"ADE" in lib.fdtd_last_error()
     solver.close()
     solver = wm.solver.B200FDTD(wm.compile_scene(_design_scene(wm, np.full((4, 4, 3), 2.0)), 10)).init_field()
     bad = (ctypes.c_int * 18)(*([1, 5, 3, 6, 3, 6] + [0] * 12))  # reaches into the CPML slab

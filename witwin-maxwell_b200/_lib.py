@@ -62,6 +62,7 @@ _SIGNATURES = {
     "fdtd_engine_unpack_psi": ([_vp, _i, _i, _vp], _i),
     "fdtd_engine_add_pole": ([_vp, _i, _i, _c_int_p, _vp, _vp, _f, _f, _c_int_p], _i),
     "fdtd_engine_pole_state": ([_vp, _i, _vp, _vp], _i),
+    "fdtd_engine_set_pole_state": ([_vp, _i, _vp, _vp], _i),
     "fdtd_engine_add_patch": ([_vp, _i, _c_int_p, _vp, _vp, _i, _f], _i),
     "fdtd_engine_add_aux_line": ([_vp, _i, _vp, _vp, _vp, _vp, _i, _vp, _i, _c_int_p], _i),
     "fdtd_engine_add_line_patch": ([_vp, _i, _c_int_p, _vp, _i, _i, _vp, _i, _f], _i),

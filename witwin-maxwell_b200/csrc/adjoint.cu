@@ -208,6 +208,41 @@ __global__ void adj_pass_b_kernel(const StepParams p, const AdjParams q) {
           d.grad[l] += -gp * (e_next - de * e_now) * ce * q.inv_dt;
         }
       }
+      // ADE poles of this component at this cell (every E mode: the forward
+      // subtracts dt J' / eps after the edge treatment, dispersive.cu:18-83).
+      // With u = gE' the adjoint of E^{n+1} and the pole's carried adjoint
+      // state of step n + 1:
+      //   Drude:   J' = a J + b E;             E' -= dt inv J'
+      //   Lorentz: J' = a J - r P + b E; P' = P + dt J';  E' -= dt inv J'
+      //   Debye:   P' = a P + b E;             E' -= inv (P' - P)
+      if (p.n_poles && (__ldg(p.plane_bits + i) & kPlanePoles)) {
+        const int pb = __ldg(p.pole_plane_ptr + i), pe = __ldg(p.pole_plane_ptr + i + 1);
+        for (int xx = pb; xx < pe; ++xx) {
+          const int id = __ldg(p.pole_plane_ids + xx);
+          const PoleTerm& pt = p.poles[id];
+          if (pt.comp != c || j < pt.j0 || j >= pt.j1 || k < pt.k0 || k >= pt.k1) continue;
+          const int64_t o = (static_cast<int64_t>(i - pt.i0) * (pt.j1 - pt.j0) + (j - pt.j0)) * pt.nkk + (k - pt.kk0);
+          const float inv = __ldg(pt.inv_eps + o), b = __ldg(pt.drive + o);
+          if (pt.kind == 1) {
+            float* gj = q.gcur[id] + o;
+            const float ge = *gj - pt.dt * inv * gp;
+            g += b * ge;
+            *gj = pt.decay * ge;
+          } else if (pt.kind == 2) {
+            float* gj = q.gcur[id] + o;
+            float* gq = q.gpol[id] + o;
+            const float ge = *gj + pt.dt * *gq - pt.dt * inv * gp;
+            g += b * ge;
+            *gj = pt.decay * ge;
+            *gq = *gq - pt.restoring * ge;
+          } else {
+            float* gq = q.gpol[id] + o;
+            const float ge = *gq - inv * gp;
+            g += b * ge;
+            *gq = pt.decay * ge + inv * gp;
+          }
+        }
+      }
       q.gE[c][x] = g;
     }
   }

@@ -26,6 +26,10 @@ struct AdjParams {
   DesignBox design[3];
   int hist_slot;  // history slot of E^n for the reverse step of step n
   float inv_dt;
+  // Adjoint ADE pole state, per pole id in the forward pole-state layout:
+  // gpol (adjoint of P; Debye, Lorentz) and gcur (adjoint of J; Drude, Lorentz).
+  float* const* gpol;
+  float* const* gcur;
 };
 
 // Reverse step of step n: seeds of step n, then passes A, B, C.

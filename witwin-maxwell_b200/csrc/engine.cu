@@ -343,6 +343,7 @@ struct AdjointHost {
   bool ready = false;
   AdjParams q{};
   std::vector<float*> bufs;  // everything allocated for the adjoint
+  std::vector<float*> gpol_host, gcur_host;  // adjoint pole state per pole id
   int max_segment = 0;
   int replay_n0 = -1, replay_n1 = -1;
 };
@@ -1251,6 +1252,17 @@ int fdtd_engine_pole_state(fdtd_engine* h, int pole_id, float* pol_out, float* c
   return 0;
 }
 
+int fdtd_engine_set_pole_state(fdtd_engine* h, int pole_id, const float* pol, const float* cur) {
+  if (!h || pole_id < 0 || pole_id >= static_cast<int>(h->poles.size()))
+    return fail(FDTD_ERR_INVALID_ARG, "bad pole id");
+  if (h->storage == kStoreBF16) return fail(FDTD_ERR_UNSUPPORTED, "pole state is BF16 here: set it through FP32 storage");
+  const PoleHost& ph = h->poles[pole_id];
+  const size_t w = ph.nk * sizeof(float), pitch = ph.nkk * sizeof(float);
+  if (pol) CUDA_TRY(cudaMemcpy2DAsync(ph.pol + ph.koff, pitch, pol, w, w, ph.rows, cudaMemcpyDefault, h->stream));
+  if (cur) CUDA_TRY(cudaMemcpy2DAsync(ph.cur + ph.koff, pitch, cur, w, w, ph.rows, cudaMemcpyDefault, h->stream));
+  return 0;
+}
+
 int fdtd_engine_add_patch(fdtd_engine* h, int comp, const int* box, const float* coeff, const float* signal,
                           int n_signal, float scale) {
   if (!h || comp < 0 || comp > 5 || !box || !coeff || !signal || n_signal <= 0)
@@ -1860,7 +1872,6 @@ static int adj_alloc(fdtd_engine* h, float** out, size_t n) {
 int fdtd_engine_adjoint_init(fdtd_engine* h, const int* design_boxes, int max_segment) {
   if (!h || max_segment < 1) return fail(FDTD_ERR_INVALID_ARG, "bad adjoint arguments");
   if (!h->finalized) return fail(FDTD_ERR_STATE, "engine not finalized");
-  if (!h->poles.empty()) return fail(FDTD_ERR_UNSUPPORTED, "the adjoint of dispersive (ADE) media is not supported");
   if (h->storage != kStoreF32) return fail(FDTD_ERR_UNSUPPORTED, "the adjoint runs on FP32 field storage only");
   if (h->wrap) return fail(FDTD_ERR_UNSUPPORTED, "the adjoint of periodic and Bloch faces is not supported");
   if (h->adj.ready) return fail(FDTD_ERR_STATE, "adjoint already initialised");
@@ -1878,6 +1889,27 @@ int fdtd_engine_adjoint_init(fdtd_engine* h, const int* design_boxes, int max_se
       if (rc) return rc;
     }
   }
+  if (!h->poles.empty()) {
+    // adjoint pole state, laid out as the forward pole state
+    std::vector<float*> gp(h->poles.size()), gc(h->poles.size());
+    for (size_t id = 0; id < h->poles.size(); ++id) {
+      int rc = adj_alloc(h, &gp[id], static_cast<size_t>(h->poles[id].state_floats));
+      if (!rc) rc = adj_alloc(h, &gc[id], static_cast<size_t>(h->poles[id].state_floats));
+      if (rc) return rc;
+    }
+    float** dgp = nullptr;
+    float** dgc = nullptr;
+    CUDA_TRY(cudaMalloc(&dgp, sizeof(float*) * gp.size()));
+    a.bufs.push_back(reinterpret_cast<float*>(dgp));
+    CUDA_TRY(cudaMalloc(&dgc, sizeof(float*) * gc.size()));
+    a.bufs.push_back(reinterpret_cast<float*>(dgc));
+    CUDA_TRY(cudaMemcpy(dgp, gp.data(), sizeof(float*) * gp.size(), cudaMemcpyHostToDevice));
+    CUDA_TRY(cudaMemcpy(dgc, gc.data(), sizeof(float*) * gc.size(), cudaMemcpyHostToDevice));
+    a.q.gpol = dgp;
+    a.q.gcur = dgc;
+    a.gpol_host = gp;
+    a.gcur_host = gc;
+  }
   a.q.n_samples = h->n_samples;
   a.q.inv_dt = static_cast<float>(1.0 / static_cast<double>(static_cast<float>(h->desc.dt)));
   a.max_segment = max_segment;
@@ -1893,6 +1925,12 @@ int fdtd_engine_adjoint_init(fdtd_engine* h, const int* design_boxes, int max_se
       const int n_ax = ax == 0 ? h->NX : (ax == 1 ? h->NY : h->NZ);
       if (b[2 * ax] < h->desc.pml_lo[ax] || b[2 * ax + 1] > n_ax - 1 - h->desc.pml_hi[ax])
         return fail(FDTD_ERR_INVALID_ARG, "design box reaches into a CPML slab or the domain edge");
+    }
+    // dE'/deps of a design cell assumes no ADE current there
+    for (const auto& ph : h->poles) {
+      const PoleTerm& t = ph.t;
+      if (t.comp == c && b[0] < t.i1 && t.i0 < b[1] && b[2] < t.j1 && t.j0 < b[3] && b[4] < t.k1 && t.k0 < b[5])
+        return fail(FDTD_ERR_INVALID_ARG, "design box overlaps a dispersive (ADE) region");
     }
     for (int ax = 0; ax < 3; ++ax) {
       d.lo[ax] = b[2 * ax];
@@ -2012,7 +2050,23 @@ static int adj_geometry(fdtd_engine* h, int kind, int comp, int which, float** b
   return L;
 }
 
+// Adjoint pole state (kind 2): comp = pole id, which = 0 (adjoint of P) or 1 (adjoint of J);
+// dense box-shaped [i][j][k] on the caller's side, z-padded rows in the engine.
+static int adj_pole_copy(fdtd_engine* h, int id, int which, float* dst, const float* src) {
+  if (id < 0 || id >= static_cast<int>(h->poles.size())) return fail(FDTD_ERR_INVALID_ARG, "bad pole id");
+  const PoleHost& ph = h->poles[id];
+  float* buf = which == 0 ? h->adj.gpol_host[id] : h->adj.gcur_host[id];
+  const size_t w = ph.nk * sizeof(float), pitch = ph.nkk * sizeof(float);
+  if (src)
+    CUDA_TRY(cudaMemcpy2DAsync(buf + ph.koff, pitch, src, w, w, ph.rows, cudaMemcpyDefault, h->stream));
+  else
+    CUDA_TRY(cudaMemcpy2DAsync(dst, w, buf + ph.koff, pitch, w, ph.rows, cudaMemcpyDefault, h->stream));
+  return 0;
+}
+
 int fdtd_engine_adjoint_pack(fdtd_engine* h, int kind, int comp, int which, const float* src) {
+  if (h && h->adj.ready && kind == 2 && src && (which == 0 || which == 1))
+    return adj_pole_copy(h, comp, which, nullptr, src);
   if (!h || !h->adj.ready || kind < 0 || kind > 1 || comp < 0 || comp > 5 || which < 0 || which > 1 || !src)
     return fail(FDTD_ERR_INVALID_ARG, "bad adjoint pack arguments");
   float* buf;
@@ -2025,6 +2079,8 @@ int fdtd_engine_adjoint_pack(fdtd_engine* h, int kind, int comp, int which, cons
 }
 
 int fdtd_engine_adjoint_unpack(fdtd_engine* h, int kind, int comp, int which, float* dst) {
+  if (h && h->adj.ready && kind == 2 && dst && (which == 0 || which == 1))
+    return adj_pole_copy(h, comp, which, dst, nullptr);
   if (!h || !h->adj.ready || kind < 0 || kind > 1 || comp < 0 || comp > 5 || which < 0 || which > 1 || !dst)
     return fail(FDTD_ERR_INVALID_ARG, "bad adjoint unpack arguments");
   float* buf;
