@@ -96,6 +96,9 @@ __device__ __forceinline__ void march(const StepParams& p, int n, int lane, int 
       if (j >= pt.j0 && j < pt.j1 && k >= pt.k0 && k < pt.k1) lane_poles |= 1u << b;
     }
   }
+  // warp-uniform: some pole box covers one of this warp's (row, z) cells
+  // (poles beyond the 32 of the lane mask are checked inside ade)
+  const bool warp_poles = __any_sync(kFull, lane_poles != 0) || p.n_poles > 32;
 
   // E^n(i) registers: row j-1 (x, y, z), row j (x, y, z), row j+1 (x, z)
   float em0, em1, em2, ec0, ec1, ec2, ep0, ep2;
@@ -285,7 +288,7 @@ __device__ __forceinline__ void march(const StepParams& p, int n, int lane, int 
       float v2 = pick(m2, ec2 * g2 + c2 * (d2a - d2b), ec2);
       // ADE subtraction, TFSF electric corrections and soft sources: the
       // additive terms of witwin/maxwell/fdtd/runtime/stepping.py:2295-2320.
-      if (pb & kPlanePoles) {
+      if ((pb & kPlanePoles) && warp_poles) {
         const unsigned upd = (m0 != kModeDeferred ? 1u : 0u) | (m1 != kModeDeferred ? 2u : 0u) |
                              (m2 != kModeDeferred ? 4u : 0u);
         ade<TA>(p, lane_poles, i, j, k, ec0, ec1, ec2, v0, v1, v2, upd);
