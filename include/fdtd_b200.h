@@ -188,6 +188,11 @@ int fdtd_engine_autotune(fdtd_engine* h, int* tile_rows, int* chunk_planes);
  * for compatibility and ignored. */
 int fdtd_engine_set_launch(fdtd_engine* h, int variant, int tile_rows, int chunk_planes);
 int fdtd_engine_get_launch(fdtd_engine* h, int* variant, int* tile_rows, int* chunk_planes);
+/* L2 prefetch distance of the scalar step kernels (variants 1-3; default 2):
+ * warps whose footprint has no CPML and no coefficient-array cell prefetch
+ * their row of the E/H fields `planes` x planes (0..16; 0 disables) ahead of
+ * their march.  Results do not depend on it. */
+int fdtd_engine_set_prefetch(fdtd_engine* h, int planes);
 /* Launch configuration and launch count bookkeeping. */
 int fdtd_engine_info(fdtd_engine* h, int* tile_rows, int* chunk_planes, int* grid_x, int* grid_y,
                      int* block, int64_t* launches);

@@ -289,6 +289,9 @@ struct DevBuf {
 };
 
 constexpr int kDefaultVariant = 2;
+// Planes ahead of the x march whose field rows the scalar step kernels
+// prefetch into L2 (0 disables).
+constexpr int kDefaultPrefetch = 2;
 
 constexpr int kMaxVariant = 9;
 
@@ -377,6 +380,7 @@ struct fdtd_engine {
   // of up to 128 / 64 / 85 per thread; 4 = TMA-fed kernel; 5..9 = z-vectorised
   // warp kernels (vec_launcher).
   int variant = kDefaultVariant;
+  int pf_dist = kDefaultPrefetch;
   int cur = 0;  // index of the buffer holding the current state
   float* E[2][3] = {};
   float* H[2][3] = {};
@@ -542,6 +546,7 @@ void fill_params(const fdtd_engine* h, StepParams& p) {
   p.zhs4 = h->zhs4;
   p.TY = h->TY;
   p.CX = h->CX;
+  p.pf_dist = h->pf_dist;
   p.Q = h->P / 4;
   p.ROWS = 1;
   const int src = h->cur, dst = 1 - h->cur;
@@ -1853,6 +1858,13 @@ int fdtd_engine_set_launch(fdtd_engine* h, int variant, int tile_rows, int chunk
   h->variant = variant;
   if (chunk_planes > 0) h->CX = chunk_planes;
   else default_tiles(h);
+  return 0;
+}
+
+// L2 prefetch distance of the scalar step kernels (launch variants 1-3).
+int fdtd_engine_set_prefetch(fdtd_engine* h, int planes) {
+  if (!h || planes < 0 || planes > 16) return fail(FDTD_ERR_INVALID_ARG, "prefetch distance must be 0..16 planes");
+  h->pf_dist = planes;
   return 0;
 }
 

@@ -71,6 +71,7 @@ struct BoxIndex {
 struct StepParams {
   int NX, NY, NZ, P, SZ;  // node counts, padded z pitch, z-slab row length
   int TY, CX, Q, ROWS;    // tile rows, planes per chunk, float4 per row, thread rows (TY + 2)
+  int pf_dist;            // L2 prefetch distance of the x march in planes (0: none)
   const float* Ein[3];
   float* Eout[3];
   const float* Hin[3];

@@ -56,6 +56,13 @@ __device__ __forceinline__ void stf(float* base, int64_t off, float v, float inv
   }
 }
 
+// L2 prefetch of the element at base + off of an array of stored type T (a
+// hint: no register, no wait; callers pass in-bounds offsets only).
+template <typename T>
+__device__ __forceinline__ void pf_l2(const void* base, int64_t off) {
+  asm volatile("prefetch.global.L2 [%0];" ::"l"(reinterpret_cast<const T*>(base) + off));
+}
+
 // ADE state element of type TA (FP32 or BF16, unscaled).
 template <typename TA>
 __device__ __forceinline__ float lda(const float* base, int64_t off) {

@@ -26,6 +26,24 @@
 
 namespace fdtdb200 {
 
+// L2 prefetch of row j's fields for the plane ip of an x march: H^{n-1/2} of
+// plane ip and E^n of plane ip + 1 (row offset rc, plane stride ps; nothing
+// past the chunk end i1).  The neighbour rows j +- 1 are prefetched by the
+// warps that own them.
+template <typename TS>
+__device__ __forceinline__ void prefetch_row(const StepParams& p, int ip, int i1, int ps, int rc, bool kok) {
+  if (!kok || ip >= i1) return;
+  const int64_t q = static_cast<int64_t>(ip) * ps + rc;
+  pf_l2<TS>(p.Hin[0], q);
+  pf_l2<TS>(p.Hin[1], q);
+  pf_l2<TS>(p.Hin[2], q);
+  if (ip + 1 < p.NX) {
+    pf_l2<TS>(p.Ein[0], q + ps);
+    pf_l2<TS>(p.Ein[1], q + ps);
+    pf_l2<TS>(p.Ein[2], q + ps);
+  }
+}
+
 // The march of one warp task (row j, z block blockIdx.y, x chunk blockIdx.z).
 // kCpml: run the CPML psi code (the task's footprint touches a slab).  kCoef:
 // read the per-cell decay/curl arrays (some coefficient of the footprint
@@ -34,8 +52,9 @@ namespace fdtdb200 {
 // TS: stored field type (float = the exact FP32 path; __half / __nv_bfloat16 =
 // reduced storage with per-component scales).  ADE pole state is BF16 with
 // BF16 fields and FP32 otherwise (FP16 would need per-pole scales that the
-// source tables do not bound).
-template <typename TS, bool kCpml, bool kCoef, bool kUniform>
+// source tables do not bound).  kPf: L2 prefetch of the fields p.pf_dist planes
+// ahead of the march.
+template <typename TS, bool kCpml, bool kCoef, bool kUniform, bool kPf = false>
 __device__ __forceinline__ void march(const StepParams& p, int n, int lane, int j) {
   using TA = typename std::conditional<std::is_same<TS, __nv_bfloat16>::value, __nv_bfloat16, float>::type;
   const int NX = p.NX, NY = p.NY, NZ = p.NZ, P = p.P;
@@ -114,12 +133,18 @@ __device__ __forceinline__ void march(const StepParams& p, int n, int lane, int 
     ep2 = ldf<TS>(p.Ein[2], o + rp, kok && jp_ok, p.fscale[2]);
   }
   float hpz = 0.f, hpy = 0.f;  // Hz, Hy of row j at plane i-1
+  if constexpr (kPf) {
+    for (int d = 1; d < p.pf_dist; ++d) prefetch_row<TS>(p, istart + d, i1, ps, rc, kok);
+  }
 
   for (int i = istart; i < i1; ++i) {
     const bool own = i >= i0;
     const bool inext = i + 1 < NX;
     const int o = i * ps;
     const int on = o + ps;
+    if constexpr (kPf) {
+      if (p.pf_dist) prefetch_row<TS>(p, i + p.pf_dist, i1, ps, rc, kok);
+    }
     const unsigned pb = __ldg(p.plane_bits + i);
     // E^n(i+1) of rows j-1, j, j+1 (the next plane's E^n(i))
     const float nm0 = ldf<TS>(p.Ein[0], on + rm, kok && jm_ok && inext, p.fscale[0]);
@@ -316,10 +341,15 @@ __device__ __forceinline__ void march(const StepParams& p, int n, int lane, int 
 // kAnyCpml / kAnyCoef: the scene has CPML slabs / some coefficient array.
 // Each warp reads its class and runs the cheapest march that is exact for its
 // footprint, so the CPML and coefficient code runs only where it changes the
-// result.  kMinBlocks trades registers for occupancy.
+// result.  kMinBlocks trades registers for occupancy.  The plain body (no
+// CPML, no coefficient arrays) prefetches its fields into L2 ahead of the
+// march, except in the kernel that also holds the CPML + coefficient body:
+// there the extra code shifts the register allocation of the heavy bodies and
+// costs more than the prefetch gains (measured on the dispersive workload).
 template <bool kAnyCpml, bool kAnyCoef, bool kUniform, int kMinBlocks>
 __global__ void __launch_bounds__(256, kMinBlocks) warp_step_kernel(const StepParams p, int n, int slot) {
   (void)slot;
+  constexpr bool kPlainPrefetch = !(kAnyCpml && kAnyCoef);
   if (p.step_base) n += __ldg(p.step_base);
   const int lane = threadIdx.x & 31;
   const int j = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
@@ -332,7 +362,7 @@ __global__ void __launch_bounds__(256, kMinBlocks) warp_step_kernel(const StepPa
     else march<float, true, false, kUniform>(p, n, lane, j);
   } else {
     if (kAnyCoef && (cls & kClassCoef)) march<float, false, true, kUniform>(p, n, lane, j);
-    else march<float, false, false, kUniform>(p, n, lane, j);
+    else march<float, false, false, kUniform, kPlainPrefetch>(p, n, lane, j);
   }
 }
 

@@ -237,6 +237,10 @@ class B200FDTD:
     def set_launch(self, variant: int, tile_rows: int = 0, chunk_planes: int = 0) -> None:
         _lib.check(self.lib.fdtd_engine_set_launch(self.handle, int(variant), int(tile_rows), int(chunk_planes)), "set_launch")
 
+    def set_prefetch(self, planes: int) -> None:
+        """L2 prefetch distance of the scalar step kernels in x planes (0 disables)."""
+        _lib.check(self.lib.fdtd_engine_set_prefetch(self.handle, int(planes)), "set_prefetch")
+
     def storage_scales(self) -> tuple[str, list[float]]:
         """The engine's field storage kind and per-component scales (Ex..Hz)."""
         kind = ctypes.c_int()
