@@ -188,6 +188,14 @@ int fdtd_engine_autotune(fdtd_engine* h, int* tile_rows, int* chunk_planes);
  * for compatibility and ignored. */
 int fdtd_engine_set_launch(fdtd_engine* h, int variant, int tile_rows, int chunk_planes);
 int fdtd_engine_get_launch(fdtd_engine* h, int* variant, int* tile_rows, int* chunk_planes);
+/* Where the Debye / Drude / Lorentz poles advance: on (1, the default) in a
+ * separate streaming pass after the step kernel, over the cells the pole boxes
+ * cover, in the reference's order (E update, TFSF and source terms, then the
+ * dispersive correction: witwin/maxwell/fdtd/runtime/stepping.py:2290-2316);
+ * off (0) inside the fused step kernel.  The pass is used with FP32 storage,
+ * launch variants 1-3 and no periodic / Bloch face; elsewhere the poles stay
+ * in the step kernel.  The two orders agree to FP32 rounding. */
+int fdtd_engine_set_ade_pass(fdtd_engine* h, int on);
 /* L2 prefetch distance of the scalar step kernels (variants 1-3; default 2):
  * warps whose footprint has no CPML and no coefficient-array cell prefetch
  * their row of the E/H fields `planes` x planes (0..16; 0 disables) ahead of

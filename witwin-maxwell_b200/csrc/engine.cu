@@ -10,6 +10,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <climits>
 #include <type_traits>
 #include <cmath>
 #include <cstdio>
@@ -416,6 +417,11 @@ struct fdtd_engine {
   int n_regions_ph[2] = {0, 0};
   int* d_pole_ptr = nullptr;
   int* d_pole_ids = nullptr;
+  // ADE pass work list (int4 tiles over the union of the pole boxes) and its switch
+  const int* d_ade_tiles = nullptr;
+  int n_ade_tiles = 0;
+  bool ade_pass = true;
+  AdeParams ade{};
   const int* d_plane_bits = nullptr;
   unsigned char* d_warp_class = nullptr;  // sized for chunk length 1 (the largest table)
   TmaMaps maps[2] = {};                    // tensor maps of E[cur], H[cur] for cur = 0, 1
@@ -675,10 +681,18 @@ int ensure_classified(fdtd_engine* h, const StepParams& p) {
   return 0;
 }
 
+// The poles run in the ADE pass after the step kernel (instead of inside it)
+// on FP32 storage with the scalar step kernels and no wrapped face.
+bool ade_pass_active(const fdtd_engine* h) {
+  return h->ade_pass && h->n_ade_tiles > 0 && h->poles.size() <= static_cast<size_t>(kAdeMaxPoles) &&
+         h->storage == kStoreF32 && !h->wrap && h->variant >= 1 && h->variant <= 3;
+}
+
 int launch_step(fdtd_engine* h, int n, int slot) {
   StepParams p;
   fill_params(h, p);
   const dim3 grid = step_grid(h);
+  const bool ade_pass = ade_pass_active(h);
   bool coef = false;
   for (int c = 0; c < 6; ++c) coef = coef || h->ecoef[c][0] || h->ecoef[c][1];
   const int block = kWarpRows * 32;
@@ -688,6 +702,7 @@ int launch_step(fdtd_engine* h, int n, int slot) {
     const int rc = ensure_classified(h, p);
     if (rc) return rc;
   }
+  if (ade_pass) p.n_poles = 0;  // the step kernel skips the poles
   if (h->storage != kStoreF32) {
     const int err = launch_step_reduced(p, n, grid, h->cpml, coef, h->uniform_grid, h->stream);
     if (err != 0) return cuda_fail(static_cast<cudaError_t>(err), "warp_step_kernel_rs launch");
@@ -725,6 +740,15 @@ int launch_step(fdtd_engine* h, int n, int slot) {
   cudaError_t err = cudaGetLastError();
   if (err != cudaSuccess) return cuda_fail(err, "warp_step_kernel launch");
   ++h->launches;
+  if (ade_pass) {
+    for (int c = 0; c < 3; ++c) {
+      h->ade.Ein[c] = p.Ein[c];
+      h->ade.Eout[c] = p.Eout[c];
+    }
+    const int e2 = launch_ade_pass(h->ade, h->d_ade_tiles, h->n_ade_tiles, h->stream);
+    if (e2 != 0) return cuda_fail(static_cast<cudaError_t>(e2), "ade_pass_kernel launch");
+    ++h->launches;
+  }
   h->cur = 1 - h->cur;
   if (h->in_pair) return 0;  // the Bloch pair runs the wrap kernel and the gather
   if (h->wrap) {
@@ -1516,6 +1540,67 @@ int fdtd_engine_finalize(fdtd_engine* h) {
     h->d_pole_ptr = const_cast<int*>(dp);
     h->d_pole_ids = const_cast<int*>(di);
   }
+  if (!h->poles.empty() && h->poles.size() <= static_cast<size_t>(kAdeMaxPoles)) {
+    // ADE pass: the pole table, and tiles over the z range of each (i, j) row
+    // covered by any pole box, cut into 32-cell pieces (one warp each), with
+    // the mask of the poles that meet each piece
+    AdeParams& a = h->ade;
+    a.NY = h->NY;
+    a.P = h->P;
+    for (size_t b = 0; b < h->poles.size(); ++b) {
+      const PoleTerm& t = h->poles[b].t;
+      AdePole& q = a.poles[b];
+      q.comp = t.comp;
+      q.kind = t.kind;
+      q.i0 = t.i0;
+      q.j0 = t.j0;
+      q.nj = t.j1 - t.j0;
+      q.k0 = t.k0;
+      q.k1 = t.k1;
+      q.kk0 = t.kk0;
+      q.nkk = t.nkk;
+      q.decay = t.decay;
+      q.restoring = t.restoring;
+      q.dt = t.dt;
+      q.inv_dt = t.inv_dt;
+      q.drive = t.drive;
+      q.inv_eps = t.inv_eps;
+      q.pol = t.pol;
+      q.cur = t.cur;
+    }
+    const int64_t rows = static_cast<int64_t>(h->NX) * h->NY;
+    std::vector<int> kmin(static_cast<size_t>(rows), INT_MAX), kmax(static_cast<size_t>(rows), -1);
+    std::vector<unsigned> rmask(static_cast<size_t>(rows), 0u);
+    for (size_t b = 0; b < h->poles.size(); ++b) {
+      const PoleTerm& t = h->poles[b].t;
+      for (int i = t.i0; i < t.i1; ++i)
+        for (int j = t.j0; j < t.j1; ++j) {
+          const size_t r = static_cast<size_t>(i) * h->NY + j;
+          kmin[r] = std::min(kmin[r], t.k0);
+          kmax[r] = std::max(kmax[r], t.k1);
+          rmask[r] |= 1u << b;
+        }
+    }
+    std::vector<int> tiles;
+    for (int64_t r = 0; r < rows; ++r)
+      for (int k0 = kmin[r]; k0 < kmax[r]; k0 += 32) {
+        const int k1 = std::min(k0 + 32, kmax[r]);
+        unsigned m = 0;
+        for (unsigned rm = rmask[r]; rm; rm &= rm - 1) {
+          const int b = __builtin_ctz(rm);
+          if (h->poles[b].t.k0 < k1 && h->poles[b].t.k1 > k0) m |= 1u << b;
+        }
+        if (!m) continue;
+        tiles.push_back(static_cast<int>(r));
+        tiles.push_back(k0);
+        tiles.push_back(k1);
+        tiles.push_back(static_cast<int>(m));
+      }
+    if (tiles.size() / 4 > static_cast<size_t>(INT_MAX)) return fail(FDTD_ERR_INVALID_ARG, "pole boxes too large");
+    rc = upload_ints(h, tiles, &h->d_ade_tiles);
+    if (rc) return rc;
+    h->n_ade_tiles = static_cast<int>(tiles.size() / 4);
+  }
   rc = upload_vec(h, &h->d_regions, h->regions);
   if (rc) return rc;
   for (int ph = 0; ph < 2; ++ph) {
@@ -1858,6 +1943,13 @@ int fdtd_engine_set_launch(fdtd_engine* h, int variant, int tile_rows, int chunk
   h->variant = variant;
   if (chunk_planes > 0) h->CX = chunk_planes;
   else default_tiles(h);
+  return 0;
+}
+
+// Poles in the ADE pass after the step kernel (on) or inside it (off).
+int fdtd_engine_set_ade_pass(fdtd_engine* h, int on) {
+  if (!h) return fail(FDTD_ERR_INVALID_ARG, "null engine");
+  h->ade_pass = on != 0;
   return 0;
 }
 

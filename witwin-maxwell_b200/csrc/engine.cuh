@@ -156,6 +156,28 @@ struct WrapFields {
   const float* hnew[3];
 };
 int64_t wrap_cell_count(const StepParams& p);
+// Pole table of the ADE pass (ade_pass.cu), passed in the kernel parameters.
+constexpr int kAdeMaxPoles = 32;
+struct AdePole {
+  int comp, kind;
+  int i0, j0, nj;  // box origin and row count (j1 - j0)
+  int k0, k1;      // cells of the box along z
+  int kk0, nkk;    // stored z range (PoleTerm)
+  float decay, restoring, dt, inv_dt;
+  const float* drive;
+  const float* inv_eps;
+  float* pol;
+  float* cur;
+};
+struct AdeParams {
+  const float* Ein[3];
+  float* Eout[3];
+  int NY, P;
+  AdePole poles[kAdeMaxPoles];
+};
+// ADE pass after the step kernel: tiles are int4 {i * NY + j, k0, k1, pole
+// mask}, one warp each.
+int launch_ade_pass(const AdeParams& a, const int* tiles, int n_tiles, cudaStream_t stream);
 // pim / fi: the imaginary channel of a Bloch pair, or nullptr (real periodic).
 int launch_wrap_fixup(const StepParams& pr, const StepParams* pim, const WrapFields& fr, const WrapFields* fi,
                       const float* phase_cos, const float* phase_sin, int n, cudaStream_t stream);

@@ -241,6 +241,10 @@ class B200FDTD:
         """L2 prefetch distance of the scalar step kernels in x planes (0 disables)."""
         _lib.check(self.lib.fdtd_engine_set_prefetch(self.handle, int(planes)), "set_prefetch")
 
+    def set_ade_pass(self, on: bool) -> None:
+        """Advance the dispersive poles in a pass after the step kernel (True) or inside it."""
+        _lib.check(self.lib.fdtd_engine_set_ade_pass(self.handle, 1 if on else 0), "set_ade_pass")
+
     def storage_scales(self) -> tuple[str, list[float]]:
         """The engine's field storage kind and per-component scales (Ex..Hz)."""
         kind = ctypes.c_int()
