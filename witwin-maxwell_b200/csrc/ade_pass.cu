@@ -11,99 +11,106 @@
 // 18-83).  Inside the 64-register step kernel the pole loads of a cell are
 // consumed as they arrive, one pole after another.  Here a thread's only
 // dependent read is its tile; the pole table sits in the kernel parameters
-// (constant cache), so E^n, E^{n+1} and the state of up to four poles are
-// loaded together and the pole state streams at HBM speed.
+// (constant cache) and is read once per pole per tile, and each lane loads the
+// state of a pole for all its cells together.
 //
-// Work list: one warp per tile {row = i * NY + j, k0, k1, pole mask}: lane l
-// takes the cell k = k0 + l when k < k1; the mask holds the poles whose box
-// covers row (i, j) and meets [k0, k1).  The host builds the tiles from the
-// union of the pole boxes per row, 32 cells each.
+// Work list: one warp per tile {row = i * NY + j, k0, k1, pole mask} of up to
+// 32 * kAdeCellsPerLane cells [k0, k1) of one row; the mask holds the poles
+// whose box covers row (i, j) and meets [k0, k1).  The host builds the tiles
+// from the union of the pole boxes per row.  A cell that no pole of a touched
+// component covers is written back unchanged (every cell lies in one tile).
 #include "step_device.cuh"
 
 namespace fdtdb200 {
 
 namespace {
 
-constexpr int kAdePoleBatch = 4;  // poles whose state loads are issued together
+// Cells per lane: a tile is kAdeCellsPerLane * 32 consecutive z cells of a row,
+// lane l taking k0 + l + 32 q.  Each pole's table entry is then read once per
+// tile, and a lane has the state loads of all its cells in flight together.
+constexpr int kQ = kAdeCellsPerLane;
 
 __global__ void __launch_bounds__(256) ade_pass_kernel(const __grid_constant__ AdeParams a,
                                                        const int4* __restrict__ tiles, int n_tiles) {
   const int t = static_cast<int>(blockIdx.x) * (blockDim.x >> 5) + static_cast<int>(threadIdx.x >> 5);
-  if (t >= n_tiles) return;
+  if (t >= n_tiles) return;  // whole warp
   const int4 tl = __ldg(tiles + t);
-  const int k = tl.y + static_cast<int>(threadIdx.x & 31);
-  if (k >= tl.z) return;
+  const int lane = static_cast<int>(threadIdx.x & 31);
   const int i = tl.x / a.NY;
   const int j = tl.x - i * a.NY;
-  const int64_t x = static_cast<int64_t>(tl.x) * a.P + k;
-  const unsigned mask = static_cast<unsigned>(tl.w);
-  // poles covering this lane's cell, and the components they touch
-  unsigned cov = 0, comps = 0;
-  for (unsigned m = mask; m; m &= m - 1) {
-    const int b = __ffs(m) - 1;
-    if (k >= a.poles[b].k0 && k < a.poles[b].k1) {
-      cov |= 1u << b;
-      comps |= 1u << a.poles[b].comp;
+  const int64_t row = static_cast<int64_t>(tl.x) * a.P;
+  const unsigned mask = static_cast<unsigned>(tl.w);  // the same for every lane
+  unsigned comps = 0;
+  for (unsigned m = mask; m; m &= m - 1) comps |= 1u << a.poles[__ffs(m) - 1].comp;
+  bool in[kQ];
+#pragma unroll
+  for (int q = 0; q < kQ; ++q) in[q] = tl.y + lane + 32 * q < tl.z;
+  // E^n and E^{n+1} of the touched components
+  float eo[kQ][3], v[kQ][3];
+#pragma unroll
+  for (int c = 0; c < 3; ++c) {
+    const bool use = (comps >> c) & 1u;
+#pragma unroll
+    for (int q = 0; q < kQ; ++q) {
+      const int64_t x = row + tl.y + lane + 32 * q;
+      eo[q][c] = use && in[q] ? __ldg(a.Ein[c] + x) : 0.f;
+      v[q][c] = use && in[q] ? a.Eout[c][x] : 0.f;
     }
   }
-  float eo[3], v[3];
-  for (int c = 0; c < 3; ++c) {
-    eo[c] = ((comps >> c) & 1u) ? __ldg(a.Ein[c] + x) : 0.f;
-    v[c] = ((comps >> c) & 1u) ? a.Eout[c][x] : 0.f;
-  }
-  for (unsigned m = cov; m;) {
-    int ids[kAdePoleBatch];
-    int64_t offs[kAdePoleBatch];
-    float drive[kAdePoleBatch], ie[kAdePoleBatch], pol[kAdePoleBatch], cur[kAdePoleBatch];
+  // poles in id order (the order of the subtractions)
+  for (unsigned m = mask; m; m &= m - 1) {
+    const AdePole& pt = a.poles[__ffs(m) - 1];
+    const int c = pt.comp, kind = pt.kind;
+    const int64_t rbase = (static_cast<int64_t>(i - pt.i0) * pt.nj + (j - pt.j0)) * pt.nkk - pt.kk0;
+    bool act[kQ];
+    float drive[kQ], ie[kQ], pol[kQ], cur[kQ];
 #pragma unroll
-    for (int u = 0; u < kAdePoleBatch; ++u) {
-      ids[u] = -1;
-      offs[u] = 0;
-      drive[u] = ie[u] = pol[u] = cur[u] = 0.f;
-      if (m) {
-        const int b = __ffs(m) - 1;
-        m &= m - 1;
-        const AdePole& pt = a.poles[b];
-        const int64_t o = (static_cast<int64_t>(i - pt.i0) * pt.nj + (j - pt.j0)) * pt.nkk + (k - pt.kk0);
-        ids[u] = b;
-        offs[u] = o;
-        drive[u] = __ldg(pt.drive + o);
-        ie[u] = __ldg(pt.inv_eps + o);
-        if (pt.kind != 1) pol[u] = pt.pol[o];
-        if (pt.kind != 0) cur[u] = pt.cur[o];
+    for (int q = 0; q < kQ; ++q) {
+      const int k = tl.y + lane + 32 * q;
+      act[q] = in[q] && k >= pt.k0 && k < pt.k1;
+      drive[q] = ie[q] = pol[q] = cur[q] = 0.f;
+      if (act[q]) {
+        drive[q] = __ldg(pt.drive + rbase + k);
+        ie[q] = __ldg(pt.inv_eps + rbase + k);
+        if (kind != 1) pol[q] = pt.pol[rbase + k];
+        if (kind != 0) cur[q] = pt.cur[rbase + k];
       }
     }
+    const float decay = pt.decay, restoring = pt.restoring, dt = pt.dt, inv_dt = pt.inv_dt;
 #pragma unroll
-    for (int u = 0; u < kAdePoleBatch; ++u) {
-      if (ids[u] < 0) continue;
-      const AdePole& pt = a.poles[ids[u]];
-      const int64_t o = offs[u];
-      const int c = pt.comp;
-      const float ec = c == 0 ? eo[0] : (c == 1 ? eo[1] : eo[2]);
+    for (int q = 0; q < kQ; ++q) {
+      if (!act[q]) continue;
+      const int64_t o = rbase + tl.y + lane + 32 * q;
+      const float ec = c == 0 ? eo[q][0] : (c == 1 ? eo[q][1] : eo[q][2]);
       float jn;
-      if (pt.kind == 0) {
-        const float prev = pol[u];
-        const float next = pt.decay * prev + drive[u] * ec;
+      if (kind == 0) {
+        const float prev = pol[q];
+        const float next = decay * prev + drive[q] * ec;
         pt.pol[o] = next;
-        jn = (next - prev) * pt.inv_dt;
+        jn = (next - prev) * inv_dt;
         pt.cur[o] = jn;
-      } else if (pt.kind == 1) {
-        jn = pt.decay * cur[u] + drive[u] * ec;
+      } else if (kind == 1) {
+        jn = decay * cur[q] + drive[q] * ec;
         pt.cur[o] = jn;
       } else {
-        const float pl = pol[u];
-        jn = pt.decay * cur[u] - pt.restoring * pl + drive[u] * ec;
+        const float pl = pol[q];
+        jn = decay * cur[q] - restoring * pl + drive[q] * ec;
         pt.cur[o] = jn;
-        pt.pol[o] = pl + pt.dt * jn;
+        pt.pol[o] = pl + dt * jn;
       }
-      const float s = pt.dt * jn * ie[u];
-      if (c == 0) v[0] -= s;
-      else if (c == 1) v[1] -= s;
-      else v[2] -= s;
+      const float s = dt * jn * ie[q];
+      if (c == 0) v[q][0] -= s;
+      else if (c == 1) v[q][1] -= s;
+      else v[q][2] -= s;
     }
   }
-  for (int c = 0; c < 3; ++c)
-    if ((comps >> c) & 1u) __stcg(a.Eout[c] + x, v[c]);
+#pragma unroll
+  for (int c = 0; c < 3; ++c) {
+    if (!((comps >> c) & 1u)) continue;
+#pragma unroll
+    for (int q = 0; q < kQ; ++q)
+      if (in[q]) __stcg(a.Eout[c] + row + tl.y + lane + 32 * q, v[q][c]);
+  }
 }
 
 }  // namespace

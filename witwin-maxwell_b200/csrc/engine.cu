@@ -1542,8 +1542,8 @@ int fdtd_engine_finalize(fdtd_engine* h) {
   }
   if (!h->poles.empty() && h->poles.size() <= static_cast<size_t>(kAdeMaxPoles)) {
     // ADE pass: the pole table, and tiles over the z range of each (i, j) row
-    // covered by any pole box, cut into 32-cell pieces (one warp each), with
-    // the mask of the poles that meet each piece
+    // covered by any pole box, cut into 32 * kAdeCellsPerLane-cell pieces (one
+    // warp each), with the mask of the poles that meet each piece
     AdeParams& a = h->ade;
     a.NY = h->NY;
     a.P = h->P;
@@ -1583,8 +1583,8 @@ int fdtd_engine_finalize(fdtd_engine* h) {
     }
     std::vector<int> tiles;
     for (int64_t r = 0; r < rows; ++r)
-      for (int k0 = kmin[r]; k0 < kmax[r]; k0 += 32) {
-        const int k1 = std::min(k0 + 32, kmax[r]);
+      for (int k0 = kmin[r]; k0 < kmax[r]; k0 += 32 * kAdeCellsPerLane) {
+        const int k1 = std::min(k0 + 32 * kAdeCellsPerLane, kmax[r]);
         unsigned m = 0;
         for (unsigned rm = rmask[r]; rm; rm &= rm - 1) {
           const int b = __builtin_ctz(rm);

@@ -158,6 +158,7 @@ struct WrapFields {
 int64_t wrap_cell_count(const StepParams& p);
 // Pole table of the ADE pass (ade_pass.cu), passed in the kernel parameters.
 constexpr int kAdeMaxPoles = 32;
+constexpr int kAdeCellsPerLane = 4;  // a tile is 32 * kAdeCellsPerLane z cells of one row
 struct AdePole {
   int comp, kind;
   int i0, j0, nj;  // box origin and row count (j1 - j0)
