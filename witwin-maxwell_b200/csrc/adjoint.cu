@@ -150,7 +150,9 @@ __global__ void adj_pass_a_kernel(const StepParams p, const AdjParams q) {
 }
 
 // ---- pass B: gE = de gE' - C_E^T g(d_H); adjoint E psi; design gradient ----
-template <bool kUniform>
+// kPoles: the scene has ADE poles (their transpose is compiled only then: in
+// the per-component loop it slows the pole-free kernel by a third).
+template <bool kUniform, bool kPoles>
 __global__ void adj_pass_b_kernel(const StepParams p, const AdjParams q) {
   {
     // one thread per cell: k from the x-dimension, rows and planes from y and z
@@ -215,7 +217,7 @@ __global__ void adj_pass_b_kernel(const StepParams p, const AdjParams q) {
       //   Drude:   J' = a J + b E;             E' -= dt inv J'
       //   Lorentz: J' = a J - r P + b E; P' = P + dt J';  E' -= dt inv J'
       //   Debye:   P' = a P + b E;             E' -= inv (P' - P)
-      if (p.n_poles && (__ldg(p.plane_bits + i) & kPlanePoles)) {
+      if (kPoles && (__ldg(p.plane_bits + i) & kPlanePoles)) {
         const int pb = __ldg(p.pole_plane_ptr + i), pe = __ldg(p.pole_plane_ptr + i + 1);
         for (int xx = pb; xx < pe; ++xx) {
           const int id = __ldg(p.pole_plane_ids + xx);
@@ -348,12 +350,15 @@ int launch_adjoint_step(const StepParams& p, const AdjParams& q, const RegionFlu
     adj_seed_kernel<<<grid, 256, 0, stream>>>(p, q, regions, n_regions, w_e, w_h, n_freq, n);
   }
   const dim3 cells((p.P + 127) / 128, p.NY, p.NX);
+  const bool poles = p.n_poles > 0;
   if (p.uniform_grid) {
     adj_pass_a_kernel<true><<<cells, 128, 0, stream>>>(p, q);
-    adj_pass_b_kernel<true><<<cells, 128, 0, stream>>>(p, q);
+    if (poles) adj_pass_b_kernel<true, true><<<cells, 128, 0, stream>>>(p, q);
+    else adj_pass_b_kernel<true, false><<<cells, 128, 0, stream>>>(p, q);
   } else {
     adj_pass_a_kernel<false><<<cells, 128, 0, stream>>>(p, q);
-    adj_pass_b_kernel<false><<<cells, 128, 0, stream>>>(p, q);
+    if (poles) adj_pass_b_kernel<false, true><<<cells, 128, 0, stream>>>(p, q);
+    else adj_pass_b_kernel<false, false><<<cells, 128, 0, stream>>>(p, q);
   }
   adj_pass_c_kernel<<<cells, 128, 0, stream>>>(p, q);
   return static_cast<int>(cudaGetLastError());
