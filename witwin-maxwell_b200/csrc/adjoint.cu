@@ -318,19 +318,23 @@ __global__ void adj_seed_kernel(const StepParams p, const AdjParams q, const Reg
   }
 }
 
-// Copy the current E of every design box into history slot `slot`.
+// Copy the current E of every design box into history slot `slot`.  Index
+// arithmetic in 32 bits: a design box holds fewer than 2^31 cells (the host
+// rejects larger ones).
 __global__ void design_record_kernel(const StepParams p, const AdjParams q, int slot) {
   const int c = blockIdx.y;
   const DesignBox& d = q.design[c];
   if (!d.grad) return;
   const float* e = p.Ein[c];
   const int nj = d.hi[1] - d.lo[1], nk = d.hi[2] - d.lo[2];
-  for (int64_t l = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; l < d.cells;
-       l += static_cast<int64_t>(gridDim.x) * blockDim.x) {
-    const int k = d.lo[2] + static_cast<int>(l % nk);
-    const int j = d.lo[1] + static_cast<int>((l / nk) % nj);
-    const int i = d.lo[0] + static_cast<int>(l / (static_cast<int64_t>(nk) * nj));
-    d.hist[static_cast<int64_t>(slot) * d.cells + l] = e[cell(p, i, j, k)];
+  const int cells = static_cast<int>(d.cells);
+  float* hist = d.hist + static_cast<int64_t>(slot) * d.cells;
+  for (int l = blockIdx.x * blockDim.x + threadIdx.x; l < cells; l += gridDim.x * blockDim.x) {
+    const int r = l / nk;
+    const int k = d.lo[2] + (l - r * nk);
+    const int i = d.lo[0] + r / nj;
+    const int j = d.lo[1] + (r - (r / nj) * nj);
+    hist[l] = e[cell(p, i, j, k)];
   }
 }
 

@@ -2041,6 +2041,7 @@ int fdtd_engine_adjoint_init(fdtd_engine* h, const int* design_boxes, int max_se
       d.hi[ax] = b[2 * ax + 1];
     }
     d.cells = static_cast<int64_t>(b[1] - b[0]) * (b[3] - b[2]) * (b[5] - b[4]);
+    if (d.cells >= INT_MAX) return fail(FDTD_ERR_INVALID_ARG, "design box holds 2^31 cells or more");
     int rc = adj_alloc(h, &d.hist, static_cast<size_t>(d.cells) * (max_segment + 1));
     if (!rc) rc = adj_alloc(h, &d.grad, static_cast<size_t>(d.cells));
     if (rc) return rc;
