@@ -213,16 +213,18 @@ def run_reference_arm(args, wm, world, rank):
 
 
 def measured_traffic(info, cells):
-    """DRAM bytes of one step-kernel launch from the committed ncu capture
-    (profiles/step_kernel_traffic.json), when it was taken on this launch shape
-    and grid size; None otherwise."""
+    """DRAM bytes of one step (the step kernel and the ADE pass after it) from
+    the committed ncu capture (profiles/step_kernel_traffic.json), when it was
+    taken on this launch shape and grid size; None otherwise."""
     path = ROOT / "profiles" / "step_kernel_traffic.json"
     if not path.exists():
         return None
     rec = json.loads(path.read_text())
     if (rec.get("variant"), rec.get("chunk_planes"), rec.get("cells")) != (info["variant"], info["chunk_planes"], int(cells)):
         return None
-    return int(rec["dram_bytes_read"] + rec["dram_bytes_write"])
+    if "kernels" not in rec:
+        return None
+    return int(sum(k["dram_bytes_read"] + k["dram_bytes_write"] for k in rec["kernels"]))
 
 
 def run_b200_arm(args, wm, world, rank, local):
@@ -286,7 +288,7 @@ def run_b200_arm(args, wm, world, rank, local):
         },
         "roofline": {
             "bound": "hbm",
-            "kernel": "fused_step_kernel",
+            "kernel": "step kernels: warp_step_kernel + ade_pass_kernel (one step)",
             "achieved": achieved,
             "peak": peaks["hbm_gbs"],
             "unit": "GB/s",
@@ -295,7 +297,7 @@ def run_b200_arm(args, wm, world, rank, local):
             "bytes_per_cell_update": bytes_alg["step_kernel"],
             "kernel_ms": kernel_ms,
             "traffic": measured_traffic(info1, cells),
-            "traffic_unit": "bytes per launch (dram__bytes_read.sum + dram__bytes_write.sum)",
+            "traffic_unit": "bytes per step, both kernels (dram__bytes_read.sum + dram__bytes_write.sum)",
         },
         "algorithmic_bytes_per_cell_update": {k: round(v, 3) for k, v in bytes_alg.items() if k != "cells"},
         "hbm_frac_whole_step": bytes_alg["total"] * cells * args.steps / (elapsed_s / world if world else elapsed_s) / 1e9 / peaks["hbm_gbs"],

@@ -24,7 +24,7 @@
 #include "adjoint.cuh"
 
 namespace fdtdb200 {
-template <bool kCpml, bool kCoef, bool kUniform, int kMinBlocks>
+template <bool kCpml, bool kCoef, bool kUniform, int kMinBlocks, bool kAde>
 __global__ void warp_step_kernel(const StepParams p, int n, int slot);
 int launch_classify_vec(const StepParams& p, int V, int n_kblocks, int n_chunks, unsigned char* out,
                         cudaStream_t stream);
@@ -714,9 +714,11 @@ int launch_step(fdtd_engine* h, int n, int slot) {
   do {                                                                                           \
     if (h->variant == 4)                                                                          \
       tma_step_kernel<CPML, COEF, UNI><<<grid, kTmaThreads, tma_smem_bytes(), h->stream>>>(p, h->maps[h->cur], n); \
-    else if (h->variant == 2) warp_step_kernel<CPML, COEF, UNI, 4><<<grid, block, 0, h->stream>>>(p, n, slot); \
-    else if (h->variant == 3) warp_step_kernel<CPML, COEF, UNI, 3><<<grid, block, 0, h->stream>>>(p, n, slot); \
-    else warp_step_kernel<CPML, COEF, UNI, 1><<<grid, block, 0, h->stream>>>(p, n, slot);            \
+    else if (h->variant == 2 && ade_pass) warp_step_kernel<CPML, COEF, UNI, 4, false><<<grid, block, 0, h->stream>>>(p, n, slot); \
+    else if (h->variant == 2) warp_step_kernel<CPML, COEF, UNI, 4, true><<<grid, block, 0, h->stream>>>(p, n, slot); \
+    else if (h->variant == 3 && ade_pass) warp_step_kernel<CPML, COEF, UNI, 3, false><<<grid, block, 0, h->stream>>>(p, n, slot); \
+    else if (h->variant == 3) warp_step_kernel<CPML, COEF, UNI, 3, true><<<grid, block, 0, h->stream>>>(p, n, slot); \
+    else warp_step_kernel<CPML, COEF, UNI, 1, true><<<grid, block, 0, h->stream>>>(p, n, slot);            \
   } while (0)
   if (h->uniform_grid) {
     if (h->cpml) {

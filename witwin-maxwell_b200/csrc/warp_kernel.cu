@@ -53,8 +53,9 @@ __device__ __forceinline__ void prefetch_row(const StepParams& p, int ip, int i1
 // reduced storage with per-component scales).  ADE pole state is BF16 with
 // BF16 fields and FP32 otherwise (FP16 would need per-pole scales that the
 // source tables do not bound).  kPf: L2 prefetch of the fields p.pf_dist planes
-// ahead of the march.
-template <typename TS, bool kCpml, bool kCoef, bool kUniform, bool kPf = false>
+// ahead of the march.  kAde: the ADE poles run here (false when the ADE pass
+// after the step kernel advances them; the pole code is then not compiled).
+template <typename TS, bool kCpml, bool kCoef, bool kUniform, bool kPf = false, bool kAde = true>
 __device__ __forceinline__ void march(const StepParams& p, int n, int lane, int j) {
   using TA = typename std::conditional<std::is_same<TS, __nv_bfloat16>::value, __nv_bfloat16, float>::type;
   const int NX = p.NX, NY = p.NY, NZ = p.NZ, P = p.P;
@@ -108,7 +109,7 @@ __device__ __forceinline__ void march(const StepParams& p, int n, int lane, int 
   }
 
   unsigned lane_poles = 0;
-  if (p.n_poles && out_lane) {
+  if (kAde && p.n_poles && out_lane) {
     const int np_ = min(p.n_poles, 32);
     for (int b = 0; b < np_; ++b) {
       const PoleTerm& pt = p.poles[b];
@@ -117,7 +118,8 @@ __device__ __forceinline__ void march(const StepParams& p, int n, int lane, int 
   }
   // warp-uniform: some pole box covers one of this warp's (row, z) cells
   // (poles beyond the 32 of the lane mask are checked inside ade)
-  const bool warp_poles = __any_sync(kFull, lane_poles != 0) || p.n_poles > 32;
+  bool warp_poles = false;
+  if constexpr (kAde) warp_poles = __any_sync(kFull, lane_poles != 0) || p.n_poles > 32;
 
   // E^n(i) registers: row j-1 (x, y, z), row j (x, y, z), row j+1 (x, z)
   float em0, em1, em2, ec0, ec1, ec2, ep0, ep2;
@@ -313,7 +315,7 @@ __device__ __forceinline__ void march(const StepParams& p, int n, int lane, int 
       float v2 = pick(m2, ec2 * g2 + c2 * (d2a - d2b), ec2);
       // ADE subtraction, TFSF electric corrections and soft sources: the
       // additive terms of witwin/maxwell/fdtd/runtime/stepping.py:2295-2320.
-      if ((pb & kPlanePoles) && warp_poles) {
+      if (kAde && (pb & kPlanePoles) && warp_poles) {
         const unsigned upd = (m0 != kModeDeferred ? 1u : 0u) | (m1 != kModeDeferred ? 2u : 0u) |
                              (m2 != kModeDeferred ? 4u : 0u);
         ade<TA>(p, lane_poles, i, j, k, ec0, ec1, ec2, v0, v1, v2, upd);
@@ -346,7 +348,7 @@ __device__ __forceinline__ void march(const StepParams& p, int n, int lane, int 
 // march, except in the kernel that also holds the CPML + coefficient body:
 // there the extra code shifts the register allocation of the heavy bodies and
 // costs more than the prefetch gains (measured on the dispersive workload).
-template <bool kAnyCpml, bool kAnyCoef, bool kUniform, int kMinBlocks>
+template <bool kAnyCpml, bool kAnyCoef, bool kUniform, int kMinBlocks, bool kAde>
 __global__ void __launch_bounds__(256, kMinBlocks) warp_step_kernel(const StepParams p, int n, int slot) {
   (void)slot;
   constexpr bool kPlainPrefetch = !(kAnyCpml && kAnyCoef);
@@ -358,11 +360,11 @@ __global__ void __launch_bounds__(256, kMinBlocks) warp_step_kernel(const StepPa
   if (kAnyCpml || kAnyCoef)
     cls = __ldg(p.warp_class + (static_cast<int64_t>(blockIdx.z) * gridDim.y + blockIdx.y) * p.NY + j);
   if (kAnyCpml && (cls & kClassCpml)) {
-    if (kAnyCoef && (cls & kClassCoef)) march<float, true, true, kUniform>(p, n, lane, j);
-    else march<float, true, false, kUniform>(p, n, lane, j);
+    if (kAnyCoef && (cls & kClassCoef)) march<float, true, true, kUniform, false, kAde>(p, n, lane, j);
+    else march<float, true, false, kUniform, false, kAde>(p, n, lane, j);
   } else {
-    if (kAnyCoef && (cls & kClassCoef)) march<float, false, true, kUniform>(p, n, lane, j);
-    else march<float, false, false, kUniform, kPlainPrefetch>(p, n, lane, j);
+    if (kAnyCoef && (cls & kClassCoef)) march<float, false, true, kUniform, false, kAde>(p, n, lane, j);
+    else march<float, false, false, kUniform, kPlainPrefetch, kAde>(p, n, lane, j);
   }
 }
 
@@ -474,10 +476,12 @@ int launch_classify(const StepParams& p, int n_kblocks, int n_chunks, unsigned c
   return static_cast<int>(cudaGetLastError());
 }
 
-#define FDTD_INSTANTIATE(CPML, COEF, UNI)                                                  \
-  template __global__ void warp_step_kernel<CPML, COEF, UNI, 1>(const StepParams, int, int); \
-  template __global__ void warp_step_kernel<CPML, COEF, UNI, 3>(const StepParams, int, int); \
-  template __global__ void warp_step_kernel<CPML, COEF, UNI, 4>(const StepParams, int, int);
+#define FDTD_INSTANTIATE(CPML, COEF, UNI)                                                         \
+  template __global__ void warp_step_kernel<CPML, COEF, UNI, 1, true>(const StepParams, int, int);  \
+  template __global__ void warp_step_kernel<CPML, COEF, UNI, 3, true>(const StepParams, int, int);  \
+  template __global__ void warp_step_kernel<CPML, COEF, UNI, 4, true>(const StepParams, int, int);  \
+  template __global__ void warp_step_kernel<CPML, COEF, UNI, 3, false>(const StepParams, int, int); \
+  template __global__ void warp_step_kernel<CPML, COEF, UNI, 4, false>(const StepParams, int, int);
 FDTD_INSTANTIATE(false, false, false)
 FDTD_INSTANTIATE(false, true, false)
 FDTD_INSTANTIATE(true, false, false)
