@@ -345,13 +345,14 @@ __device__ __forceinline__ void march(const StepParams& p, int n, int lane, int 
 // footprint, so the CPML and coefficient code runs only where it changes the
 // result.  kMinBlocks trades registers for occupancy.  The plain body (no
 // CPML, no coefficient arrays) prefetches its fields into L2 ahead of the
-// march, except in the kernel that also holds the CPML + coefficient body:
-// there the extra code shifts the register allocation of the heavy bodies and
-// costs more than the prefetch gains (measured on the dispersive workload).
+// march, except in the kernel that also holds the CPML + coefficient body and
+// the pole code: there the extra code shifts the register allocation of the
+// heavy bodies and costs more than the prefetch gains (measured on the
+// dispersive workload; without the pole code the prefetch gains 3 %).
 template <bool kAnyCpml, bool kAnyCoef, bool kUniform, int kMinBlocks, bool kAde>
 __global__ void __launch_bounds__(256, kMinBlocks) warp_step_kernel(const StepParams p, int n, int slot) {
   (void)slot;
-  constexpr bool kPlainPrefetch = !(kAnyCpml && kAnyCoef);
+  constexpr bool kPlainPrefetch = !(kAnyCpml && kAnyCoef) || !kAde;
   if (p.step_base) n += __ldg(p.step_base);
   const int lane = threadIdx.x & 31;
   const int j = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
