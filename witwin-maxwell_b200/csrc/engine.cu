@@ -223,18 +223,35 @@ __device__ __forceinline__ float load_field(const FieldPtrs& fp, int comp, int64
   return __ldg(fp.f[comp] + off);
 }
 
+// Cells a thread of the gather loads before it stores any: a z-normal region
+// reads one value per z row (one DRAM sector each), so the gather is bound by
+// load latency unless several loads are in flight per thread.
+constexpr int kGatherIlp = 4;
+
 __global__ void sample_gather_kernel(const RegionFlush* regions, const FieldPtrs fields, int NY, int P,
                                      float* samples, int64_t n_samples, int slot) {
   const RegionFlush rg = regions[blockIdx.y];
   float* out = samples + static_cast<int64_t>(slot) * n_samples + rg.base;
   // 32-bit cell arithmetic: a region holds fewer than 2^31 cells (checked at set-up)
   const int count = static_cast<int>(rg.count), nk = rg.nk, nj = rg.nj;
-  for (int x = blockIdx.x * blockDim.x + threadIdx.x; x < count; x += gridDim.x * blockDim.x) {
-    const int r = x / nk;
-    const int lk = x - r * nk;
-    const int li = r / nj;
-    const int lj = r - li * nj;
-    out[x] = load_field(fields, rg.comp, (static_cast<int64_t>(rg.i0 + li) * NY + rg.j0 + lj) * P + rg.k0 + lk);
+  const int stride = gridDim.x * blockDim.x;
+  for (int x0 = blockIdx.x * blockDim.x + threadIdx.x; x0 < count; x0 += stride * kGatherIlp) {
+    float v[kGatherIlp];
+#pragma unroll
+    for (int u = 0; u < kGatherIlp; ++u) {
+      const int x = x0 + u * stride;
+      v[u] = 0.0f;
+      if (x < count) {
+        const int r = x / nk;
+        const int lk = x - r * nk;
+        const int li = r / nj;
+        const int lj = r - li * nj;
+        v[u] = load_field(fields, rg.comp, (static_cast<int64_t>(rg.i0 + li) * NY + rg.j0 + lj) * P + rg.k0 + lk);
+      }
+    }
+#pragma unroll
+    for (int u = 0; u < kGatherIlp; ++u)
+      if (x0 + u * stride < count) out[x0 + u * stride] = v[u];
   }
 }
 
@@ -788,7 +805,7 @@ int launch_gather(fdtd_engine* h, int slot) {
     }
     fields.storage = h->storage;
     for (int c = 0; c < 6; ++c) fields.scale[c] = h->fscale[c];
-    const int gx = static_cast<int>(std::min<int64_t>((h->max_region + 255) / 256, 2048));
+    const int gx = static_cast<int>(std::min<int64_t>((h->max_region + 256 * kGatherIlp - 1) / (256 * kGatherIlp), 2048));
     sample_gather_kernel<<<dim3(std::max(gx, 1), h->n_flush), 256, 0, h->stream>>>(
         h->d_flush, fields, h->NY, h->P, h->samples, h->n_samples, slot);
     err = cudaGetLastError();
