@@ -28,9 +28,12 @@ namespace {
 // Cells per lane: a tile is kAdeCellsPerLane * 32 consecutive z cells of a row,
 // lane l taking k0 + l + 32 q.  Each pole's table entry is then read once per
 // tile, and a lane has the state loads of all its cells in flight together.
+// Four CTAs per SM (64 registers): measured 2.3 % faster per step on the
+// dispersive workload than the unbounded 70-register build (three CTAs), and
+// than two cells per lane.
 constexpr int kQ = kAdeCellsPerLane;
 
-__global__ void __launch_bounds__(256) ade_pass_kernel(const __grid_constant__ AdeParams a,
+__global__ void __launch_bounds__(256, 4) ade_pass_kernel(const __grid_constant__ AdeParams a,
                                                        const int4* __restrict__ tiles, int n_tiles) {
   const int t = static_cast<int>(blockIdx.x) * (blockDim.x >> 5) + static_cast<int>(threadIdx.x >> 5);
   if (t >= n_tiles) return;  // whole warp
