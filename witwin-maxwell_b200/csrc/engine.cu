@@ -462,6 +462,16 @@ struct fdtd_engine {
   int64_t launches = 0;
   float last_ms = 0.0f;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  // Inside step_range the monitor gather and the DFT flush run on a second
+  // (high-priority) stream, so they overlap the next step's kernels: the
+  // gather of step n reads the buffer set step n wrote, which only step n + 2
+  // overwrites (ping-pong), so step n + 2 waits for ev_gat[set] and nothing
+  // else waits.  The flush stays ordered behind the gathers on the same stream,
+  // and the streams are joined before step_range returns.
+  cudaStream_t aux = nullptr;
+  cudaEvent_t ev_fork = nullptr, ev_join = nullptr, ev_gat[2] = {nullptr, nullptr};
+  bool gat_pending[2] = {false, false};
+  bool async_gather = false;
   std::vector<Checkpoint> checkpoints;
   AdjointHost adj;
 };
@@ -720,6 +730,11 @@ int launch_step(fdtd_engine* h, int n, int slot) {
     if (rc) return rc;
   }
   if (ade_pass) p.n_poles = 0;  // the step kernel skips the poles
+  if (h->async_gather && h->gat_pending[1 - h->cur]) {
+    // the set this step writes was read by the gather of two steps ago
+    CUDA_TRY(cudaStreamWaitEvent(h->stream, h->ev_gat[1 - h->cur], 0));
+    h->gat_pending[1 - h->cur] = false;
+  }
   if (h->storage != kStoreF32) {
     const int err = launch_step_reduced(p, n, grid, h->cpml, coef, h->uniform_grid, h->stream);
     if (err != 0) return cuda_fail(static_cast<cudaError_t>(err), "warp_step_kernel_rs launch");
@@ -806,10 +821,20 @@ int launch_gather(fdtd_engine* h, int slot) {
     fields.storage = h->storage;
     for (int c = 0; c < 6; ++c) fields.scale[c] = h->fscale[c];
     const int gx = static_cast<int>(std::min<int64_t>((h->max_region + 256 * kGatherIlp - 1) / (256 * kGatherIlp), 2048));
-    sample_gather_kernel<<<dim3(std::max(gx, 1), h->n_flush), 256, 0, h->stream>>>(
+    cudaStream_t s = h->stream;
+    if (h->async_gather) {
+      CUDA_TRY(cudaEventRecord(h->ev_fork, h->stream));
+      CUDA_TRY(cudaStreamWaitEvent(h->aux, h->ev_fork, 0));
+      s = h->aux;
+    }
+    sample_gather_kernel<<<dim3(std::max(gx, 1), h->n_flush), 256, 0, s>>>(
         h->d_flush, fields, h->NY, h->P, h->samples, h->n_samples, slot);
     err = cudaGetLastError();
     if (err != cudaSuccess) return cuda_fail(err, "sample_gather_kernel launch");
+    if (h->async_gather) {
+      CUDA_TRY(cudaEventRecord(h->ev_gat[h->cur], h->aux));
+      h->gat_pending[h->cur] = true;
+    }
     ++h->launches;
   }
   return 0;
@@ -826,7 +851,7 @@ int flush_samples(fdtd_engine* h) {
     const size_t smem = sizeof(float2) * static_cast<size_t>(h->pending) * h->n_freq;
     // In a captured step block the weights start at the block's device-side base step.
     const int n_base = h->graph_base ? h->pending_base - h->graph_n0 : h->pending_base;
-    dft_flush_kernel<<<grid, threads, smem, h->stream>>>(h->samples, h->n_samples, h->pending, n_base, h->n_freq,
+    dft_flush_kernel<<<grid, threads, smem, h->async_gather ? h->aux : h->stream>>>(h->samples, h->n_samples, h->pending, n_base, h->n_freq,
                                                            h->w_e, h->w_h, h->d_flush, h->acc_re, h->acc_im,
                                                            h->cmp_re, h->cmp_im, h->graph_base ? h->d_base : nullptr);
     cudaError_t err = cudaGetLastError();
@@ -997,6 +1022,16 @@ int fdtd_engine_create(const fdtd_grid_desc* desc, void* stream, fdtd_engine** o
     cudaError_t e2 = cudaEventCreate(&h->ev1);
     if (e1 != cudaSuccess || e2 != cudaSuccess) rc = cuda_fail(e1 != cudaSuccess ? e1 : e2, "cudaEventCreate");
   }
+  if (!rc) {
+    int least = 0, greatest = 0;
+    cudaError_t e = cudaDeviceGetStreamPriorityRange(&least, &greatest);
+    if (e == cudaSuccess) e = cudaStreamCreateWithPriority(&h->aux, cudaStreamNonBlocking, greatest);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&h->ev_fork, cudaEventDisableTiming);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&h->ev_join, cudaEventDisableTiming);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&h->ev_gat[0], cudaEventDisableTiming);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&h->ev_gat[1], cudaEventDisableTiming);
+    if (e != cudaSuccess) rc = cuda_fail(e, "gather stream and events");
+  }
   if (rc) {
     fdtd_engine_destroy(h);
     return rc;
@@ -1037,6 +1072,10 @@ int fdtd_engine_destroy(fdtd_engine* h) {
   cudaFree(h->acc_im);
   cudaFree(h->cmp_re);
   cudaFree(h->cmp_im);
+  if (h->aux) cudaStreamSynchronize(h->aux);
+  for (cudaEvent_t e : {h->ev_fork, h->ev_join, h->ev_gat[0], h->ev_gat[1]})
+    if (e) cudaEventDestroy(e);
+  if (h->aux) cudaStreamDestroy(h->aux);
   if (h->ev0) cudaEventDestroy(h->ev0);
   if (h->ev1) cudaEventDestroy(h->ev1);
   delete h;
@@ -1723,6 +1762,32 @@ int fdtd_engine_finalize(fdtd_engine* h) {
 
 static int step_range_impl(fdtd_engine* h, int n0, int n1, bool record);
 
+// Scope of the second-stream gather inside step_range: forks the gather
+// stream from the engine stream on entry (work queued before the call is
+// visible to it) and joins it back on join() or on any early return.
+struct AsyncGather {
+  fdtd_engine* h;
+  bool on;
+  AsyncGather(fdtd_engine* e, bool enable) : h(e), on(enable) {
+    if (!on) return;
+    if (cudaEventRecord(h->ev_fork, h->stream) != cudaSuccess || cudaStreamWaitEvent(h->aux, h->ev_fork, 0) != cudaSuccess) {
+      on = false;
+      return;
+    }
+    h->async_gather = true;
+  }
+  int join() {
+    if (!on) return 0;
+    on = false;
+    h->async_gather = false;
+    h->gat_pending[0] = h->gat_pending[1] = false;
+    CUDA_TRY(cudaEventRecord(h->ev_join, h->aux));
+    CUDA_TRY(cudaStreamWaitEvent(h->stream, h->ev_join, 0));
+    return 0;
+  }
+  ~AsyncGather() { join(); }
+};
+
 int fdtd_engine_step_range(fdtd_engine* h, int n0, int n1) { return step_range_impl(h, n0, n1, false); }
 
 int fdtd_engine_step_range_recorded(fdtd_engine* h, int n0, int n1) {
@@ -1746,6 +1811,12 @@ static int step_range_impl(fdtd_engine* h, int n0, int n1, bool record) {
   if (h->n_samples > 0 && h->n_freq > 0 && n1 > h->dft_steps)
     return fail(FDTD_ERR_INVALID_ARG, "DFT weight table shorter than the range");
   CUDA_TRY(cudaEventRecord(h->ev0, h->stream));
+  // Gather and flush on the second stream unless the engine's stream is being
+  // captured into a graph (batches capture their own single-stream steps).
+  cudaStreamCaptureStatus capturing = cudaStreamCaptureStatusNone;
+  CUDA_TRY(cudaStreamIsCapturing(h->stream, &capturing));
+  AsyncGather overlap(h, h->aux && h->n_flush > 0 && h->n_samples > 0 && !h->graph_base &&
+                             capturing == cudaStreamCaptureStatusNone);
   if (record) {
     StepParams p;
     fill_params(h, p);
@@ -1774,6 +1845,10 @@ static int step_range_impl(fdtd_engine* h, int n0, int n1, bool record) {
         if (rc) return rc;
       }
     }
+  }
+  {
+    const int rc = overlap.join();
+    if (rc) return rc;
   }
   CUDA_TRY(cudaEventRecord(h->ev1, h->stream));
   CUDA_TRY(cudaEventSynchronize(h->ev1));
