@@ -235,6 +235,39 @@ def test_ade_pass_matches_poles_in_step_kernel():
     ref32.close()
 
 
+def test_pinned_scene_and_host_results_match():
+    """An engine built from pin_scene's copy (coefficient and pole arrays in
+    pinned memory, uploaded asynchronously) steps to bit-identical fields and
+    spectra, and monitor_results(host=True) returns the same values on the host
+    as the device tensors."""
+    wm = load_package()
+    steps = 120
+    sc = wm.Scene(cells=(40, 36, 36), spacing=25e-9, pml_cells=6)
+    sc.structures.append(wm.Structure(wm.Sphere((21, 18, 18), 6.0), wm.Medium.lorentz(2.0, 3.0, 250e12, 20e12)))
+    sc.structures.append(wm.Structure(wm.Box((8, 8, 8), (14, 28, 28)), wm.Medium(eps_r=3.0)))
+    sc.sources.append(wm.PointDipole((26, 18, 18), "Ez", wm.GaussianPulse(300e12, 100e12), width=25e-9))
+    sc.monitors.append(wm.flux_monitor("flux", 2, 24, (250e12, 300e12)))
+    cs = wm.compile_scene(sc, steps)
+    ref = wm.solver.B200FDTD(cs).init_field()
+    ref.step_range(0, steps)
+    ref_fields = {n: ref.field(n).cpu().numpy() for n in FIELDS}
+    ref_mons = {k: {c: v.cpu().numpy() for c, v in d.items()} for k, d in ref.monitor_results().items()}
+    ref.close()
+    pinned = wm.solver.pin_scene(cs)
+    assert all(v is None or v.is_pinned() for v in pinned.curl.values())
+    assert all(p.drive.is_pinned() for p in pinned.poles)
+    solver = wm.solver.B200FDTD(pinned).init_field()
+    solver.step_range(0, steps)
+    for n in FIELDS:
+        np.testing.assert_array_equal(solver.field(n).cpu().numpy(), ref_fields[n], err_msg=n)
+    host = solver.monitor_results(host=True)
+    for name, comps in ref_mons.items():
+        for comp, v in comps.items():
+            assert host[name][comp].device.type == "cpu" and host[name][comp].is_pinned()
+            np.testing.assert_array_equal(host[name][comp].numpy(), v, err_msg=f"{name} {comp}")
+    solver.close()
+
+
 def test_checkpoint_roundtrip_and_autotune_restore_state():
     wm = load_package()
     steps = 60

@@ -34,6 +34,24 @@ def _require_cuda(device: torch.device) -> None:
 STORAGE_KINDS = {"fp32": 0, "fp16": 1, "bf16": 2}
 
 
+def pin_scene(cs):
+    """A copy of a compiled scene whose large per-cell arrays (the decay / curl
+    coefficient arrays and the pole drive / 1/eps boxes) are CPU tensors in
+    pinned memory, so that building an engine from it uploads them
+    asynchronously at full PCIe / C2C speed.  The small arrays stay numpy."""
+    import dataclasses
+
+    def pin(a):
+        return None if a is None else torch.from_numpy(np.ascontiguousarray(a)).pin_memory()
+
+    return dataclasses.replace(
+        cs,
+        decay={k: pin(v) for k, v in cs.decay.items()},
+        curl={k: pin(v) for k, v in cs.curl.items()},
+        poles=[dataclasses.replace(p, drive=pin(p.drive), inv_eps=pin(p.inv_eps)) for p in cs.poles],
+    )
+
+
 class B200FDTD:
     def __init__(
         self,
@@ -68,7 +86,12 @@ class B200FDTD:
 
     # ------------------------------------------------------------------ setup
     def _dev(self, array, dtype=torch.float32) -> torch.Tensor:
-        t = torch.as_tensor(np.ascontiguousarray(array)).to(device=self.device, dtype=dtype).contiguous()
+        if isinstance(array, torch.Tensor):
+            # a CPU tensor (pinned by pin_scene) uploads asynchronously on the
+            # engine's stream, which every later use of it is ordered behind
+            t = array.to(device=self.device, dtype=dtype, non_blocking=True).contiguous()
+        else:
+            t = torch.as_tensor(np.ascontiguousarray(array)).to(device=self.device, dtype=dtype).contiguous()
         self._keep.append(t)
         return t
 
@@ -315,8 +338,11 @@ class B200FDTD:
         _lib.check(self.lib.fdtd_engine_read_dft(h, _lib.ptr(re), _lib.ptr(im)), "read_dft")
         return re, im
 
-    def monitor_results(self) -> dict:
-        """{monitor: {component: complex64 tensor [F, *box shape]}} scaled by 2/sum(window)."""
+    def monitor_results(self, host: bool = False) -> dict:
+        """{monitor: {component: complex64 tensor [F, *box shape]}} scaled by 2/sum(window).
+        host=True returns CPU tensors in pinned memory (torch's caching host
+        allocator), copied asynchronously on the engine stream and synchronized
+        once: several times faster than .cpu() on each device tensor."""
         cs = self.compiled
         if not cs.regions or not cs.frequencies:
             return {}
@@ -335,6 +361,16 @@ class B200FDTD:
             fidx = [cs.frequencies.index(f) for f in cs.monitor_frequencies[reg.monitor]]
             data = torch.complex(re[fidx, base:base + count], im[fidx, base:base + count]) * scale
             out.setdefault(reg.monitor, {})[reg.component] = data.reshape((len(fidx),) + shape)
+        if host:
+            staged: dict = {}
+            for name, comps in out.items():
+                staged[name] = {}
+                for comp, v in comps.items():
+                    hv = torch.empty(v.shape, dtype=v.dtype, pin_memory=True)
+                    hv.copy_(v, non_blocking=True)
+                    staged[name][comp] = hv
+            torch.cuda.current_stream(self.device).synchronize()
+            return staged
         return out
 
     def close(self) -> None:
