@@ -151,9 +151,14 @@ __global__ void adj_pass_a_kernel(const StepParams p, const AdjParams q) {
 
 // ---- pass B: gE = de gE' - C_E^T g(d_H); adjoint E psi; design gradient ----
 // kPoles: the scene has ADE poles (their transpose is compiled only then: in
-// the per-component loop it slows the pole-free kernel by a third).
+// the per-component loop it slows the pole-free kernel by a third).  The
+// pole-free kernel runs twelve 128-thread CTAs per SM (40 registers, no
+// spills): the pass is latency-bound, and 48 resident warps against 32 at 64
+// registers took the backward of the 160x160x96 design workload from 910 to
+// 782 ms.  The pole kernel spills at that budget and runs five CTAs per SM
+// (at most 102 registers, 70-72 used).
 template <bool kUniform, bool kPoles>
-__global__ void adj_pass_b_kernel(const StepParams p, const AdjParams q) {
+__global__ void __launch_bounds__(128, kPoles ? 5 : 12) adj_pass_b_kernel(const StepParams p, const AdjParams q) {
   {
     // one thread per cell: k from the x-dimension, rows and planes from y and z
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
