@@ -149,48 +149,118 @@ def barrier(world: int):
         dist.barrier()
 
 
-def cpu_reference_step_time(wm, cells: int, steps: int, threads: int) -> tuple[float, int]:
-    """Seconds per step and cell count of the oracle (FP32) on a scaled-down copy
-    (cells^3, same materials, sources and monitors scaled with the grid)."""
+def cpu_model() -> str:
+    try:
+        for line in Path("/proc/cpuinfo").read_text().splitlines():
+            if line.lower().startswith("model name"):
+                return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    import platform
+
+    return platform.processor() or "unknown"
+
+
+def cpu_workload_run(wm, steps: int, warmup: int, threads: int, budget_s: float | None = None) -> dict:
+    """The workload (full 256^3 grid) stepped by the oracle in FP32 on `threads`
+    host threads: `warmup` untimed steps, then `steps` timed ones, or as many as
+    fit in `budget_s` seconds when that is given (at least two)."""
     from oracle import oracle as orc
 
     orc.build()
-    cs = wm.compile_scene(wm.workloads.dispersive_256(cells=cells), steps + 2)
+    total = warmup + max(steps, 2) + (64 if budget_s else 2)
+    cs = wm.compile_scene(wm.workloads.dispersive_256(), total)
     sim = orc.OracleSimulation(cs, "f32", threads=threads)
-    sim.step_once()  # warm
-    t0 = time.perf_counter()
-    for _ in range(steps):
+    for _ in range(warmup):
         sim.step_once()
-    dt = (time.perf_counter() - t0) / steps
+    done = 0
+    t0 = time.perf_counter()
+    while True:
+        sim.step_once()
+        done += 1
+        elapsed = time.perf_counter() - t0
+        if budget_s is None and done >= steps:
+            break
+        if budget_s is not None and done >= 2 and (elapsed >= budget_s or done >= total - warmup - 2):
+            break
     sim.close()
-    return dt, cs.cells
+    return {"cells": int(cs.cells), "steps": done, "elapsed_s": elapsed, "value": cs.cells * done / elapsed / 1e9,
+            "compiled": cs}
+
+
+def cpu_baseline_entry(run: dict, threads: int, what: str) -> dict:
+    return {
+        "value": run["value"], "unit": METRIC, "cores": threads, "kind": "port",
+        "cpu_model": cpu_model(), "host_threads": os.cpu_count(),
+        "sample": f"{run['steps']} steps of the full 256^3 workload ({what}), FP32 C oracle (the reference's "
+                  f"algorithm restated), {threads} threads, {run['elapsed_s']:.1f} s",
+    }
+
+
+def reference_gpu_bar(wm, cs, span: int = 8, reps: int = 5) -> dict:
+    """The reference's own CUDA ops (built from its sources into oracle/_ref) on
+    the same scene tensors, stepped in the reference's order with its own FP32
+    observer kernels (monitors on), captured into CUDA graphs of `span` and
+    2 * `span` steps; ms per step = (T(2 span) - T(span)) / span, the two-point
+    slope of the median replay times (CUDA events)."""
+    import torch
+
+    from oracle import ref_gpu
+
+    if not ref_gpu.available():
+        return {"unavailable": "oracle/_ref not built"}
+    if not torch.cuda.is_available():
+        return {"unavailable": "no CUDA device"}
+    sim = ref_gpu.RefGpuSimulation(cs, monitor_ops=True)
+    sim.run(3)
+    torch.cuda.synchronize()
+    side = torch.cuda.Stream()
+    graphs = {}
+    for n in (span, 2 * span):
+        side.wait_stream(torch.cuda.current_stream())
+        with torch.cuda.stream(side):
+            sim.run(1)
+        torch.cuda.current_stream().wait_stream(side)
+        g = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(g):
+            sim.run(n)
+        graphs[n] = g
+    times = {}
+    for n, g in graphs.items():
+        g.replay()
+        torch.cuda.synchronize()
+        samples = []
+        for _ in range(reps):
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record()
+            g.replay()
+            b.record()
+            b.synchronize()
+            samples.append(a.elapsed_time(b))
+        times[n] = statistics.median(samples)
+    ms = (times[2 * span] - times[span]) / span
+    del graphs, sim
+    torch.cuda.empty_cache()
+    return {
+        "ms_per_step": ms,
+        "value": cs.cells / (ms * 1e-3) / 1e9,
+        "unit": METRIC,
+        "what": "the reference's CUDA ops compiled for sm_100 from its own sources, stepped in its order "
+                "(stepping.py:1740-1815, 2295-2330) with its FP32 observer kernels per (region, frequency), "
+                "CUDA-graph captured, two-point slope of graph replays",
+        "graph_ms": {str(k): v for k, v in times.items()},
+    }
 
 
 def run_reference_arm(args, wm, world, rank):
-    """CPU restatement of the reference path, all host threads, bounded sample per step."""
+    """The reference's algorithm on the host cores (the FP32 C oracle, all host
+    threads) over the full workload, and beside it the reference's own CUDA ops
+    from oracle/_ref on the GPU (graph-captured, monitors on)."""
     if rank != 0:
         return None
     threads = os.cpu_count() or 1
-    from oracle import oracle as orc
-
-    orc.build()
-    full_cells = 256 ** 3
-    # size the per-step sample (a scaled copy of the workload) so the run stays within ~3 minutes
-    probe_dt, probe_cells = cpu_reference_step_time(wm, 48, 2, threads)
-    per_cell = probe_dt / probe_cells
-    budget_cells = 150.0 / max(args.steps + args.warmup, 1) / per_cell
-    n = int(max(32, min(256, round(budget_cells ** (1.0 / 3.0) / 8) * 8)))
-    cs = wm.compile_scene(wm.workloads.dispersive_256(cells=n), args.steps + args.warmup + 2)
-    sim = orc.OracleSimulation(cs, "f32", threads=threads)
-    for _ in range(args.warmup):
-        sim.step_once()
-    t0 = time.perf_counter()
-    for _ in range(args.steps):
-        sim.step_once()
-    elapsed = time.perf_counter() - t0
-    sim.close()
-    value = cs.cells * args.steps / elapsed / 1e9
-    sample = f"{args.steps} steps of the workload scaled to {n}^3 cells (same materials, sources, monitors, scaled geometry)"
+    run = cpu_workload_run(wm, args.steps, args.warmup, threads)
+    value = run["value"]
     line = {
         "impl": "reference",
         "metric": METRIC,
@@ -199,32 +269,43 @@ def run_reference_arm(args, wm, world, rank):
         "n_gpus": world,
         "steps": args.steps,
         "warmup": args.warmup,
-        "ms_per_step": elapsed * 1e3 / args.steps,
+        "ms_per_step": run["elapsed_s"] * 1e3 / run["steps"],
         "higher_is_better": True,
         "scaling": "weak",
         "vs_baseline": None,
         "dtype": "f32",
         "data": "synthetic",
-        "config": {"workload": WORKLOAD, "cells_full": int(full_cells), "cells_sample": int(cs.cells)},
-        "cpu_baseline": {"value": value, "unit": METRIC, "cores": threads, "kind": "port", "sample": sample},
+        "config": {"workload": WORKLOAD, "cells": run["cells"]},
+        "cpu_baseline": cpu_baseline_entry(run, threads, f"after {args.warmup} warm-up steps"),
         "e2e": {"value": value, "unit": METRIC, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
+    if args.reference_gpu:
+        try:
+            line["reference_gpu"] = reference_gpu_bar(wm, run["compiled"])
+        except Exception as exc:  # reported beside the CPU value, never fatal
+            line["reference_gpu"] = {"unavailable": f"{type(exc).__name__}: {exc}"}
     return line
 
 
+# DRAM bytes per launch (dram__bytes_read.sum + dram__bytes_write.sum) of the
+# step kernels of one step of the full 256^3 workload, from one ncu capture of
+# this launch shape (kernel name -> bytes); the capture and its command are
+# summarised in profiles/.  Reported as `traffic` only when the run used the
+# same kernels and grid; null otherwise.
+NCU_TRAFFIC = {
+    "cells": 256 ** 3,
+    "kernels": {"warp_step_kernel<1,1,1,4,0>": 1055.3e6, "ade_pass_kernel": 372.1e6},
+    "launch": {"variant": 2, "chunk_planes": 13},
+}
+
+
 def measured_traffic(info, cells):
-    """DRAM bytes of one step (the step kernel and the ADE pass after it) from
-    the committed ncu capture (profiles/step_kernel_traffic.json), when it was
-    taken on this launch shape and grid size; None otherwise."""
-    path = ROOT / "profiles" / "step_kernel_traffic.json"
-    if not path.exists():
+    rec = NCU_TRAFFIC
+    if (info["variant"], info["chunk_planes"]) != (rec["launch"]["variant"], rec["launch"]["chunk_planes"]):
         return None
-    rec = json.loads(path.read_text())
-    if (rec.get("variant"), rec.get("chunk_planes"), rec.get("cells")) != (info["variant"], info["chunk_planes"], int(cells)):
+    if int(cells) != rec["cells"]:
         return None
-    if "kernels" not in rec:
-        return None
-    return int(sum(k["dram_bytes_read"] + k["dram_bytes_write"] for k in rec["kernels"]))
+    return int(sum(rec["kernels"].values()))
 
 
 def run_b200_arm(args, wm, world, rank, local):
@@ -300,7 +381,11 @@ def run_b200_arm(args, wm, world, rank, local):
             "traffic_unit": "bytes per step, both kernels (dram__bytes_read.sum + dram__bytes_write.sum)",
         },
         "algorithmic_bytes_per_cell_update": {k: round(v, 3) for k, v in bytes_alg.items() if k != "cells"},
-        "hbm_frac_whole_step": bytes_alg["total"] * cells * args.steps / (elapsed_s / world if world else elapsed_s) / 1e9 / peaks["hbm_gbs"],
+        # algorithmic bytes of the whole step (the per-step DFT read-modify-write
+        # of every monitor point counted as the reference does it) over the timed
+        # steps, which include every DFT flush of those steps; the engine moves
+        # fewer bytes (the flush accumulates 32 steps per pass)
+        "whole_step_alg_frac": bytes_alg["total"] * cells * args.steps * world / elapsed_s / 1e9 / peaks["hbm_gbs"],
         "clocks": clock_info,
         "gpu_launches": int(launches),
         "compile_s": t_compile,
@@ -322,12 +407,8 @@ def run_b200_arm(args, wm, world, rank, local):
     if rank == 0 and args.cpu_baseline:
         try:
             threads = os.cpu_count() or 1
-            step_dt, sample_cells = cpu_reference_step_time(wm, 96, 3, threads)
-            cpu_value = sample_cells / step_dt / 1e9
-            result["cpu_baseline"] = {
-                "value": cpu_value, "unit": METRIC, "cores": threads, "kind": "port",
-                "sample": "3 steps (after 1 warm-up) of the workload scaled to 96^3 cells, FP32 oracle, all host threads",
-            }
+            run = cpu_workload_run(wm, 0, 2, threads, budget_s=12.0)
+            result["cpu_baseline"] = cpu_baseline_entry(run, threads, "after 2 warm-up steps, about 12 s")
         except Exception as exc:  # the CPU baseline is reported, never fatal
             result["cpu_baseline"] = {"value": None, "unit": METRIC, "cores": os.cpu_count(), "kind": "port",
                                       "sample": f"failed: {exc}"}
@@ -578,6 +659,8 @@ def main():
                     help="skip the 512x512x384 Bloch grating timing")
     ap.add_argument("--no-adjoint", dest="adjoint", action="store_false",
                     help="skip the forward+adjoint timing of the 160x160x96 design workload")
+    ap.add_argument("--no-reference-gpu", dest="reference_gpu", action="store_false",
+                    help="reference arm: skip the timing of the reference's own CUDA ops")
     ap.add_argument("--cells", type=int, default=256,
                     help="cells per axis of the (scaled) workload; 256 is the benchmark, smaller sizes are for profiling")
     args = ap.parse_args()

@@ -201,6 +201,15 @@ int fdtd_engine_set_ade_pass(fdtd_engine* h, int on);
  * their row of the E/H fields `planes` x planes (0..16; 0 disables) ahead of
  * their march.  Results do not depend on it. */
 int fdtd_engine_set_prefetch(fdtd_engine* h, int planes);
+/* Failure detection: polling rounds (default 1 << 20) a bounded pipeline wait
+ * inside a step kernel makes before it gives up, records FDTD_ERR_TIMEOUT in
+ * the device status word and returns; the next step_range then returns
+ * FDTD_ERR_TIMEOUT.  The TMA variant (4) waits on its mbarrier ring this way;
+ * its producer still waits for every copy it issued before the block exits
+ * (that drain has its own fixed bound).  0 makes every pipeline wait run out
+ * at once, which is how the timeout path is tested.  No counterpart in the
+ * reference (its kernels have no device-side waits). */
+int fdtd_engine_set_wait_limit(fdtd_engine* h, int rounds);
 /* Launch configuration and launch count bookkeeping. */
 int fdtd_engine_info(fdtd_engine* h, int* tile_rows, int* chunk_planes, int* grid_x, int* grid_y,
                      int* block, int64_t* launches);
@@ -336,6 +345,8 @@ int fdtd_op_add_line_patch(float* field, const int* fshape, const float* coeff, 
 /* Auxiliary 1-D grid (sources.cu:803-839). */
 int fdtd_op_aux_magnetic(int n_e, float* h, const float* e, const float* h_decay, const float* h_curl,
                          void* stream);
+/* The last cell (n_e - 1) is pinned to zero before the source cell is
+ * considered; a negative source_index injects nothing. */
 int fdtd_op_aux_electric(int n_e, float* e, const float* h, const float* e_decay, const float* e_curl,
                          int source_index, float source_value, void* stream);
 
@@ -354,13 +365,16 @@ int fdtd_op_aux_electric(int n_e, float* e, const float* h, const float* e_decay
  * the source cell), and the outputs e_hist and h_hist (n_steps x n_e, row n =
  * the line before E/after H of step n; the last entry of each H row is zero).
  * Same recurrence as fdtd_op_aux_magnetic followed by fdtd_op_aux_electric,
- * stepped n_steps times from a zero line.
+ * stepped n_steps times from a zero line.  A negative source_index injects
+ * nothing; a source on the last cell (n_e - 1) is overridden by that cell's
+ * zero, as in the reference's update_auxiliary_electric_kernel.
  *
  * Limit: n_e <= FDTD_AUX_STATIC_MAX_CELLS; larger lines return
  * FDTD_ERR_INVALID_ARG.  The line state starts at zero on every call (the
- * kernel clears it); nothing else needs clearing.  The first call on each
- * device looks up the array's device address (which may load the module); make
- * it once per device, with that device current, before any stream capture.
+ * kernel clears it); nothing else needs clearing.  Every call looks up the
+ * array's device address on the current device (no allocation); the first call
+ * on a device may load the module, so make one call per device, with that
+ * device current, before any stream capture.
  * The array is shared by every call on a device: calls that can overlap
  * (different streams, or unordered host threads) race on it and both results
  * are undefined, so order them on one stream. */

@@ -8,7 +8,10 @@ the list in witwin/maxwell/fdtd/cuda/build.py:181-197), with the defines that
 file passes (build.py:300-310), for sm_100.  Nothing is copied; the outputs
 (objects, ninja files, the .so) go to oracle/_ref/, which git ignores.
 
-Usage: python oracle/build_ref.py [reference checkout, default /root/reference]
+Usage: python oracle/build_ref.py [reference checkout]
+
+The checkout is the argument, else the WITWIN_MAXWELL_REFERENCE environment
+variable, else the build container's read-only copy (REFERENCE_DEFAULT).
 """
 from __future__ import annotations
 
@@ -17,6 +20,15 @@ import sys
 from pathlib import Path
 
 HERE = Path(__file__).resolve().parent
+# where the build container mounts the reference checkout (read-only); this
+# recipe and the golden-vector scripts are the only files that name it
+REFERENCE_DEFAULT = "/root/reference"
+
+
+def reference_checkout(arg: str | None = None) -> Path | None:
+    """The reference checkout to read, or None when none is present."""
+    path = Path(arg or os.environ.get("WITWIN_MAXWELL_REFERENCE") or REFERENCE_DEFAULT)
+    return path if (path / "witwin" / "maxwell").is_dir() else None
 OUT = HERE / "_ref"
 LIB_NAME = "witwin_maxwell_fdtd_cuda"
 SOURCES = ("extension.cpp", "kernels/common.cu", "kernels/magnetic.cu", "kernels/electric.cu", "kernels/boundary.cu",
@@ -52,5 +64,7 @@ def build(reference: Path) -> Path:
 
 
 if __name__ == "__main__":
-    ref = Path(sys.argv[1]) if len(sys.argv) > 1 else Path("/root/reference")
+    ref = reference_checkout(sys.argv[1] if len(sys.argv) > 1 else None)
+    if ref is None:
+        sys.exit("no reference checkout: pass its path or set WITWIN_MAXWELL_REFERENCE")
     print(build(ref))

@@ -260,8 +260,10 @@ void oracle_aux_electric(int ne, real *e, const real *h, const real *edecay, con
     if (x == src_index) continue;
     e[x] = edecay[x] * e[x] - ecurl[x] * (h[x] - h[x - 1]);
   }
-  if (ne > 0) e[ne - 1] = (real)0;
+  /* the source cell first, then the last cell pinned to zero: the reference's
+     kernel checks the last cell before the source cell (sources.cu:829-835) */
   if (src_index >= 0 && src_index < ne) e[src_index] = src_value;
+  if (ne > 0) e[ne - 1] = (real)0;
 }
 
 /* ------------------------------------------------------------------------- */

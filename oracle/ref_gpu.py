@@ -1,4 +1,4 @@
-"""The reference's own CUDA FDTD ops, stepped in the reference's order (test checker).
+"""The reference's own CUDA FDTD ops, stepped in the reference's order (checker).
 
 Loads the library that ``oracle/build_ref.py`` compiles from the reference's
 sources into ``oracle/_ref/`` and drives its torch ops
@@ -8,8 +8,16 @@ compiled scene, one op per launch, in the order of
 witwin/maxwell/fdtd/runtime/stepping.py:1740-1815 and :2295-2330: H update,
 TFSF magnetic corrections, aux H, ADE advance, E update, TFSF electric
 corrections, aux E, soft sources, ADE subtraction, PEC clamp.  The monitor
-DFT is accumulated here in float64 from the stepped fields (phase recurrence
-as observers.py:577-659).  Only tests import this module.
+DFT is accumulated in float64 from the stepped fields (phase recurrence as
+observers.py:577-659), or -- with ``monitor_ops=True``, for timing the
+reference -- by the reference's own FP32 observer kernels, one
+accumulate_plane_observer launch per (plane region, frequency) and one
+accumulate_point_observers launch per (point group, frequency), with the
+weights evaluated on the host per step as accumulate_observers does
+(observers.py:577-659).
+
+Test and measurement infrastructure: only tests/ and bench.py's reference
+arm import this module.
 """
 from __future__ import annotations
 
@@ -47,7 +55,7 @@ def _shape(name, nodes):
 
 
 class RefGpuSimulation:
-    def __init__(self, compiled, device: str = "cuda", channel: int = 0):
+    def __init__(self, compiled, device: str = "cuda", channel: int = 0, monitor_ops: bool = False):
         self.cs = cs = compiled
         self.op = ops()
         dev = torch.device(device)
@@ -121,6 +129,33 @@ class RefGpuSimulation:
         self.window_sum = 0.0
         self.step = 0
         self.monitors = True
+        self.monitor_ops = bool(monitor_ops)
+        self.ops_groups = self._observer_groups(nf) if self.monitor_ops else []
+
+    def _observer_groups(self, nf):
+        """The reference's observer launch groups: a region one cell thick along
+        an axis is a plane observer over the component's whole plane
+        (observers.cu accumulate_plane_observer); every other region's cells
+        form a point group of that component (accumulate_point_observers).
+        FP32 accumulators, one per frequency."""
+        groups = []
+        nodes = self.cs.nodes
+        for r, reg in enumerate(self.cs.regions):
+            b = reg.box
+            ext = _shape(reg.component, nodes)
+            sizes = [b[1] - b[0], b[3] - b[2], b[5] - b[4]]
+            axis = next((a for a in (2, 0, 1) if sizes[a] == 1), None)
+            if axis is not None and sizes.count(1) < 3:
+                plane = [ext[a] for a in range(3) if a != axis]
+                acc = [torch.zeros((nf, *plane), device=self.dev) for _ in range(2)]
+                groups.append(("plane", r, reg.component, axis, b[2 * axis], acc))
+            else:
+                ii, jj, kk = np.meshgrid(np.arange(b[0], b[1]), np.arange(b[2], b[3]), np.arange(b[4], b[5]),
+                                         indexing="ij")
+                idx = [torch.as_tensor(v.ravel().astype(np.int64), device=self.dev) for v in (ii, jj, kk)]
+                acc = [torch.zeros((nf, idx[0].numel()), device=self.dev) for _ in range(2)]
+                groups.append(("points", r, reg.component, idx, None, acc))
+        return groups
 
     # ------------------------------------------------------------------ ops
     def _update_h(self):
@@ -192,6 +227,20 @@ class RefGpuSimulation:
         wc, ws = w * self.pc, w * self.ps
         hc = wc * self.hoff_c - ws * self.hoff_s
         hs = ws * self.hoff_c + wc * self.hoff_s
+        if self.monitor_ops:
+            for kind, _r, comp, where, index, (re, im) in self.ops_groups:
+                cc, ss = (wc, ws) if comp[0] == "E" else (hc, hs)
+                for f in range(self.freqs.size):
+                    if kind == "plane":
+                        self.op.accumulate_plane_observer(self.F[comp], re[f], im[f], int(where), int(index),
+                                                          float(cc[f]), float(ss[f]))
+                    else:
+                        self.op.accumulate_point_observers(self.F[comp], where[0], where[1], where[2], re[f], im[f],
+                                                           float(cc[f]), float(ss[f]))
+            self.window_sum += w
+            self.pc, self.ps = (self.pc * self.step_c - self.ps * self.step_s,
+                                self.ps * self.step_c + self.pc * self.step_s)
+            return
         for reg, (re, im) in zip(cs.regions, self.acc):
             b = reg.box
             v = self.F[reg.component][b[0]:b[1], b[2]:b[3], b[4]:b[5]].double()
@@ -235,6 +284,19 @@ class RefGpuSimulation:
         cs = self.cs
         scale = 2.0 / self.window_sum if self.window_sum > 0 else 0.0
         out: dict = {}
+        if self.monitor_ops:
+            for kind, r, comp, where, index, (re, im) in self.ops_groups:
+                reg = cs.regions[r]
+                b = reg.box
+                shape = (b[1] - b[0], b[3] - b[2], b[5] - b[4])
+                if kind == "plane":
+                    sl = [slice(b[2 * a], b[2 * a + 1]) for a in range(3) if a != where]
+                    data = (re[(slice(None), *sl)].double() + 1j * im[(slice(None), *sl)].double()).cpu().numpy()
+                else:
+                    data = (re.double() + 1j * im.double()).cpu().numpy()
+                fidx = [cs.frequencies.index(f) for f in cs.monitor_frequencies[reg.monitor]]
+                out.setdefault(reg.monitor, {})[comp] = data[fidx].reshape((len(fidx),) + shape) * scale
+            return out
         for reg, (re, im) in zip(cs.regions, self.acc):
             fidx = [cs.frequencies.index(f) for f in cs.monitor_frequencies[reg.monitor]]
             data = (re[fidx].cpu().numpy() + 1j * im[fidx].cpu().numpy()) * scale

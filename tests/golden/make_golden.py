@@ -3,7 +3,10 @@
 Run from the repository root in a container where the reference checkout is
 available (it is not needed anywhere else):
 
-    python tests/golden/make_golden.py --reference /root/reference
+    python tests/golden/make_golden.py [--reference CHECKOUT]
+
+(the checkout defaults to WITWIN_MAXWELL_REFERENCE or the build container's
+copy, as oracle/build_ref.py resolves it)
 
 It imports the reference's frozen Torch implementation of the FDTD kernels
 (tests/fdtd/cuda/torch_reference.py, "a snapshot of the pre-CUDA-only backend
@@ -459,10 +462,16 @@ def step_vectors(tr) -> dict:
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--reference", default="/root/reference")
+    ap.add_argument("--reference", default=None)
     args = ap.parse_args()
+    sys.path.insert(0, str(HERE.parents[1]))
+    from oracle.build_ref import reference_checkout
+
+    ref = reference_checkout(args.reference)
+    if ref is None:
+        sys.exit("no reference checkout: pass --reference or set WITWIN_MAXWELL_REFERENCE")
     torch.set_default_dtype(torch.float64)
-    tr = load_reference(Path(args.reference))
+    tr = load_reference(ref)
     rng = np.random.default_rng(20261203)
     np.savez_compressed(HERE / "ops.npz", **op_vectors(tr, rng))
     np.savez_compressed(HERE / "steps.npz", **step_vectors(tr))

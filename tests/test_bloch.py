@@ -3,7 +3,7 @@
 The step kernel defers the E cells on a wrapped face and the wrap kernel
 updates them from the whole new H (phase e^{ikL} across the wrap, the real and
 imaginary channels coupled only there).  Checked against the reference's own
-CUDA ops compiled from its sources (oracle/_ref, tests/ref_gpu.py): the
+CUDA ops compiled from its sources (oracle/_ref, oracle/ref_gpu.py): the
 standard / compressed-CPML ops with periodic boundary modes for periodic
 scenes, and its complex Bloch E kernels for Bloch scenes.  Tolerance as the
 other engine parity tests: joint relative L2 <= 1e-5 on fields and monitors.
@@ -13,7 +13,7 @@ from __future__ import annotations
 import numpy as np
 import pytest
 
-import ref_gpu
+from oracle import ref_gpu
 from conftest import load_package
 from oracle import oracle as orc
 

@@ -332,3 +332,35 @@ def test_engine_rejects_bad_inputs():
     dummy = torch.zeros(64, device="cuda")
     assert lib.fdtd_engine_add_patch(handle, 0, box, dummy.data_ptr(), dummy.data_ptr(), 1, 1.0) == -1
     assert lib.fdtd_engine_destroy(handle) == 0
+
+
+def test_bounded_waits_report_timeout_and_leave_the_context_usable():
+    """Failure detection without a GPU fault: the TMA-fed step kernel (variant
+    4) waits on its mbarrier ring with a bounded number of polling rounds.
+    With the bound at zero every pipeline wait runs out at once: the kernel
+    records FDTD_ERR_TIMEOUT in the device status word and returns (its
+    producer still waits for the copies it issued), and step_range reports
+    the timeout.  With the default bound restored the same engine steps again
+    without error, and a fresh engine still matches the register kernel
+    bit for bit (the context is intact)."""
+    wm = load_package()
+    steps = 20
+    cs = wm.compile_scene(_c1_scene(wm, cells=40, pml=6), steps + 4)
+    solver = wm.solver.B200FDTD(cs).init_field()
+    solver.set_launch(4, 1, 0)
+    solver.set_wait_limit(0)
+    with pytest.raises(wm._lib.FdtdError) as err:
+        solver.step_range(0, 2)
+    assert "status -5" in str(err.value)
+    solver.set_wait_limit(1 << 20)
+    solver.step_range(2, 4)  # no timeout once the bound is back
+    solver.close()
+    fields = []
+    for variant in (4, 2):
+        solver = wm.solver.B200FDTD(cs).init_field()
+        solver.set_launch(variant, 1, 0)
+        solver.step_range(0, steps)
+        fields.append({n: solver.field(n).cpu().numpy() for n in FIELDS})
+        solver.close()
+    for n in FIELDS:
+        np.testing.assert_array_equal(fields[0][n], fields[1][n])

@@ -1,7 +1,7 @@
 """GPU parity of the fused engine against the reference's own CUDA kernels.
 
 The reference's torch ops are compiled from its sources by oracle/build_ref.py
-into oracle/_ref/ and stepped op by op in the reference's order (ref_gpu.py)
+into oracle/_ref/ and stepped op by op in the reference's order (oracle/ref_gpu.py)
 on the same compiled scene tensors.  Tolerance: relative L2 <= 1e-5 over all
 six field components together and over each monitor (both sides are FP32 on
 the same GPU; they differ only in FMA contraction and summation order).
@@ -17,7 +17,7 @@ import numpy as np
 import pytest
 import torch
 
-import ref_gpu
+from oracle import ref_gpu
 from conftest import load_package
 from test_engine_parity import FIELDS, TOL, _c1_scene, assert_monitors_close, joint_rel_l2
 

@@ -74,6 +74,35 @@ def test_static_history_matches_stepped_ops_twice_in_a_row():
         assert np.all(got_h[:, -1] == 0.0)
 
 
+def test_static_history_source_on_the_last_cell_and_no_source():
+    """A source placed on the last line cell is overridden by that cell's zero
+    (the reference's update_auxiliary_electric_kernel checks the last cell
+    first), in the static entry point and in the per-step op alike; a negative
+    source index injects nothing."""
+    import dataclasses
+
+    wm = load_package()
+    lib = wm._lib.load()
+    aux = _line(wm, 40, (1, 0, 0), 96)
+    ne = len(aux.e_decay)
+    # drive the last cell: its history stays zero and nothing propagates
+    last = dataclasses.replace(aux, source_index=ne - 1)
+    got_e, got_h = _static(lib, last)
+    want_e, want_h = _stepped(lib, last)
+    np.testing.assert_allclose(got_e, want_e, rtol=RTOL, atol=ATOL)
+    np.testing.assert_allclose(got_h[:, :-1], want_h[:, :-1], rtol=RTOL, atol=ATOL)
+    assert np.all(got_e == 0.0) and np.all(got_h == 0.0)
+    # a source on the second-to-last cell still drives the line
+    near = dataclasses.replace(aux, source_index=ne - 2)
+    got_e, _ = _static(lib, near)
+    want_e, _ = _stepped(lib, near)
+    np.testing.assert_allclose(got_e, want_e, rtol=RTOL, atol=ATOL)
+    assert np.abs(got_e).max() > 1e-3 and np.all(got_e[:, -1] == 0.0)
+    none = dataclasses.replace(aux, source_index=-1)
+    got_e, got_h = _static(lib, none)
+    assert np.all(got_e == 0.0) and np.all(got_h == 0.0)
+
+
 def test_static_history_rejects_lines_beyond_the_scratch_maximum():
     wm = load_package()
     lib = wm._lib.load()

@@ -81,6 +81,7 @@ _SIGNATURES = {
     "fdtd_engine_set_launch": ([_vp, _i, _i, _i], _i),
     "fdtd_engine_get_launch": ([_vp, _c_int_p, _c_int_p, _c_int_p], _i),
     "fdtd_engine_set_prefetch": ([_vp, _i], _i),
+    "fdtd_engine_set_wait_limit": ([_vp, _i], _i),
     "fdtd_engine_set_ade_pass": ([_vp, _i], _i),
     "fdtd_engine_checkpoint_reserve": ([_vp, _i], _i),
     "fdtd_engine_adjoint_init": ([_vp, _c_int_p, _i], _i),

@@ -20,7 +20,6 @@
 // results are undefined; order such calls on one stream.
 #include <cuda_runtime.h>
 
-#include <mutex>
 #include <string>
 
 #include "../../include/fdtd_b200.h"
@@ -31,20 +30,19 @@ using namespace fdtdb200;
 namespace {
 
 constexpr int kAuxStaticMaxCells = FDTD_AUX_STATIC_MAX_CELLS;
-constexpr int kMaxDevices = 64;
 
 // Running line state: E in [0, n_e), H in [kAuxStaticMaxCells, +n_e - 1).
 // Every call clears the part it uses before its first step.
 static __device__ __align__(256) float g_aux_line_scratch[2 * kAuxStaticMaxCells];
 
-std::mutex g_setup_mutex;
-float* g_scratch_ptr[kMaxDevices] = {};
 
 // One 256-thread block marches the line in time.  Same recurrence as the
 // engine's history kernel (AuxiliaryGrid1D.advance_magnetic/advance_electric,
 // witwin/maxwell/fdtd/excitation/spatial.py:443-462, sources.cu:803-839): the
 // E row is recorded before the step, H is advanced and recorded, then E is
-// advanced, its last cell pinned to zero and the source cell overwritten.
+// advanced, the source cell overwritten and the last cell pinned to zero (a
+// source on the last cell is overridden by the zero, as in the reference's
+// update_auxiliary_electric_kernel).  A negative source index injects nothing.
 // The last entry of each H row (no H cell there) is written as zero.
 __global__ void aux_history_static_kernel(int ne, const float* __restrict__ e_decay, const float* __restrict__ e_curl,
                                           const float* __restrict__ h_decay, const float* __restrict__ h_curl,
@@ -71,8 +69,10 @@ __global__ void aux_history_static_kernel(int ne, const float* __restrict__ e_de
     }
     __syncthreads();
     if (threadIdx.x == 0) {
-      e[ne - 1] = 0.0f;
+      // the source cell first, then the last cell pinned to zero: a source
+      // placed on the last cell is overridden, as in the reference's op
       if (src_index >= 0 && src_index < ne) e[src_index] = source[n];
+      e[ne - 1] = 0.0f;
     }
     __syncthreads();
   }
@@ -83,25 +83,18 @@ int static_fail(int code, const std::string& msg) {
   return code;
 }
 
-// Device address of the scratch array for the current device, looked up once
-// per device (cudaGetSymbolAddress may load this file's module on first use).
+// Device address of the scratch array on the current device.  Looked up on
+// every call (cheap and allocation-free), so the address stays valid after the
+// device's primary context is reset and this file's module is loaded again;
+// the first call on a device may load the module, so make it before any
+// stream capture.
 int scratch_for_current_device(float** out) {
-  int dev = -1;
-  cudaError_t err = cudaGetDevice(&dev);
-  if (err != cudaSuccess)
-    return static_fail(FDTD_ERR_CUDA, std::string("aux_line_history_static: cudaGetDevice: ") + cudaGetErrorString(err));
-  if (dev < 0 || dev >= kMaxDevices)
-    return static_fail(FDTD_ERR_UNSUPPORTED, "aux_line_history_static: device ordinal beyond 63");
-  std::lock_guard<std::mutex> lock(g_setup_mutex);
-  if (!g_scratch_ptr[dev]) {
-    float* ptr = nullptr;
-    err = cudaGetSymbolAddress(reinterpret_cast<void**>(&ptr), g_aux_line_scratch);
-    if (err != cudaSuccess || !ptr)
-      return static_fail(FDTD_ERR_CUDA, std::string("aux_line_history_static: cudaGetSymbolAddress: ") +
-                                            cudaGetErrorString(err));
-    g_scratch_ptr[dev] = ptr;
-  }
-  *out = g_scratch_ptr[dev];
+  float* ptr = nullptr;
+  const cudaError_t err = cudaGetSymbolAddress(reinterpret_cast<void**>(&ptr), g_aux_line_scratch);
+  if (err != cudaSuccess || !ptr)
+    return static_fail(FDTD_ERR_CUDA, std::string("aux_line_history_static: cudaGetSymbolAddress: ") +
+                                          cudaGetErrorString(err));
+  *out = ptr;
   return 0;
 }
 

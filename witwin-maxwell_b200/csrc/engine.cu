@@ -179,8 +179,10 @@ __global__ void aux_history_kernel(int ne, const float* e_decay, const float* e_
     }
     __syncthreads();
     if (threadIdx.x == 0) {
-      e[ne - 1] = 0.0f;
+      // the source cell first, then the last cell pinned to zero: a source
+      // placed on the last cell is overridden, as in the reference's op
       if (src_index >= 0 && src_index < ne) e[src_index] = source[n];
+      e[ne - 1] = 0.0f;
     }
     __syncthreads();
   }
@@ -444,6 +446,7 @@ struct fdtd_engine {
   TmaMaps maps[2] = {};                    // tensor maps of E[cur], H[cur] for cur = 0, 1
   bool tma_ready = false;
   int* d_status = nullptr;                 // timeout flag written by bounded waits
+  int wait_limit = 1 << 20;                // polling rounds of a bounded pipeline wait
   int class_key = 0;                      // (chunk length, lane width) the table was built for (0 = stale)
   std::vector<int*> index_bufs;
   RegionFlush* d_flush = nullptr;
@@ -625,6 +628,7 @@ void fill_params(const fdtd_engine* h, StepParams& p) {
   p.plane_bits = reinterpret_cast<const unsigned*>(h->d_plane_bits);
   p.warp_class = h->d_warp_class;
   p.status = h->d_status;
+  p.wait_limit = h->wait_limit;
   for (int ph = 0; ph < 2; ++ph) {
     p.term_index[ph] = h->term_ix[ph];
     p.n_terms[ph] = h->n_terms_ph[ph];
@@ -1846,6 +1850,12 @@ static int step_range_impl(fdtd_engine* h, int n0, int n1, bool record) {
       }
     }
   }
+  // The DFT of every step in the range is accumulated before the range ends,
+  // so the range's device time holds all of its monitor work.
+  {
+    const int rc = flush_samples(h);
+    if (rc) return rc;
+  }
   {
     const int rc = overlap.join();
     if (rc) return rc;
@@ -2044,6 +2054,12 @@ int fdtd_engine_set_launch(fdtd_engine* h, int variant, int tile_rows, int chunk
 int fdtd_engine_set_ade_pass(fdtd_engine* h, int on) {
   if (!h) return fail(FDTD_ERR_INVALID_ARG, "null engine");
   h->ade_pass = on != 0;
+  return 0;
+}
+
+int fdtd_engine_set_wait_limit(fdtd_engine* h, int rounds) {
+  if (!h || rounds < 0) return fail(FDTD_ERR_INVALID_ARG, "bad wait limit");
+  h->wait_limit = rounds;
   return 0;
 }
 
@@ -2706,6 +2722,11 @@ int fdtd_bloch_step_range(fdtd_bloch* p, int n0, int n1) {
         if (rc) return rc;
       }
     }
+  }
+  // the DFT of every step of the range lands inside the range
+  for (fdtd_engine* h : hs) {
+    const int rc = flush_samples(h);
+    if (rc) return rc;
   }
   CUDA_TRY(cudaEventRecord(p->ev1, st));
   CUDA_TRY(cudaEventSynchronize(p->ev1));

@@ -136,6 +136,9 @@ struct StepParams {
   // Device status word: a kernel whose bounded wait ran out stores
   // FDTD_ERR_TIMEOUT here (read back by the host after stepping).
   int* status;
+  // Polling rounds of a bounded pipeline wait before it gives up and reports
+  // FDTD_ERR_TIMEOUT (fdtd_engine_set_wait_limit; the default is 1 << 20).
+  int wait_limit;
 };
 
 // A warp task needs the CPML code (some cell of its footprint lies in a slab)

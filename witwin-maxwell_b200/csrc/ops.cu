@@ -231,10 +231,10 @@ __global__ void op_aux_e_kernel(int ne, float* e, const float* h, const float* e
                                 float value) {
   const int x = blockIdx.x * blockDim.x + threadIdx.x;
   if (x >= ne) return;
-  if (x == src) {
+  if (x == ne - 1) {
+    e[x] = 0.0f;  // checked before the source cell, as the reference's op does
+  } else if (x == src) {
     e[x] = value;
-  } else if (x == ne - 1) {
-    e[x] = 0.0f;
   } else if (x >= 1) {
     e[x] = ed[x] * e[x] - ec[x] * (h[x] - h[x - 1]);
   }

@@ -44,7 +44,9 @@ constexpr int kHPad = 352;             // floats per H component tile (>= 9 x 36
 constexpr int kStageFloats = 3 * kEPad + 3 * kHPad;
 constexpr uint32_t kEBytes = kCols * kERows * 4;  // one E component box
 constexpr uint32_t kHBytes = kCols * kHRows * 4;  // one H component box
-constexpr uint32_t kSpinLimit = 1u << 20;  // try_wait rounds before a wait reports a timeout
+// try_wait rounds of the final drain (the producer waiting for its own issued
+// copies before the block exits); the pipeline waits use p.wait_limit.
+constexpr uint32_t kSpinLimit = 1u << 20;
 
 static_assert(kERows * kCols <= kEPad && kHRows * kCols <= kHPad, "tile pads too small");
 static_assert((kEPad * 4) % 128 == 0 && (kHPad * 4) % 128 == 0, "tiles must stay 128-byte aligned");
@@ -66,8 +68,8 @@ __device__ __forceinline__ void mbar_arrive(uint32_t bar) {
 }
 
 // Bounded wait for the phase of parity `parity` to complete.
-__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity) {
-  for (uint32_t it = 0; it < kSpinLimit; ++it) {
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity, uint32_t limit) {
+  for (uint32_t it = 0; it < limit; ++it) {
     uint32_t done;
     asm volatile(
         "{\n\t.reg .pred p;\n\t"
@@ -99,12 +101,13 @@ struct Ring {
   uint32_t full0;     // shared address of full[0] (8 bytes apart)
   uint32_t empty0;    // shared address of empty[0]
   int istart, i1;     // planes consumed: istart .. i1 (i1 read as the last "next" plane)
+  uint32_t limit;     // try_wait rounds of a pipeline wait (StepParams::wait_limit)
 };
 
 // Consumer side: wait until the stage of plane q has landed.
 __device__ __forceinline__ bool ring_wait_full(const Ring& r, int q) {
   const int u = q - r.istart;
-  return mbar_wait(r.full0 + 8u * (u % kStages), (u / kStages) & 1);
+  return mbar_wait(r.full0 + 8u * (u % kStages), (u / kStages) & 1, r.limit);
 }
 
 }  // namespace
@@ -399,6 +402,7 @@ __global__ void __launch_bounds__(kTmaThreads, 3) tma_step_kernel(const StepPara
   ring.empty0 = smem_addr(bars + kStages);
   ring.istart = max(i0 - 1, 0);
   ring.i1 = min(i0 + p.CX, p.NX);
+  ring.limit = static_cast<uint32_t>(p.wait_limit);
   if (threadIdx.x == 0) {
     for (int s = 0; s < kStages; ++s) {
       mbar_init(ring.full0 + 8u * s, 1);
@@ -419,7 +423,7 @@ __global__ void __launch_bounds__(kTmaThreads, 3) tma_step_kernel(const StepPara
     bool ok = true;
     for (int u = 0; u < planes && ok; ++u) {
       const int s = u % kStages, q = ring.istart + u;
-      if (u >= kStages && !mbar_wait(ring.empty0 + 8u * s, ((u / kStages) - 1) & 1)) {
+      if (u >= kStages && !mbar_wait(ring.empty0 + 8u * s, ((u / kStages) - 1) & 1, ring.limit)) {
         report_timeout(p.status);
         ok = false;
         break;
@@ -435,7 +439,7 @@ __global__ void __launch_bounds__(kTmaThreads, 3) tma_step_kernel(const StepPara
     }
     // Every issued copy has landed before the block can exit.
     for (int u = max(0, issued - kStages); u < issued; ++u) {
-      if (!mbar_wait(ring.full0 + 8u * (u % kStages), (u / kStages) & 1)) {
+      if (!mbar_wait(ring.full0 + 8u * (u % kStages), (u / kStages) & 1, kSpinLimit)) {
         report_timeout(p.status);
         break;
       }

@@ -264,6 +264,11 @@ class B200FDTD:
         """L2 prefetch distance of the scalar step kernels in x planes (0 disables)."""
         _lib.check(self.lib.fdtd_engine_set_prefetch(self.handle, int(planes)), "set_prefetch")
 
+    def set_wait_limit(self, rounds: int) -> None:
+        """Polling rounds of a bounded pipeline wait in the step kernels before it
+        reports FDTD_ERR_TIMEOUT (failure detection; 0 makes every wait run out)."""
+        _lib.check(self.lib.fdtd_engine_set_wait_limit(self.handle, int(rounds)), "set_wait_limit")
+
     def set_ade_pass(self, on: bool) -> None:
         """Advance the dispersive poles in a pass after the step kernel (True) or inside it."""
         _lib.check(self.lib.fdtd_engine_set_ade_pass(self.handle, 1 if on else 0), "set_ade_pass")
