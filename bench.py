@@ -558,7 +558,7 @@ def run_adjoint_bench(wm, device):
                     "300 THz ramped CW, |E|^2 over a 16x16 patch",
         "steps": steps,
         "design_cells": int(np.prod(eps_r.shape)),
-        "gradient_check": "tests/test_adjoint.py: exact transpose (dot-product test) and central finite differences",
+        "gradient_check": "tests/test_adjoint_golden.py: the reference's adjoint ops (golden, 1e-4); tests/test_adjoint.py: exact transpose and FP64 central differences on 16 seeded cells of the half-size layout",
     }
     cs = None
     grads = {}

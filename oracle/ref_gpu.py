@@ -305,22 +305,48 @@ class RefGpuSimulation:
 
 
 class RefGpuBloch:
-    """A complex field on x / y Bloch faces with PEC (or NONE) z faces, stepped
-    with the reference's own ops: per channel the standard H updates, ADE,
-    source patches and PEC clamps of RefGpuSimulation, and for E the
-    reference's complex Bloch kernels update_electric_ex_bloch_y_standard_z,
-    update_electric_ey_bloch_x_standard_z and update_electric_ez_bloch
-    (electric.cu:356-453, 1164-1229), as stepping.py:1118-1173 and 1790 order
-    them.  Monitors are the complex DFT A + iB of the two channels' spectra."""
+    """A complex field on x / y Bloch faces with PEC, NONE or CPML z faces,
+    stepped with the reference's own ops: per channel the H updates (standard,
+    or compressed CPML with slabs on z only), ADE, source patches and PEC
+    clamps of RefGpuSimulation, and for E the reference's complex Bloch kernels
+    update_electric_ex_bloch_y_standard_z, update_electric_ey_bloch_x_standard_z
+    and update_electric_ez_bloch (electric.cu:356-453, 1164-1229), as
+    stepping.py:1118-1173 and 1790 order them; with CPML on z the Ex / Ey
+    stretch is folded in afterwards by apply_electric_e{x,y}_cpml_z_correction
+    over each z slab of each channel (update_electric_fields_bloch_cpml,
+    stepping.py:1373-1387 and 1236-1277; the ops take contiguous copies of the
+    slab views and write them back, as the reference's launcher does,
+    cuda/backend.py:54-70).  Monitors are the complex DFT A + iB of the two
+    channels' spectra."""
 
     def __init__(self, compiled, device: str = "cuda"):
         cs = compiled
-        if cs.cpml and (any(cs.pml_lo) or any(cs.pml_hi)):
-            raise ValueError("the Bloch checker covers scenes without CPML")
+        if cs.cpml and (any(cs.pml_lo[:2]) or any(cs.pml_hi[:2])):
+            raise ValueError("the Bloch checker covers CPML on z only")
         self.cs = cs
         self.re = RefGpuSimulation(cs, device, channel=0)
         self.im = RefGpuSimulation(cs, device, channel=1)
         self.op = self.re.op
+        self.z_cpml = bool(cs.cpml and (cs.pml_lo[2] or cs.pml_hi[2]))
+
+    def _z_cpml_corrections(self, sim):
+        bnd = self.cs.boundary
+        cp, F = sim.cp, sim.F
+        for comp, h, op, modes, tangent in (("Ex", "Hy", self.op.apply_electric_ex_cpml_z_correction, (bnd[2], bnd[3]), 1),
+                                            ("Ey", "Hx", self.op.apply_electric_ey_cpml_z_correction, (bnd[0], bnd[1]), 0)):
+            low, hstart, high = sim.slab[(comp, 1)]
+            psi = sim.psi[(comp, 1)]
+            for local, start, length in ((0, 0, low), (low, hstart, high)):
+                if length <= 0:
+                    continue
+                view = F[comp].narrow(2, start, length)
+                pview = psi.narrow(2, local, length)
+                field, psi_c = view.contiguous(), pview.contiguous()
+                curl = sim.curl[comp].narrow(2, start, length).contiguous()
+                op(field, F[h], curl, psi_c, cp["ik_e"][2], cp["b_e"][2], cp["c_e"][2], sim.inv_e[2], 0, 0, start,
+                   int(modes[0]), int(modes[1]), int(F[comp].shape[tangent]), int(F[comp].shape[2]))
+                view.copy_(field)
+                pview.copy_(psi_c)
 
     def _update_e(self):
         cs, R, I = self.cs, self.re.F, self.im.F
@@ -336,6 +362,9 @@ class RefGpuBloch:
         self.op.update_electric_ez_bloch(
             R["Ez"], I["Ez"], R["Hx"], I["Hx"], R["Hy"], I["Hy"], self.re.decay["Ez"], self.re.curl["Ez"],
             float(c[0]), float(s[0]), float(c[1]), float(s[1]), inv[0], inv[1])
+        if self.z_cpml:
+            self._z_cpml_corrections(self.re)
+            self._z_cpml_corrections(self.im)
 
     def step_once(self):
         re, im = self.re, self.im

@@ -18,6 +18,7 @@ import pytest
 import torch
 
 from conftest import load_package
+from oracle import oracle as orc
 
 pytestmark = pytest.mark.gpu
 FIELDS = ("Ex", "Ey", "Ez", "Hx", "Hy", "Hz")
@@ -211,3 +212,53 @@ def test_adjoint_rejects_designs_on_ade_cells_and_edges():
     bad = (ctypes.c_int * 18)(*([1, 5, 3, 6, 3, 6] + [0] * 12))  # reaches into the CPML slab
     assert lib.fdtd_engine_adjoint_init(solver.handle, bad, 4) == -1
     solver.close()
+
+
+def test_design_workload_gradient_against_fp64_finite_differences():
+    """The 160x160x96 design workload's layout at half size (80x80x48 cells,
+    10-cell CPML, eps 2.1 substrate, 32x32x8 design block with eps_r ~ U[1, 12)
+    seed 0, ramped 300 THz CW source, 8x8 patch objective), 400 steps, the
+    reverse pass replaying checkpoints every 100 steps: dL/deps_r of 16 design
+    cells drawn with numpy.random.default_rng(0) against central differences
+    (h = 1e-3 on eps_r) of L = sum |E|^2 over the patch computed by the FP64
+    oracle (FP32 forward runs are too noisy at this h: a single cell moves L by
+    about 1e-6 of itself).  The scene's coefficients are FP32, which limits the
+    differences to about 1e-4 relative; tolerance 2e-3 of the largest checked
+    gradient."""
+    wm = load_package()
+    adj = wm.adjoint
+    steps = 400
+    scene = wm.workloads.adjoint_160(steps, scale=2)
+    eps_r = scene.material_regions[0].eps_r
+    problem = adj.DesignProblem(scene, steps, stride=100, history="replay")
+    mons = problem.forward(eps_r)
+    g = problem.backward({"patch": {c: 2.0 * v for c, v in mons["patch"].items()}})
+    problem.close()
+    rng = np.random.default_rng(0)
+    picks = rng.choice(eps_r.size, size=16, replace=False)
+    h = 1e-3
+
+    def loss(e):
+        sc = wm.workloads.adjoint_160(steps, scale=2)
+        region = sc.material_regions[0]
+        sc.material_regions[0] = wm.MaterialRegion(region.lo, region.hi, e)
+        cs = wm.compile_scene(sc, steps)
+        sim = orc.OracleSimulation(cs, "f64").run(steps)
+        m = sim.monitor_results()
+        sim.close()
+        return float(sum(np.sum(np.abs(v) ** 2) for v in m["patch"].values()))
+
+    fds, gs = [], []
+    for flat in picks:
+        idx = np.unravel_index(flat, eps_r.shape)
+        vals = []
+        for sgn in (1.0, -1.0):
+            e = eps_r.copy()
+            e[idx] += sgn * h
+            vals.append(loss(e))
+        fds.append((vals[0] - vals[1]) / (2 * h))
+        gs.append(g[idx])
+    fds, gs = np.array(fds), np.array(gs)
+    scale = np.abs(fds).max()
+    assert scale > 0
+    np.testing.assert_allclose(gs, fds, rtol=0, atol=2e-3 * scale)

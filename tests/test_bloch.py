@@ -115,6 +115,36 @@ def test_bloch_matches_reference_bloch_kernels():
         assert joint(mons[m], refm[m]) < TOL, m
 
 
+def test_bloch_grating_shape_with_z_cpml_matches_reference_kernels():
+    """The large grating's boundary set on a small copy: Bloch x / y faces
+    (k_x = 0.1 * 2 pi / L_x), 8-cell CPML on z only, the Debye grating layer
+    and the phased current sheet (64 x 64 x 48 cells, 4 frequencies, 300
+    steps), against the reference's Bloch-xy / standard-z E kernels followed by
+    its z-CPML corrections of Ex and Ey on both channels."""
+    wm = load_package()
+    steps = 300
+    cs = wm.compile_scene(wm.workloads.bloch_grating(cells=(64, 64, 48), pml=8, n_freq=4), steps)
+    assert cs.complex_fields and cs.pml_lo[2] == 8 and cs.pml_lo[0] == 0
+    assert {p.kind for p in cs.poles} == {0}
+    solver = wm.solver.B200FDTD(cs).init_field()
+    solver.step_range(0, steps)
+    got_re = {n: solver.field(n).cpu().numpy() for n in FIELDS}
+    got_im = {n: solver.field(n, imag=True).cpu().numpy() for n in FIELDS}
+    mons = {k: {c: v.cpu().numpy() for c, v in d.items()} for k, d in solver.monitor_results().items()}
+    solver.close()
+    ref = ref_gpu.RefGpuBloch(cs)
+    assert ref.z_cpml
+    ref.run(steps)
+    ref_re, ref_im = ref.fields()
+    got = {**{f"re_{n}": got_re[n] for n in FIELDS}, **{f"im_{n}": got_im[n] for n in FIELDS}}
+    want = {**{f"re_{n}": ref_re[n] for n in FIELDS}, **{f"im_{n}": ref_im[n] for n in FIELDS}}
+    assert np.linalg.norm(want["re_Ex"]) > 0 and np.linalg.norm(want["im_Ex"]) > 1e-3 * np.linalg.norm(want["re_Ex"])
+    assert joint(got, want) < TOL
+    refm = ref.monitor_results()
+    for m in refm:
+        assert joint(mons[m], refm[m]) < TOL, m
+
+
 def test_bloch_at_zero_wavevector_is_periodic():
     """k = 0: the Bloch pair's real channel equals the periodic engine and the
     imaginary channel stays zero (a real source)."""

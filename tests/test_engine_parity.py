@@ -143,6 +143,34 @@ def test_engine_dispersive_tfsf_against_fp64_oracle():
     solver.close()
 
 
+def test_batched_design_scene_against_fp64_oracle():
+    """One scene of the batched design workload as generated (seed 1): the
+    smallest of the 32, diagonal anisotropic eps boxes (a different
+    coefficient array per E component), 8-cell CPML, Ez dipole, 8-frequency
+    point monitor; 600 steps of the FP32 engine against the FP32 and FP64
+    oracles."""
+    wm = load_package()
+    steps = 600
+    scenes = wm.workloads.batched_designs()
+    sc = min(scenes, key=lambda s: int(np.prod(s.cells)))
+    assert any(st.medium.eps_diag is not None and len(set(st.medium.eps_diag)) == 3 for st in sc.structures)
+    cs = wm.compile_scene(sc, steps)
+    curls = [cs.curl[n] for n in ("Ex", "Ey", "Ez")]
+    assert all(c is not None for c in curls) and not np.array_equal(curls[0][:-1, :-1, :-1], curls[1][:-1, :-1, :-1])
+    solver, fields, mons = _run_engine(cs, steps)
+    ref32 = orc.OracleSimulation(cs, "f32").run(steps)
+    ref64 = orc.OracleSimulation(cs, "f64").run(steps)
+    assert_fields_close(fields, ref32.fields)
+    assert joint_rel_l2(fields, ref64.fields) < 2.0 * joint_rel_l2(ref32.fields, ref64.fields) + 1e-7
+    assert_monitors_close(mons, ref32.monitor_results())
+    m64 = ref64.monitor_results()
+    for name in m64:
+        assert joint_rel_l2(mons[name], m64[name]) < TOL, name
+    ref32.close()
+    ref64.close()
+    solver.close()
+
+
 @pytest.mark.parametrize(
     "tiles",
     [

@@ -60,6 +60,27 @@ def test_dispersive_tfsf_matches_reference_kernels():
     _compare(cs, 300)
 
 
+def test_dispersive_full_size_matches_reference_kernels():
+    """The dispersive workload at its full 256^3 size (12-cell CPML, Lorentz
+    sphere, Drude slab, TFSF plane wave, 16-frequency flux planes and box),
+    200 steps, against the reference's kernels on the same tensors."""
+    wm = load_package()
+    cs = wm.compile_scene(wm.workloads.dispersive_256(), 200)
+    assert cs.nodes == (257, 257, 257) and len(cs.frequencies) == 16
+    _compare(cs, 200)
+
+
+def test_reference_observer_ops_match_float64_accumulation():
+    """The reference-timing mode of the checker (its own FP32 observer kernels
+    per region and frequency) against the float64 accumulation the parity tests
+    use, on the 40^3 scene: relative L2 <= 1e-5 per monitor."""
+    wm = load_package()
+    cs = wm.compile_scene(_c1_scene(wm, cells=40, pml=6), 120)
+    a = ref_gpu.RefGpuSimulation(cs).run(120).monitor_results()
+    b = ref_gpu.RefGpuSimulation(cs, monitor_ops=True).run(120).monitor_results()
+    assert_monitors_close(b, a)
+
+
 def test_small_scene_matches_reference_kernels():
     wm = load_package()
     cs = wm.compile_scene(_c1_scene(wm, cells=40, pml=6), 200)

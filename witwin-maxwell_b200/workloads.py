@@ -73,23 +73,30 @@ def dispersive_256(cells: int = 256, pml: int = 12, n_freq: int = 16, slab_throu
     return sc
 
 
-def adjoint_160(steps: int = 3000, seed: int = 0) -> Scene:
+def adjoint_160(steps: int = 3000, seed: int = 0, scale: int = 1) -> Scene:
     """Adjoint-gradient workload: 160x160x96 cells, 10-cell CPML; eps 2.1 substrate for
     z < 40; a 64x64x16 MaterialRegion design block at x, y in [48, 112), z in [40, 56)
     with eps_r ~ U[1, 12) i.i.d. (torch.Generator().manual_seed(seed)); an Ey source at
     300 THz, CW after a 200-step raised-cosine ramp (sampled table); the objective's
     monitor is the 16x16 patch of E on the plane z = 80 at 300 THz.  A point dipole below
-    the design block stands in for the reference's Gaussian beam (not built here)."""
+    the design block stands in for the reference's Gaussian beam (not built here).
+    ``scale`` > 1 divides every length but the 10-cell CPML by it (the same layout on a
+    smaller grid, for checks that cannot afford the full size)."""
     import torch
 
-    sc = Scene(cells=(160, 160, 96), spacing=SPACING, pml_cells=10)
-    sc.structures.append(Structure(Box((0, 0, 0), (160, 160, 39)), Medium(eps_r=2.1)))
+    def s_(v):
+        return int(v) // scale
+
+    sc = Scene(cells=(s_(160), s_(160), s_(96)), spacing=SPACING, pml_cells=10)
+    sc.structures.append(Structure(Box((0, 0, 0), (s_(160), s_(160), s_(40) - 1)), Medium(eps_r=2.1)))
     gen = torch.Generator().manual_seed(seed)
-    eps_r = (1.0 + 11.0 * torch.rand((64, 64, 16), generator=gen, dtype=torch.float64)).numpy()
-    sc.material_regions.append(MaterialRegion((48, 48, 40), (112, 112, 56), eps_r))
+    shape = (s_(64), s_(64), s_(16))
+    eps_r = (1.0 + 11.0 * torch.rand(shape, generator=gen, dtype=torch.float64)).numpy()
+    sc.material_regions.append(MaterialRegion((s_(48), s_(48), s_(40)), (s_(112), s_(112), s_(56)), eps_r))
     dt = sc.resolve_dt()
-    sc.sources.append(PointDipole((80, 80, 30), "Ey", ramped_cw(300e12, 200, dt, steps), width=SPACING))
-    sc.monitors.append(PlaneMonitor("patch", 2, 80, ("Ex", "Ey", "Ez"), (300e12,), (72, 72), (87, 87)))
+    sc.sources.append(PointDipole((s_(80), s_(80), s_(30)), "Ey", ramped_cw(300e12, 200, dt, steps), width=SPACING))
+    sc.monitors.append(PlaneMonitor("patch", 2, s_(80), ("Ex", "Ey", "Ez"), (300e12,), (s_(72), s_(72)),
+                                    (s_(72) + 16 // scale - 1, s_(72) + 16 // scale - 1)))
     return sc
 
 
