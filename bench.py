@@ -281,7 +281,7 @@ def run_reference_arm(args, wm, world, rank):
     }
     if args.reference_gpu:
         try:
-            line["reference_gpu"] = reference_gpu_bar(wm, run["compiled"])
+            line["reference_gpu"] = reference_gpu_bar(wm, wm.compile_scene(wm.workloads.dispersive_256(), 64))
         except Exception as exc:  # reported beside the CPU value, never fatal
             line["reference_gpu"] = {"unavailable": f"{type(exc).__name__}: {exc}"}
     return line

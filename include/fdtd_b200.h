@@ -179,13 +179,20 @@ int fdtd_engine_checkpoint_load(fdtd_engine* h, int slot);
 int fdtd_engine_autotune(fdtd_engine* h, int* tile_rows, int* chunk_planes);
 /* Launch configuration of the fused step kernel.  Variants 1-3: the scalar
  * warp kernel (one z cell per lane) with a register budget of about 100 (1),
- * 64 (2, the default: four 256-thread CTAs per SM) or 85 (3) per thread;
- * 4: the same warp decomposition fed by TMA plane tiles; 5-9: the z-vectorised
- * warp kernel (5: four cells per lane, 6: two cells per lane, direct loads;
- * 7 / 8: two cells per lane fed by a 4- / 3-plane cp.async ring; 9: four cells
- * per lane, 3-plane ring).  chunk_planes is the number of x planes each warp
- * marches through (0 picks the variant's default).  tile_rows is accepted
- * for compatibility and ignored. */
+ * 64 (2: four 256-thread CTAs per SM) or 85 (3) per thread; 4: the same warp
+ * decomposition fed by TMA plane tiles; 5-9: the z-vectorised warp kernel (5:
+ * four cells per lane, 6: two cells per lane, direct loads; 7 / 8: two cells
+ * per lane fed by a 4- / 3-plane cp.async ring; 9: four cells per lane, 3-plane
+ * ring); 10: the row-tile kernel (a TMA-fed ring of plane tiles, eight row
+ * warps and a halo warp per CTA sharing y-neighbour rows through shared
+ * memory; with CPML in the scene the CTAs that meet a slab run in the warp
+ * kernel of variant 2 after it; poles run in the ADE pass, and variant 2 runs
+ * in its place where that pass cannot take them).  Default: 10 for FP32
+ * engines without CPML, periodic or Bloch faces, 2 otherwise; reduced storage
+ * runs 2 only.
+ * chunk_planes is the number of x planes each warp marches through (0 picks
+ * the variant's default).  tile_rows is accepted for compatibility and
+ * ignored. */
 int fdtd_engine_set_launch(fdtd_engine* h, int variant, int tile_rows, int chunk_planes);
 int fdtd_engine_get_launch(fdtd_engine* h, int* variant, int* tile_rows, int* chunk_planes);
 /* Where the Debye / Drude / Lorentz poles advance: on (1, the default) in a

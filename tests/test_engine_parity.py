@@ -176,7 +176,7 @@ def test_batched_design_scene_against_fp64_oracle():
     [
         (1, 1, 8), (3, 1, 5), (2, 1, 64), (2, 1, 13), (4, 1, 8), (4, 1, 3), (4, 1, 41),
         (5, 1, 8), (5, 1, 13), (6, 1, 8), (6, 1, 41), (7, 1, 8), (7, 1, 3), (7, 1, 41), (8, 1, 13), (9, 1, 8),
-        (9, 1, 41),
+        (9, 1, 41), (10, 1, 8), (10, 1, 3), (10, 1, 41), (10, 1, 1), (10, 1, 2),
     ],
 )
 def test_tile_shape_does_not_change_results(tiles):
@@ -189,7 +189,7 @@ def test_tile_shape_does_not_change_results(tiles):
     wm = load_package()
     steps = 50
     cs = wm.compile_scene(_c1_scene(wm, cells=40, pml=6), steps)
-    family = (lambda v: v >= 5)
+    family = (lambda v: 5 <= v <= 9)
     base_variant = 7 if family(tiles[0]) else 2  # one member of the tile's family
     solver = wm.solver.B200FDTD(cs).init_field()
     solver.set_launch(base_variant, 1, 32)
@@ -200,28 +200,37 @@ def test_tile_shape_does_not_change_results(tiles):
     solver.set_launch(*tiles)
     assert solver.get_launch() == (tiles[0], 1, tiles[2])
     solver.step_range(0, steps)
+    scale = max(float(np.abs(v).max()) for v in base.values())
     for n in FIELDS:
-        np.testing.assert_array_equal(solver.field(n).cpu().numpy(), base[n])
+        got = solver.field(n).cpu().numpy()
+        if tiles[0] == 10:
+            # the row-tile kernel: same arithmetic, the compiler's own choice of
+            # fused multiply-adds, so agreement to FP32 rounding of the field scale
+            np.testing.assert_allclose(got, base[n], rtol=0, atol=1e-6 * scale)
+        else:
+            np.testing.assert_array_equal(got, base[n])
     solver.close()
 
 
 def test_kernel_families_agree():
-    """The scalar warp kernel and the z-vectorised ring kernel give the same
-    fields after 200 steps of a CPML + dielectric scene: relative L2 within
-    1e-5 per component (the engine's parity bar against the FP32 oracle)."""
+    """The scalar warp kernel, the z-vectorised ring kernel and the row-tile
+    kernel give the same fields after 200 steps of a CPML + dielectric scene:
+    relative L2 within 1e-5 per component (the engine's parity bar against the
+    FP32 oracle)."""
     wm = load_package()
     steps = 200
     cs = wm.compile_scene(_c1_scene(wm, cells=40, pml=6), steps)
     out = []
-    for variant in (2, 7):
+    for variant in (2, 7, 10):
         solver = wm.solver.B200FDTD(cs).init_field()
         solver.set_launch(variant, 1, 0)
         solver.step_range(0, steps)
         out.append({n: solver.field(n).cpu().numpy() for n in FIELDS})
         solver.close()
-    for n in FIELDS:
-        a, b = out[1][n].astype(np.float64), out[0][n].astype(np.float64)
-        assert np.linalg.norm(a - b) <= 1e-5 * np.linalg.norm(b), n
+    for other in out[1:]:
+        for n in FIELDS:
+            a, b = other[n].astype(np.float64), out[0][n].astype(np.float64)
+            assert np.linalg.norm(a - b) <= 1e-5 * np.linalg.norm(b), n
 
 
 def test_ade_pass_matches_poles_in_step_kernel():

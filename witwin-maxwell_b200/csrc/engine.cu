@@ -29,6 +29,9 @@ __global__ void warp_step_kernel(const StepParams p, int n, int slot);
 int launch_classify_vec(const StepParams& p, int V, int n_kblocks, int n_chunks, unsigned char* out,
                         cudaStream_t stream);
 int launch_step_reduced(const StepParams& p, int n, dim3 grid, bool cpml, bool coef, bool uni, cudaStream_t stream);
+int launch_tile_step(const StepParams& p, const TmaMaps& maps, int n, dim3 grid, bool cpml, bool coef, bool uni,
+                     cudaStream_t stream);
+int tile_block_threads();
 using VecLauncher = int (*)(const StepParams&, int, dim3, bool, bool, bool, cudaStream_t);
 int launch_vec_v4(const StepParams&, int, dim3, bool, bool, bool, cudaStream_t);
 int launch_vec_v2(const StepParams&, int, dim3, bool, bool, bool, cudaStream_t);
@@ -313,7 +316,11 @@ constexpr int kDefaultVariant = 2;
 // prefetch into L2 (0 disables).
 constexpr int kDefaultPrefetch = 2;
 
-constexpr int kMaxVariant = 9;
+constexpr int kMaxVariant = 10;
+// The row-tile kernel (tile_kernel.cu): the default launch of FP32 engines
+// without wrapped faces.
+constexpr int kTileVariant = 10;
+constexpr int kTileMaxChunk = 63;  // planes per chunk of the row-tile kernel (chunk + halo plane <= 64)
 
 // z cells per lane of a launch variant (1 for the scalar kernels 1-4).
 int variant_v(int variant) {
@@ -398,7 +405,8 @@ struct fdtd_engine {
   int TY = 0, CX = 0;
   // Fused kernel: 1..3 = register-prefetch warp kernel with a register budget
   // of up to 128 / 64 / 85 per thread; 4 = TMA-fed kernel; 5..9 = z-vectorised
-  // warp kernels (vec_launcher).
+  // warp kernels (vec_launcher); 10 = row-tile kernel (shared-memory row
+  // exchange, tile_kernel.cu).
   int variant = kDefaultVariant;
   int pf_dist = kDefaultPrefetch;
   int cur = 0;  // index of the buffer holding the current state
@@ -660,6 +668,15 @@ void default_tiles(fdtd_engine* h) {
     const int64_t want_chunks = std::max<int64_t>(1, (148 * per_sm * 6 + cols - 1) / cols);
     CX = static_cast<int>(std::max<int64_t>(8, (h->NX + want_chunks - 1) / want_chunks));
   }
+  if (CX <= 0 && h->variant == kTileVariant) {
+    // Row-tile kernel (three 320-thread CTAs per SM): about thirteen waves of
+    // CTAs; 12-13 plane chunks measured fastest at 256^3 (chunks of 29 planes
+    // were 8 % slower: fewer CTAs to fill the last waves), so chunks stay short
+    // down to 12 planes.
+    const int64_t cols = static_cast<int64_t>((h->NY + kWarpRows - 1) / kWarpRows) * ((h->NZ + kWarpOut - 1) / kWarpOut);
+    const int64_t want_chunks = std::max<int64_t>(1, (148 * 3 * 13 + cols - 1) / cols);
+    CX = static_cast<int>(std::min<int64_t>(kTileMaxChunk, std::max<int64_t>(12, (h->NX + want_chunks - 1) / want_chunks)));
+  }
   if (CX <= 0) {
     // Split x into chunks until the grid holds about ten waves of the
     // 64-register variant (four 256-thread CTAs per SM on 148 SMs).  Shorter
@@ -716,7 +733,15 @@ int ensure_classified(fdtd_engine* h, const StepParams& p) {
 // on FP32 storage with the scalar step kernels and no wrapped face.
 bool ade_pass_active(const fdtd_engine* h) {
   return h->ade_pass && h->n_ade_tiles > 0 && h->poles.size() <= static_cast<size_t>(kAdeMaxPoles) &&
-         h->storage == kStoreF32 && !h->wrap && h->variant >= 1 && h->variant <= 3;
+         h->storage == kStoreF32 && !h->wrap && ((h->variant >= 1 && h->variant <= 3) || h->variant == kTileVariant);
+}
+
+// The row-tile kernel has no pole code: with poles that the ADE pass cannot
+// take (more than its table holds, or the pass switched off) the 64-register
+// warp kernel runs instead.
+bool tile_runs(const fdtd_engine* h) {
+  return h->variant == kTileVariant && h->storage == kStoreF32 && !h->wrap && h->tma_ready &&
+         (h->poles.empty() || ade_pass_active(h));
 }
 
 int launch_step(fdtd_engine* h, int n, int slot) {
@@ -742,6 +767,27 @@ int launch_step(fdtd_engine* h, int n, int slot) {
   if (h->storage != kStoreF32) {
     const int err = launch_step_reduced(p, n, grid, h->cpml, coef, h->uniform_grid, h->stream);
     if (err != 0) return cuda_fail(static_cast<cudaError_t>(err), "warp_step_kernel_rs launch");
+  } else if (tile_runs(h)) {
+    // the row-tile kernel, then (scenes with CPML) the warp kernel over the
+    // CTAs that meet a slab, which the row-tile kernel leaves alone
+    const int err = launch_tile_step(p, h->maps[h->cur], n, grid, h->cpml, coef, h->uniform_grid, h->stream);
+    if (err != 0) return cuda_fail(static_cast<cudaError_t>(err), "tile_step_kernel launch");
+    if (h->cpml) {
+      ++h->launches;
+      StepParams q = p;
+      q.shell_only = 1;
+#define FDTD_SHELL(COEF, UNI) warp_step_kernel<true, COEF, UNI, 4, false><<<grid, block, 0, h->stream>>>(q, n, slot)
+      if (h->uniform_grid) {
+        if (coef) FDTD_SHELL(true, true);
+        else FDTD_SHELL(false, true);
+      } else {
+        if (coef) FDTD_SHELL(true, false);
+        else FDTD_SHELL(false, false);
+      }
+#undef FDTD_SHELL
+      const cudaError_t e2 = cudaGetLastError();
+      if (e2 != cudaSuccess) return cuda_fail(e2, "warp_step_kernel (CPML shell) launch");
+    }
   } else if (VecLauncher vl = vec_launcher(h->variant)) {
     const int err = vl(p, n, grid, h->cpml, coef, h->uniform_grid, h->stream);
     if (err != 0) return cuda_fail(static_cast<cudaError_t>(err), "vec_step_kernel launch");
@@ -750,8 +796,8 @@ int launch_step(fdtd_engine* h, int n, int slot) {
   do {                                                                                           \
     if (h->variant == 4)                                                                          \
       tma_step_kernel<CPML, COEF, UNI><<<grid, kTmaThreads, tma_smem_bytes(), h->stream>>>(p, h->maps[h->cur], n); \
-    else if (h->variant == 2 && ade_pass) warp_step_kernel<CPML, COEF, UNI, 4, false><<<grid, block, 0, h->stream>>>(p, n, slot); \
-    else if (h->variant == 2) warp_step_kernel<CPML, COEF, UNI, 4, true><<<grid, block, 0, h->stream>>>(p, n, slot); \
+    else if ((h->variant == 2 || h->variant == kTileVariant) && ade_pass) warp_step_kernel<CPML, COEF, UNI, 4, false><<<grid, block, 0, h->stream>>>(p, n, slot); \
+    else if (h->variant == 2 || h->variant == kTileVariant) warp_step_kernel<CPML, COEF, UNI, 4, true><<<grid, block, 0, h->stream>>>(p, n, slot); \
     else if (h->variant == 3 && ade_pass) warp_step_kernel<CPML, COEF, UNI, 3, false><<<grid, block, 0, h->stream>>>(p, n, slot); \
     else if (h->variant == 3) warp_step_kernel<CPML, COEF, UNI, 3, true><<<grid, block, 0, h->stream>>>(p, n, slot); \
     else warp_step_kernel<CPML, COEF, UNI, 1, true><<<grid, block, 0, h->stream>>>(p, n, slot);            \
@@ -1040,6 +1086,12 @@ int fdtd_engine_create(const fdtd_grid_desc* desc, void* stream, fdtd_engine** o
     fdtd_engine_destroy(h);
     return rc;
   }
+  // The row-tile kernel is the default where it measured fastest: FP32 scenes
+  // without CPML or wrapped faces (256^3 vacuum: 0.201 against 0.253 ms).  With
+  // CPML the slab CTAs run in the warp kernel either way and the hybrid launch
+  // measured no faster (CPML vacuum 0.389 against 0.393 ms, the dispersive
+  // workload 0.520 against 0.509 ms), so those engines keep variant 2.
+  if (!h->wrap && !h->cpml) h->variant = kTileVariant;
   default_tiles(h);
   *out = h;
   return 0;
@@ -2047,6 +2099,8 @@ int fdtd_engine_set_launch(fdtd_engine* h, int variant, int tile_rows, int chunk
   h->variant = variant;
   if (chunk_planes > 0) h->CX = chunk_planes;
   else default_tiles(h);
+  // the row-tile kernel gathers its chunk's plane bits into 64-bit masks
+  if (variant == kTileVariant) h->CX = std::min(h->CX, kTileMaxChunk);
   return 0;
 }
 
@@ -2323,7 +2377,7 @@ int fdtd_engine_info(fdtd_engine* h, int* tile_rows, int* chunk_planes, int* gri
   const dim3 g = step_grid(h);
   if (grid_x) *grid_x = static_cast<int>(g.x);
   if (grid_y) *grid_y = static_cast<int>(g.y * g.z);
-  if (block) *block = kWarpRows * 32;
+  if (block) *block = tile_runs(h) ? tile_block_threads() : kWarpRows * 32;
   if (launches) *launches = h->launches;
   return 0;
 }
@@ -2528,9 +2582,9 @@ int fdtd_batch_step_range(fdtd_batch* b, int n0, int n1) {
   }
   CUDA_TRY(cudaEventRecord(b->ev0, b->stream));
   // Monitor samples are flushed into the DFT sums in the same groups as
-  // fdtd_engine_step_range would (a partial block stays pending across calls),
+  // fdtd_engine_step_range would (every 32 steps and at the end of the range),
   // so a batch gives the spectra of the engines stepped one by one.  Samples
-  // that do not continue at n0, or engines whose pending counts differ, are
+  // left pending by other calls, or engines whose pending counts differ, are
   // flushed first.
   bool aligned = true;
   for (fdtd_engine* h : b->eng) {
@@ -2585,8 +2639,13 @@ int fdtd_batch_step_range(fdtd_batch* b, int n0, int n1) {
     for (fdtd_engine* h : b->eng) h->pending_base = n;
   }
   {
-    // tail steps (fewer than a block) run as direct launches; their samples stay pending
+    // tail steps (fewer than a block) run as direct launches
     const int rc = direct(n, n1);
+    if (rc) return rc;
+  }
+  // as fdtd_engine_step_range: the DFT of every step of the range lands inside it
+  for (fdtd_engine* h : b->eng) {
+    const int rc = flush_samples(h);
     if (rc) return rc;
   }
   CUDA_TRY(cudaEventRecord(b->ev1, b->stream));

@@ -139,6 +139,10 @@ struct StepParams {
   // Polling rounds of a bounded pipeline wait before it gives up and reports
   // FDTD_ERR_TIMEOUT (fdtd_engine_set_wait_limit; the default is 1 << 20).
   int wait_limit;
+  // Warp kernel only: run just the CTAs (8 rows, one z block, one x chunk)
+  // in which some warp task has the CPML class; the row-tile kernel runs the
+  // others (launch variant 10 on scenes with CPML).
+  int shell_only;
 };
 
 // A warp task needs the CPML code (some cell of its footprint lies in a slab)

@@ -356,10 +356,13 @@ __global__ void __launch_bounds__(256, kMinBlocks) warp_step_kernel(const StepPa
   if (p.step_base) n += __ldg(p.step_base);
   const int lane = threadIdx.x & 31;
   const int j = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
-  if (j >= p.NY) return;  // whole warp; this kernel has no block-level barrier
   unsigned cls = 0;
-  if (kAnyCpml || kAnyCoef)
+  if ((kAnyCpml || kAnyCoef) && j < p.NY)
     cls = __ldg(p.warp_class + (static_cast<int64_t>(blockIdx.z) * gridDim.y + blockIdx.y) * p.NY + j);
+  // shell_only: the CTAs without a CPML warp belong to the row-tile kernel
+  // (its CTAs cover the same rows, z block and chunk)
+  if (kAnyCpml && p.shell_only && !__syncthreads_or(cls & kClassCpml)) return;
+  if (j >= p.NY) return;  // whole warp; no block-level barrier follows
   if (kAnyCpml && (cls & kClassCpml)) {
     if (kAnyCoef && (cls & kClassCoef)) march<float, true, true, kUniform, false, kAde>(p, n, lane, j);
     else march<float, true, false, kUniform, false, kAde>(p, n, lane, j);
