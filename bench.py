@@ -369,7 +369,9 @@ def run_b200_arm(args, wm, world, rank, local):
         },
         "roofline": {
             "bound": "hbm",
-            "kernel": "step kernels: warp_step_kernel + ade_pass_kernel (one step)",
+            "kernel": ("step kernels: tile_step_kernel (+ warp_step_kernel on the CTAs that meet a CPML slab) "
+                       "+ ade_pass_kernel (one step)") if info1["variant"] == 10 else
+                      "step kernels: warp_step_kernel + ade_pass_kernel (one step)",
             "achieved": achieved,
             "peak": peaks["hbm_gbs"],
             "unit": "GB/s",
@@ -398,6 +400,8 @@ def run_b200_arm(args, wm, world, rank, local):
         result["e2e"] = run_e2e(args, wm, cs, device, world)
     if args.reduced:
         result["reduced_storage"] = run_reduced_bench(args, wm, cs, device, kernel_ms, elapsed_s * 1e3 / args.steps)
+    if args.vacuum:
+        result["vacuum_kernels"] = run_vacuum_kernels(wm, device)
     if args.batched:
         result["batched"] = run_batched_bench(wm, device)
     if args.grating:
@@ -467,6 +471,35 @@ def run_reduced_bench(args, wm, cs, device, fp32_kernel_ms, fp32_step_ms):
         out[st]["monitor_rel_l2_vs_fp32"] = {m: float(f"{e:.3e}") for m, e in errs.items()}
         out[st]["max_monitor_rel_l2_vs_fp32"] = max(errs.values())
         out[st]["algorithmic_bytes_per_cell_update"] = round(wm.workloads.algorithmic_bytes(cs, storage_bytes=2)["step_kernel"], 3)
+    return out
+
+
+def run_vacuum_kernels(wm, device, cells: int = 256):
+    """The step kernels on a CPML-free scene (cells^3 vacuum, PEC faces, Ez
+    dipole): the row-tile kernel (launch variant 10, the default of such
+    engines) against the warp kernel (variant 2), device time of one launch
+    (CUDA events over 10 back-to-back launches, best of 3), with the HBM
+    fraction of the 48 B/cell field traffic."""
+    import torch
+
+    sc = wm.Scene(cells=(cells,) * 3, spacing=25e-9, pml_cells=0, boundary=(4,) * 6)
+    sc.sources.append(wm.PointDipole((cells // 2,) * 3, "Ez", wm.GaussianPulse(300e12, 100e12), width=25e-9))
+    cs = wm.compile_scene(sc, 64)
+    peak = measured_peaks()["hbm_gbs"]
+    bytes_cell = wm.workloads.algorithmic_bytes(cs)["step_kernel"]
+    out = {"workload": f"vacuum_{cells}: {cells}^3 cells, PEC faces, Ez dipole", "bytes_per_cell_update": bytes_cell}
+    for variant in (10, 2):
+        s = wm.solver.B200FDTD(cs, device=device).init_field()
+        s.set_launch(variant, 1, 0)
+        s.step_range(0, 8)
+        ms = min(s.time_kernel(8, 10) for _ in range(3))
+        info = s.info()
+        s.close()
+        torch.cuda.empty_cache()
+        gbs = bytes_cell * cs.cells / (ms * 1e-3) / 1e9
+        out[f"variant_{variant}"] = {"kernel_ms": ms, "chunk_planes": info["chunk_planes"], "achieved_gbs": gbs,
+                                     "frac": gbs / peak}
+    out["speedup_tile_over_warp"] = out["variant_2"]["kernel_ms"] / out["variant_10"]["kernel_ms"]
     return out
 
 
@@ -653,6 +686,8 @@ def main():
     ap.add_argument("--no-e2e", dest="e2e", action="store_false")
     ap.add_argument("--no-reduced", dest="reduced", action="store_false",
                     help="skip the FP16 / BF16 field-storage timing and error")
+    ap.add_argument("--no-vacuum", dest="vacuum", action="store_false",
+                    help="skip the row-tile against warp kernel timing on a 256^3 vacuum scene")
     ap.add_argument("--no-batched", dest="batched", action="store_false",
                     help="skip the 32-scene batched design workload")
     ap.add_argument("--no-grating", dest="grating", action="store_false",
