@@ -294,6 +294,17 @@ int fdtd_engine_step_range_recorded(fdtd_engine* h, int n0, int n1);
 /* Reverse steps n1-1 down to n0; with design boxes the last replay must cover
  * [n0, n1). */
 int fdtd_engine_adjoint_range(fdtd_engine* h, int n1, int n0);
+/* The whole reverse pass of an n_steps forward run that saved checkpoint slot s
+ * at step s * stride (fdtd_engine_checkpoint_save before stepping segment s;
+ * stride <= max_segment): for each segment from the last to the first, replay
+ * it from its checkpoint (recording the design-box E history) and run its
+ * reverse steps.  The reverse of segment s runs on a second stream while the
+ * engine stream replays segment s - 1 (double-buffered histories), so the two
+ * latency-bound passes overlap; the call returns when both are done.  The
+ * result equals fdtd_engine_replay_range + fdtd_engine_adjoint_range per
+ * segment (the reference's segment replay, witwin/maxwell/fdtd/adjoint/
+ * core.py:3527-3565, with its checkpoints, checkpoint.py:365-568). */
+int fdtd_engine_backward_replay(fdtd_engine* h, int n_steps, int stride);
 /* Accumulated dL/deps (absolute permittivity) of the design box of E
  * component comp (0..2), box-dense [i][j][k]. */
 int fdtd_engine_adjoint_grad(fdtd_engine* h, int comp, float* out);

@@ -176,11 +176,8 @@ class DesignProblem:
         if self.stored:
             _lib.check(lib.fdtd_engine_adjoint_range(h, self.steps, 0), "adjoint_range")
         else:
-            for s0 in reversed(range(0, self.steps, self.stride)):
-                s1 = min(s0 + self.stride, self.steps)
-                solver.checkpoint_load(s0 // self.stride)
-                _lib.check(lib.fdtd_engine_replay_range(h, s0, s1), "replay_range")
-                _lib.check(lib.fdtd_engine_adjoint_range(h, s1, s0), "adjoint_range")
+            # segment replays overlapped with the reverse steps of the segment after
+            _lib.check(lib.fdtd_engine_backward_replay(h, self.steps, self.stride), "backward_replay")
         ev[1].record(solver.stream)
         ev[1].synchronize()
         self.timings["backward_ms"] = ev[0].elapsed_time(ev[1])

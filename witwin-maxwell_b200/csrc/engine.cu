@@ -376,6 +376,12 @@ struct AdjointHost {
   std::vector<float*> gpol_host, gcur_host;  // adjoint pole state per pole id
   int max_segment = 0;
   int replay_n0 = -1, replay_n1 = -1;
+  // Pipelined checkpoint replay (fdtd_engine_backward_replay): a second design
+  // history per box, and the stream and events on which the reverse steps of
+  // one segment run while the engine stream replays the segment before it.
+  float* hist2[3] = {nullptr, nullptr, nullptr};
+  cudaStream_t rev = nullptr;
+  cudaEvent_t ev_rep[2] = {nullptr, nullptr}, ev_rev[2] = {nullptr, nullptr};
 };
 
 struct fdtd_engine {
@@ -1132,6 +1138,10 @@ int fdtd_engine_destroy(fdtd_engine* h) {
   for (cudaEvent_t e : {h->ev_fork, h->ev_join, h->ev_gat[0], h->ev_gat[1]})
     if (e) cudaEventDestroy(e);
   if (h->aux) cudaStreamDestroy(h->aux);
+  if (h->adj.rev) cudaStreamSynchronize(h->adj.rev);
+  for (cudaEvent_t e : {h->adj.ev_rep[0], h->adj.ev_rep[1], h->adj.ev_rev[0], h->adj.ev_rev[1]})
+    if (e) cudaEventDestroy(e);
+  if (h->adj.rev) cudaStreamDestroy(h->adj.rev);
   if (h->ev0) cudaEventDestroy(h->ev0);
   if (h->ev1) cudaEventDestroy(h->ev1);
   delete h;
@@ -2283,6 +2293,112 @@ int fdtd_engine_adjoint_range(fdtd_engine* h, int n1, int n0) {
   }
   CUDA_TRY(cudaStreamSynchronize(h->stream));
   return 0;
+}
+
+// Segments [s * stride, min((s + 1) * stride, n_steps)) from the last to the
+// first.  Segment s needs its design-box E history, which a replay from
+// checkpoint slot s rebuilds on the engine stream; its reverse steps run on a
+// second stream.  The reverse of segment s and the replay of segment s - 1 are
+// independent (the reverse reads only adjoint state, static coefficients and
+// the history of segment s; the replay writes only forward state and the
+// history of segment s - 1, kept in the other of two buffers), so they run at
+// the same time: each is latency-bound well below the HBM roof, and together
+// they use it better than one after the other.
+int fdtd_engine_backward_replay(fdtd_engine* h, int n_steps, int stride) {
+  if (!h || !h->adj.ready) return fail(FDTD_ERR_STATE, "adjoint not initialised");
+  AdjointHost& a = h->adj;
+  if (n_steps < 1 || stride < 1 || stride > a.max_segment)
+    return fail(FDTD_ERR_INVALID_ARG, "bad replay stride (at most the max_segment of fdtd_engine_adjoint_init)");
+  const int S = (n_steps + stride - 1) / stride;
+  if (static_cast<int>(h->checkpoints.size()) < S)
+    return fail(FDTD_ERR_STATE, "one checkpoint per segment (slot s = step s * stride) is needed");
+  for (int s = 0; s < S; ++s)
+    if (!h->checkpoints[s].valid) return fail(FDTD_ERR_STATE, "a segment checkpoint was never saved");
+  if (a.q.seed_re && n_steps > h->dft_steps) return fail(FDTD_ERR_INVALID_ARG, "DFT weight table shorter than the range");
+  for (const auto& t : h->terms)
+    if (t.signal && n_steps > t.aux_len) return fail(FDTD_ERR_INVALID_ARG, "source signal table shorter than the range");
+  for (const auto& l : h->lines)
+    if (n_steps > l.n_steps) return fail(FDTD_ERR_INVALID_ARG, "incident line history shorter than the range");
+  int rc = flush_samples(h);  // buffered forward samples belong to the forward run
+  if (rc) return rc;
+  if (!a.rev) {
+    int prio_lo = 0, prio_hi = 0;
+    CUDA_TRY(cudaDeviceGetStreamPriorityRange(&prio_lo, &prio_hi));
+    CUDA_TRY(cudaStreamCreateWithPriority(&a.rev, cudaStreamNonBlocking, prio_lo));
+    for (int b = 0; b < 2; ++b) {
+      CUDA_TRY(cudaEventCreateWithFlags(&a.ev_rep[b], cudaEventDisableTiming));
+      CUDA_TRY(cudaEventCreateWithFlags(&a.ev_rev[b], cudaEventDisableTiming));
+    }
+  }
+  bool design = false;
+  for (int c = 0; c < 3; ++c) {
+    DesignBox& d = a.q.design[c];
+    if (!d.grad) continue;
+    design = true;
+    if (!a.hist2[c]) {
+      rc = adj_alloc(h, &a.hist2[c], static_cast<size_t>(d.cells) * (a.max_segment + 1));
+      if (rc) return rc;
+    }
+  }
+  // the history buffers of segment s: the engine's for even s, the second for odd s
+  auto with_hist = [&](int s) {
+    AdjParams q = a.q;
+    if (s & 1)
+      for (int c = 0; c < 3; ++c)
+        if (q.design[c].grad) q.design[c].hist = a.hist2[c];
+    return q;
+  };
+  auto replay = [&](int s) -> int {
+    const int n0 = s * stride, n1 = std::min(n_steps, n0 + stride);
+    int r = fdtd_engine_checkpoint_load(h, s);
+    if (r) return r;
+    const AdjParams q = with_hist(s);
+    StepParams p;
+    fill_params(h, p);
+    int err = design ? launch_design_record(p, q, 0, h->stream) : 0;
+    if (err) return cuda_fail(static_cast<cudaError_t>(err), "design record");
+    for (int n = n0; n < n1; ++n) {
+      r = launch_step(h, n, -1);
+      if (r) return r;
+      if (design) {
+        fill_params(h, p);
+        err = launch_design_record(p, q, n + 1 - n0, h->stream);
+        if (err) return cuda_fail(static_cast<cudaError_t>(err), "design record");
+      }
+    }
+    CUDA_TRY(cudaEventRecord(a.ev_rep[s & 1], h->stream));
+    return 0;
+  };
+  // the reverse stream starts after everything queued so far on the engine stream
+  CUDA_TRY(cudaEventRecord(a.ev_rev[0], h->stream));
+  CUDA_TRY(cudaStreamWaitEvent(a.rev, a.ev_rev[0], 0));
+  rc = replay(S - 1);
+  if (rc) return rc;
+  StepParams p;
+  fill_params(h, p);
+  for (int s = S - 1; s >= 0; --s) {
+    const int n0 = s * stride, n1 = std::min(n_steps, n0 + stride);
+    CUDA_TRY(cudaStreamWaitEvent(a.rev, a.ev_rep[s & 1], 0));
+    const AdjParams qs = with_hist(s);
+    for (int n = n1 - 1; n >= n0; --n) {
+      AdjParams q = qs;
+      q.hist_slot = design ? n - n0 : 0;
+      const int err = launch_adjoint_step(p, q, h->d_flush, q.seed_re ? h->n_flush : 0, h->w_e, h->w_h, h->n_freq,
+                                          n, a.rev);
+      if (err) return cuda_fail(static_cast<cudaError_t>(err), "adjoint step");
+    }
+    CUDA_TRY(cudaEventRecord(a.ev_rev[s & 1], a.rev));
+    if (s > 0) {
+      // the history buffer of segment s - 1 was read by the reverse of segment s + 1
+      if (s + 1 < S) CUDA_TRY(cudaStreamWaitEvent(h->stream, a.ev_rev[(s + 1) & 1], 0));
+      rc = replay(s - 1);
+      if (rc) return rc;
+    }
+  }
+  CUDA_TRY(cudaStreamWaitEvent(h->stream, a.ev_rev[0], 0));
+  CUDA_TRY(cudaStreamSynchronize(h->stream));
+  a.replay_n0 = a.replay_n1 = -1;
+  return check_status(h);
 }
 
 int fdtd_engine_adjoint_grad(fdtd_engine* h, int comp, float* out) {
