@@ -131,6 +131,17 @@ int fdtd_engine_set_pole_state(fdtd_engine* h, int pole_id, const float* pol, co
  * holds the host-evaluated waveform, excitation/temporal.py:408-491). */
 int fdtd_engine_add_patch(fdtd_engine* h, int comp, const int* box, const float* coeff, const float* signal,
                           int n_signal, float scale);
+/* Time-shifted patch (sources.cu:173-221, excitation/temporal.py:232-251; the
+ * pulsed soft GaussianBeam of injection.py:920-949): comp gets
+ * scale[cell] * w(n * dt + t_offset - delay[cell]) at step n, w of kind 0 (CW,
+ * amplitude cos(2 pi frequency t + phase)) or 1 (Gaussian pulse,
+ * amplitude exp(-(tau 2 pi fwidth)^2 / 2) cos(2 pi frequency tau + phase),
+ * tau = t - wdelay).  scale and delay (seconds) are box-dense; the engine
+ * evaluates the waveform per cell on the GPU before every step; n_steps bounds
+ * the steps it may run.  At most 8 per engine. */
+int fdtd_engine_add_shifted_patch(fdtd_engine* h, int comp, const int* box, const float* scale, const float* delay,
+                                  double t_offset, int kind, double frequency, double fwidth, double amplitude,
+                                  double phase, double wdelay, int n_steps);
 
 /* 1-D incident line for TFSF (witwin/maxwell/fdtd/excitation/spatial.py:311-469):
  * the engine precomputes its whole history for n_steps steps.  Coefficient
@@ -356,6 +367,20 @@ int fdtd_op_apply_polarization(int64_t n, const float* cur, const float* inv_eps
  * cells outside the field are skipped.  fshape/pshape/offset are int[3]. */
 int fdtd_op_add_source_patch(float* field, const int* fshape, const float* patch, const int* pshape,
                              const int* offset, float signal, void* stream);
+/* addCwPhasedSourcePatch3D (sources.cu:156-171, launched by excitation/
+ * temporal.py:133-144): value = signal_cos * patch_cos + signal_sin * patch_sin. */
+int fdtd_op_add_cw_patch(float* field, const int* fshape, const float* patch_cos, const float* patch_sin,
+                         const int* pshape, const int* offset, float signal_cos, float signal_sin, void* stream);
+/* addTimeShiftedSourcePatch3D (sources.cu:173-221, excitation/temporal.py:232-251):
+ * value = patch * w(time - delay[idx]), w of kind 0 (CW, amplitude
+ * cos(2 pi frequency t + phase)), 1 (Gaussian pulse of width fwidth centred at
+ * wdelay) or 2 (Ricker centred at wdelay), waveforms.py:83-107; with causal_gate
+ * a cell adds nothing while time < activation[idx] (activation may be NULL
+ * without the gate). */
+int fdtd_op_add_shifted_patch(float* field, const int* fshape, const float* patch, const float* delay,
+                              const float* activation, int causal_gate, const int* pshape, const int* offset, int kind,
+                              float time, float frequency, float fwidth, float amplitude, float phase, float wdelay,
+                              void* stream);
 /* add_scaled_line_source_patch (sources.cu:485-545): value = coeff * incident[sample_idx[a]] * scale. */
 int fdtd_op_add_line_patch(float* field, const int* fshape, const float* coeff, const int* pshape,
                            const int* offset, const float* incident, const int64_t* sample_idx, int axis,

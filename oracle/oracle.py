@@ -79,6 +79,22 @@ def _p(a):
     return None if a is None else a.ctypes.data_as(_vp)
 
 
+def shifted_waveform(source_time, t):
+    """Waveform of a time-shifted patch (witwin/maxwell/waveforms.py:83-107) at
+    times t: CW A cos(2 pi f t + phase); Gaussian pulse A exp(-(tau 2 pi fwidth)^2 / 2)
+    cos(2 pi f tau + phase) with tau = t - delay (delay 6 / (2 pi fwidth) unless
+    given)."""
+    t = np.asarray(t, dtype=np.float64)
+    f = float(source_time.frequency)
+    if source_time.kind == "cw":
+        return source_time.amplitude * np.cos(2.0 * np.pi * f * t + source_time.phase)
+    fw = float(source_time.fwidth)
+    centre = 6.0 / (2.0 * np.pi * fw) if source_time.delay is None else float(source_time.delay)
+    tau = t - centre
+    return source_time.amplitude * np.exp(-0.5 * (tau * 2.0 * np.pi * fw) ** 2) * np.cos(2.0 * np.pi * f * tau
+                                                                                        + source_time.phase)
+
+
 def component_shape(name, nodes):
     nx, ny, nz = nodes
     return {
@@ -144,6 +160,10 @@ class OracleSimulation:
                 "drive": drive, "inv_eps": inv_eps, "P": np.zeros(shape, dt), "J": np.zeros(shape, dt),
             })
         self.patches = [(p.component, p.box, p.coeff.astype(dt), p.signal) for p in cs.patches]
+        # time-shifted patches: scale * w(n dt + t_offset - delay) per cell, the
+        # waveform evaluated in FP64 here (sources.cu:173-221)
+        self.shifted = [(p.component, p.box, p.scale.astype(np.float64), p.delay.astype(np.float64), p.t_offset,
+                         p.source_time) for p in getattr(cs, "shifted", [])]
         self.aux = None
         if cs.aux_line is not None:
             a = cs.aux_line
@@ -273,14 +293,32 @@ class OracleSimulation:
             self.lib.oracle_add_line_patch(f.shape[0], f.shape[1], f.shape[2], _p(f), pshape[0], pshape[1], pshape[2],
                                            _p(coeff), _p(sample), _p(idx), axis, box[0], box[2], box[4], scale)
 
+    def _soft_terms(self, n: int, magnetic: bool):
+        """Soft patches of one phase: H components right after the H update
+        (stepping.py:1776-1777), E components after the E update (:2300-2308)."""
+        F = self.fields
+        for comp, box, coeff, signal in self.patches:
+            if (comp[0] == "H") != magnetic:
+                continue
+            f = F[comp]
+            self.lib.oracle_add_patch(f.shape[0], f.shape[1], f.shape[2], _p(f), coeff.shape[0], coeff.shape[1],
+                                      coeff.shape[2], _p(coeff), box[0], box[2], box[4], float(signal[n]))
+        for comp, box, scale, delay, t_off, st in self.shifted:
+            if (comp[0] == "H") != magnetic:
+                continue
+            value = np.ascontiguousarray(scale * shifted_waveform(st, n * self.cs.dt + t_off - delay), dtype=self.dtype)
+            f = F[comp]
+            self.lib.oracle_add_patch(f.shape[0], f.shape[1], f.shape[2], _p(f), value.shape[0], value.shape[1],
+                                      value.shape[2], _p(value), box[0], box[2], box[4], 1.0)
+
     def step_once(self):
         n = self.step
-        F = self.fields
         self.update_h()
         if self.aux is not None:
             self._line_corrections(True)
             a = self.aux
             self.lib.oracle_aux_magnetic(a["e"].size, _p(a["h"]), _p(a["e"]), _p(a["hd"]), _p(a["hc"]))
+        self._soft_terms(n, True)
         self.advance_ade()
         self.update_e()
         if self.aux is not None:
@@ -288,10 +326,7 @@ class OracleSimulation:
             a = self.aux
             self.lib.oracle_aux_electric(a["e"].size, _p(a["e"]), _p(a["h"]), _p(a["ed"]), _p(a["ec"]), a["src"],
                                          float(a["signal"][n]))
-        for comp, box, coeff, signal in self.patches:
-            f = F[comp]
-            self.lib.oracle_add_patch(f.shape[0], f.shape[1], f.shape[2], _p(f), coeff.shape[0], coeff.shape[1],
-                                      coeff.shape[2], _p(coeff), box[0], box[2], box[4], float(signal[n]))
+        self._soft_terms(n, False)
         self.apply_ade()
         if self.aux is None:
             self._clamp_pec()

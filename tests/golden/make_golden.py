@@ -285,6 +285,24 @@ def op_vectors(tr, rng) -> dict:
                                           EzImagAccum=acc_i["Ez"], weightedCos=t(wc), weightedSin=t(ws))
     for k in ("Ex", "Ey", "Ez"):
         out[f"out_dft_{k}_re"], out[f"out_dft_{k}_im"] = acc[k].numpy(), acc_i[k].numpy()
+    # CW-phased and time-shifted patches (sources.cu:156-221), partially outside
+    fld, patch = out["patch_field"], out["patch"]
+    pc, ps = rng.standard_normal((3, 3, 3)), rng.standard_normal((3, 3, 3))
+    out.update(cw_cos=pc, cw_sin=ps)
+    f = t(fld)
+    K["addCwPhasedSourcePatch3D"](field=f, sourcePatchCos=t(pc), sourcePatchSin=t(ps), offsetI=3, offsetJ=-1,
+                                  offsetK=2, signalCos=0.6, signalSin=-0.3)
+    out["out_cw_patch"] = f.numpy()
+    delay = rng.uniform(0.0, 2e-15, (3, 3, 3))
+    act = rng.uniform(0.0, 2e-14, (3, 3, 3))
+    out.update(shift_delay=delay, shift_act=act)
+    for kind, gate in ((0, 0), (1, 0), (1, 1), (2, 1)):
+        f = t(fld)
+        K["addTimeShiftedSourcePatch3D"](field=f, sourcePatch=t(patch), delayPatch=t(delay),
+                                         activationDelayPatch=t(act), offsetI=3, offsetJ=-1, offsetK=2, timeKind=kind,
+                                         time=1.1e-14, frequency=300e12, fwidth=100e12, amplitude=1.3, phase=0.2,
+                                         delay=9.5e-15, causalGate=gate)
+        out[f"out_shift_{kind}_{gate}"] = f.numpy()
     return out
 
 

@@ -140,6 +140,17 @@ def test_patch_line_aux_ops(ops, mod):
     mod.addSourcePatch3D(field=f, sourcePatch=g(ops["patch"]), offsetI=3, offsetJ=-1, offsetK=2, signal=0.75).launchRaw()
     close(f, ops["out_patch"])
     f = g(ops["patch_field"])
+    mod.addCwPhasedSourcePatch3D(field=f, sourcePatchCos=g(ops["cw_cos"]), sourcePatchSin=g(ops["cw_sin"]), offsetI=3,
+                                 offsetJ=-1, offsetK=2, signalCos=0.6, signalSin=-0.3).launchRaw()
+    close(f, ops["out_cw_patch"])
+    for kind, gate in ((0, 0), (1, 0), (1, 1), (2, 1)):
+        f = g(ops["patch_field"])
+        mod.addTimeShiftedSourcePatch3D(field=f, sourcePatch=g(ops["patch"]), delayPatch=g(ops["shift_delay"]),
+                                        activationDelayPatch=g(ops["shift_act"]), offsetI=3, offsetJ=-1, offsetK=2,
+                                        timeKind=kind, time=1.1e-14, frequency=300e12, fwidth=100e12, amplitude=1.3,
+                                        phase=0.2, delay=9.5e-15, causalGate=gate).launchRaw()
+        close(f, ops[f"out_shift_{kind}_{gate}"])
+    f = g(ops["patch_field"])
     mod.addScaledLineSourcePatch3D(field=f, coeffPatch=g(ops["line_coeff"]), incidentField=g(ops["line_inc"]),
                                    sampleIndices=g(ops["line_idx"], torch.int64), sampleAxisCode=0, offsetI=1,
                                    offsetJ=1, offsetK=1, scale=-0.6).launchRaw()

@@ -20,6 +20,7 @@ from .scene import (
     CW,
     Box,
     CustomSourceTime,
+    GaussianBeam,
     GaussianPulse,
     MaterialRegion,
     Medium,

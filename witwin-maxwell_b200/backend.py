@@ -145,6 +145,33 @@ def _add_source_patch(*, field, sourcePatch, offsetI, offsetJ, offsetK, signal):
         _lib.int_array([offsetI, offsetJ, offsetK]), float(signal), _stream(field)), "add source patch")
 
 
+def _add_cw_patch(*, field, sourcePatchCos, sourcePatchSin, offsetI, offsetJ, offsetK, signalCos, signalSin):
+    _check_tensor(field, "field")
+    _check_tensor(sourcePatchCos, "sourcePatchCos")
+    _check_tensor(sourcePatchSin, "sourcePatchSin")
+    _lib.check(_lib.load().fdtd_op_add_cw_patch(
+        _lib.ptr(field), _lib.int_array(field.shape), _lib.ptr(sourcePatchCos), _lib.ptr(sourcePatchSin),
+        _lib.int_array(sourcePatchCos.shape), _lib.int_array([offsetI, offsetJ, offsetK]), float(signalCos),
+        float(signalSin), _stream(field)), "add CW-phased patch")
+
+
+def _add_shifted_patch(*, field, sourcePatch, delayPatch, activationDelayPatch, offsetI, offsetJ, offsetK, timeKind,
+                       time, frequency, fwidth, amplitude, phase, delay, causalGate):
+    _check_tensor(field, "field")
+    _check_tensor(sourcePatch, "sourcePatch")
+    _check_tensor(delayPatch, "delayPatch")
+    if int(timeKind) not in (0, 1, 2):
+        raise ValueError("timeKind must be 0 (CW), 1 (Gaussian pulse) or 2 (Ricker)")
+    gate = int(causalGate) != 0
+    if gate:
+        _check_tensor(activationDelayPatch, "activationDelayPatch")
+    _lib.check(_lib.load().fdtd_op_add_shifted_patch(
+        _lib.ptr(field), _lib.int_array(field.shape), _lib.ptr(sourcePatch), _lib.ptr(delayPatch),
+        _lib.ptr(activationDelayPatch) if gate else None, 1 if gate else 0, _lib.int_array(sourcePatch.shape),
+        _lib.int_array([offsetI, offsetJ, offsetK]), int(timeKind), float(time), float(frequency), float(fwidth),
+        float(amplitude), float(phase), float(delay), _stream(field)), "add time-shifted patch")
+
+
 def _add_line_patch(*, field, coeffPatch, incidentField, sampleIndices, sampleAxisCode, offsetI, offsetJ, offsetK, scale):
     _check_tensor(field, "field")
     idx = sampleIndices.to(dtype=torch.int64).contiguous()
@@ -207,6 +234,8 @@ _KERNELS.update({
     "updateLorentzCurrent3D": _lorentz,
     "applyPolarizationCurrent3D": _apply_polarization,
     "addSourcePatch3D": _add_source_patch,
+    "addCwPhasedSourcePatch3D": _add_cw_patch,
+    "addTimeShiftedSourcePatch3D": _add_shifted_patch,
     "addScaledLineSourcePatch3D": _add_line_patch,
     "updateAuxiliaryMagnetic1D": _aux_magnetic,
     "updateAuxiliaryElectric1D": _aux_electric,

@@ -369,6 +369,49 @@ struct Checkpoint {
 
 // Adjoint state (reverse-time pass): adjoint fields and CPML psi in the
 // forward layouts, monitor seeds, design boxes with their replayed E history.
+// Time-shifted patches (witwin/maxwell/fdtd/cuda/kernels/sources.cu:173-221):
+// comp gets scale[cell] * w(n dt + t_offset - delay[cell]) at step n.  Each one
+// is an ordinary injection term whose coefficient array the shift kernel
+// rewrites before every step, with a signal table of ones.
+constexpr int kMaxShifted = 8;
+struct ShiftedHost {
+  float* coeff;  // the injection term's coefficient array
+  const float* scale;
+  const float* delay;
+  int64_t cells;
+  double t_offset, wdelay;
+  int kind;  // 0 CW, 1 Gaussian pulse
+  float omega, inv_sigma, amplitude, phase;
+};
+
+struct ShiftedLaunch {
+  int count;
+  float* coeff[kMaxShifted];
+  const float* scale[kMaxShifted];
+  const float* delay[kMaxShifted];
+  int64_t cells[kMaxShifted];
+  float tau0[kMaxShifted];  // n dt + t_offset (- the pulse centre), formed in FP64
+  int kind[kMaxShifted];
+  float omega[kMaxShifted], inv_sigma[kMaxShifted], amplitude[kMaxShifted], phase[kMaxShifted];
+};
+
+// blockIdx.y picks the term; CW: A cos(omega tau + phase); Gaussian pulse:
+// A exp(-(tau inv_sigma)^2 / 2) cos(omega tau + phase) (waveforms.py:83-103).
+__global__ void __launch_bounds__(256) shifted_patch_kernel(const __grid_constant__ ShiftedLaunch s) {
+  const int t = blockIdx.y;
+  const int64_t cells = s.cells[t];
+  for (int64_t c = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; c < cells;
+       c += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    const float tau = s.tau0[t] - __ldg(s.delay[t] + c);
+    float w = s.amplitude[t] * cosf(s.omega[t] * tau + s.phase[t]);
+    if (s.kind[t] == 1) {
+      const float a = tau * s.inv_sigma[t];
+      w *= expf(-0.5f * a * a);
+    }
+    s.coeff[t][c] = __ldg(s.scale[t] + c) * w;
+  }
+}
+
 struct AdjointHost {
   bool ready = false;
   AdjParams q{};
@@ -435,6 +478,7 @@ struct fdtd_engine {
   bool uniform_grid = false;
   float inv_e_u[3] = {0, 0, 0}, inv_h_u[3] = {0, 0, 0};
   std::vector<InjectionTerm> terms;
+  std::vector<ShiftedHost> shifted;
   std::vector<float*> owned;
   std::vector<PoleHost> poles;
   std::vector<SampleRegion> regions;
@@ -750,7 +794,37 @@ bool tile_runs(const fdtd_engine* h) {
          (h->poles.empty() || ade_pass_active(h));
 }
 
+int launch_shifted(fdtd_engine* h, int n) {
+  ShiftedLaunch s{};
+  s.count = static_cast<int>(h->shifted.size());
+  int64_t most = 0;
+  for (int t = 0; t < s.count; ++t) {
+    const ShiftedHost& x = h->shifted[t];
+    s.coeff[t] = x.coeff;
+    s.scale[t] = x.scale;
+    s.delay[t] = x.delay;
+    s.cells[t] = x.cells;
+    s.tau0[t] = static_cast<float>(n * h->desc.dt + x.t_offset - (x.kind == 1 ? x.wdelay : 0.0));
+    s.kind[t] = x.kind;
+    s.omega[t] = x.omega;
+    s.inv_sigma[t] = x.inv_sigma;
+    s.amplitude[t] = x.amplitude;
+    s.phase[t] = x.phase;
+    most = std::max(most, x.cells);
+  }
+  const int gx = static_cast<int>(std::min<int64_t>((most + 255) / 256, 4 * 148));
+  shifted_patch_kernel<<<dim3(gx, s.count), 256, 0, h->stream>>>(s);
+  const cudaError_t err = cudaGetLastError();
+  if (err != cudaSuccess) return cuda_fail(err, "shifted_patch_kernel launch");
+  ++h->launches;
+  return 0;
+}
+
 int launch_step(fdtd_engine* h, int n, int slot) {
+  if (!h->shifted.empty()) {
+    const int rc = launch_shifted(h, n);
+    if (rc) return rc;
+  }
   StepParams p;
   fill_params(h, p);
   const dim3 grid = step_grid(h);
@@ -1441,6 +1515,55 @@ int fdtd_engine_add_patch(fdtd_engine* h, int comp, const int* box, const float*
   t.aux_len = n_signal;  // bound of the signal table
   t.scale = scale;
   h->terms.push_back(t);
+  return 0;
+}
+
+int fdtd_engine_add_shifted_patch(fdtd_engine* h, int comp, const int* box, const float* scale, const float* delay,
+                                  double t_offset, int kind, double frequency, double fwidth, double amplitude,
+                                  double phase, double wdelay, int n_steps) {
+  if (!h || comp < 0 || comp > 5 || !box || !scale || !delay || kind < 0 || kind > 1 || n_steps <= 0)
+    return fail(FDTD_ERR_INVALID_ARG, "bad shifted patch arguments");
+  if (h->finalized) return fail(FDTD_ERR_STATE, "engine already finalized");
+  if (static_cast<int>(h->shifted.size()) >= kMaxShifted) return fail(FDTD_ERR_UNSUPPORTED, "too many shifted patches");
+  if (!box_ok(h, comp, box)) return fail(FDTD_ERR_INVALID_ARG, "patch box outside the component extent");
+  const int64_t cnt = static_cast<int64_t>(box[1] - box[0]) * (box[3] - box[2]) * (box[5] - box[4]);
+  float *c = nullptr, *sc = nullptr, *dl = nullptr, *ones = nullptr;
+  int rc = dev_copy(h, &c, scale, cnt);  // the step-0 coefficients are replaced before the first step
+  if (!rc) rc = dev_copy(h, &sc, scale, cnt);
+  if (!rc) rc = dev_copy(h, &dl, delay, cnt);
+  if (!rc) {
+    const std::vector<float> one(static_cast<size_t>(n_steps), 1.0f);
+    rc = dev_copy(h, &ones, one.data(), one.size());
+    if (!rc) CUDA_TRY(cudaStreamSynchronize(h->stream));
+  }
+  if (rc) return rc;
+  InjectionTerm t{};
+  t.comp = comp;
+  t.i0 = box[0];
+  t.i1 = box[1];
+  t.j0 = box[2];
+  t.j1 = box[3];
+  t.k0 = box[4];
+  t.k1 = box[5];
+  t.coeff = c;
+  t.signal = ones;
+  t.aux_len = n_steps;
+  t.scale = 1.0f;
+  h->terms.push_back(t);
+  constexpr double kTwoPi = 6.283185307179586;
+  ShiftedHost x{};
+  x.coeff = c;
+  x.scale = sc;
+  x.delay = dl;
+  x.cells = cnt;
+  x.t_offset = t_offset;
+  x.wdelay = wdelay;
+  x.kind = kind;
+  x.omega = static_cast<float>(kTwoPi * frequency);
+  x.inv_sigma = static_cast<float>(std::max(kTwoPi * fwidth, 1e-30));
+  x.amplitude = static_cast<float>(amplitude);
+  x.phase = static_cast<float>(phase);
+  h->shifted.push_back(x);
   return 0;
 }
 

@@ -5,6 +5,7 @@
 // index (z fastest), 256-thread blocks, launched on the caller's stream.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <string>
 
 #include "../../include/fdtd_b200.h"
@@ -207,6 +208,55 @@ __global__ void op_patch_kernel(float* field, int fx, int fy, int fz, const floa
   }
 }
 
+// CW-phased patch: value = signal_cos * patch_cos + signal_sin * patch_sin
+// (witwin/maxwell/fdtd/cuda/kernels/sources.cu:156-171).
+__global__ void op_cw_patch_kernel(float* field, int fx, int fy, int fz, const float* pc, const float* ps, int px,
+                                   int py, int pz, int oi, int oj, int ok, float sc, float ss) {
+  const int64_t total = static_cast<int64_t>(px) * py * pz;
+  for (int64_t x = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; x < total;
+       x += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    int i, j, k;
+    unflatten(x, py, pz, i, j, k);
+    const int gi = oi + i, gj = oj + j, gk = ok + k;
+    if (gi < 0 || gj < 0 || gk < 0 || gi >= fx || gj >= fy || gk >= fz) continue;
+    field[off3(gi, gj, gk, fy, fz)] += sc * pc[x] + ss * ps[x];
+  }
+}
+
+// Time-shifted patch: value = patch * w(time - delay[cell]) with the analytic
+// waveform w of kind 0 (CW: A cos(omega t + phase)), 1 (Gaussian pulse:
+// A exp(-(tau inv_sigma)^2 / 2) cos(omega tau + phase), tau = t - wdelay) or
+// 2 (Ricker: A (1 - 2 a^2) exp(-a^2), a = pi f tau); with the causal gate a cell
+// adds nothing before its activation time (witwin/maxwell/fdtd/cuda/kernels/
+// sources.cu:173-221, waveforms.py:83-107).
+__global__ void op_shifted_patch_kernel(float* field, int fx, int fy, int fz, const float* patch, const float* delay,
+                                        const float* activation, int gate, int px, int py, int pz, int oi, int oj,
+                                        int ok, int kind, float time, float omega, float inv_sigma, float pi_f,
+                                        float amplitude, float phase, float wdelay) {
+  const int64_t total = static_cast<int64_t>(px) * py * pz;
+  for (int64_t x = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; x < total;
+       x += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    int i, j, k;
+    unflatten(x, py, pz, i, j, k);
+    const int gi = oi + i, gj = oj + j, gk = ok + k;
+    if (gi < 0 || gj < 0 || gk < 0 || gi >= fx || gj >= fy || gk >= fz) continue;
+    if (gate && time < activation[x]) continue;
+    const float t = time - delay[x];
+    float w;
+    if (kind == 0) {
+      w = amplitude * cosf(omega * t + phase);
+    } else if (kind == 1) {
+      const float tau = t - wdelay;
+      const float a = tau * inv_sigma;
+      w = amplitude * expf(-0.5f * a * a) * cosf(omega * tau + phase);
+    } else {
+      const float a = pi_f * (t - wdelay);
+      w = amplitude * (1.0f - 2.0f * a * a) * expf(-a * a);
+    }
+    field[off3(gi, gj, gk, fy, fz)] += w * patch[x];
+  }
+}
+
 __global__ void op_line_patch_kernel(float* field, int fx, int fy, int fz, const float* coeff, int px, int py, int pz,
                                      int oi, int oj, int ok, const float* inc, const int64_t* sidx, int axis,
                                      float scale) {
@@ -404,6 +454,36 @@ int fdtd_op_add_source_patch(float* field, const int* fshape, const float* patch
   op_patch_kernel<<<blocks_for(n), kThreads, 0, static_cast<cudaStream_t>(stream)>>>(
       field, fshape[0], fshape[1], fshape[2], patch, pshape[0], pshape[1], pshape[2], offset[0], offset[1], offset[2], signal);
   return op_launch_check("add_source_patch");
+}
+
+int fdtd_op_add_cw_patch(float* field, const int* fshape, const float* patch_cos, const float* patch_sin,
+                         const int* pshape, const int* offset, float signal_cos, float signal_sin, void* stream) {
+  if (!field || !fshape || !patch_cos || !patch_sin || !pshape || !offset)
+    return op_fail(FDTD_ERR_INVALID_ARG, "add_cw_patch: bad arguments");
+  const int64_t n = static_cast<int64_t>(pshape[0]) * pshape[1] * pshape[2];
+  if (n <= 0) return 0;
+  op_cw_patch_kernel<<<blocks_for(n), kThreads, 0, static_cast<cudaStream_t>(stream)>>>(
+      field, fshape[0], fshape[1], fshape[2], patch_cos, patch_sin, pshape[0], pshape[1], pshape[2], offset[0],
+      offset[1], offset[2], signal_cos, signal_sin);
+  return op_launch_check("add_cw_patch");
+}
+
+int fdtd_op_add_shifted_patch(float* field, const int* fshape, const float* patch, const float* delay,
+                              const float* activation, int causal_gate, const int* pshape, const int* offset, int kind,
+                              float time, float frequency, float fwidth, float amplitude, float phase, float wdelay,
+                              void* stream) {
+  if (!field || !fshape || !patch || !delay || !pshape || !offset || kind < 0 || kind > 2 ||
+      (causal_gate && !activation))
+    return op_fail(FDTD_ERR_INVALID_ARG, "add_shifted_patch: bad arguments");
+  const int64_t n = static_cast<int64_t>(pshape[0]) * pshape[1] * pshape[2];
+  if (n <= 0) return 0;
+  constexpr double kPi = 3.141592653589793;
+  const float inv_sigma = static_cast<float>(std::max(2.0 * kPi * fwidth, 1e-30));
+  op_shifted_patch_kernel<<<blocks_for(n), kThreads, 0, static_cast<cudaStream_t>(stream)>>>(
+      field, fshape[0], fshape[1], fshape[2], patch, delay, activation, causal_gate ? 1 : 0, pshape[0], pshape[1],
+      pshape[2], offset[0], offset[1], offset[2], kind, time, static_cast<float>(2.0 * kPi * frequency), inv_sigma,
+      static_cast<float>(kPi * frequency), amplitude, phase, wdelay);
+  return op_launch_check("add_shifted_patch");
 }
 
 int fdtd_op_add_line_patch(float* field, const int* fshape, const float* coeff, const int* pshape,

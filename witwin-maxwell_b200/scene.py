@@ -94,13 +94,23 @@ class GaussianPulse:
 
 @dataclass(frozen=True)
 class CW:
+    """Continuous wave A cos(2 pi f t + phase).  ``ramp_time`` > 0 multiplies it by a
+    raised-cosine turn-on 0.5 (1 - cos(pi t / ramp_time)) for t < ramp_time; the
+    reference's CW (ramp_time 0) starts at full amplitude."""
+
     frequency: float
     amplitude: float = 1.0
     phase: float = 0.0
+    ramp_time: float = 0.0
     kind: str = "cw"
 
+    def ramp(self, t: float) -> float:
+        if self.ramp_time <= 0.0 or t >= self.ramp_time:
+            return 1.0
+        return 0.5 * (1.0 - math.cos(math.pi * max(float(t), 0.0) / self.ramp_time))
+
     def evaluate(self, t: float) -> float:
-        return self.amplitude * math.cos(2.0 * math.pi * self.frequency * float(t) + self.phase)
+        return self.ramp(t) * self.amplitude * math.cos(2.0 * math.pi * self.frequency * float(t) + self.phase)
 
     @property
     def characteristic_frequency(self) -> float:
@@ -255,6 +265,28 @@ class PlaneSource:
 
 
 @dataclass(frozen=True)
+class GaussianBeam:
+    """Soft Gaussian beam (witwin/maxwell/sources.py:615-655) launched by the
+    surface-equivalent currents of one face, J_s = n x H_inc on the E components and
+    M_s = -n x E_inc on the H components, over the whole plane normal to the
+    injection axis (excitation/injection.py:807-968), with the beam's amplitude and
+    per-cell delay (excitation/spatial.py:175-251) and unit forward power.
+
+    ``focus`` is in node-index coordinates (node i at x = i * spacing), ``beam_waist``
+    in metres.  The launch plane sits 5 % of the physical span inside the CPML edge
+    on the side the beam comes from (spatial.py:64-77).  A CW source time gives
+    cos / sin phased patches (the delay folded into their phase), a pulse gives
+    time-shifted patches (the waveform evaluated at t - delay per cell)."""
+
+    direction: tuple[float, float, float]
+    polarization: tuple[float, float, float]
+    beam_waist: float
+    focus: tuple[float, float, float]
+    source_time: object
+    injection_axis: int | None = None
+
+
+@dataclass(frozen=True)
 class PlaneWaveTFSF:
     """Axis-aligned plane wave injected through a TFSF box (or slab along the propagation axis)."""
 
@@ -380,6 +412,20 @@ class CompiledPatch:
 
 
 @dataclass
+class CompiledShiftedPatch:
+    """Time-shifted patch (witwin/maxwell/fdtd/cuda/kernels/sources.cu:173-221): comp
+    gets scale[cell] * w(n * dt + t_offset - delay[cell]) at step n, w the analytic
+    waveform of ``source_time`` (a GaussianPulse, or a CW without ramp)."""
+
+    component: str
+    box: tuple[int, int, int, int, int, int]
+    scale: np.ndarray  # box-dense float32
+    delay: np.ndarray  # box-dense float32, seconds
+    t_offset: float  # 0 for H components, dt / 2 for E components
+    source_time: object
+
+
+@dataclass
 class CompiledLinePatch:
     component: str
     box: tuple[int, int, int, int, int, int]
@@ -437,6 +483,7 @@ class CompiledScene:
     complex_fields: bool = False
     bloch_cos: tuple[float, float, float] = (1.0, 1.0, 1.0)
     bloch_sin: tuple[float, float, float] = (0.0, 0.0, 0.0)
+    shifted: list = field(default_factory=list)  # CompiledShiftedPatch
 
     @property
     def cells(self) -> int:
@@ -769,13 +816,19 @@ def compile_scene(scene: Scene, time_steps: int) -> CompiledScene:
             poles.append(CompiledPole(name, kind, float(decay_v), float(restoring), box,
                                       np.ascontiguousarray(drive), np.ascontiguousarray(inv_eps)))
     # --- sources ---
-    patches, line_patches, aux_line = [], [], None
+    patches, line_patches, aux_line, shifted = [], [], None, []
     for src in scene.sources:
         if isinstance(src, PointDipole):
             box, coeff = _dipole_patch(scene, src, eps, dt)
             patches.append(CompiledPatch(src.polarization, box, coeff, _source_signal(src.source_time, dt, time_steps)))
         elif isinstance(src, PlaneSource):
             patches.extend(_plane_source_patches(scene, src, eps, dt, time_steps))
+        elif isinstance(src, GaussianBeam):
+            curl_full = {name: curl[name] if curl[name] is not None else np.float32(uniform[name][1])
+                         for name in COMPONENTS}
+            beam_patches, beam_shifted = _beam_patches(scene, src, curl_full, dt, time_steps)
+            patches.extend(beam_patches)
+            shifted.extend(beam_shifted)
         elif isinstance(src, PlaneWaveTFSF):
             if any(b == BOUNDARY_BLOCH for b in scene.boundary):
                 raise ValueError("TFSF sources with Bloch faces are not supported; use PlaneSource")
@@ -828,7 +881,7 @@ def compile_scene(scene: Scene, time_steps: int) -> CompiledScene:
         pml_hi=pml_hi, inv_e=inv_e, inv_h=inv_h, cpml=cp, eps=eps, decay=decay, curl=curl, uniform=uniform,
         poles=poles, patches=patches, aux_line=aux_line, line_patches=line_patches, regions=regions,
         frequencies=tuple(freq_list), monitor_frequencies=mon_freqs, window=window, design=design,
-        complex_fields=complex_fields, bloch_cos=tuple(bcos), bloch_sin=tuple(bsin),
+        complex_fields=complex_fields, bloch_cos=tuple(bcos), bloch_sin=tuple(bsin), shifted=shifted,
     )
 
 
@@ -859,3 +912,172 @@ def _plane_source_patches(scene: Scene, src: PlaneSource, eps: dict, dt: float, 
         out.append(CompiledPatch(name, tuple(box), np.ascontiguousarray((base * np.sin(phase)).astype(np.float32)),
                                  signal, 1))
     return out
+
+
+def _numerical_wavenumber(omega: float, dt: float, direction, d: float) -> float:
+    """|k| of the discrete dispersion relation sum_a sin^2(k |u_a| d / 2) / d^2 =
+    sin^2(omega dt / 2) / (c dt)^2 on a uniform grid, by 80 bisection steps over
+    (0, min_a 2 pi / (|u_a| d)) (witwin/maxwell/fdtd/dispersion.py:6-48)."""
+    if omega <= 0.0:
+        return 0.0
+    target = math.sin(0.5 * omega * dt) ** 2 / (C_0 ** 2 * dt ** 2)
+    comps = [abs(float(u)) for u in direction if abs(float(u)) > 1e-12]
+    if target <= 0.0 or not comps:
+        return omega / C_0
+    lo, hi = 0.0, min(2.0 * math.pi / max(u * d, 1e-30) for u in comps)
+    for _ in range(80):
+        mid = 0.5 * (lo + hi)
+        if sum(math.sin(0.5 * mid * u * d) ** 2 / (d * d) for u in comps) - target >= 0.0:
+            hi = mid
+        else:
+            lo = mid
+    return 0.5 * (lo + hi)
+
+
+def _beam_profile(pos, direction, polarization, waist: float, focus, frequency: float, speed: float):
+    """Amplitude and delay of a Gaussian beam at positions pos[..., 3] (metres):
+    w(z) = w0 sqrt(1 + (z / z_R)^2), amplitude (w0 / w) exp(-(u^2 + v^2) / w^2),
+    delay z / c + (u^2 + v^2) / (2 R c) - atan(z / z_R) / omega with the wavefront
+    radius R = z (1 + (z_R / z)^2) (zero curvature within 1 nm of the waist plane),
+    u along the polarization, v along direction x polarization
+    (witwin/maxwell/fdtd/excitation/spatial.py:175-251)."""
+    dvec = np.asarray(direction, dtype=np.float64)
+    pvec = np.asarray(polarization, dtype=np.float64)
+    bvec = np.cross(dvec, pvec)
+    rel = pos - np.asarray(focus, dtype=np.float64)
+    z = rel @ dvec
+    u = rel @ pvec
+    v = rel @ bvec
+    wavelength = speed / frequency
+    z_r = math.pi * waist * waist / max(wavelength, 1e-30)
+    radius = waist * np.sqrt(1.0 + (z / max(z_r, 1e-30)) ** 2)
+    amplitude = (waist / radius) * np.exp(-(u * u) / (radius * radius) - (v * v) / (radius * radius))
+    curved = np.abs(z) > 1e-9
+    with np.errstate(divide="ignore", invalid="ignore"):
+        r_curv = z * (1.0 + (z_r / np.maximum(np.abs(z), 1e-30)) ** 2)
+        curvature = np.where(curved, (u * u + v * v) / (2.0 * r_curv * speed), 0.0)
+    gouy = np.arctan(z / max(z_r, 1e-30))
+    delay = z / speed + curvature - gouy / (2.0 * math.pi * frequency)
+    return amplitude, delay
+
+
+def _component_positions(name: str, offsets, shape, d: float) -> np.ndarray:
+    """Metres of the Yee samples of ``name`` over the box at ``offsets`` with ``shape``:
+    E components sit half a cell along their own axis, H components half a cell along
+    the other two (witwin/maxwell/fdtd/solver.py:406-424)."""
+    own = "xyz".index(name[1])
+    axes = []
+    for a in range(3):
+        half = (a == own) if name[0] == "E" else (a != own)
+        axes.append((np.arange(offsets[a], offsets[a] + shape[a], dtype=np.float64) + (0.5 if half else 0.0)) * d)
+    grid = np.meshgrid(*axes, indexing="ij")
+    return np.stack(grid, axis=-1)
+
+
+def _beam_launch_plane(scene: Scene, axis: int, forward: bool) -> int:
+    """Node index of the soft launch plane: 5 % of the physical (CPML-free) span from
+    its edge on the side the beam comes from, the nearest node, ties to the lower
+    index (witwin/maxwell/fdtd/excitation/spatial.py:49-77)."""
+    pml_lo, pml_hi = scene.pml_lengths()
+    n = scene.nodes[axis]
+    lo, hi = pml_lo[axis], n - pml_hi[axis] - 1
+    if hi <= lo:
+        raise ValueError("the scene has no physical interior along the injection axis")
+    target = lo + 0.05 * (hi - lo) if forward else hi - 0.05 * (hi - lo)
+    below = int(math.floor(target))
+    return below if target - below <= (below + 1) - target else below + 1
+
+
+def _beam_patches(scene: Scene, src: GaussianBeam, curl: dict, dt: float, steps: int):
+    """Face terms of a soft GaussianBeam (witwin/maxwell/fdtd/excitation/injection.py:807-968):
+    the E components of the launch face carry J_s from the magnetic incident vector,
+    the H components M_s from the electric one, each scaled by the curl coefficient
+    over the spacing, the face sign, the unit-power amplitude 1 / sqrt(pi w0^2 cos /
+    (4 eta0)) / sqrt(cos(k_n d / 2)) and the beam profile evaluated with the numerical
+    phase speed omega / k; the delay of the plane centre is removed (injection.py:
+    907-941).  E terms sample the waveform at (n + 1/2) dt, H terms at n dt
+    (runtime/stepping.py:1776, 2300-2306)."""
+    if any(b in (BOUNDARY_BLOCH, BOUNDARY_PERIODIC) for b in scene.boundary):
+        raise ValueError("a soft GaussianBeam supports CPML, PEC and open faces only")
+    st = src.source_time
+    if not isinstance(st, (CW, GaussianPulse)):
+        raise TypeError("a GaussianBeam takes a CW or GaussianPulse source time")
+    if src.beam_waist <= 0.0:
+        raise ValueError("beam_waist must be > 0")
+    dvec = np.asarray(src.direction, dtype=np.float64)
+    dvec = dvec / np.linalg.norm(dvec)
+    pvec = np.asarray(src.polarization, dtype=np.float64)
+    pvec = pvec / np.linalg.norm(pvec)
+    if abs(float(dvec @ pvec)) > 1e-6:
+        raise ValueError("the polarization must be transverse to the direction")
+    axis = int(np.argmax(np.abs(dvec))) if src.injection_axis is None else int(src.injection_axis)
+    if abs(dvec[axis]) <= 1e-6:
+        raise ValueError("the direction needs a component along the injection axis")
+    forward = dvec[axis] >= 0.0
+    d = float(scene.spacing)
+    nodes = scene.nodes
+    plane = _beam_launch_plane(scene, axis, forward)
+    lower = [0, 0, 0]
+    upper = [n - 1 for n in nodes]
+    lower[axis], upper[axis] = (plane, plane + 1) if forward else (plane - 1, plane)
+    ele, mag = _tfsf_specs(lower, upper)
+    face = 4 * axis + (0 if forward else 2)  # the x-low, x-high, y-low, ... pairs of the spec table
+    ele, mag = ele[face:face + 2], mag[face:face + 2]
+
+    freq = float(st.frequency)
+    omega = 2.0 * math.pi * freq
+    k_num = _numerical_wavenumber(omega, dt, dvec, d)
+    speed = omega / k_num if k_num > 1e-12 else C_0
+    power = 1.0 / math.sqrt(math.pi * src.beam_waist ** 2 * abs(dvec[axis]) / (4.0 * ETA_0))
+    factor = math.cos(0.5 * k_num * dvec[axis] * d)
+    if factor <= 0.0:
+        raise ValueError("the grid is too coarse for a positive discrete normal power")
+    power /= math.sqrt(factor)
+    e_vec = {n: power * float(pvec[i]) for i, n in enumerate(("Ex", "Ey", "Ez"))}
+    h_vec = {n: power * v / ETA_0 for n, v in _magnetic_unit_vector(dvec, pvec).items()}
+    pml_lo, pml_hi = scene.pml_lengths()
+    centre = np.array([0.5 * (pml_lo[a] + nodes[a] - 1 - pml_hi[a]) * d for a in range(3)])
+    centre[axis] = plane * d
+    focus = np.asarray(src.focus, dtype=np.float64) * d
+    _, ref_delay = _beam_profile(centre[None, :], dvec, pvec, src.beam_waist, focus, freq, speed)
+
+    patches, shifted = [], []
+    for specs, vector, t_off in ((ele, h_vec, 0.5 * dt), (mag, e_vec, 0.0)):
+        for fname, iname, offs, shape, soffs, _delta_axis, sgn in specs:
+            comp_scale = float(vector[iname])
+            if abs(sgn * comp_scale) <= 1e-12:
+                continue
+            box = (offs[0], offs[0] + shape[0], offs[1], offs[1] + shape[1], offs[2], offs[2] + shape[2])
+            c = curl[fname]
+            c_arr = np.broadcast_to(c, component_shape(fname, nodes)) if np.ndim(c) == 0 else c
+            coeff = c_arr[box[0]:box[1], box[2]:box[3], box[4]:box[5]].astype(np.float64) / d
+            amp, delay = _beam_profile(_component_positions(iname, soffs, shape, d), dvec, pvec, src.beam_waist,
+                                       focus, freq, speed)
+            delay = delay - ref_delay[0]
+            scale = sgn * comp_scale * amp * coeff
+            if float(np.max(np.abs(scale))) <= 1e-12:
+                continue
+            if isinstance(st, CW):
+                times = np.arange(steps, dtype=np.float64) * dt + t_off
+                ramp = np.array([st.ramp(t) for t in times])
+                phase = omega * times + st.phase
+                for patch, sig in ((scale * np.cos(omega * delay), np.cos(phase)),
+                                   (scale * np.sin(omega * delay), np.sin(phase))):
+                    patches.append(CompiledPatch(fname, box, np.ascontiguousarray(patch.astype(np.float32)),
+                                                 (st.amplitude * ramp * sig).astype(np.float32)))
+            else:
+                shifted.append(CompiledShiftedPatch(fname, box, np.ascontiguousarray(scale.astype(np.float32)),
+                                                    np.ascontiguousarray(delay.astype(np.float32)), t_off, st))
+    return patches, shifted
+
+
+def shifted_waveform(source_time, t):
+    """Waveform of a time-shifted patch at times t (array): A cos(2 pi f t + phase) for
+    a CW, A exp(-(tau 2 pi fwidth)^2 / 2) cos(2 pi f tau + phase), tau = t - delay, for
+    a GaussianPulse (witwin/maxwell/waveforms.py:83-107)."""
+    t = np.asarray(t, dtype=np.float64)
+    if isinstance(source_time, CW):
+        return source_time.amplitude * np.cos(2.0 * math.pi * source_time.frequency * t + source_time.phase)
+    tau = t - source_time.resolved_delay
+    env = np.exp(-0.5 * (tau * 2.0 * math.pi * source_time.fwidth) ** 2)
+    return source_time.amplitude * env * np.cos(2.0 * math.pi * source_time.frequency * tau + source_time.phase)

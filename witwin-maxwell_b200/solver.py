@@ -19,7 +19,7 @@ import numpy as np
 import torch
 
 from . import _lib
-from .scene import COMP_INDEX, CompiledScene, component_shape
+from .scene import COMP_INDEX, CompiledScene, GaussianPulse, component_shape
 
 
 def _require_cuda(device: torch.device) -> None:
@@ -185,6 +185,18 @@ class B200FDTD:
                         _lib.ptr(sig), int(sig.numel()), 1.0,
                     ),
                     "add_patch",
+                )
+            for sp in getattr(cs, "shifted", []) if channel == 0 else []:
+                st = sp.source_time
+                pulse = isinstance(st, GaussianPulse)
+                _lib.check(
+                    lib.fdtd_engine_add_shifted_patch(
+                        h, COMP_INDEX[sp.component], _lib.int_array(sp.box), _lib.ptr(self._dev(sp.scale)),
+                        _lib.ptr(self._dev(sp.delay)), float(sp.t_offset), 1 if pulse else 0, float(st.frequency),
+                        float(st.fwidth) if pulse else 0.0, float(st.amplitude), float(st.phase),
+                        float(st.resolved_delay) if pulse else 0.0, int(cs.time_steps),
+                    ),
+                    "add_shifted_patch",
                 )
             if cs.aux_line is not None and channel == 0:
                 aux = cs.aux_line

@@ -9,7 +9,9 @@ from __future__ import annotations
 import numpy as np
 
 from .scene import (
+    CW,
     Box,
+    GaussianBeam,
     GaussianPulse,
     MaterialRegion,
     Medium,
@@ -23,7 +25,6 @@ from .scene import (
     Structure,
     closed_box_monitor,
     flux_monitor,
-    ramped_cw,
 )
 
 SPACING = 25e-9
@@ -76,12 +77,12 @@ def dispersive_256(cells: int = 256, pml: int = 12, n_freq: int = 16, slab_throu
 def adjoint_160(steps: int = 3000, seed: int = 0, scale: int = 1) -> Scene:
     """Adjoint-gradient workload: 160x160x96 cells, 10-cell CPML; eps 2.1 substrate for
     z < 40; a 64x64x16 MaterialRegion design block at x, y in [48, 112), z in [40, 56)
-    with eps_r ~ U[1, 12) i.i.d. (torch.Generator().manual_seed(seed)); an Ey source at
-    300 THz, CW after a 200-step raised-cosine ramp (sampled table); the objective's
-    monitor is the 16x16 patch of E on the plane z = 80 at 300 THz.  A point dipole below
-    the design block stands in for the reference's Gaussian beam (not built here).
-    ``scale`` > 1 divides every length but the 10-cell CPML by it (the same layout on a
-    smaller grid, for checks that cannot afford the full size)."""
+    with eps_r ~ U[1, 12) i.i.d. (torch.Generator().manual_seed(seed)); a soft +z Ey
+    GaussianBeam (waist 0.5 um, focused on the design block's centre) launched from the
+    substrate, 300 THz CW after a 200-step raised-cosine ramp; the objective's monitor is
+    the 16x16 patch of E on the plane z = 80 at 300 THz.  ``scale`` > 1 divides every
+    length but the 10-cell CPML by it (the same layout on a smaller grid, for checks
+    that cannot afford the full size)."""
     import torch
 
     def s_(v):
@@ -94,7 +95,8 @@ def adjoint_160(steps: int = 3000, seed: int = 0, scale: int = 1) -> Scene:
     eps_r = (1.0 + 11.0 * torch.rand(shape, generator=gen, dtype=torch.float64)).numpy()
     sc.material_regions.append(MaterialRegion((s_(48), s_(48), s_(40)), (s_(112), s_(112), s_(56)), eps_r))
     dt = sc.resolve_dt()
-    sc.sources.append(PointDipole((s_(80), s_(80), s_(30)), "Ey", ramped_cw(300e12, 200, dt, steps), width=SPACING))
+    sc.sources.append(GaussianBeam((0.0, 0.0, 1.0), (0.0, 1.0, 0.0), 0.5e-6 / scale, (s_(80), s_(80), s_(48)),
+                                   CW(300e12, ramp_time=200 * dt)))
     sc.monitors.append(PlaneMonitor("patch", 2, s_(80), ("Ex", "Ey", "Ez"), (300e12,), (s_(72), s_(72)),
                                     (s_(72) + 16 // scale - 1, s_(72) + 16 // scale - 1)))
     return sc
