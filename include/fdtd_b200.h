@@ -285,8 +285,9 @@ int fdtd_bloch_last_ms(fdtd_bloch* p, float* ms);
  * fdtd_engine_adjoint_init: allocate and zero the adjoint state.
  * design_boxes holds 6 ints per E component ([i0,i1,j0,j1,k0,k1] in that
  * component's Yee index space; an empty box means none) or is NULL.  Boxes
- * must stay clear of CPML slabs and domain edges, and of the boxes of ADE
- * poles of their component.  max_segment is the longest replay (steps).
+ * must stay clear of CPML slabs and domain edges; they may cover ADE cells
+ * (the design variable is then eps_inf).  max_segment is the longest replay
+ * (steps).
  * Dispersive (ADE) media carry adjoint pole state through the exact transpose
  * of the Debye / Drude / Lorentz recursions (the reference's dispersive reverse
  * runner, witwin/maxwell/fdtd/adjoint/native.py:2104). */

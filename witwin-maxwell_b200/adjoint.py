@@ -110,9 +110,12 @@ class DesignProblem:
         new_region = MaterialRegion(region.lo, region.hi, np.asarray(eps_r, dtype=np.float64))
         return dataclasses.replace(self.scene, material_regions=[new_region] + list(self.scene.material_regions[1:]))
 
-    def forward(self, eps_r: np.ndarray) -> dict:
+    def prepare(self, eps_r: np.ndarray) -> B200FDTD:
+        """Compile the scene with ``eps_r``, create its engine with the adjoint
+        state and (replay) the checkpoint slots; nothing is stepped yet."""
         if self.solver is not None:
             self.solver.close()
+            self.solver = None
         scene = self._scene_with(eps_r)
         cs = compile_scene(scene, self.steps)
         self.region = cs.design
@@ -128,6 +131,12 @@ class DesignProblem:
         if not self.stored:
             n_slots = (self.steps + self.stride - 1) // self.stride
             _lib.check(lib.fdtd_engine_checkpoint_reserve(h, n_slots), "checkpoint_reserve")
+        self.solver = solver
+        return solver
+
+    def forward(self, eps_r: np.ndarray) -> dict:
+        solver = self.prepare(eps_r)
+        lib, h = solver.lib, solver.handle
         ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
         ev[0].record(solver.stream)
         if self.stored:
@@ -140,7 +149,6 @@ class DesignProblem:
         ev[1].record(solver.stream)
         ev[1].synchronize()
         self.timings = {"forward_ms": ev[0].elapsed_time(ev[1])}
-        self.solver = solver
         return solver.monitor_results()
 
     def _seeds(self, grad: dict) -> tuple[torch.Tensor, torch.Tensor]:
@@ -193,6 +201,70 @@ class DesignProblem:
         if self.solver is not None:
             self.solver.close()
             self.solver = None
+
+
+class BatchDesignProblem:
+    """Forward and adjoint gradients of many independent design scenes.
+
+    The forward run steps every scene together through ``B200Batch`` (one CUDA
+    graph per sample block, the scenes' kernels concurrent on their own
+    streams), saving each scene's full-state checkpoint at the start of every
+    ``stride``-step segment; ``backward`` then runs each scene's pipelined
+    checkpoint replay and reverse steps (``fdtd_engine_backward_replay``).
+    Gradients equal those of one ``DesignProblem`` per scene (the reference's
+    per-simulation differentiable runs over its ensemble,
+    witwin/maxwell/execution/ensemble.py:166 and fdtd/adjoint/bridge.py:1444)."""
+
+    def __init__(self, scenes, steps: int, stride: int = 100, device: str = "cuda"):
+        self.problems = [DesignProblem(sc, steps, stride=stride, device=device, history="replay") for sc in scenes]
+        if not self.problems:
+            raise ValueError("empty batch")
+        self.steps = int(steps)
+        self.stride = self.problems[0].stride
+        self.batch = None
+        self.timings: dict = {}
+
+    def forward(self, eps_list) -> list[dict]:
+        from .solver import B200Batch
+
+        if len(eps_list) != len(self.problems):
+            raise ValueError("one eps_r array per scene")
+        self._close_batch()
+        solvers = [p.prepare(e) for p, e in zip(self.problems, eps_list)]
+        self.batch = B200Batch(solvers)
+        stream = solvers[0].stream
+        ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+        ev[0].record(stream)
+        for s0 in range(0, self.steps, self.stride):
+            for s in solvers:
+                s.checkpoint_save(s0 // self.stride)
+            self.batch.step_range(s0, min(s0 + self.stride, self.steps))
+        ev[1].record(stream)
+        ev[1].synchronize()
+        self.timings = {"forward_ms": ev[0].elapsed_time(ev[1])}
+        return [s.monitor_results() for s in solvers]
+
+    def backward(self, grads) -> list[np.ndarray]:
+        if self.batch is None:
+            raise RuntimeError("backward before forward")
+        stream = self.problems[0].solver.stream
+        ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+        ev[0].record(stream)
+        out = [p.backward(g) for p, g in zip(self.problems, grads)]
+        ev[1].record(stream)
+        ev[1].synchronize()
+        self.timings["backward_ms"] = ev[0].elapsed_time(ev[1])
+        return out
+
+    def _close_batch(self):
+        if self.batch is not None:
+            self.batch.close()
+            self.batch = None
+
+    def close(self):
+        self._close_batch()
+        for p in self.problems:
+            p.close()
 
 
 class _DesignFunction(torch.autograd.Function):

@@ -16,10 +16,11 @@
 // with, for a slab term of effective adjoint g_eff and old adjoint psi gq:
 //   g(d) = ik g_eff + c (gq + g_eff),   gq <- b (gq + g_eff).
 // dL/deps of an E cell (ce = dt/eps, de = 1): the update E' = de E + ce curl
-// + S, where every E-phase source coefficient carries the same dt/eps (point
-// dipole current patches -dt/eps J, injection.py:214-396; TFSF corrections,
-// the curl coefficient times an inverse spacing), so
-//   dE'/deps = -(ce curl + S) / eps = -(E^{n+1} - de E^n) ce / dt,
+// + S - A, where every E-phase source coefficient carries the same dt/eps
+// (point dipole current patches -dt/eps J, injection.py:214-396; TFSF and soft
+// surface terms, the curl coefficient times an inverse spacing) and so does
+// the ADE correction A (dt J' / eps, or (P' - P) / eps for Debye), so
+//   dE'/deps = -(ce curl + S - A) / eps = -(E^{n+1} - de E^n) ce / dt,
 // evaluated from the replayed E history of the box.  Sources are affine in the
 // fields: they add nothing to the adjoint recursion itself.
 #include <cuda_runtime.h>
@@ -110,6 +111,25 @@ __device__ __forceinline__ float inv_at(const float* arr, int idx, int n, float 
   return (idx >= 0 && idx < n) ? __ldg(arr + idx) : 0.0f;
 }
 
+// True when every coordinate of (i, j, k) lies in [lo_a + a0, N_a - hi_a - a1]
+// with lo_a, hi_a the CPML slab lengths raised to at least `floor_` (the edge
+// planes are then excluded as well).  Pass A takes a0 = 0, a1 = 2 with floor 1:
+// every E neighbour an H cell reads (coordinates c and c + 1) is then an
+// interior, non-slab E cell of edge mode 0, so each transposed term is +-ce gE.
+// Pass B takes a0 = 1, a1 = 2 with floor 0: the H neighbours (c - 1 and c) are
+// in their extent and outside the slabs, and the E cell itself has edge mode 0
+// and no psi.
+__device__ __forceinline__ bool plain_cell(const StepParams& p, int i, int j, int k, int floor_, int a0, int a1) {
+  const int c[3] = {i, j, k};
+  const int n[3] = {p.NX, p.NY, p.NZ};
+#pragma unroll
+  for (int a = 0; a < 3; ++a) {
+    const int lo = max(p.cpml ? p.slab_lo[a] : 0, floor_), hi = max(p.cpml ? p.slab_hi[a] : 0, floor_);
+    if (c[a] < lo + a0 || c[a] > n[a] - hi - a1) return false;
+  }
+  return true;
+}
+
 // ---- pass A: gH_mid = gH + C_H^T g(d_E) (in place in q.gH) ----
 template <bool kUniform>
 __global__ void adj_pass_a_kernel(const StepParams p, const AdjParams q) {
@@ -122,6 +142,35 @@ __global__ void adj_pass_a_kernel(const StepParams p, const AdjParams q) {
     const float* iex = p.inv_e[0];
     const float* iey = p.inv_e[1];
     const float* iez = p.inv_e[2];
+    if (plain_cell(p, i, j, k, 1, 0, 2)) {
+      // the same sums as below with every term +-u, u = ce gE of the neighbour
+      const int64_t sy = p.P, sx = static_cast<int64_t>(p.NY) * p.P;
+      const float uxk = coef(p.ecurl[0], p.ecurl_u[0], x) * q.gE[0][x];
+      const float uxk1 = coef(p.ecurl[0], p.ecurl_u[0], x + 1) * q.gE[0][x + 1];
+      const float uxj1 = coef(p.ecurl[0], p.ecurl_u[0], x + sy) * q.gE[0][x + sy];
+      const float uyk = coef(p.ecurl[1], p.ecurl_u[1], x) * q.gE[1][x];
+      const float uyk1 = coef(p.ecurl[1], p.ecurl_u[1], x + 1) * q.gE[1][x + 1];
+      const float uyi1 = coef(p.ecurl[1], p.ecurl_u[1], x + sx) * q.gE[1][x + sx];
+      const float uzj1 = coef(p.ecurl[2], p.ecurl_u[2], x + sy) * q.gE[2][x + sy];
+      const float uzi1 = coef(p.ecurl[2], p.ecurl_u[2], x + sx) * q.gE[2][x + sx];
+      const float uz = coef(p.ecurl[2], p.ecurl_u[2], x) * q.gE[2][x];
+      const float ez0 = inv_at<kUniform>(iez, k, p.NZ, p.inv_e_u[2]), ez1 = inv_at<kUniform>(iez, k + 1, p.NZ, p.inv_e_u[2]);
+      const float ey0 = inv_at<kUniform>(iey, j, p.NY, p.inv_e_u[1]), ey1 = inv_at<kUniform>(iey, j + 1, p.NY, p.inv_e_u[1]);
+      const float ex0 = inv_at<kUniform>(iex, i, p.NX, p.inv_e_u[0]), ex1 = inv_at<kUniform>(iex, i + 1, p.NX, p.inv_e_u[0]);
+      float g = q.gH[0][x];
+      g += ez0 * uyk - ez1 * uyk1;
+      g += ey0 * -uz - ey1 * -uzj1;
+      q.gH[0][x] = g;
+      g = q.gH[1][x];
+      g += ez0 * -uxk - ez1 * -uxk1;
+      g += ex0 * uz - ex1 * uzi1;
+      q.gH[1][x] = g;
+      g = q.gH[2][x];
+      g += ey0 * uxk - ey1 * uxj1;
+      g += ex0 * -uyk - ex1 * -uyi1;
+      q.gH[2][x] = g;
+      return;
+    }
     if (h_in_extent(p, 0, i, j, k)) {  // Hx: Ey d1b (z), Ez d2b (y)
       float g = q.gH[0][x];
       g += inv_at<kUniform>(iez, k, p.NZ, p.inv_e_u[2]) * e_term_adjoint(p, q, 1, 1, i, j, k) -
@@ -168,13 +217,46 @@ __global__ void __launch_bounds__(128, kPoles ? 5 : 12) adj_pass_b_kernel(const 
     const float* ihx = p.inv_h[0];
     const float* ihy = p.inv_h[1];
     const float* ihz = p.inv_h[2];
+    // interior cells: the same sums with every term +-v, v = ch gH of the neighbour
+    const bool plain = plain_cell(p, i, j, k, 0, 1, 2);
+    float vx0 = 0.f, vxk = 0.f, vxj = 0.f, vy0 = 0.f, vyk = 0.f, vyi = 0.f, vz0 = 0.f, vzj = 0.f, vzi = 0.f;
+    float hz0 = 0.f, hz1 = 0.f, hy0 = 0.f, hy1 = 0.f, hx0 = 0.f, hx1 = 0.f;
+    if (plain) {
+      const int64_t sy = p.P, sx = static_cast<int64_t>(p.NY) * p.P;
+      vx0 = coef(p.hcurl[0], p.hcurl_u[0], x) * q.gH[0][x];
+      vxk = coef(p.hcurl[0], p.hcurl_u[0], x - 1) * q.gH[0][x - 1];
+      vxj = coef(p.hcurl[0], p.hcurl_u[0], x - sy) * q.gH[0][x - sy];
+      vy0 = coef(p.hcurl[1], p.hcurl_u[1], x) * q.gH[1][x];
+      vyk = coef(p.hcurl[1], p.hcurl_u[1], x - 1) * q.gH[1][x - 1];
+      vyi = coef(p.hcurl[1], p.hcurl_u[1], x - sx) * q.gH[1][x - sx];
+      vz0 = coef(p.hcurl[2], p.hcurl_u[2], x) * q.gH[2][x];
+      vzj = coef(p.hcurl[2], p.hcurl_u[2], x - sy) * q.gH[2][x - sy];
+      vzi = coef(p.hcurl[2], p.hcurl_u[2], x - sx) * q.gH[2][x - sx];
+      hz0 = inv_at<kUniform>(ihz, k, p.NZ - 1, p.inv_h_u[2]);
+      hz1 = inv_at<kUniform>(ihz, k - 1, p.NZ - 1, p.inv_h_u[2]);
+      hy0 = inv_at<kUniform>(ihy, j, p.NY - 1, p.inv_h_u[1]);
+      hy1 = inv_at<kUniform>(ihy, j - 1, p.NY - 1, p.inv_h_u[1]);
+      hx0 = inv_at<kUniform>(ihx, i, p.NX - 1, p.inv_h_u[0]);
+      hx1 = inv_at<kUniform>(ihx, i - 1, p.NX - 1, p.inv_h_u[0]);
+    }
     for (int c = 0; c < 3; ++c) {
-      const int m = e_mode(p, c, i, j, k);
+      const int m = plain ? 0 : e_mode(p, c, i, j, k);
       if (m == 3 || k >= p.NZ) continue;
       const float gp = q.gE[c][x];
       float g = m == 0 ? coef(p.edecay[c], p.edecay_u[c], x) * gp : (m == 1 ? gp : 0.0f);
       // H-update terms reading this E cell (forward differences of E)
-      if (c == 0) {  // Hy cyb (z), Hz czb (y)
+      if (plain) {
+        if (c == 0) {
+          g += -hz0 * -vy0 + hz1 * -vyk;
+          g += -hy0 * vz0 + hy1 * vzj;
+        } else if (c == 1) {
+          g += -hz0 * vx0 + hz1 * vxk;
+          g += -hx0 * -vz0 + hx1 * -vzi;
+        } else {
+          g += -hy0 * -vx0 + hy1 * -vxj;
+          g += -hx0 * vy0 + hx1 * vyi;
+        }
+      } else if (c == 0) {  // Hy cyb (z), Hz czb (y)
         g += -inv_at<kUniform>(ihz, k, p.NZ - 1, p.inv_h_u[2]) * h_term_adjoint(p, q, 1, 1, i, j, k) +
              inv_at<kUniform>(ihz, k - 1, p.NZ - 1, p.inv_h_u[2]) * h_term_adjoint(p, q, 1, 1, i, j, k - 1);
         g += -inv_at<kUniform>(ihy, j, p.NY - 1, p.inv_h_u[1]) * h_term_adjoint(p, q, 2, 1, i, j, k) +
@@ -193,7 +275,7 @@ __global__ void __launch_bounds__(128, kPoles ? 5 : 12) adj_pass_b_kernel(const 
       if (m == 0) {
         const float ce = coef(p.ecurl[c], p.ecurl_u[c], x);
         const float u = ce * gp;
-        if (p.cpml) {
+        if (p.cpml && !plain) {
           for (int w = 0; w < 2; ++w) {
             const int axis = w == 0 ? (c == 0 ? 1 : 0) : (c == 2 ? 1 : 2);
             const int extent = axis == 0 ? p.NX : (axis == 1 ? p.NY : p.NZ);
@@ -263,6 +345,10 @@ __global__ void adj_pass_c_kernel(const StepParams p, const AdjParams q) {
     const int j = blockIdx.y, i = blockIdx.z;
     if (k >= p.P) return;
     const int64_t x = (static_cast<int64_t>(i) * p.NY + j) * p.P + k;
+    // cells outside every slab have nothing to do when no H component decays
+    bool unit = true;
+    for (int c = 0; c < 3; ++c) unit = unit && !p.hdecay[c] && p.hdecay_u[c] == 1.0f;
+    if (unit && plain_cell(p, i, j, k, 0, 0, 2)) return;
     for (int c = 0; c < 3; ++c) {
       if (!h_in_extent(p, c, i, j, k)) continue;
       // With unit magnetic decay (no magnetic loss) gH = gH_mid already: only

@@ -2327,12 +2327,12 @@ int fdtd_engine_adjoint_init(fdtd_engine* h, const int* design_boxes, int max_se
       if (b[2 * ax] < h->desc.pml_lo[ax] || b[2 * ax + 1] > n_ax - 1 - h->desc.pml_hi[ax])
         return fail(FDTD_ERR_INVALID_ARG, "design box reaches into a CPML slab or the domain edge");
     }
-    // dE'/deps of a design cell assumes no ADE current there
-    for (const auto& ph : h->poles) {
-      const PoleTerm& t = ph.t;
-      if (t.comp == c && b[0] < t.i1 && t.i0 < b[1] && b[2] < t.j1 && t.j0 < b[3] && b[4] < t.k1 && t.k0 < b[5])
-        return fail(FDTD_ERR_INVALID_ARG, "design box overlaps a dispersive (ADE) region");
-    }
+    // Design cells may sit in ADE media (the design variable is then eps_inf):
+    // the pole correction -dt inv J' (Drude, Lorentz) or -inv (P' - P) (Debye)
+    // carries inv = 1 / eps like the curl and source terms, so
+    // dE'/deps = -(E^{n+1} - de E^n) / eps covers it, and the pole states
+    // themselves depend on eps only through E (witwin/maxwell/fdtd/adjoint/
+    // native.py:2104-2290, reverseDispersiveCorrection3D).
     for (int ax = 0; ax < 3; ++ax) {
       d.lo[ax] = b[2 * ax];
       d.hi[ax] = b[2 * ax + 1];

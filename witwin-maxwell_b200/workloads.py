@@ -78,7 +78,7 @@ def adjoint_160(steps: int = 3000, seed: int = 0, scale: int = 1) -> Scene:
     """Adjoint-gradient workload: 160x160x96 cells, 10-cell CPML; eps 2.1 substrate for
     z < 40; a 64x64x16 MaterialRegion design block at x, y in [48, 112), z in [40, 56)
     with eps_r ~ U[1, 12) i.i.d. (torch.Generator().manual_seed(seed)); a soft +z Ey
-    GaussianBeam (waist 0.5 um, focused on the design block's centre) launched from the
+    GaussianBeam (waist 1 um, focused on the design block's centre) launched from the
     substrate, 300 THz CW after a 200-step raised-cosine ramp; the objective's monitor is
     the 16x16 patch of E on the plane z = 80 at 300 THz.  ``scale`` > 1 divides every
     length but the 10-cell CPML by it (the same layout on a smaller grid, for checks
@@ -95,7 +95,7 @@ def adjoint_160(steps: int = 3000, seed: int = 0, scale: int = 1) -> Scene:
     eps_r = (1.0 + 11.0 * torch.rand(shape, generator=gen, dtype=torch.float64)).numpy()
     sc.material_regions.append(MaterialRegion((s_(48), s_(48), s_(40)), (s_(112), s_(112), s_(56)), eps_r))
     dt = sc.resolve_dt()
-    sc.sources.append(GaussianBeam((0.0, 0.0, 1.0), (0.0, 1.0, 0.0), 0.5e-6 / scale, (s_(80), s_(80), s_(48)),
+    sc.sources.append(GaussianBeam((0.0, 0.0, 1.0), (0.0, 1.0, 0.0), 1.0e-6 / scale, (s_(80), s_(80), s_(48)),
                                    CW(300e12, ramp_time=200 * dt)))
     sc.monitors.append(PlaneMonitor("patch", 2, s_(80), ("Ex", "Ey", "Ez"), (300e12,), (s_(72), s_(72)),
                                     (s_(72) + 16 // scale - 1, s_(72) + 16 // scale - 1)))
@@ -103,13 +103,17 @@ def adjoint_160(steps: int = 3000, seed: int = 0, scale: int = 1) -> Scene:
 
 
 def batched_designs(n_scenes: int = 32, seed: int = 1, size_range: tuple[int, int] = (64, 192), pml: int = 8,
-                    n_freq: int = 8) -> list[Scene]:
+                    n_freq: int = 8, design: bool = False) -> list[Scene]:
     """Batched design workload: ``n_scenes`` independent scenes whose cell counts per axis
     are drawn uniformly from ``size_range`` (numpy.random.default_rng(seed)); 8-cell CPML;
     4-8 boxes per scene (seeded positions and sizes) of diagonal anisotropic permittivity
     with eps_xx, eps_yy, eps_zz ~ U[1, 6]; an Ez point dipole (300/100 THz pulse) at the
-    centre; an 8-frequency (250-350 THz) point monitor of all six components."""
+    centre; an 8-frequency (250-350 THz) point monitor of all six components.  With
+    ``design`` each scene also gets an 8x8x8-cell MaterialRegion (eps_r ~ U[1, 6) from
+    numpy.random.default_rng([seed, 7]), so the scenes are the same with or without it)
+    between the dipole and the probe, for per-scene adjoint gradients."""
     rng = np.random.default_rng(seed)
+    design_rng = np.random.default_rng([seed, 7])
     lo_n, hi_n = size_range
     freqs = tuple(np.linspace(250e12, 350e12, n_freq))
     scenes = []
@@ -127,6 +131,10 @@ def batched_designs(n_scenes: int = 32, seed: int = 1, size_range: tuple[int, in
         sc.sources.append(PointDipole(centre, "Ez", GaussianPulse(300e12, 100e12), width=SPACING))
         probe = (centre[0] + cells[0] // 4, centre[1], centre[2])
         sc.monitors.append(PointMonitor("probe", probe, frequencies=freqs))
+        if design:
+            lo = (centre[0] + 2, centre[1] - 4, centre[2] - 4)
+            eps_r = design_rng.uniform(1.0, 6.0, size=(8, 8, 8))
+            sc.material_regions.append(MaterialRegion(lo, tuple(v + 8 for v in lo), eps_r))
         scenes.append(sc)
     return scenes
 
