@@ -77,6 +77,32 @@ def test_bf16_storage_error_bound():
     assert errs and max(errs.values()) <= BF16_TOL, errs
 
 
+def test_dispersive_workload_2000_steps_against_fp64():
+    """The dispersive workload's layout at 96^3 (8-cell CPML, the Drude slab stopped
+    at the CPML) over its 2000 steps: each monitor's relative L2 against the FP64
+    oracle for FP32, FP16 and BF16 storage.  Bars: FP32 <= 1e-5 (the parity form),
+    FP16 <= 5e-3, BF16 <= 5e-2; the measured values are printed."""
+    wm = load_package()
+    steps = 2000
+    scene = wm.workloads.dispersive_256(cells=96, pml=8, slab_through_pml=False)
+    cs = wm.compile_scene(scene, steps)
+    ref = orc.OracleSimulation(cs, "f64").run(steps)
+    refm = ref.monitor_results()
+    ref.close()
+    norms = {m: sum(float(np.linalg.norm(v)) ** 2 for v in d.values()) ** 0.5 for m, d in refm.items()}
+    live = [m for m in refm if norms[m] > 1e-3 * max(norms.values())]
+    report = {}
+    for storage, bar in (("fp32", 1e-5), ("fp16", 5e-3), ("bf16", 5e-2)):
+        solver = wm.solver.B200FDTD(cs, storage=storage).init_field()
+        solver.step_range(0, steps)
+        got = {k: {c: v.cpu().numpy() for c, v in d.items()} for k, d in solver.monitor_results().items()}
+        solver.close()
+        errs = {m: joint_rel_l2(got[m], refm[m]) for m in live}
+        report[storage] = {m: float(f"{e:.3e}") for m, e in errs.items()}
+        assert max(errs.values()) <= bar, (storage, errs)
+    print("monitor rel. L2 vs FP64, dispersive layout 96^3, 2000 steps:", report)
+
+
 def test_reduced_storage_state_round_trip_and_limits():
     """Packing a field into FP16 storage and reading it back rounds each value
     to FP16 relative precision (scales are exact powers of two); scales are
