@@ -619,6 +619,43 @@ def run_adjoint_bench(wm, device):
     return out
 
 
+def run_xslab_arm(args, wm, world, rank, local):
+    """Strong scaling of one dispersive workload split into x slabs over the ranks
+    (``--decomp xslab``; witwin-maxwell_b200/distributed.py): every rank steps its
+    slab with one ghost plane per cut and exchanges halo planes with its chain
+    neighbours once per step (NCCL point-to-point).  Only the one-rank form runs
+    on a single GPU; the exchange itself is tested on CPU ranks (gloo) and as
+    ranks of one process on one GPU."""
+    import torch
+
+    device = torch.device("cuda", local)
+    torch.cuda.set_device(device)
+    total = args.warmup + args.steps + 4
+    cs = wm.compile_scene(wm.workloads.dispersive_256(cells=args.cells), total)
+    run = wm.distributed.XSlabRun(cs, rank, world, device=device, sample_block=args.sample_block)
+    for n in range(args.warmup):
+        run.step(n)
+    torch.cuda.synchronize(device)
+    barrier(world)
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+    ev[0].record()
+    for n in range(args.warmup, args.warmup + args.steps):
+        run.step(n)
+    ev[1].record()
+    ev[1].synchronize()
+    barrier(world)
+    elapsed_s = max_over_ranks(ev[0].elapsed_time(ev[1]) * 1e-3, world, device)
+    run.close()
+    return {
+        "metric": METRIC, "value": cs.cells * args.steps / elapsed_s / 1e9, "unit": METRIC, "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": elapsed_s * 1e3 / args.steps,
+        "higher_is_better": True, "scaling": "strong", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "cells": int(cs.cells), "parallelism": f"x-slabs x{world}",
+                   "slab_planes": [list(r) for r in wm.distributed.split_planes(cs.nodes[0], world)],
+                   "l2": "working set far larger than the 126 MB L2; no flush needed"},
+    }
+
+
 def run_e2e(args, wm, cs, device, world):
     """Gcell-updates/s of Simulation-style solve from host buffers: upload the compiled
     scene tensors from host memory, run the steps, read the monitor spectra back."""
@@ -696,6 +733,8 @@ def main():
                     help="skip the forward+adjoint timing of the 160x160x96 design workload")
     ap.add_argument("--no-reference-gpu", dest="reference_gpu", action="store_false",
                     help="reference arm: skip the timing of the reference's own CUDA ops")
+    ap.add_argument("--decomp", choices=("replicas", "xslab"), default="replicas",
+                    help="N > 1: independent replicas (the default) or one workload split into x slabs")
     ap.add_argument("--cells", type=int, default=256,
                     help="cells per axis of the (scaled) workload; 256 is the benchmark, smaller sizes are for profiling")
     args = ap.parse_args()
@@ -707,6 +746,8 @@ def main():
     try:
         if args.impl == "reference":
             line = run_reference_arm(args, wm, world, rank)
+        elif args.decomp == "xslab":
+            line = run_xslab_arm(args, wm, world, rank, local)
         else:
             line = run_b200_arm(args, wm, world, rank, local)
         if rank == 0 and line is not None:

@@ -176,6 +176,18 @@ int fdtd_engine_finalize(fdtd_engine* h);
 int fdtd_engine_step_range(fdtd_engine* h, int n0, int n1);
 /* Flush buffered monitor samples into the DFT accumulators now. */
 int fdtd_engine_flush(fdtd_engine* h);
+/* on = 0: fdtd_engine_step_range no longer flushes at the end of every range
+ * (only every sample_block steps); call fdtd_engine_flush before reading the
+ * spectra.  For callers that advance one step per call (the x-slab halo
+ * exchange). */
+int fdtd_engine_set_range_flush(fdtd_engine* h, int on);
+/* One x plane i of component comp's current state in the component's Yee
+ * shape [ny_c][nz_c], to (get) or from (set) a device or host buffer, on the
+ * engine's stream; FP32 storage.  The x-slab decomposition moves its halo
+ * planes with them (witwin/maxwell/fdtd/distributed/nccl_transport.py:14-24,
+ * one plane per face per step). */
+int fdtd_engine_get_plane(fdtd_engine* h, int comp, int i, float* dst);
+int fdtd_engine_set_plane(fdtd_engine* h, int comp, int i, const float* src);
 
 /* Checkpoints of the full time-stepping state (fields, psi, ADE state),
  * witwin/maxwell/fdtd/checkpoint.py:365-568. */

@@ -91,6 +91,9 @@ _SIGNATURES = {
     "fdtd_engine_step_range_recorded": ([_vp, _i, _i], _i),
     "fdtd_engine_adjoint_range": ([_vp, _i, _i], _i),
     "fdtd_engine_backward_replay": ([_vp, _i, _i], _i),
+    "fdtd_engine_set_range_flush": ([_vp, _i], _i),
+    "fdtd_engine_get_plane": ([_vp, _i, _i, _vp], _i),
+    "fdtd_engine_set_plane": ([_vp, _i, _i, _vp], _i),
     "fdtd_engine_adjoint_grad": ([_vp, _i, _vp], _i),
     "fdtd_engine_adjoint_pack": ([_vp, _i, _i, _i, _vp], _i),
     "fdtd_engine_adjoint_unpack": ([_vp, _i, _i, _i, _vp], _i),

@@ -513,6 +513,7 @@ struct fdtd_engine {
   float* samples = nullptr;
   int M = 32;
   int pending = 0;
+  bool range_flush = true;  // flush the buffered monitor samples at the end of every step range
   int pending_base = 0;
   // DFT
   int n_freq = 0, dft_steps = 0;
@@ -2037,7 +2038,7 @@ static int step_range_impl(fdtd_engine* h, int n0, int n1, bool record) {
   }
   // The DFT of every step in the range is accumulated before the range ends,
   // so the range's device time holds all of its monitor work.
-  {
+  if (h->range_flush) {
     const int rc = flush_samples(h);
     if (rc) return rc;
   }
@@ -2242,6 +2243,39 @@ int fdtd_engine_set_ade_pass(fdtd_engine* h, int on) {
   if (!h) return fail(FDTD_ERR_INVALID_ARG, "null engine");
   h->ade_pass = on != 0;
   return 0;
+}
+
+int fdtd_engine_set_range_flush(fdtd_engine* h, int on) {
+  if (!h) return fail(FDTD_ERR_INVALID_ARG, "null engine");
+  h->range_flush = on != 0;
+  return 0;
+}
+
+// One x plane of a component's current state, in the component's Yee shape
+// [ny_c][nz_c], to or from a device or host buffer (one strided 2-D copy on
+// the engine's stream).
+static int plane_copy(fdtd_engine* h, int comp, int i, float* out, const float* in) {
+  if (!h || comp < 0 || comp > 5 || (!out && !in)) return fail(FDTD_ERR_INVALID_ARG, "bad plane arguments");
+  if (!h->finalized) return fail(FDTD_ERR_STATE, "engine not finalized");
+  if (h->storage != kStoreF32) return fail(FDTD_ERR_UNSUPPORTED, "plane copies need FP32 field storage");
+  int ext[3];
+  comp_extent(comp, h->NX, h->NY, h->NZ, ext);
+  if (i < 0 || i >= ext[0]) return fail(FDTD_ERR_INVALID_ARG, "plane index outside the component's x extent");
+  float* base = (comp < 3 ? h->E[h->cur][comp] : h->H[h->cur][comp - 3]) + static_cast<int64_t>(i) * h->NY * h->P;
+  const size_t row = sizeof(float) * ext[2], pitch = sizeof(float) * h->P;
+  if (out)
+    CUDA_TRY(cudaMemcpy2DAsync(out, row, base, pitch, row, ext[1], cudaMemcpyDefault, h->stream));
+  else
+    CUDA_TRY(cudaMemcpy2DAsync(base, pitch, in, row, row, ext[1], cudaMemcpyDefault, h->stream));
+  return 0;
+}
+
+int fdtd_engine_get_plane(fdtd_engine* h, int comp, int i, float* dst) {
+  return dst ? plane_copy(h, comp, i, dst, nullptr) : fail(FDTD_ERR_INVALID_ARG, "null plane buffer");
+}
+
+int fdtd_engine_set_plane(fdtd_engine* h, int comp, int i, const float* src) {
+  return src ? plane_copy(h, comp, i, nullptr, src) : fail(FDTD_ERR_INVALID_ARG, "null plane buffer");
 }
 
 int fdtd_engine_set_wait_limit(fdtd_engine* h, int rounds) {
