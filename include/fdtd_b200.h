@@ -356,6 +356,37 @@ int fdtd_op_update_magnetic(int comp, int mode, int nx, int ny, int nz, float* f
                             const float* ika, const float* ba, const float* ca, const float* ikb,
                             const float* bb, const float* cb, const int* slab, void* stream);
 
+/* Complex E update on Bloch faces (electric.cu:356-453, update_electric_e*_bloch;
+ * z_standard = 1: Ex / Ey with Bloch y / x and a standard z difference with
+ * boundary modes z_low_mode / z_high_mode, electric.cu:1164-1528,
+ * update_electric_e{x,y}_bloch_{y,x}_standard_z).  (nx, ny, nz) is the E
+ * component's shape; first/second as in fdtd_op_update_electric (Ex: Hy, Hz;
+ * Ey: Hx, Hz; Ez: Hx, Hy), each as real and imaginary arrays; phases a / b and
+ * inv_a / inv_b in the reference's order (Ex: y, z; Ey: x, z; Ez: x, y); decay
+ * and curl are E-shaped arrays. */
+int fdtd_op_update_electric_bloch(int comp, int z_standard, int nx, int ny, int nz, float* e_re, float* e_im,
+                                  const float* first_re, const float* first_im, const float* second_re,
+                                  const float* second_im, const float* decay, const float* curl, float phase_cos_a,
+                                  float phase_sin_a, float phase_cos_b, float phase_sin_b, const float* inv_a,
+                                  const float* inv_b, int z_low_mode, int z_high_mode, void* stream);
+/* z-CPML correction of Ex (comp 0, its H is Hy, t axis y) or Ey (comp 1, Hx,
+ * t axis x) over a region of fshape at offset in the full grid (the per-axis
+ * CPML corrections of the Bloch-x/y + CPML-z scenes, electric.cu:1164-1528,
+ * apply_electric_e{x,y}_cpml_z_correction): field, curl and psi are
+ * region-shaped, h has the full shape hshape, inv_kappa / b / c / inv_dz are
+ * full-length z profiles; full_size_t / full_size_z are the full E extents
+ * along t and z. */
+int fdtd_op_apply_cpml_z_correction(int comp, float* field, const int* fshape, const float* h, const int* hshape,
+                                    const float* curl, float* psi, const float* inv_kappa, const float* b,
+                                    const float* c, const float* inv_dz, const int* offset, int low_mode,
+                                    int high_mode, int full_size_t, int full_size_z, void* stream);
+/* Face projection of a periodic field along axis (projection.cu:43-60,
+ * project_periodic_boundary) and of a Bloch field with phase e^{ikL}
+ * (projection.cu:62-125, project_bloch_boundary). */
+int fdtd_op_project_periodic(float* field, const int* fshape, int axis, void* stream);
+int fdtd_op_project_bloch(float* field_re, float* field_im, const int* fshape, int axis, float phase_cos,
+                          float phase_sin, void* stream);
+
 /* Electric update of component comp (0 Ex, 1 Ey, 2 Ez) with boundary-mode-aware
  * backward differences; modes = {a_low, a_high, b_low, b_high} boundary codes;
  * witwin/maxwell/fdtd/cuda/kernels/electric.cu:242-941 (update_electric_e*_{standard,cpml,cpml_compressed}).

@@ -303,6 +303,65 @@ def op_vectors(tr, rng) -> dict:
                                          time=1.1e-14, frequency=300e12, fwidth=100e12, amplitude=1.3, phase=0.2,
                                          delay=9.5e-15, causalGate=gate)
         out[f"out_shift_{kind}_{gate}"] = f.numpy()
+    # complex E updates on Bloch faces (electric.cu:356-453, 1164-1528)
+    cplx = {n: (rng.standard_normal(sh), rng.standard_normal(sh)) for n, sh in S.items()}
+    for n, (re_, im_) in cplx.items():
+        out[f"bl_{n}_re"], out[f"bl_{n}_im"] = re_, im_
+    phase = {a: (float(np.cos(0.3 + 0.5 * i)), float(np.sin(0.3 + 0.5 * i))) for i, a in enumerate("XYZ")}
+    bl_coef = {n: (rng.uniform(0.5, 1.0, S[n]), rng.uniform(0.1, 0.5, S[n])) for n in ("Ex", "Ey", "Ez")}
+    for n, (dcy, crl) in bl_coef.items():
+        out[f"bl_{n}_decay"], out[f"bl_{n}_curl"] = dcy, crl
+    spec = {"Ex": ("Hy", "Hz", "Y", "Z"), "Ey": ("Hx", "Hz", "X", "Z"), "Ez": ("Hx", "Hy", "X", "Y")}
+    variants = [(n, None) for n in ("Ex", "Ey", "Ez")] + [("Ex", (5, 2)), ("Ey", (0, 5))]
+    for comp, zmodes in variants:
+        first, second, a, b = spec[comp]
+        kw = {f"{comp}Real": t(cplx[comp][0]), f"{comp}Imag": t(cplx[comp][1]),
+              f"{first}Real": t(cplx[first][0]), f"{first}Imag": t(cplx[first][1]),
+              f"{second}Real": t(cplx[second][0]), f"{second}Imag": t(cplx[second][1]),
+              f"{comp}Decay": t(bl_coef[comp][0]), f"{comp}Curl": t(bl_coef[comp][1]),
+              f"phaseCos{a}": phase[a][0], f"phaseSin{a}": phase[a][1],
+              f"invD{a.lower()}": t(inv[a.lower()]), f"invD{b.lower()}": t(inv[b.lower()])}
+        if zmodes is None:
+            kw[f"phaseCos{b}"], kw[f"phaseSin{b}"] = phase[b]
+            name = f"updateElectricField{comp}Bloch3D"
+            key = f"out_bl_{comp}"
+        else:
+            kw["zLowBoundaryMode"], kw["zHighBoundaryMode"] = zmodes
+            name = "updateElectricFieldExBlochYStandardZ3D" if comp == "Ex" else "updateElectricFieldEyBlochXStandardZ3D"
+            key = f"out_blz_{comp}"
+        K[name](**kw)
+        out[f"{key}_re"], out[f"{key}_im"] = kw[f"{comp}Real"].numpy(), kw[f"{comp}Imag"].numpy()
+    out["bl_phase"] = np.array([phase[a] for a in "XYZ"])
+    # z-CPML corrections of Ex / Ey over a region (Bloch-x/y + CPML-z scenes)
+    nzf = nodes[2]
+    prof = {k: rng.uniform(0.2, 1.0, nzf) for k in ("ik", "b", "c")}
+    out.update(cz_ik=prof["ik"], cz_b=prof["b"], cz_c=prof["c"])
+    for comp, h, off, region, t_ax, modes in (("Ex", "Hy", (1, 0, 0), (4, 6, 5), "Y", (1, 5)),
+                                               ("Ey", "Hx", (0, 1, 0), (7, 3, 5), "X", (5, 4))):
+        fld = rng.standard_normal(region)
+        crl = rng.uniform(0.1, 0.5, region)
+        psi = rng.standard_normal(region)
+        hh = rng.standard_normal(S[h])
+        out.update({f"cz_{comp}_field": fld, f"cz_{comp}_curl": crl, f"cz_{comp}_psi": psi, f"cz_{comp}_h": hh})
+        f, pz = t(fld), t(psi)
+        K[f"applyElectricField{comp}CpmlZCorrection3D"](
+            **{comp: f, h: t(hh), f"{comp}Curl": t(crl), f"Psi{comp}Z": pz, f"InvKappa{comp}Z": t(prof["ik"]),
+               f"B{comp}Z": t(prof["b"]), f"C{comp}Z": t(prof["c"]), "invDz": t(inv["z"]), "offsetI": off[0],
+               "offsetJ": off[1], "offsetK": off[2], f"{t_ax.lower()}LowBoundaryMode": modes[0],
+               f"{t_ax.lower()}HighBoundaryMode": modes[1], f"fullSize{t_ax}": S[comp][0 if t_ax == "X" else 1],
+               "fullSizeZ": nzf})
+        out[f"out_cz_{comp}"], out[f"out_cz_{comp}_psi"] = f.numpy(), pz.numpy()
+    # periodic and Bloch face projections (projection.cu:43-125)
+    pf = rng.standard_normal((5, 4, 6))
+    pim = rng.standard_normal((5, 4, 6))
+    out.update(proj_re=pf, proj_im=pim)
+    for axis in range(3):
+        f = t(pf)
+        K["projectPeriodicBoundary3D"](field=f, axis=axis)
+        out[f"out_proj_per_{axis}"] = f.numpy()
+        fr, fi = t(pf), t(pim)
+        K["projectBlochBoundary3D"](fieldReal=fr, fieldImag=fi, axis=axis, phaseCos=0.6, phaseSin=0.8)
+        out[f"out_proj_bl_{axis}_re"], out[f"out_proj_bl_{axis}_im"] = fr.numpy(), fi.numpy()
     return out
 
 

@@ -194,3 +194,55 @@ def test_backend_rejects_bad_arguments(mod):
     h = torch.zeros((4, 3, 3), device="cuda", dtype=torch.float64)
     with pytest.raises(ValueError):
         mod.updateMagneticFieldHxStandard3D(Hx=h, Ey=h, Ez=h, HxDecay=h, HxCurl=h, invDy=h, invDz=h).launchRaw()
+
+
+_BLOCH_E = {"Ex": ("Hy", "Hz", "Y", "Z"), "Ey": ("Hx", "Hz", "X", "Z"), "Ez": ("Hx", "Hy", "X", "Y")}
+
+
+@pytest.mark.parametrize("comp,zmodes", [("Ex", None), ("Ey", None), ("Ez", None), ("Ex", (5, 2)), ("Ey", (0, 5))])
+def test_bloch_electric_ops(ops, mod, comp, zmodes):
+    first, second, a, b = _BLOCH_E[comp]
+    phase = {ax: tuple(ops["bl_phase"][i]) for i, ax in enumerate("XYZ")}
+    inv = {a: ops[f"inv_e_{a}"] for a in "xyz"}
+    kw = {f"{comp}Real": g(ops[f"bl_{comp}_re"]), f"{comp}Imag": g(ops[f"bl_{comp}_im"]),
+          f"{first}Real": g(ops[f"bl_{first}_re"]), f"{first}Imag": g(ops[f"bl_{first}_im"]),
+          f"{second}Real": g(ops[f"bl_{second}_re"]), f"{second}Imag": g(ops[f"bl_{second}_im"]),
+          f"{comp}Decay": g(ops[f"bl_{comp}_decay"]), f"{comp}Curl": g(ops[f"bl_{comp}_curl"]),
+          f"phaseCos{a}": phase[a][0], f"phaseSin{a}": phase[a][1],
+          f"invD{a.lower()}": g(inv[a.lower()]), f"invD{b.lower()}": g(inv[b.lower()])}
+    if zmodes is None:
+        kw[f"phaseCos{b}"], kw[f"phaseSin{b}"] = phase[b]
+        name, key = f"updateElectricField{comp}Bloch3D", f"out_bl_{comp}"
+    else:
+        kw["zLowBoundaryMode"], kw["zHighBoundaryMode"] = zmodes
+        name = "updateElectricFieldExBlochYStandardZ3D" if comp == "Ex" else "updateElectricFieldEyBlochXStandardZ3D"
+        key = f"out_blz_{comp}"
+    getattr(mod, name)(**kw).launchRaw()
+    close(kw[f"{comp}Real"], ops[f"{key}_re"])
+    close(kw[f"{comp}Imag"], ops[f"{key}_im"])
+
+
+@pytest.mark.parametrize("comp", ["Ex", "Ey"])
+def test_cpml_z_correction_ops(ops, mod, comp):
+    h, off, t_ax, modes, full_t = (("Hy", (1, 0, 0), "Y", (1, 5), 6) if comp == "Ex" else
+                                   ("Hx", (0, 1, 0), "X", (5, 4), 7))
+    f, psi = g(ops[f"cz_{comp}_field"]), g(ops[f"cz_{comp}_psi"])
+    getattr(mod, f"applyElectricField{comp}CpmlZCorrection3D")(
+        **{comp: f, h: g(ops[f"cz_{comp}_h"]), f"{comp}Curl": g(ops[f"cz_{comp}_curl"]), f"Psi{comp}Z": psi,
+           f"InvKappa{comp}Z": g(ops["cz_ik"]), f"B{comp}Z": g(ops["cz_b"]), f"C{comp}Z": g(ops["cz_c"]),
+           "invDz": g(ops["inv_e_z"]), "offsetI": off[0], "offsetJ": off[1], "offsetK": off[2],
+           f"{t_ax.lower()}LowBoundaryMode": modes[0], f"{t_ax.lower()}HighBoundaryMode": modes[1],
+           f"fullSize{t_ax}": full_t, "fullSizeZ": int(ops["nodes"][2])}).launchRaw()
+    close(f, ops[f"out_cz_{comp}"])
+    close(psi, ops[f"out_cz_{comp}_psi"])
+
+
+@pytest.mark.parametrize("axis", [0, 1, 2])
+def test_projection_ops(ops, mod, axis):
+    f = g(ops["proj_re"])
+    mod.projectPeriodicBoundary3D(field=f, axis=axis).launchRaw()
+    close(f, ops[f"out_proj_per_{axis}"])
+    fr, fi = g(ops["proj_re"]), g(ops["proj_im"])
+    mod.projectBlochBoundary3D(fieldReal=fr, fieldImag=fi, axis=axis, phaseCos=0.6, phaseSin=0.8).launchRaw()
+    close(fr, ops[f"out_proj_bl_{axis}_re"])
+    close(fi, ops[f"out_proj_bl_{axis}_im"])

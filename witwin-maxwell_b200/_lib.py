@@ -110,6 +110,12 @@ _SIGNATURES = {
     "fdtd_op_update_lorentz": ([_i64, _vp, _vp, _f, _f, _f, _vp, _vp, _vp], _i),
     "fdtd_op_apply_polarization": ([_i64, _vp, _vp, _f, _vp, _vp], _i),
     "fdtd_op_add_source_patch": ([_vp, _c_int_p, _vp, _c_int_p, _c_int_p, _f, _vp], _i),
+    "fdtd_op_update_electric_bloch": ([_i, _i, _i, _i, _i, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _f, _f, _f, _f,
+                                      _vp, _vp, _i, _i, _vp], _i),
+    "fdtd_op_apply_cpml_z_correction": ([_i, _vp, _c_int_p, _vp, _c_int_p, _vp, _vp, _vp, _vp, _vp, _vp, _c_int_p,
+                                         _i, _i, _i, _i, _vp], _i),
+    "fdtd_op_project_periodic": ([_vp, _c_int_p, _i, _vp], _i),
+    "fdtd_op_project_bloch": ([_vp, _vp, _c_int_p, _i, _f, _f, _vp], _i),
     "fdtd_op_add_cw_patch": ([_vp, _c_int_p, _vp, _vp, _c_int_p, _c_int_p, _f, _f, _vp], _i),
     "fdtd_op_add_shifted_patch": ([_vp, _c_int_p, _vp, _vp, _vp, _i, _c_int_p, _c_int_p, _i, _f, _f, _f, _f, _f, _f,
                                    _vp], _i),

@@ -14,6 +14,7 @@ from __future__ import annotations
 
 import ctypes
 
+import numpy as np
 import torch
 
 from . import _lib
@@ -137,6 +138,81 @@ def _apply_polarization(*, ElectricField, PolarizationCurrent, InvPermittivity, 
                                                       _stream(ElectricField)), "apply polarization")
 
 
+def _full(t, like, n=None):
+    """A coefficient or spacing argument as a contiguous float32 CUDA tensor: full
+    E-shaped (or n-long) from a one-element tensor or a Python float."""
+    shape = like.shape if n is None else (n,)
+    if not isinstance(t, torch.Tensor):
+        return torch.full(shape, float(t), device=like.device, dtype=torch.float32)
+    if t.numel() == 1 and t.numel() != int(np.prod(shape)):
+        return t.reshape(1).to(device=like.device, dtype=torch.float32).expand(*shape).contiguous()
+    _check_tensor(t, "coefficient")
+    return t
+
+
+# (component, first H, second H, axis a, axis b) of the Bloch E kernels
+_BLOCH_E = {"Ex": ("Hy", "Hz", "Y", "Z"), "Ey": ("Hx", "Hz", "X", "Z"), "Ez": ("Hx", "Hy", "X", "Y")}
+
+
+def _electric_bloch(comp: str, z_standard: bool):
+    first, second, a, b = _BLOCH_E[comp]
+
+    def run(**kw):
+        er, ei = kw[f"{comp}Real"], kw[f"{comp}Imag"]
+        for key in (f"{comp}Real", f"{comp}Imag", f"{first}Real", f"{first}Imag", f"{second}Real", f"{second}Imag"):
+            _check_tensor(kw[key], key)
+        nx, ny, nz = er.shape
+        sizes = {"X": nx, "Y": ny, "Z": nz}
+        decay = _full(kw[f"{comp}Decay"], er)
+        curl = _full(kw[f"{comp}Curl"], er)
+        inv_a = _full(kw[f"invD{a.lower()}"], er, sizes[a])
+        inv_b = _full(kw[f"invD{b.lower()}"], er, sizes[b])
+        pcb = float(kw.get(f"phaseCos{b}", 1.0))
+        psb = float(kw.get(f"phaseSin{b}", 0.0))
+        _lib.check(_lib.load().fdtd_op_update_electric_bloch(
+            "xyz".index(comp[1].lower()), 1 if z_standard else 0, nx, ny, nz, _lib.ptr(er), _lib.ptr(ei),
+            _lib.ptr(kw[f"{first}Real"]), _lib.ptr(kw[f"{first}Imag"]), _lib.ptr(kw[f"{second}Real"]),
+            _lib.ptr(kw[f"{second}Imag"]), _lib.ptr(decay), _lib.ptr(curl), float(kw[f"phaseCos{a}"]),
+            float(kw[f"phaseSin{a}"]), pcb, psb, _lib.ptr(inv_a), _lib.ptr(inv_b),
+            int(kw.get("zLowBoundaryMode", 0)), int(kw.get("zHighBoundaryMode", 0)), _stream(er)),
+            f"update electric {comp} Bloch")
+
+    return run
+
+
+def _cpml_z_correction(comp: str):
+    h, t = ("Hy", "Y") if comp == "Ex" else ("Hx", "X")
+
+    def run(**kw):
+        field = kw[comp]
+        for key in (comp, h, f"{comp}Curl", f"Psi{comp}Z", f"InvKappa{comp}Z", f"B{comp}Z", f"C{comp}Z"):
+            _check_tensor(kw[key], key)
+        inv_dz = _full(kw["invDz"], field, int(kw["fullSizeZ"]))
+        _lib.check(_lib.load().fdtd_op_apply_cpml_z_correction(
+            0 if comp == "Ex" else 1, _lib.ptr(field), _lib.int_array(field.shape), _lib.ptr(kw[h]),
+            _lib.int_array(kw[h].shape), _lib.ptr(kw[f"{comp}Curl"]), _lib.ptr(kw[f"Psi{comp}Z"]),
+            _lib.ptr(kw[f"InvKappa{comp}Z"]), _lib.ptr(kw[f"B{comp}Z"]), _lib.ptr(kw[f"C{comp}Z"]), _lib.ptr(inv_dz),
+            _lib.int_array([kw["offsetI"], kw["offsetJ"], kw["offsetK"]]), int(kw[f"{t.lower()}LowBoundaryMode"]),
+            int(kw[f"{t.lower()}HighBoundaryMode"]), int(kw[f"fullSize{t}"]), int(kw["fullSizeZ"]), _stream(field)),
+            f"{comp} CPML z correction")
+
+    return run
+
+
+def _project_periodic(*, field, axis):
+    _check_tensor(field, "field")
+    _lib.check(_lib.load().fdtd_op_project_periodic(_lib.ptr(field), _lib.int_array(field.shape), int(axis),
+                                                   _stream(field)), "periodic projection")
+
+
+def _project_bloch(*, fieldReal, fieldImag, axis, phaseCos, phaseSin):
+    _check_tensor(fieldReal, "fieldReal")
+    _check_tensor(fieldImag, "fieldImag")
+    _lib.check(_lib.load().fdtd_op_project_bloch(_lib.ptr(fieldReal), _lib.ptr(fieldImag),
+                                                _lib.int_array(fieldReal.shape), int(axis), float(phaseCos),
+                                                float(phaseSin), _stream(fieldReal)), "Bloch projection")
+
+
 def _add_source_patch(*, field, sourcePatch, offsetI, offsetJ, offsetK, signal):
     _check_tensor(field, "field")
     _check_tensor(sourcePatch, "sourcePatch")
@@ -228,7 +304,15 @@ for _c in ("Ex", "Ey", "Ez"):
     _KERNELS[f"updateElectricField{_c}Standard3D"] = _electric(_c, 0)
     _KERNELS[f"updateElectricField{_c}Cpml3D"] = _electric(_c, 1)
     _KERNELS[f"updateElectricField{_c}CpmlCompressed3D"] = _electric(_c, 2)
+for _c in ("Ex", "Ey", "Ez"):
+    _KERNELS[f"updateElectricField{_c}Bloch3D"] = _electric_bloch(_c, False)
+_KERNELS["updateElectricFieldExBlochYStandardZ3D"] = _electric_bloch("Ex", True)
+_KERNELS["updateElectricFieldEyBlochXStandardZ3D"] = _electric_bloch("Ey", True)
 _KERNELS.update({
+    "applyElectricFieldExCpmlZCorrection3D": _cpml_z_correction("Ex"),
+    "applyElectricFieldEyCpmlZCorrection3D": _cpml_z_correction("Ey"),
+    "projectPeriodicBoundary3D": _project_periodic,
+    "projectBlochBoundary3D": _project_bloch,
     "updateDebyeCurrent3D": _debye,
     "updateDrudeCurrent3D": _drude,
     "updateLorentzCurrent3D": _lorentz,

@@ -117,6 +117,36 @@ __device__ __forceinline__ float bdiff(const float* src, int axis, int i, int j,
   return (src[cur] - src[prv]) * iv;
 }
 
+// Bloch-periodic backward difference along `axis` of the complex source
+// (re, im) at the target cell (i, j, k), target extent tsize along the axis:
+// across the wrap the far face enters with the phase e^{-ikL} at the low end
+// and the near face with e^{+ikL} at the high end
+// (witwin/maxwell/fdtd/cuda/kernels/electric.cu:120-240, 356-453).
+__device__ __forceinline__ void bloch_bdiff(const float* re, const float* im, int axis, int i, int j, int k, int tsize,
+                                            int sy, int sz, float pc, float ps, const float* inv, float& dr, float& di) {
+  const int coord = axis == 0 ? i : (axis == 1 ? j : k);
+  const float iv = inv[coord];
+  if (coord == 0 || coord + 1 == tsize) {
+    const int last = tsize - 2;
+    const int64_t l = axis == 0 ? off3(0, j, k, sy, sz) : (axis == 1 ? off3(i, 0, k, sy, sz) : off3(i, j, 0, sy, sz));
+    const int64_t h = axis == 0 ? off3(last, j, k, sy, sz) : (axis == 1 ? off3(i, last, k, sy, sz) : off3(i, j, last, sy, sz));
+    if (coord == 0) {
+      const float nr = pc * re[h] + ps * im[h], ni = pc * im[h] - ps * re[h];
+      dr = (re[l] - nr) * iv;
+      di = (im[l] - ni) * iv;
+    } else {
+      const float pr = pc * re[l] - ps * im[l], pi = ps * re[l] + pc * im[l];
+      dr = (pr - re[h]) * iv;
+      di = (pi - im[h]) * iv;
+    }
+    return;
+  }
+  const int64_t cur = off3(i, j, k, sy, sz);
+  const int64_t prv = axis == 0 ? off3(i - 1, j, k, sy, sz) : (axis == 1 ? off3(i, j - 1, k, sy, sz) : off3(i, j, k - 1, sy, sz));
+  dr = (re[cur] - re[prv]) * iv;
+  di = (im[cur] - im[prv]) * iv;
+}
+
 // witwin/maxwell/fdtd/cuda/kernels/electric.cu:18-119, 242-311, 462-941
 __global__ void op_electric_kernel(int comp, int mode, int nx, int ny, int nz, float* field, const float* first,
                                    const float* second, const float* decay, const float* curl, float decay_u,
@@ -205,6 +235,105 @@ __global__ void op_patch_kernel(float* field, int fx, int fy, int fz, const floa
     const int gi = oi + i, gj = oj + j, gk = ok + k;
     if (gi < 0 || gj < 0 || gk < 0 || gi >= fx || gj >= fy || gk >= fz) continue;
     field[off3(gi, gj, gk, fy, fz)] += signal * patch[x];
+  }
+}
+
+// Complex E update on Bloch faces: E = E decay + curl (d_A second - d_B first)
+// (Ey: d_B first - d_A second), both differences Bloch-wrapped, or the B (z)
+// difference standard with z boundary modes (z_std: the Bloch-x/y,
+// standard-z kernels), electric.cu:356-453, 1164-1528.
+__global__ void op_electric_bloch_kernel(int comp, int z_std, int nx, int ny, int nz, float* er, float* ei,
+                                         const float* fr, const float* fi, const float* sr, const float* si,
+                                         const float* decay, const float* curl, float pca, float psa, float pcb,
+                                         float psb, const float* inv_a, const float* inv_b, int z_lo, int z_hi) {
+  const int64_t total = static_cast<int64_t>(nx) * ny * nz;
+  const int A = comp == 0 ? 1 : 0, B = comp == 2 ? 1 : 2;
+  const int sy2 = ny - (A == 1), sz2 = nz - (A == 2);
+  const int sy1 = ny - (B == 1), sz1 = nz - (B == 2);
+  const int size_a = A == 0 ? nx : (A == 1 ? ny : nz);
+  const int size_b = B == 0 ? nx : (B == 1 ? ny : nz);
+  for (int64_t x = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; x < total;
+       x += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    int i, j, k;
+    unflatten(x, ny, nz, i, j, k);
+    float dar, dai, dbr, dbi;
+    bloch_bdiff(sr, si, A, i, j, k, size_a, sy2, sz2, pca, psa, inv_a, dar, dai);
+    if (z_std) {
+      dbr = bdiff(fr, B, i, j, k, size_b, sy1, sz1, z_lo, z_hi, inv_b);
+      dbi = bdiff(fi, B, i, j, k, size_b, sy1, sz1, z_lo, z_hi, inv_b);
+    } else {
+      bloch_bdiff(fr, fi, B, i, j, k, size_b, sy1, sz1, pcb, psb, inv_b, dbr, dbi);
+    }
+    const float cr = comp == 1 ? (dbr - dar) : (dar - dbr);
+    const float ci = comp == 1 ? (dbi - dai) : (dai - dbi);
+    er[x] = er[x] * decay[x] + curl[x] * cr;
+    ei[x] = ei[x] * decay[x] + curl[x] * ci;
+  }
+}
+
+// z-CPML correction of Ex (t axis y) or Ey (t axis x) over a region at
+// (oi, oj, ok) of the full grid: psi = b psi + c dH/dz, E -/+= curl (dH/dz
+// (1 / kappa - 1) + psi), skipped on inactive t faces (NONE, PEC, PML) and on
+// the first and last global z planes (electric.cu:1164-1528).
+__global__ void op_cpml_z_kernel(int comp, float* field, int sx, int sy, int sz, const float* h, int hy, int hz,
+                                 const float* curl, float* psi, const float* ik, const float* b, const float* c,
+                                 const float* inv_dz, int oi, int oj, int ok, int lo_mode, int hi_mode, int full_t,
+                                 int k0, int k1) {
+  const int nk = k1 - k0;
+  const int64_t total = static_cast<int64_t>(sx) * sy * nk;
+  for (int64_t x = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; x < total;
+       x += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    int li, lj, lk;
+    unflatten(x, sy, nk, li, lj, lk);
+    lk += k0;
+    const int gi = oi + li, gj = oj + lj, gk = ok + lk;
+    const int t = comp == 0 ? gj : gi;
+    const bool lo_off = lo_mode == BND_NONE || lo_mode == BND_PEC || lo_mode == BND_PML;
+    const bool hi_off = hi_mode == BND_NONE || hi_mode == BND_PEC || hi_mode == BND_PML;
+    if ((lo_off && t == 0) || (hi_off && t + 1 == full_t)) continue;
+    const float d = (h[off3(gi, gj, gk, hy, hz)] - h[off3(gi, gj, gk - 1, hy, hz)]) * inv_dz[gk];
+    const int64_t o = off3(li, lj, lk, sy, sz);
+    const float v = b[gk] * psi[o] + c[gk] * d;
+    psi[o] = v;
+    // the z difference enters Ex's curl with a minus sign and Ey's with a plus
+    const float corr = curl[o] * (d * (ik[gk] - 1.0f) + v);
+    field[o] = comp == 0 ? field[o] - corr : field[o] + corr;
+  }
+}
+
+// Face projection of a periodic (im == nullptr: average of the two faces) or
+// Bloch field (the low face least-squares consistent with high = e^{ikL} low,
+// then the high face set from it), projection.cu:43-125.
+__global__ void op_project_kernel(float* re, float* im, int nx, int ny, int nz, int axis, float pc, float ps) {
+  const int da = axis == 0 ? ny : nx, db = axis == 2 ? ny : nz;
+  const int64_t total = static_cast<int64_t>(da) * db;
+  for (int64_t x = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; x < total;
+       x += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    const int a = static_cast<int>(x / db), bb = static_cast<int>(x % db);
+    int64_t lo, hi;
+    if (axis == 0) {
+      lo = off3(0, a, bb, ny, nz);
+      hi = lo + static_cast<int64_t>(nx - 1) * ny * nz;
+    } else if (axis == 1) {
+      lo = off3(a, 0, bb, ny, nz);
+      hi = lo + static_cast<int64_t>(ny - 1) * nz;
+    } else {
+      lo = off3(a, bb, 0, ny, nz);
+      hi = lo + nz - 1;
+    }
+    if (!im) {
+      const float avg = 0.5f * (re[lo] + re[hi]);
+      re[lo] = avg;
+      re[hi] = avg;
+      continue;
+    }
+    const float lr = re[lo], li = im[lo], hr = re[hi], hi_i = im[hi];
+    const float pr = 0.5f * (lr + pc * hr + ps * hi_i);
+    const float pi = 0.5f * (li + pc * hi_i - ps * hr);
+    re[lo] = pr;
+    im[lo] = pi;
+    re[hi] = pc * pr - ps * pi;
+    im[hi] = ps * pr + pc * pi;
   }
 }
 
@@ -454,6 +583,58 @@ int fdtd_op_add_source_patch(float* field, const int* fshape, const float* patch
   op_patch_kernel<<<blocks_for(n), kThreads, 0, static_cast<cudaStream_t>(stream)>>>(
       field, fshape[0], fshape[1], fshape[2], patch, pshape[0], pshape[1], pshape[2], offset[0], offset[1], offset[2], signal);
   return op_launch_check("add_source_patch");
+}
+
+int fdtd_op_update_electric_bloch(int comp, int z_standard, int nx, int ny, int nz, float* e_re, float* e_im,
+                                  const float* first_re, const float* first_im, const float* second_re,
+                                  const float* second_im, const float* decay, const float* curl, float phase_cos_a,
+                                  float phase_sin_a, float phase_cos_b, float phase_sin_b, const float* inv_a,
+                                  const float* inv_b, int z_low_mode, int z_high_mode, void* stream) {
+  if (comp < 0 || comp > 2 || (z_standard && comp == 2) || nx < 2 || ny < 2 || nz < 2 || !e_re || !e_im ||
+      !first_re || !first_im || !second_re || !second_im || !decay || !curl || !inv_a || !inv_b)
+    return op_fail(FDTD_ERR_INVALID_ARG, "update_electric_bloch: bad arguments");
+  const int64_t n = static_cast<int64_t>(nx) * ny * nz;
+  op_electric_bloch_kernel<<<blocks_for(n), kThreads, 0, static_cast<cudaStream_t>(stream)>>>(
+      comp, z_standard ? 1 : 0, nx, ny, nz, e_re, e_im, first_re, first_im, second_re, second_im, decay, curl,
+      phase_cos_a, phase_sin_a, phase_cos_b, phase_sin_b, inv_a, inv_b, z_low_mode, z_high_mode);
+  return op_launch_check("update_electric_bloch");
+}
+
+int fdtd_op_apply_cpml_z_correction(int comp, float* field, const int* fshape, const float* h, const int* hshape,
+                                    const float* curl, float* psi, const float* inv_kappa, const float* b,
+                                    const float* c, const float* inv_dz, const int* offset, int low_mode,
+                                    int high_mode, int full_size_t, int full_size_z, void* stream) {
+  if (comp < 0 || comp > 1 || !field || !fshape || !h || !hshape || !curl || !psi || !inv_kappa || !b || !c ||
+      !inv_dz || !offset)
+    return op_fail(FDTD_ERR_INVALID_ARG, "apply_cpml_z_correction: bad arguments");
+  const int k0 = std::max(0, 1 - offset[2]);
+  const int k1 = std::min(fshape[2], full_size_z - 1 - offset[2]);
+  if (k1 <= k0 || fshape[0] <= 0 || fshape[1] <= 0) return 0;
+  const int64_t n = static_cast<int64_t>(fshape[0]) * fshape[1] * (k1 - k0);
+  op_cpml_z_kernel<<<blocks_for(n), kThreads, 0, static_cast<cudaStream_t>(stream)>>>(
+      comp, field, fshape[0], fshape[1], fshape[2], h, hshape[1], hshape[2], curl, psi, inv_kappa, b, c, inv_dz,
+      offset[0], offset[1], offset[2], low_mode, high_mode, full_size_t, k0, k1);
+  return op_launch_check("apply_cpml_z_correction");
+}
+
+int fdtd_op_project_periodic(float* field, const int* fshape, int axis, void* stream) {
+  if (!field || !fshape || axis < 0 || axis > 2) return op_fail(FDTD_ERR_INVALID_ARG, "project_periodic: bad arguments");
+  const int64_t n = static_cast<int64_t>(axis == 0 ? fshape[1] : fshape[0]) * (axis == 2 ? fshape[1] : fshape[2]);
+  if (n <= 0) return 0;
+  op_project_kernel<<<blocks_for(n), kThreads, 0, static_cast<cudaStream_t>(stream)>>>(
+      field, nullptr, fshape[0], fshape[1], fshape[2], axis, 1.0f, 0.0f);
+  return op_launch_check("project_periodic");
+}
+
+int fdtd_op_project_bloch(float* field_re, float* field_im, const int* fshape, int axis, float phase_cos,
+                          float phase_sin, void* stream) {
+  if (!field_re || !field_im || !fshape || axis < 0 || axis > 2)
+    return op_fail(FDTD_ERR_INVALID_ARG, "project_bloch: bad arguments");
+  const int64_t n = static_cast<int64_t>(axis == 0 ? fshape[1] : fshape[0]) * (axis == 2 ? fshape[1] : fshape[2]);
+  if (n <= 0) return 0;
+  op_project_kernel<<<blocks_for(n), kThreads, 0, static_cast<cudaStream_t>(stream)>>>(
+      field_re, field_im, fshape[0], fshape[1], fshape[2], axis, phase_cos, phase_sin);
+  return op_launch_check("project_bloch");
 }
 
 int fdtd_op_add_cw_patch(float* field, const int* fshape, const float* patch_cos, const float* patch_sin,
