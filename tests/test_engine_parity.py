@@ -350,9 +350,15 @@ def test_engine_rejects_bad_inputs():
     rc = lib.fdtd_engine_create(ctypes.byref(desc), None, ctypes.byref(handle))
     assert rc == -1 and b"at least 3" in lib.fdtd_last_error()
     desc.nx = desc.ny = desc.nz = 10
-    desc.boundary[0] = 5  # PMC face: the per-op path only
+    desc.boundary[0] = 5  # a PMC face with a CPML slab
+    desc.pml_lo[0] = 2
+    rc = lib.fdtd_engine_create(ctypes.byref(desc), None, ctypes.byref(handle))
+    assert rc == -1 and b"PMC" in lib.fdtd_last_error()
+    desc.pml_lo[0] = 0
+    desc.boundary[2] = desc.boundary[3] = 2  # PMC beside periodic faces
     rc = lib.fdtd_engine_create(ctypes.byref(desc), None, ctypes.byref(handle))
     assert rc == -3
+    desc.boundary[2] = desc.boundary[3] = 0
     desc.boundary[0] = 3  # a Bloch low face needs a Bloch high face
     rc = lib.fdtd_engine_create(ctypes.byref(desc), None, ctypes.byref(handle))
     assert rc == -1 and b"must match" in lib.fdtd_last_error()
@@ -401,3 +407,36 @@ def test_bounded_waits_report_timeout_and_leave_the_context_usable():
         solver.close()
     for n in FIELDS:
         np.testing.assert_array_equal(fields[0][n], fields[1][n])
+
+
+@pytest.mark.parametrize("faces", ["mixed", "closed"])
+def test_pmc_faces_against_oracle(faces):
+    """PMC faces in the fused engine (the tangential E on the face updated with
+    the difference across it doubled, electric.cu:18-119) against the FP32 / FP64
+    oracle: PMC beside CPML and PEC faces, and a closed PMC / PEC box with no
+    CPML (the scalar warp kernel then replaces the row-tile default)."""
+    wm = load_package()
+    steps = 300
+    pml, pec, pmc = wm.BOUNDARY_PML, wm.BOUNDARY_PEC, wm.BOUNDARY_PMC
+    boundary = (pmc, pml, pmc, pmc, pec, pml) if faces == "mixed" else (pmc, pmc, pec, pmc, pmc, pec)
+    sc = wm.Scene(cells=(30, 26, 24), spacing=25e-9, pml_cells=6, boundary=boundary)
+    sc.structures.append(wm.Structure(wm.Box((8, 6, 6), (16, 14, 12)), wm.Medium(eps_r=3.0)))
+    sc.structures.append(wm.Structure(wm.Sphere((18, 13, 12), 3.5), wm.Medium.lorentz(2.0, 3.0, 250e12, 20e12)))
+    sc.sources.append(wm.PointDipole((5, 4, 5), "Ey", wm.GaussianPulse(300e12, 100e12), width=25e-9))
+    sc.sources.append(wm.PointDipole((12, 20, 3), "Ex", wm.GaussianPulse(300e12, 100e12), width=25e-9))
+    freqs = (250e12, 300e12)
+    sc.monitors.append(wm.PlaneMonitor("x0", 0, 0, ("Ey", "Ez", "Hx"), freqs))
+    sc.monitors.append(wm.PlaneMonitor("zmid", 2, 12, ("Ex", "Ey", "Hz"), freqs))
+    cs = wm.compile_scene(sc, steps)
+    solver, fields, mons = _run_engine(cs, steps)
+    assert solver.info()["variant"] in (1, 2, 3)
+    ref32 = orc.OracleSimulation(cs, "f32").run(steps)
+    ref64 = orc.OracleSimulation(cs, "f64").run(steps)
+    assert_fields_close(fields, ref32.fields)
+    assert joint_rel_l2(fields, ref64.fields) < 2.0 * joint_rel_l2(ref32.fields, ref64.fields) + 1e-7
+    assert_monitors_close(mons, ref32.monitor_results())
+    # the tangential E on a PMC face is live (a PEC or CPML face would keep it zero)
+    assert float(np.abs(fields["Ey"][0]).max()) > 1e-3 * float(np.abs(fields["Ey"]).max())
+    ref32.close()
+    ref64.close()
+    solver.close()

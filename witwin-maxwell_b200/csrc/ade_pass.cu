@@ -107,6 +107,21 @@ __global__ void __launch_bounds__(256, 4) ade_pass_kernel(const __grid_constant_
       else v[q][2] -= s;
     }
   }
+  // tangential E on PEC faces stays zero (scenes without TFSF,
+  // witwin/maxwell/fdtd/runtime/stepping.py:2316-2318)
+  if (a.pec_faces) {
+    const int pf = a.pec_faces;
+    const bool xf = (i == 0 && (pf & 1)) || (i == a.NX - 1 && (pf & 2));
+    const bool yf = (j == 0 && (pf & 4)) || (j == a.NY - 1 && (pf & 8));
+#pragma unroll
+    for (int q = 0; q < kQ; ++q) {
+      const int k = tl.y + lane + 32 * q;
+      const bool zf = (k == 0 && (pf & 16)) || (k == a.NZ - 1 && (pf & 32));
+      if (yf || zf) v[q][0] = 0.f;
+      if (xf || zf) v[q][1] = 0.f;
+      if (xf || yf) v[q][2] = 0.f;
+    }
+  }
 #pragma unroll
   for (int c = 0; c < 3; ++c) {
     if (!((comps >> c) & 1u)) continue;

@@ -305,6 +305,9 @@ __global__ void __launch_bounds__(128, kPoles ? 5 : 12) adj_pass_b_kernel(const 
       //   Lorentz: J' = a J - r P + b E; P' = P + dt J';  E' -= dt inv J'
       //   Debye:   P' = a P + b E;             E' -= inv (P' - P)
       if (kPoles && (__ldg(p.plane_bits + i) & kPlanePoles)) {
+        // a PEC cell that the forward zeroes after the ADE correction
+        // (pec_clamp) passes no adjoint to the pole currents
+        const float gpc = (m == 2 && p.pec_clamp) ? 0.0f : gp;
         const int pb = __ldg(p.pole_plane_ptr + i), pe = __ldg(p.pole_plane_ptr + i + 1);
         for (int xx = pb; xx < pe; ++xx) {
           const int id = __ldg(p.pole_plane_ids + xx);
@@ -314,21 +317,21 @@ __global__ void __launch_bounds__(128, kPoles ? 5 : 12) adj_pass_b_kernel(const 
           const float inv = __ldg(pt.inv_eps + o), b = __ldg(pt.drive + o);
           if (pt.kind == 1) {
             float* gj = q.gcur[id] + o;
-            const float ge = *gj - pt.dt * inv * gp;
+            const float ge = *gj - pt.dt * inv * gpc;
             g += b * ge;
             *gj = pt.decay * ge;
           } else if (pt.kind == 2) {
             float* gj = q.gcur[id] + o;
             float* gq = q.gpol[id] + o;
-            const float ge = *gj + pt.dt * *gq - pt.dt * inv * gp;
+            const float ge = *gj + pt.dt * *gq - pt.dt * inv * gpc;
             g += b * ge;
             *gj = pt.decay * ge;
             *gq = *gq - pt.restoring * ge;
           } else {
             float* gq = q.gpol[id] + o;
-            const float ge = *gq - inv * gp;
+            const float ge = *gq - inv * gpc;
             g += b * ge;
-            *gq = pt.decay * ge + inv * gp;
+            *gq = pt.decay * ge + inv * gpc;
           }
         }
       }

@@ -448,6 +448,7 @@ struct fdtd_engine {
   // the real channel or imaginary channel of an fdtd_bloch pair); in_pair: the
   // pair runs the wrap kernel and the monitor gather of this engine.
   bool wrap = false;
+  bool pmc = false;  // some face is PMC: the scalar warp kernels (launch variants 1-3) only
   bool bloch = false;
   bool in_pair = false;
   int64_t plane = 0, vol = 0;
@@ -688,6 +689,10 @@ void fill_params(const fdtd_engine* h, StepParams& p) {
   p.warp_class = h->d_warp_class;
   p.status = h->d_status;
   p.wait_limit = h->wait_limit;
+  p.pmc = 0;
+  for (int f = 0; f < 6; ++f)
+    if (h->desc.boundary[f] == FDTD_BND_PMC) p.pmc |= 1 << f;
+  p.pec_clamp = h->lines.empty() ? 1 : 0;
   for (int ph = 0; ph < 2; ++ph) {
     p.term_index[ph] = h->term_ix[ph];
     p.n_terms[ph] = h->n_terms_ph[ph];
@@ -791,7 +796,7 @@ bool ade_pass_active(const fdtd_engine* h) {
 // take (more than its table holds, or the pass switched off) the 64-register
 // warp kernel runs instead.
 bool tile_runs(const fdtd_engine* h) {
-  return h->variant == kTileVariant && h->storage == kStoreF32 && !h->wrap && h->tma_ready &&
+  return h->variant == kTileVariant && h->storage == kStoreF32 && !h->wrap && !h->pmc && h->tma_ready &&
          (h->poles.empty() || ade_pass_active(h));
 }
 
@@ -1085,9 +1090,19 @@ int fdtd_engine_create(const fdtd_grid_desc* desc, void* stream, fdtd_engine** o
   for (int f = 0; f < 6; ++f) {
     const int b = desc->boundary[f];
     const bool wrap = b == FDTD_BND_PERIODIC || b == FDTD_BND_BLOCH;
-    if (b != FDTD_BND_NONE && b != FDTD_BND_PML && b != FDTD_BND_PEC && !wrap)
-      return fail(FDTD_ERR_UNSUPPORTED, "fused engine supports NONE, PML, PEC, periodic and Bloch faces; PMC faces use the per-op path");
+    if (b != FDTD_BND_NONE && b != FDTD_BND_PML && b != FDTD_BND_PEC && b != FDTD_BND_PMC && !wrap)
+      return fail(FDTD_ERR_INVALID_ARG, "unknown boundary code");
     if (wrap && f >= 4) return fail(FDTD_ERR_UNSUPPORTED, "periodic and Bloch faces are supported on x and y");
+    if (b == FDTD_BND_PMC && (f % 2 == 0 ? desc->pml_lo[f / 2] : desc->pml_hi[f / 2]) != 0)
+      return fail(FDTD_ERR_INVALID_ARG, "a PMC face has no CPML slab");
+  }
+  {
+    bool pmc = false, wraps = false;
+    for (int f = 0; f < 6; ++f) {
+      pmc = pmc || desc->boundary[f] == FDTD_BND_PMC;
+      wraps = wraps || desc->boundary[f] == FDTD_BND_PERIODIC || desc->boundary[f] == FDTD_BND_BLOCH;
+    }
+    if (pmc && wraps) return fail(FDTD_ERR_UNSUPPORTED, "PMC faces with periodic or Bloch faces are not supported");
   }
   for (int a = 0; a < 2; ++a) {
     const int lo = desc->boundary[2 * a], hi = desc->boundary[2 * a + 1];
@@ -1107,6 +1122,8 @@ int fdtd_engine_create(const fdtd_grid_desc* desc, void* stream, fdtd_engine** o
     if (desc->boundary[f] == FDTD_BND_PERIODIC || desc->boundary[f] == FDTD_BND_BLOCH) h->wrap = true;
     if (desc->boundary[f] == FDTD_BND_BLOCH) h->bloch = true;
   }
+  for (int f = 0; f < 6; ++f)
+    if (desc->boundary[f] == FDTD_BND_PMC) h->pmc = true;
   h->stream = static_cast<cudaStream_t>(stream);
   h->NX = desc->nx;
   h->NY = desc->ny;
@@ -1172,7 +1189,7 @@ int fdtd_engine_create(const fdtd_grid_desc* desc, void* stream, fdtd_engine** o
   // CPML the slab CTAs run in the warp kernel either way and the hybrid launch
   // measured no faster (CPML vacuum 0.389 against 0.393 ms, the dispersive
   // workload 0.520 against 0.509 ms), so those engines keep variant 2.
-  if (!h->wrap && !h->cpml) h->variant = kTileVariant;
+  if (!h->wrap && !h->cpml && !h->pmc) h->variant = kTileVariant;
   default_tiles(h);
   *out = h;
   return 0;
@@ -1795,6 +1812,12 @@ int fdtd_engine_finalize(fdtd_engine* h) {
     AdeParams& a = h->ade;
     a.NY = h->NY;
     a.P = h->P;
+    a.NX = h->NX;
+    a.NZ = h->NZ;
+    a.pec_faces = 0;
+    if (h->lines.empty())
+      for (int f = 0; f < 6; ++f)
+        if (h->desc.boundary[f] == FDTD_BND_PEC) a.pec_faces |= 1 << f;
     for (size_t b = 0; b < h->poles.size(); ++b) {
       const PoleTerm& t = h->poles[b].t;
       AdePole& q = a.poles[b];
@@ -2164,7 +2187,7 @@ int fdtd_engine_autotune(fdtd_engine* h, int* tile_rows, int* chunk_planes) {
   for (int var = 1; var <= kMaxVariant; ++var) {
     if (var == 4 && !h->tma_ready) continue;
     if (h->storage != kStoreF32 && var != 2) continue;  // reduced storage: the 64-register kernel only
-    if (h->wrap && var > 3) continue;                    // wrap faces: the scalar warp kernels only
+    if ((h->wrap || h->pmc) && var > 3) continue;        // wrap and PMC faces: the scalar warp kernels only
     for (int cx : cxs) {
       if (cx > 2 * h->NX) continue;
       h->variant = var;
@@ -2230,6 +2253,7 @@ int fdtd_engine_set_launch(fdtd_engine* h, int variant, int tile_rows, int chunk
     return fail(FDTD_ERR_UNSUPPORTED, "reduced field storage runs launch variant 2 only");
   if (h->wrap && variant > 3)
     return fail(FDTD_ERR_UNSUPPORTED, "periodic and Bloch faces run launch variants 1-3 only");
+  if (h->pmc && variant > 3) return fail(FDTD_ERR_UNSUPPORTED, "PMC faces run launch variants 1-3 only");
   h->variant = variant;
   if (chunk_planes > 0) h->CX = chunk_planes;
   else default_tiles(h);
@@ -2309,6 +2333,7 @@ int fdtd_engine_adjoint_init(fdtd_engine* h, const int* design_boxes, int max_se
   if (!h->finalized) return fail(FDTD_ERR_STATE, "engine not finalized");
   if (h->storage != kStoreF32) return fail(FDTD_ERR_UNSUPPORTED, "the adjoint runs on FP32 field storage only");
   if (h->wrap) return fail(FDTD_ERR_UNSUPPORTED, "the adjoint of periodic and Bloch faces is not supported");
+  if (h->pmc) return fail(FDTD_ERR_UNSUPPORTED, "the adjoint of PMC faces is not supported");
   if (h->adj.ready) return fail(FDTD_ERR_STATE, "adjoint already initialised");
   AdjointHost& a = h->adj;
   a.q = AdjParams{};

@@ -143,6 +143,15 @@ struct StepParams {
   // in which some warp task has the CPML class; the row-tile kernel runs the
   // others (launch variant 10 on scenes with CPML).
   int shell_only;
+  // PMC faces, bit f for face f (x_lo, x_hi, y_lo, y_hi, z_lo, z_hi): the
+  // tangential E on such a face is updated with the difference across it
+  // doubled (the mirrored H outside is minus the H inside, electric.cu:18-119).
+  int pmc;
+  // 1: tangential E on PEC faces is zeroed after the source terms and the ADE
+  // correction (the reference enforces PEC faces last in scenes without TFSF,
+  // witwin/maxwell/fdtd/runtime/stepping.py:2316-2318); with TFSF the
+  // corrections and sources added after the update stay (0).
+  int pec_clamp;
 };
 
 // A warp task needs the CPML code (some cell of its footprint lies in a slab)
@@ -181,6 +190,9 @@ struct AdeParams {
   const float* Ein[3];
   float* Eout[3];
   int NY, P;
+  // PEC faces (bit f for face f) whose tangential E stays zero after the pass
+  // (StepParams::pec_clamp), and the grid extents the face test needs
+  int pec_faces, NX, NZ;
   AdePole poles[kAdeMaxPoles];
 };
 // ADE pass after the step kernel: tiles are int4 {i * NY + j, k0, k1, pole

@@ -241,6 +241,12 @@ __device__ __forceinline__ void row_plane(const StepParams& p, const Ring<R>& ri
     float v2 = pick(m2, e2 * g2 + c2 * (d2a - d2b), e2);
     if (kTerms && ((pb & kPlaneETerms) || (c.lf & (kLfETermY | kLfETermZ))))
       add_terms(p, 0, 0, n, i, c.j, c.k, pb & kPlaneETerms, c.lf & kLfETermY, c.lf & kLfETermZ, v0, v1, v2);
+    // scenes without TFSF end the E update on PEC faces (stepping.py:2316-2318)
+    if (p.pec_clamp) {
+      if (m0 == 2) v0 = 0.f;
+      if (m1 == 2) v1 = 0.f;
+      if (m2 == 2) v2 = 0.f;
+    }
     __stcg(p.Hout[0] + o, hx);
     __stcg(p.Hout[1] + o, hy);
     __stcg(p.Hout[2] + o, hz);

@@ -374,6 +374,12 @@ __device__ __forceinline__ void tma_march(const StepParams& p, const Ring& ring,
       if (pb & kPlanePoles) ade(p, lane_poles, i, j, k, ec0, ec1, ec2, v0, v1, v2);
       if ((pb & kPlaneETerms) || (lf & (kLfETermY | kLfETermZ)))
         add_terms(p, 0, 0, n, i, j, k, pb & kPlaneETerms, lf & kLfETermY, lf & kLfETermZ, v0, v1, v2);
+      // scenes without TFSF end the E update on PEC faces (stepping.py:2316-2318)
+      if (p.pec_clamp) {
+        if (m0 == 2) v0 = 0.f;
+        if (m1 == 2) v1 = 0.f;
+        if (m2 == 2) v2 = 0.f;
+      }
       __stcg(p.Eout[0] + o + rc, v0);
       __stcg(p.Eout[1] + o + rc, v1);
       __stcg(p.Eout[2] + o + rc, v2);

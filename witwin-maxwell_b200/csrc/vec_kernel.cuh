@@ -798,6 +798,16 @@ __device__ __forceinline__ void vmarch(const StepParams& p, int n, int lane, int
       if ((pb & kPlanePoles) && lane_poles) ade_v(p, lane_poles, i, j, kb, ec0, ec1, ec2, v0, v1, v2);
       if ((pb & kPlaneETerms) || (lf & kLfETermY) || ze)
         add_terms_v(p, 0, 0, n, i, j, kb, pb & kPlaneETerms, lf & kLfETermY, ze, v0, v1, v2);
+      // scenes without TFSF end the E update on PEC faces (stepping.py:2316-2318):
+      // cells neither updated nor kept are PEC (or outside the extent, zero anyway)
+      if (p.pec_clamp && (u0 & u1 & u2) != kAll) {
+#pragma unroll
+        for (int t = 0; t < V; ++t) {
+          if (!((u0 | k0) >> t & 1u)) v0[t] = 0.f;
+          if (!((u1 | k1) >> t & 1u)) v1[t] = 0.f;
+          if (!((u2 | k2) >> t & 1u)) v2[t] = 0.f;
+        }
+      }
       vst_cg(p.Eout[0], o + rc, v0);
       vst_cg(p.Eout[1], o + rc, v1);
       vst_cg(p.Eout[2], o + rc, v2);

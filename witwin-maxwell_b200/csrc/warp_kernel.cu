@@ -288,10 +288,31 @@ __device__ __forceinline__ void march(const StepParams& p, int n, int lane, int 
       float d2a = (hcy - hpy) * iex, d2b = (hcx - hmx) * iey;
       int m0 = 0, m1 = 0, m2 = 0;
       if (lane_edge || i == 0 || i == NX - 1) {
-        const bool xlo = i == 0, xhi = i == NX - 1;
-        m0 = edge_mode(i < NX - 1 && ez_kok, ylo, yhi, zlo, zhi, p.bnd[2], p.bnd[3], p.bnd[4], p.bnd[5]);
-        m1 = edge_mode(yc_ok && ez_kok, xlo, xhi, zlo, zhi, p.bnd[0], p.bnd[1], p.bnd[4], p.bnd[5]);
-        m2 = edge_mode(hz_kok, xlo, xhi, ylo, yhi, p.bnd[0], p.bnd[1], p.bnd[2], p.bnd[3]);
+        // a PMC face keeps its tangential E updated: it counts as no face here
+        const int pm = p.pmc;
+        const bool xlo = i == 0 && !(pm & 1), xhi = i == NX - 1 && !(pm & 2);
+        const bool ylo_ = ylo && !(pm & 4), yhi_ = yhi && !(pm & 8);
+        const bool zlo_ = zlo && !(pm & 16), zhi_ = zhi && !(pm & 32);
+        m0 = edge_mode(i < NX - 1 && ez_kok, ylo_, yhi_, zlo_, zhi_, p.bnd[2], p.bnd[3], p.bnd[4], p.bnd[5]);
+        m1 = edge_mode(yc_ok && ez_kok, xlo, xhi, zlo_, zhi_, p.bnd[0], p.bnd[1], p.bnd[4], p.bnd[5]);
+        m2 = edge_mode(hz_kok, xlo, xhi, ylo_, yhi_, p.bnd[0], p.bnd[1], p.bnd[2], p.bnd[3]);
+        if (pm) {
+          // the H outside a PMC face mirrors the H inside with the opposite
+          // sign, so the difference across the face doubles (the missing
+          // neighbour reads as zero here)
+          if ((i == 0 && (pm & 1)) || (i == NX - 1 && (pm & 2))) {
+            d1a *= 2.0f;
+            d2a *= 2.0f;
+          }
+          if ((ylo && (pm & 4)) || (yhi && (pm & 8))) {
+            d0a *= 2.0f;
+            d2b *= 2.0f;
+          }
+          if ((zlo && (pm & 16)) || (zhi && (pm & 32))) {
+            d0b *= 2.0f;
+            d1b *= 2.0f;
+          }
+        }
       }
       if (kCpml) {
         if (sxe >= 0) {
@@ -322,6 +343,12 @@ __device__ __forceinline__ void march(const StepParams& p, int n, int lane, int 
       }
       if ((pb & kPlaneETerms) || (lf & (kLfETermY | kLfETermZ)))
         add_terms(p, 0, 0, n, i, j, k, pb & kPlaneETerms, lf & kLfETermY, lf & kLfETermZ, v0, v1, v2);
+      // scenes without TFSF end the E update on PEC faces (stepping.py:2316-2318)
+      if (p.pec_clamp) {
+        if (m0 == 2) v0 = 0.f;
+        if (m1 == 2) v1 = 0.f;
+        if (m2 == 2) v2 = 0.f;
+      }
       // deferred (wrap-face) cells are written by the wrap kernel
       if (m0 != kModeDeferred) stf<TS>(p.Eout[0], o + rc, v0, p.finv[0]);
       if (m1 != kModeDeferred) stf<TS>(p.Eout[1], o + rc, v1, p.finv[1]);
