@@ -479,6 +479,28 @@ int fdtd_op_dft_volume(int64_t n, int n_freq, const float* field, float* re, flo
 /* PEC face clamp (boundary.cu:69-168). */
 int fdtd_op_clamp_face(float* field, const int* fshape, int axis, int side, void* stream);
 
+/* ------------------------------------------------------------------------ */
+/* 3. Consumers of the DFT planes                                            */
+/* ------------------------------------------------------------------------ */
+/* Diffraction-order projection of one frequency's plane spectrum
+ * (witwin/maxwell/postprocess/diffraction.py:84-196): field holds the
+ * co-located complex components [na][nb][3] (interleaved re, im; float32) of E
+ * or of H on the plane's tangential coordinates coords_a [na], coords_b [nb];
+ * for the order grid kx[n_m] x ky[n_n] (FP64) it writes
+ * amplitudes[m][n][3] (interleaved complex) = the mean over the plane of
+ * F exp(-i (kx a + ky b)).  scratch: 2 * n_n * na * 3 doubles of device memory. */
+int fdtd_pp_diffraction(int na, int nb, const float* coords_a, const float* coords_b, const float* field, int n_m,
+                        const double* kx, int n_n, const double* ky, double* scratch, float* amplitudes,
+                        void* stream);
+/* Near-to-far-field transform (witwin/maxwell/postprocess/nfft.py:100-137):
+ * points [P][3] (metres), quadrature-weighted surface currents j_weighted /
+ * m_weighted [P][3] (interleaved complex), unit directions [D][3] and radii
+ * [D]; lossless background wavenumber k and impedance eta.  Writes the far E
+ * and H [D][3] (interleaved complex) and the radial power density [D]. */
+int fdtd_pp_nfft(int n_points, const float* points, const float* j_weighted, const float* m_weighted, int n_dirs,
+                 const float* directions, const float* radius, double k, double eta, float* e_out, float* h_out,
+                 float* power, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -44,7 +44,7 @@ __version__ = "0.1.0"
 def __getattr__(name):
     # Lazily import the CUDA-backed modules so that scene compilation and the
     # library's symbol table can be used on machines without a GPU.
-    if name in ("solver", "backend", "simulation", "adjoint", "distributed", "_lib"):
+    if name in ("solver", "backend", "simulation", "adjoint", "distributed", "postprocess", "_lib"):
         import importlib
 
         return importlib.import_module(f".{name}", __name__)

@@ -116,6 +116,8 @@ _SIGNATURES = {
                                          _i, _i, _i, _i, _vp], _i),
     "fdtd_op_project_periodic": ([_vp, _c_int_p, _i, _vp], _i),
     "fdtd_op_project_bloch": ([_vp, _vp, _c_int_p, _i, _f, _f, _vp], _i),
+    "fdtd_pp_diffraction": ([_i, _i, _vp, _vp, _vp, _i, _vp, _i, _vp, _vp, _vp, _vp], _i),
+    "fdtd_pp_nfft": ([_i, _vp, _vp, _vp, _i, _vp, _vp, _d, _d, _vp, _vp, _vp, _vp], _i),
     "fdtd_op_add_cw_patch": ([_vp, _c_int_p, _vp, _vp, _c_int_p, _c_int_p, _f, _f, _vp], _i),
     "fdtd_op_add_shifted_patch": ([_vp, _c_int_p, _vp, _vp, _vp, _i, _c_int_p, _c_int_p, _i, _f, _f, _f, _f, _f, _f,
                                    _vp], _i),
