@@ -126,6 +126,24 @@ int fdtd_engine_pole_state(fdtd_engine* h, int pole_id, float* pol_out, float* c
 /* Overwrite a pole's state (box-dense, either pointer may be NULL); FP32 or FP16 field storage. */
 int fdtd_engine_set_pole_state(fdtd_engine* h, int pole_id, const float* pol, const float* cur);
 
+/* Instantaneous nonlinear cells of E component comp (0..2): before every step
+ * the engine recomposes their E coefficients from E^n
+ * (witwin/maxwell/fdtd/runtime/materials.py:1664-1770; kernels
+ * dispersive.cu:267-400; replaces updateKerrElectricField{Ex,Ey,Ez}Curl3D and
+ * updateNonlinearElectricCoefficients3D before update_electric_fields,
+ * stepping.py:1794-1796).  cells: n_cells x (i, j, k) Yee indices of comp;
+ * params: n_cells x 6 floats (eps_lin, decay, sigma_static, chi2, chi3,
+ * tpa_sigma), with decay the static decay in the Kerr form (general = 0:
+ * curl = dt / eps_eff * decay) and the external decay in the general form
+ * (general = 1: decay and curl rewritten).  Host or device pointers.  Pass only
+ * cells with a nonzero chi2, chi3 or tpa channel, and set the component's
+ * coefficient arrays (curl; curl and decay in the general form) to the
+ * formula's values with those channels zero.  Poles in such a scene subtract
+ * J times this step's curl coefficient (materials.py:751-773).  Not with
+ * reduced storage, Bloch fields or the adjoint. */
+int fdtd_engine_set_nonlinear(fdtd_engine* h, int comp, int n_cells, const int* cells, const float* params,
+                              int general, float eps0);
+
 /* Soft source patch: comp gets coeff[cell] * signal[n] added at step n
  * (witwin/maxwell/fdtd/cuda/kernels/sources.cu:135-154; the signal table
  * holds the host-evaluated waveform, excitation/temporal.py:408-491). */
@@ -406,6 +424,24 @@ int fdtd_op_update_lorentz(int64_t n, const float* e, const float* drive, float 
                            float dt, float* pol, float* cur, void* stream);
 int fdtd_op_apply_polarization(int64_t n, const float* cur, const float* inv_eps, float dt, float* e,
                                void* stream);
+
+/* Instantaneous nonlinear E coefficients of component comp (0..2) over its
+ * whole Yee array (update_kerr_e{x,y,z}_curl and update_nonlinear_coefficients,
+ * extension.cpp:2109-2112; kernels dispersive.cu:165-400).  shapes: the
+ * Ex, Ey, Ez array shapes (9 ints); eps, decay / external_decay, sigma, chi2,
+ * chi3, tpa and the outputs have comp's shape.  E is collocated onto comp's
+ * edge (4-point averages, clamped indices); eps_eff is floored at 1e-12 eps0.
+ * Kerr: curl = dt / (eps + eps0 chi3 |E|^2) * decay.  General:
+ * eps_eff = eps + eps0 (chi2 E_comp + chi3 |E|^2), sigma = max(sigma + tpa |E|^2, 0),
+ * half = sigma dt / (2 eps_eff), decay = ext (1 - half) / (1 + half),
+ * curl = ext dt / eps_eff / (1 + half). */
+int fdtd_op_update_kerr_curl(int comp, const int* shapes, const float* ex, const float* ey, const float* ez,
+                             const float* eps, const float* decay, const float* chi3, float dt, float eps0,
+                             float* curl, void* stream);
+int fdtd_op_update_nonlinear_coefficients(int comp, const int* shapes, const float* ex, const float* ey,
+                                          const float* ez, const float* eps, const float* external_decay,
+                                          const float* sigma, const float* chi2, const float* chi3, const float* tpa,
+                                          float dt, float eps0, float* decay, float* curl, void* stream);
 
 /* add_source_patch (sources.cu:135-154): field[off + idx] += signal * patch[idx],
  * cells outside the field are skipped.  fshape/pshape/offset are int[3]. */

@@ -12,6 +12,7 @@ in ``fdtd_oracle.c`` on full Yee-shaped arrays:
     TFSF E correction, aux E advance   tfsf_apply.py:237-264
     soft sources                       sources.cu:135-154, temporal.py:408-491
     ADE subtraction E -= dt J / eps    dispersive.cu:72-83, materials.py:911
+    nonlinear E coefficients           dispersive.cu:165-400, materials.py:1664-1770
     monitor running DFT                observers.py:577-659, spectral.py:165-232
 
 The DFT phase follows the reference's observer path: a float64 rotation
@@ -103,6 +104,58 @@ def component_shape(name, nodes):
     }[name]
 
 
+def _clamped(f, i, j, k):
+    return f[np.clip(i, 0, f.shape[0] - 1), np.clip(j, 0, f.shape[1] - 1), np.clip(k, 0, f.shape[2] - 1)]
+
+
+def collocate_e(comp, ex, ey, ez):
+    """E collocated onto the Yee edges of ``comp`` (witwin/maxwell/fdtd/cuda/
+    kernels/dispersive.cu:160-265): the own component as is, the other two as
+    the mean of their four surrounding edges, indices clamped to each array."""
+    own = {"Ex": ex, "Ey": ey, "Ez": ez}[comp]
+    i, j, k = np.meshgrid(*(np.arange(n) for n in own.shape), indexing="ij")
+    if comp == "Ex":
+        vy = 0.25 * (_clamped(ey, i, j - 1, k) + _clamped(ey, i, j, k) + _clamped(ey, i + 1, j - 1, k)
+                     + _clamped(ey, i + 1, j, k))
+        vz = 0.25 * (_clamped(ez, i, j, k - 1) + _clamped(ez, i, j, k) + _clamped(ez, i + 1, j, k - 1)
+                     + _clamped(ez, i + 1, j, k))
+        return ex, vy, vz
+    if comp == "Ey":
+        vx = 0.25 * (_clamped(ex, i - 1, j, k) + _clamped(ex, i, j, k) + _clamped(ex, i - 1, j + 1, k)
+                     + _clamped(ex, i, j + 1, k))
+        vz = 0.25 * (_clamped(ez, i, j, k - 1) + _clamped(ez, i, j, k) + _clamped(ez, i, j + 1, k - 1)
+                     + _clamped(ez, i, j + 1, k))
+        return vx, ey, vz
+    vx = 0.25 * (_clamped(ex, i - 1, j, k) + _clamped(ex, i, j, k) + _clamped(ex, i - 1, j, k + 1)
+                 + _clamped(ex, i, j, k + 1))
+    vy = 0.25 * (_clamped(ey, i, j - 1, k) + _clamped(ey, i, j, k) + _clamped(ey, i, j - 1, k + 1)
+                 + _clamped(ey, i, j, k + 1))
+    return vx, vy, ez
+
+
+def kerr_curl(comp, ex, ey, ez, eps, decay, chi3, dt, eps0):
+    """Kerr curl coefficient (dispersive.cu:267-321): dt / max(eps + eps0 chi3 |E|^2,
+    1e-12 eps0) * decay."""
+    vx, vy, vz = collocate_e(comp, ex, ey, ez)
+    eff = np.maximum(eps + eps0 * chi3 * (vx * vx + vy * vy + vz * vz), 1.0e-12 * eps0)
+    return (dt / eff) * decay
+
+
+def nonlinear_coefficients(comp, ex, ey, ez, eps, external, sigma, chi2, chi3, tpa, dt, eps0):
+    """General instantaneous-nonlinear decay / curl pair (dispersive.cu:323-400):
+    eps_eff = eps + eps0 (chi2 E_own + chi3 |E|^2) (floored at 1e-12 eps0),
+    sigma_eff = max(sigma + tpa |E|^2, 0), half = sigma_eff dt / (2 eps_eff),
+    decay = ext (1 - half) / (1 + half), curl = ext dt / eps_eff / (1 + half)."""
+    vx, vy, vz = collocate_e(comp, ex, ey, ez)
+    fsq = vx * vx + vy * vy + vz * vz
+    own = {"Ex": vx, "Ey": vy, "Ez": vz}[comp]
+    eff = np.maximum(eps + eps0 * (chi2 * own + chi3 * fsq), 1.0e-12 * eps0)
+    sig = np.maximum(sigma + tpa * fsq, 0.0)
+    half = 0.5 * sig * dt / eff
+    inv = 1.0 / (1.0 + half)
+    return external * (1.0 - half) * inv, external * (dt / eff) * inv
+
+
 # (a-axis, b-axis, first, second) per component, magnetic.cu:20-212 / electric.cu:242-941
 _H_SPEC = {"Hx": (1, 2, "Ey", "Ez"), "Hy": (0, 2, "Ex", "Ez"), "Hz": (0, 1, "Ex", "Ey")}
 _E_SPEC = {"Ex": (1, 2, "Hy", "Hz"), "Ey": (0, 2, "Hx", "Hz"), "Ez": (0, 1, "Hx", "Hy")}
@@ -159,6 +212,14 @@ class OracleSimulation:
                 "comp": pole.component, "kind": pole.kind, "decay": pole.decay, "restoring": pole.restoring,
                 "drive": drive, "inv_eps": inv_eps, "P": np.zeros(shape, dt), "J": np.zeros(shape, dt),
             })
+        # instantaneous nonlinear channels: the E coefficients are recomposed
+        # from E^n over every cell before each E update (materials.py:1664-1770)
+        self.nl = None
+        if getattr(cs, "nonlinear", None) is not None:
+            nl = cs.nonlinear
+            self.nl = {"general": nl.general, "eps0": nl.eps0,
+                       "eps": {n: cs.eps[n].astype(dt) for n in ("Ex", "Ey", "Ez")},
+                       "ch": {n: {k: v.astype(dt) for k, v in nl.channels[n].items()} for n in ("Ex", "Ey", "Ez")}}
         self.patches = [(p.component, p.box, p.coeff.astype(dt), p.signal) for p in cs.patches]
         # time-shifted patches: scale * w(n dt + t_offset - delay) per cell, the
         # waveform evaluated in FP64 here (sources.cu:173-221)
@@ -278,8 +339,27 @@ class OracleSimulation:
         dt = self.cs.dt
         for p in self.poles:
             e = F[p["comp"]]
-            self._split_flat(e.size, lambda a, b, p=p, e=e: self.lib.oracle_apply_polarization(
-                a, b, _p(p["J"]), _p(p["inv_eps"]), dt, _p(e)))
+            # nonlinear scenes: J times this step's curl coefficient, dt 1 (materials.py:751-773)
+            coef, apply_dt = (self.curl[p["comp"]], 1.0) if self.nl is not None else (p["inv_eps"], dt)
+            self._split_flat(e.size, lambda a, b, p=p, e=e, coef=coef, apply_dt=apply_dt:
+                             self.lib.oracle_apply_polarization(a, b, _p(p["J"]), _p(coef), apply_dt, _p(e)))
+
+    def update_nonlinear(self):
+        F = self.fields
+        nl = self.nl
+        dt, eps0 = self.cs.dt, nl["eps0"]
+        out = {}
+        for n in ("Ex", "Ey", "Ez"):
+            ch, eps = nl["ch"][n], nl["eps"][n]
+            if nl["general"]:
+                out[n] = nonlinear_coefficients(n, F["Ex"], F["Ey"], F["Ez"], eps, ch["decay"], ch["sigma"], ch["chi2"],
+                                                ch["chi3"], ch["tpa"], dt, eps0)
+            else:
+                out[n] = (None, kerr_curl(n, F["Ex"], F["Ey"], F["Ez"], eps, ch["decay"], ch["chi3"], dt, eps0))
+        for n, (d, c) in out.items():
+            if d is not None:
+                self.decay[n][...] = d
+            self.curl[n][...] = c
 
     def _line_corrections(self, magnetic: bool):
         if self.aux is None:
@@ -320,6 +400,8 @@ class OracleSimulation:
             self.lib.oracle_aux_magnetic(a["e"].size, _p(a["h"]), _p(a["e"]), _p(a["hd"]), _p(a["hc"]))
         self._soft_terms(n, True)
         self.advance_ade()
+        if self.nl is not None:
+            self.update_nonlinear()
         self.update_e()
         if self.aux is not None:
             self._line_corrections(False)

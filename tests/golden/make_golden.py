@@ -36,6 +36,7 @@ import torch
 
 HERE = Path(__file__).resolve().parent
 ROOT = HERE.parents[1]
+REFERENCE: Path | None = None  # the reference checkout (set by main)
 
 
 def load_reference(ref_root: Path):
@@ -362,7 +363,67 @@ def op_vectors(tr, rng) -> dict:
         fr, fi = t(pf), t(pim)
         K["projectBlochBoundary3D"](fieldReal=fr, fieldImag=fi, axis=axis, phaseCos=0.6, phaseSin=0.8)
         out[f"out_proj_bl_{axis}_re"], out[f"out_proj_bl_{axis}_im"] = fr.numpy(), fi.numpy()
+    # instantaneous nonlinear coefficients: the Kerr curl ops of torch_reference
+    # (updateKerrElectricField{Ex,Ey,Ez}Curl3D) and the general chi2 / chi3 / TPA
+    # formula of the reference's own test (tests/materials/nonlinear/
+    # test_fdtd_nonlinear.py, _reference_nonlinear_coefficients), on fields large
+    # enough that every channel matters; a few cells drive eps_eff below its
+    # floor and the TPA conductivity below zero
+    nonlinear_vectors(tr, rng, out)
     return out
+
+
+def _reference_test_functions(names):
+    """The named top-level functions of the reference's nonlinear test module,
+    executed without the module's package imports."""
+    import ast
+
+    path = REFERENCE / "tests/materials/nonlinear/test_fdtd_nonlinear.py"
+    tree = ast.parse(path.read_text())
+    body = [node for node in tree.body if isinstance(node, ast.FunctionDef) and node.name in names]
+    ns = {"torch": torch}
+    exec(compile(ast.Module(body=body, type_ignores=[]), str(path), "exec"), ns)
+    return [ns[n] for n in names]
+
+
+def nonlinear_vectors(tr, rng, out):
+    nodes = (7, 6, 5)
+    S = shapes(nodes)
+    eps0, dt = 8.8541878128e-12, 4.8e-17
+    fields = {c: rng.standard_normal(S[c]) * 30.0 for c in ("Ex", "Ey", "Ez")}
+    out.update(nl_dt=np.array(dt), nl_eps0=np.array(eps0), nl_Ex=fields["Ex"], nl_Ey=fields["Ey"], nl_Ez=fields["Ez"])
+    (general,) = _reference_test_functions(["_clamped_gather", "_collocate_reference",
+                                            "_reference_nonlinear_coefficients"])[2:]
+    solver = types.SimpleNamespace(Ex=t(fields["Ex"]), Ey=t(fields["Ey"]), Ez=t(fields["Ez"]), eps0=eps0, dt=dt)
+    for comp in ("Ex", "Ey", "Ez"):
+        sh = S[comp]
+        eps = eps0 * rng.uniform(1.0, 4.0, sh)
+        dec = rng.uniform(0.5, 1.0, sh)
+        ext = rng.uniform(0.5, 1.0, sh)
+        sig = rng.uniform(0.0, 1.0e6, sh)
+        chi2 = rng.uniform(-0.01, 0.01, sh)
+        chi3 = rng.uniform(0.0, 2.0e-3, sh)
+        tpa = rng.uniform(-2.0e2, 1.0e4, sh)
+        chi3.flat[::7] = -1.0  # eps_eff below the floor
+        chi2.flat[3::11] = -2.0
+        vals = dict(eps=eps, dec=dec, ext=ext, sig=sig, chi2=chi2, chi3=chi3, tpa=tpa)
+        for k, v in vals.items():
+            out[f"nl_{comp}_{k}"] = v
+        dyn = torch.zeros(sh)
+        tr.__dict__[f"_update_kerr_{comp.lower()}"](
+            DynamicCurl=dyn, Ex=solver.Ex, Ey=solver.Ey, Ez=solver.Ez, LinearPermittivity=t(eps),
+            **{f"{comp}Decay": t(dec)}, KerrChi3=t(chi3), dt=dt, eps0=eps0)
+        out[f"out_kerr_{comp}"] = dyn.numpy()
+        low = comp.lower()
+        setattr(solver, f"eps_{comp}", t(eps))
+        setattr(solver, f"c{low}_decay_external", t(ext))
+        setattr(solver, f"sigma_e_{comp}", t(sig))
+        setattr(solver, f"nonlinear_chi2_{comp}", t(chi2))
+        setattr(solver, f"kerr_chi3_{comp}", t(chi3))
+        setattr(solver, f"tpa_sigma_{comp}", t(tpa))
+    for comp in ("Ex", "Ey", "Ez"):
+        d, c = general(solver, comp)
+        out[f"out_nl_{comp}_decay"], out[f"out_nl_{comp}_curl"] = d.numpy(), c.numpy()
 
 
 def _package():
@@ -548,6 +609,8 @@ def main():
     if ref is None:
         sys.exit("no reference checkout: pass --reference or set WITWIN_MAXWELL_REFERENCE")
     torch.set_default_dtype(torch.float64)
+    global REFERENCE
+    REFERENCE = Path(ref)
     tr = load_reference(ref)
     rng = np.random.default_rng(20261203)
     np.savez_compressed(HERE / "ops.npz", **op_vectors(tr, rng))

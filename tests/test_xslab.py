@@ -23,8 +23,12 @@ ROOT = Path(__file__).resolve().parents[1]
 STEPS = 40
 
 
-def _scene(wm):
+def _scene(wm, nonlinear=False):
     sc = wm.Scene(cells=(30, 16, 14), spacing=25e-9, pml_cells=3)
+    if nonlinear:
+        # Kerr, chi2 and TPA channels across the cut of two ranks (node plane 16)
+        sc.structures.append(wm.Structure(wm.Box((12, 3, 3), (21, 12, 11)),
+                                          wm.Medium(eps_r=2.0, kerr_chi3=0.02, chi2=0.05, tpa_beta=5e7, sigma=1e4)))
     sc.structures.append(wm.Structure(wm.Box((10, 4, 4), (20, 12, 10)), wm.Medium(eps_r=3.0)))
     sc.structures.append(wm.Structure(wm.Sphere((15, 8, 7), 3.0), wm.Medium.lorentz(2.0, 3.0, 250e12, 20e12)))
     sc.structures.append(wm.Structure(wm.Box((18, 3, 3), (21, 13, 11)),
@@ -45,7 +49,7 @@ def _free_port() -> int:
         return s.getsockname()[1]
 
 
-def _worker(rank: int, world: int, port: int, out):
+def _worker(rank: int, world: int, port: int, out, nonlinear=False):
     import torch.distributed as dist
 
     sys.path.insert(0, str(ROOT))
@@ -57,7 +61,7 @@ def _worker(rank: int, world: int, port: int, out):
     os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
     dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=60))
     try:
-        cs = wm.compile_scene(_scene(wm), STEPS)
+        cs = wm.compile_scene(_scene(wm, nonlinear), STEPS)
         run = wm.distributed.XSlabRun(cs, rank, world, stepper=lambda local: orc.OracleSimulation(local, "f64",
                                                                                                    threads=1))
         run.run(0, STEPS)
@@ -72,17 +76,17 @@ def _worker(rank: int, world: int, port: int, out):
         dist.destroy_process_group()
 
 
-@pytest.mark.parametrize("world", [2, 3])
-def test_xslab_ranks_reproduce_single_domain(world):
+@pytest.mark.parametrize("world,nonlinear", [(2, False), (3, False), (2, True)])
+def test_xslab_ranks_reproduce_single_domain(world, nonlinear):
     from oracle import oracle as orc
 
     wm = load_package()
-    cs = wm.compile_scene(_scene(wm), STEPS)
+    cs = wm.compile_scene(_scene(wm, nonlinear), STEPS)
     ref = orc.OracleSimulation(cs, "f64", threads=1).run(STEPS)
     port = _free_port()
     ctx = mp.get_context("spawn")
     q = ctx.Queue()
-    procs = [ctx.Process(target=_worker, args=(r, world, port, q)) for r in range(world)]
+    procs = [ctx.Process(target=_worker, args=(r, world, port, q, nonlinear)) for r in range(world)]
     for p in procs:
         p.start()
     fields, mons = q.get(timeout=300)
@@ -123,15 +127,15 @@ def test_slab_split_and_checks():
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("world", [2, 3])
-def test_xslab_engines_match_single_engine(world):
+@pytest.mark.parametrize("world,nonlinear", [(2, False), (3, False), (2, True)])
+def test_xslab_engines_match_single_engine(world, nonlinear):
     """The slabs as fused engines on one device (ranks of one process, halo planes
     copied device to device) against one engine over the whole grid, at the
     engine's parity bars (joint relative L2 <= 1e-5, <= 1e-4 per component)."""
     wm = load_package()
     d = wm.distributed
     steps = 200
-    cs = wm.compile_scene(_scene(wm), steps)
+    cs = wm.compile_scene(_scene(wm, nonlinear), steps)
     single = wm.solver.B200FDTD(cs).init_field()
     single.step_range(0, steps)
     ref_f = {n: single.field(n).cpu().numpy() for n in ("Ex", "Ey", "Ez", "Hx", "Hy", "Hz")}

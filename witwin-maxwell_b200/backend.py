@@ -150,6 +150,44 @@ def _full(t, like, n=None):
     return t
 
 
+def _nl_shapes(ex, ey, ez):
+    return (ctypes.c_int * 9)(*ex.shape, *ey.shape, *ez.shape)
+
+
+def _kerr_curl(comp: str):
+    """updateKerrElectricField{Ex,Ey,Ez}Curl3D (witwin/maxwell/fdtd/cuda/backend.py:2232-2275)."""
+    c = "xyz".index(comp[1].lower())
+
+    def run(*, DynamicCurl, Ex, Ey, Ez, LinearPermittivity, KerrChi3, dt, eps0, **kw):
+        decay = kw[f"{comp}Decay"]
+        for name, t in (("DynamicCurl", DynamicCurl), ("Ex", Ex), ("Ey", Ey), ("Ez", Ez),
+                        ("LinearPermittivity", LinearPermittivity), (f"{comp}Decay", decay), ("KerrChi3", KerrChi3)):
+            _check_tensor(t, name)
+        _lib.check(_lib.load().fdtd_op_update_kerr_curl(
+            c, _nl_shapes(Ex, Ey, Ez), _lib.ptr(Ex), _lib.ptr(Ey), _lib.ptr(Ez), _lib.ptr(LinearPermittivity),
+            _lib.ptr(decay), _lib.ptr(KerrChi3), float(dt), float(eps0), _lib.ptr(DynamicCurl),
+            _stream(DynamicCurl)), "kerr curl")
+
+    return run
+
+
+def _nonlinear_coefficients(*, DynamicDecay, DynamicCurl, Ex, Ey, Ez, LinearPermittivity, ExternalDecay, SigmaStatic,
+                            Chi2, Chi3, TpaSigma, component, dt, eps0):
+    """updateNonlinearElectricCoefficients3D (witwin/maxwell/fdtd/cuda/backend.py:2277-2309)."""
+    if component not in ("Ex", "Ey", "Ez"):
+        raise ValueError(f"unsupported nonlinear component {component!r}")
+    tensors = (("DynamicDecay", DynamicDecay), ("DynamicCurl", DynamicCurl), ("Ex", Ex), ("Ey", Ey), ("Ez", Ez),
+               ("LinearPermittivity", LinearPermittivity), ("ExternalDecay", ExternalDecay),
+               ("SigmaStatic", SigmaStatic), ("Chi2", Chi2), ("Chi3", Chi3), ("TpaSigma", TpaSigma))
+    for name, t in tensors:
+        _check_tensor(t, name)
+    _lib.check(_lib.load().fdtd_op_update_nonlinear_coefficients(
+        "xyz".index(component[1].lower()), _nl_shapes(Ex, Ey, Ez), _lib.ptr(Ex), _lib.ptr(Ey), _lib.ptr(Ez),
+        _lib.ptr(LinearPermittivity), _lib.ptr(ExternalDecay), _lib.ptr(SigmaStatic), _lib.ptr(Chi2), _lib.ptr(Chi3),
+        _lib.ptr(TpaSigma), float(dt), float(eps0), _lib.ptr(DynamicDecay), _lib.ptr(DynamicCurl),
+        _stream(DynamicCurl)), "nonlinear coefficients")
+
+
 # (component, first H, second H, axis a, axis b) of the Bloch E kernels
 _BLOCH_E = {"Ex": ("Hy", "Hz", "Y", "Z"), "Ey": ("Hx", "Hz", "X", "Z"), "Ez": ("Hx", "Hy", "X", "Y")}
 
@@ -317,6 +355,10 @@ _KERNELS.update({
     "updateDrudeCurrent3D": _drude,
     "updateLorentzCurrent3D": _lorentz,
     "applyPolarizationCurrent3D": _apply_polarization,
+    "updateKerrElectricFieldExCurl3D": _kerr_curl("Ex"),
+    "updateKerrElectricFieldEyCurl3D": _kerr_curl("Ey"),
+    "updateKerrElectricFieldEzCurl3D": _kerr_curl("Ez"),
+    "updateNonlinearElectricCoefficients3D": _nonlinear_coefficients,
     "addSourcePatch3D": _add_source_patch,
     "addCwPhasedSourcePatch3D": _add_cw_patch,
     "addTimeShiftedSourcePatch3D": _add_shifted_patch,

@@ -80,6 +80,9 @@ __global__ void __launch_bounds__(256, 4) ade_pass_kernel(const __grid_constant_
       }
     }
     const float decay = pt.decay, restoring = pt.restoring, dt = pt.dt, inv_dt = pt.inv_dt;
+    // nonlinear scenes: J times this step's curl coefficient (dt 1)
+    const float* nlc = a.nl_curl[c];
+    const float dt_apply = nlc ? 1.0f : dt;
 #pragma unroll
     for (int q = 0; q < kQ; ++q) {
       if (!act[q]) continue;
@@ -101,7 +104,7 @@ __global__ void __launch_bounds__(256, 4) ade_pass_kernel(const __grid_constant_
         pt.cur[o] = jn;
         pt.pol[o] = pl + dt * jn;
       }
-      const float s = dt * jn * ie[q];
+      const float s = dt_apply * jn * (nlc ? __ldg(nlc + row + tl.y + lane + 32 * q) : ie[q]);
       if (c == 0) v[q][0] -= s;
       else if (c == 1) v[q][1] -= s;
       else v[q][2] -= s;

@@ -412,6 +412,85 @@ __global__ void __launch_bounds__(256) shifted_patch_kernel(const __grid_constan
   }
 }
 
+// Instantaneous nonlinear media (witwin/maxwell/fdtd/cuda/kernels/
+// dispersive.cu:165-400, called before the E update, runtime/stepping.py:
+// 1794-1796): before every step the E coefficients of the nonlinear cells are
+// recomposed from E^n collocated onto the cell's Yee edge (the other two
+// components 4-point averaged, indices clamped to their arrays):
+//   Kerr only:  curl = dt / max(eps + eps0 chi3 |E|^2, 1e-12 eps0) * decay
+//   general:    eps_eff = eps + eps0 (chi2 E_own + chi3 |E|^2) (same floor),
+//               sigma = max(sigma_s + tpa |E|^2, 0), half = sigma dt / (2 eps_eff),
+//               decay = ext (1 - half) / (1 + half), curl = ext dt / eps_eff / (1 + half).
+// The work list holds only cells with a nonzero chi2, chi3 or TPA channel: on
+// every other cell the formula is constant and the host stores its value once.
+struct NonlinearLaunch {
+  const int4* cells;  // i, j, k, component
+  const float* prm;   // 6 x n (SoA): eps, decay (Kerr) or external decay, sigma_s, chi2, chi3, tpa
+  int64_t n;
+  const float* E[3];  // E^n
+  float* decay[3];
+  float* curl[3];
+  int NX, NY, NZ, P;
+  float dt, eps0;
+  int general;
+};
+
+// E component c at (i, j, k), each index clamped into c's Yee extent
+__device__ __forceinline__ float nl_sample(const NonlinearLaunch& a, int c, int i, int j, int k) {
+  const int ex = c == 0 ? a.NX - 1 : a.NX, ey = c == 1 ? a.NY - 1 : a.NY, ez = c == 2 ? a.NZ - 1 : a.NZ;
+  i = min(max(i, 0), ex - 1);
+  j = min(max(j, 0), ey - 1);
+  k = min(max(k, 0), ez - 1);
+  return __ldg(a.E[c] + (static_cast<int64_t>(i) * a.NY + j) * a.P + k);
+}
+
+__global__ void __launch_bounds__(256) nonlinear_kernel(const __grid_constant__ NonlinearLaunch a) {
+  for (int64_t t = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; t < a.n;
+       t += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    const int4 q = __ldg(a.cells + t);
+    const int i = q.x, j = q.y, k = q.z, c = q.w;
+    float e[3];
+    e[c] = nl_sample(a, c, i, j, k);
+    if (c == 0) {
+      e[1] = 0.25f * (nl_sample(a, 1, i, j - 1, k) + nl_sample(a, 1, i, j, k) + nl_sample(a, 1, i + 1, j - 1, k) +
+                      nl_sample(a, 1, i + 1, j, k));
+      e[2] = 0.25f * (nl_sample(a, 2, i, j, k - 1) + nl_sample(a, 2, i, j, k) + nl_sample(a, 2, i + 1, j, k - 1) +
+                      nl_sample(a, 2, i + 1, j, k));
+    } else if (c == 1) {
+      e[0] = 0.25f * (nl_sample(a, 0, i - 1, j, k) + nl_sample(a, 0, i, j, k) + nl_sample(a, 0, i - 1, j + 1, k) +
+                      nl_sample(a, 0, i, j + 1, k));
+      e[2] = 0.25f * (nl_sample(a, 2, i, j, k - 1) + nl_sample(a, 2, i, j, k) + nl_sample(a, 2, i, j + 1, k - 1) +
+                      nl_sample(a, 2, i, j + 1, k));
+    } else {
+      e[0] = 0.25f * (nl_sample(a, 0, i - 1, j, k) + nl_sample(a, 0, i, j, k) + nl_sample(a, 0, i - 1, j, k + 1) +
+                      nl_sample(a, 0, i, j, k + 1));
+      e[1] = 0.25f * (nl_sample(a, 1, i, j - 1, k) + nl_sample(a, 1, i, j, k) + nl_sample(a, 1, i, j - 1, k + 1) +
+                      nl_sample(a, 1, i, j, k + 1));
+    }
+    const float fsq = e[0] * e[0] + e[1] * e[1] + e[2] * e[2];
+    const float eps = __ldg(a.prm + t), dec = __ldg(a.prm + a.n + t);
+    const float chi3 = __ldg(a.prm + 4 * a.n + t);
+    const float floor_eps = 1.0e-12f * a.eps0;
+    const int64_t o = (static_cast<int64_t>(i) * a.NY + j) * a.P + k;
+    if (!a.general) {
+      float eff = eps + a.eps0 * chi3 * fsq;
+      if (eff < floor_eps) eff = floor_eps;
+      a.curl[c][o] = (a.dt / eff) * dec;
+    } else {
+      const float sig_s = __ldg(a.prm + 2 * a.n + t), chi2 = __ldg(a.prm + 3 * a.n + t);
+      const float tpa = __ldg(a.prm + 5 * a.n + t);
+      float eff = eps + a.eps0 * (chi2 * e[c] + chi3 * fsq);
+      if (eff < floor_eps) eff = floor_eps;
+      float sigma = sig_s + tpa * fsq;
+      if (sigma < 0.0f) sigma = 0.0f;
+      const float half = 0.5f * sigma * a.dt / eff;
+      const float inv_denom = 1.0f / (1.0f + half);
+      a.decay[c][o] = dec * (1.0f - half) * inv_denom;
+      a.curl[c][o] = dec * (a.dt / eff) * inv_denom;
+    }
+  }
+}
+
 struct AdjointHost {
   bool ready = false;
   AdjParams q{};
@@ -449,6 +528,16 @@ struct fdtd_engine {
   // pair runs the wrap kernel and the monitor gather of this engine.
   bool wrap = false;
   bool pmc = false;  // some face is PMC: the scalar warp kernels (launch variants 1-3) only
+  // Instantaneous nonlinear E cells (fdtd_engine_set_nonlinear): host lists
+  // until finalize, then one device work list over the three components.
+  std::vector<int> nl_cells_h;     // i, j, k, component per cell
+  std::vector<float> nl_prm_h[6];  // NonlinearLaunch::prm channels
+  int nl_general = -1;             // -1: no nonlinear cells; 0: Kerr (curl only); 1: general (decay and curl)
+  float nl_eps0 = 0.0f;
+  int64_t nl_n = 0;
+  int4* d_nl_cells = nullptr;
+  float* d_nl_prm = nullptr;
+  int nl_lo[3] = {0, 0, 0}, nl_hi[3] = {0, 0, 0};
   bool bloch = false;
   bool in_pair = false;
   int64_t plane = 0, vol = 0;
@@ -693,6 +782,10 @@ void fill_params(const fdtd_engine* h, StepParams& p) {
   for (int f = 0; f < 6; ++f)
     if (h->desc.boundary[f] == FDTD_BND_PMC) p.pmc |= 1 << f;
   p.pec_clamp = h->lines.empty() ? 1 : 0;
+  for (int a = 0; a < 3; ++a) {
+    p.nl_lo[a] = h->nl_lo[a];
+    p.nl_hi[a] = h->nl_hi[a];
+  }
   for (int ph = 0; ph < 2; ++ph) {
     p.term_index[ph] = h->term_ix[ph];
     p.n_terms[ph] = h->n_terms_ph[ph];
@@ -826,9 +919,38 @@ int launch_shifted(fdtd_engine* h, int n) {
   return 0;
 }
 
+int launch_nonlinear(fdtd_engine* h) {
+  NonlinearLaunch a{};
+  a.cells = h->d_nl_cells;
+  a.prm = h->d_nl_prm;
+  a.n = h->nl_n;
+  for (int c = 0; c < 3; ++c) {
+    a.E[c] = h->E[h->cur][c];
+    a.decay[c] = h->ecoef[c][0];
+    a.curl[c] = h->ecoef[c][1];
+  }
+  a.NX = h->NX;
+  a.NY = h->NY;
+  a.NZ = h->NZ;
+  a.P = h->P;
+  a.dt = static_cast<float>(h->desc.dt);
+  a.eps0 = h->nl_eps0;
+  a.general = h->nl_general;
+  const int gx = static_cast<int>(std::min<int64_t>((h->nl_n + 255) / 256, 8 * 148));
+  nonlinear_kernel<<<gx, 256, 0, h->stream>>>(a);
+  const cudaError_t err = cudaGetLastError();
+  if (err != cudaSuccess) return cuda_fail(err, "nonlinear_kernel launch");
+  ++h->launches;
+  return 0;
+}
+
 int launch_step(fdtd_engine* h, int n, int slot) {
   if (!h->shifted.empty()) {
     const int rc = launch_shifted(h, n);
+    if (rc) return rc;
+  }
+  if (h->nl_n > 0) {
+    const int rc = launch_nonlinear(h);
     if (rc) return rc;
   }
   StepParams p;
@@ -1585,6 +1707,36 @@ int fdtd_engine_add_shifted_patch(fdtd_engine* h, int comp, const int* box, cons
   return 0;
 }
 
+int fdtd_engine_set_nonlinear(fdtd_engine* h, int comp, int n_cells, const int* cells, const float* params,
+                              int general, float eps0) {
+  if (!h || comp < 0 || comp > 2 || n_cells < 0 || (n_cells > 0 && (!cells || !params)) || general < 0 ||
+      general > 1 || !(eps0 > 0.0f))
+    return fail(FDTD_ERR_INVALID_ARG, "bad nonlinear arguments");
+  if (h->finalized) return fail(FDTD_ERR_STATE, "engine already finalized");
+  if (h->nl_general >= 0 && h->nl_general != general)
+    return fail(FDTD_ERR_INVALID_ARG, "nonlinear components disagree on the general form");
+  if (h->storage != kStoreF32) return fail(FDTD_ERR_UNSUPPORTED, "nonlinear media with reduced field storage");
+  h->nl_general = general;
+  h->nl_eps0 = eps0;
+  if (n_cells == 0) return 0;
+  std::vector<int> ijk(static_cast<size_t>(3) * n_cells);
+  std::vector<float> prm(static_cast<size_t>(6) * n_cells);
+  CUDA_TRY(cudaMemcpy(ijk.data(), cells, sizeof(int) * ijk.size(), cudaMemcpyDefault));
+  CUDA_TRY(cudaMemcpy(prm.data(), params, sizeof(float) * prm.size(), cudaMemcpyDefault));
+  int ext[3];
+  comp_extent(comp, h->NX, h->NY, h->NZ, ext);
+  for (int t = 0; t < n_cells; ++t) {
+    for (int a = 0; a < 3; ++a) {
+      const int v = ijk[3 * t + a];
+      if (v < 0 || v >= ext[a]) return fail(FDTD_ERR_INVALID_ARG, "nonlinear cell outside the component extent");
+      h->nl_cells_h.push_back(v);
+    }
+    h->nl_cells_h.push_back(comp);
+    for (int q = 0; q < 6; ++q) h->nl_prm_h[q].push_back(prm[6 * static_cast<size_t>(t) + q]);
+  }
+  return 0;
+}
+
 int fdtd_engine_add_aux_line(fdtd_engine* h, int n_e, const float* e_decay, const float* e_curl,
                              const float* h_decay, const float* h_curl, int source_index, const float* source,
                              int n_steps, int* line_id) {
@@ -1790,6 +1942,45 @@ int fdtd_engine_finalize(fdtd_engine* h) {
     rc = build_box_index(h, h->terms, sel, h->term_ix[ph]);
     if (rc) return rc;
   }
+  if (h->nl_general >= 0) {
+    // nonlinear cells: their coefficient arrays must exist (the host passes
+    // arrays, not uniform values), poles run in the ADE pass, FP32 storage
+    for (int c = 0; c < 3; ++c)
+      if (!h->ecoef[c][1] || (h->nl_general == 1 && !h->ecoef[c][0]))
+        return fail(FDTD_ERR_STATE, "nonlinear media need E coefficient arrays (decay and curl)");
+    if (h->storage != kStoreF32) return fail(FDTD_ERR_UNSUPPORTED, "nonlinear media with reduced field storage");
+    if (h->bloch) return fail(FDTD_ERR_UNSUPPORTED, "nonlinear media on Bloch (complex) fields");
+    if (!h->poles.empty()) {
+      if (!h->ade_pass || h->poles.size() > static_cast<size_t>(kAdeMaxPoles))
+        return fail(FDTD_ERR_UNSUPPORTED, "nonlinear media with poles need the ADE pass (at most 32 pole components)");
+      if (h->variant >= 4 && h->variant != kTileVariant)
+        return fail(FDTD_ERR_UNSUPPORTED, "nonlinear media with poles run launch variants 1-3 and 10");
+    }
+    const int64_t n = static_cast<int64_t>(h->nl_cells_h.size() / 4);
+    CUDA_TRY(cudaMalloc(&h->d_nl_cells, sizeof(int4) * n));
+    h->owned.push_back(reinterpret_cast<float*>(h->d_nl_cells));
+    CUDA_TRY(cudaMemcpy(h->d_nl_cells, h->nl_cells_h.data(), sizeof(int4) * n, cudaMemcpyHostToDevice));
+    std::vector<float> prm;
+    prm.reserve(static_cast<size_t>(6 * n));
+    for (int q = 0; q < 6; ++q) prm.insert(prm.end(), h->nl_prm_h[q].begin(), h->nl_prm_h[q].end());
+    rc = dev_copy(h, &h->d_nl_prm, prm.data(), prm.size());
+    if (!rc) CUDA_TRY(cudaStreamSynchronize(h->stream));
+    if (rc) return rc;
+    h->nl_n = n;
+    for (int a = 0; a < 3; ++a) {
+      h->nl_lo[a] = INT_MAX;
+      h->nl_hi[a] = -1;
+    }
+    for (int64_t t = 0; t < n; ++t)
+      for (int a = 0; a < 3; ++a) {
+        h->nl_lo[a] = std::min(h->nl_lo[a], h->nl_cells_h[4 * t + a]);
+        h->nl_hi[a] = std::max(h->nl_hi[a], h->nl_cells_h[4 * t + a] + 1);
+      }
+    if (n == 0)
+      for (int a = 0; a < 3; ++a) h->nl_lo[a] = h->nl_hi[a] = 0;
+    h->nl_cells_h.clear();
+    for (int q = 0; q < 6; ++q) h->nl_prm_h[q].clear();
+  }
   std::vector<PoleTerm> pv;
   for (const auto& ph : h->poles) pv.push_back(ph.t);
   rc = upload_vec(h, &h->d_poles, pv);
@@ -1815,6 +2006,7 @@ int fdtd_engine_finalize(fdtd_engine* h) {
     a.NX = h->NX;
     a.NZ = h->NZ;
     a.pec_faces = 0;
+    for (int c = 0; c < 3; ++c) a.nl_curl[c] = h->nl_general >= 0 ? h->ecoef[c][1] : nullptr;
     if (h->lines.empty())
       for (int f = 0; f < 6; ++f)
         if (h->desc.boundary[f] == FDTD_BND_PEC) a.pec_faces |= 1 << f;
@@ -2188,6 +2380,7 @@ int fdtd_engine_autotune(fdtd_engine* h, int* tile_rows, int* chunk_planes) {
     if (var == 4 && !h->tma_ready) continue;
     if (h->storage != kStoreF32 && var != 2) continue;  // reduced storage: the 64-register kernel only
     if ((h->wrap || h->pmc) && var > 3) continue;        // wrap and PMC faces: the scalar warp kernels only
+    if (h->nl_n > 0 && !h->poles.empty() && var > 3 && var != kTileVariant) continue;  // nonlinear poles: the ADE pass
     for (int cx : cxs) {
       if (cx > 2 * h->NX) continue;
       h->variant = var;
@@ -2254,6 +2447,8 @@ int fdtd_engine_set_launch(fdtd_engine* h, int variant, int tile_rows, int chunk
   if (h->wrap && variant > 3)
     return fail(FDTD_ERR_UNSUPPORTED, "periodic and Bloch faces run launch variants 1-3 only");
   if (h->pmc && variant > 3) return fail(FDTD_ERR_UNSUPPORTED, "PMC faces run launch variants 1-3 only");
+  if (h->nl_general >= 0 && !h->poles.empty() && variant > 3 && variant != kTileVariant)
+    return fail(FDTD_ERR_UNSUPPORTED, "nonlinear media with poles run launch variants 1-3 and 10");
   h->variant = variant;
   if (chunk_planes > 0) h->CX = chunk_planes;
   else default_tiles(h);
@@ -2265,6 +2460,8 @@ int fdtd_engine_set_launch(fdtd_engine* h, int variant, int tile_rows, int chunk
 // Poles in the ADE pass after the step kernel (on) or inside it (off).
 int fdtd_engine_set_ade_pass(fdtd_engine* h, int on) {
   if (!h) return fail(FDTD_ERR_INVALID_ARG, "null engine");
+  if (!on && h->nl_general >= 0 && !h->poles.empty())
+    return fail(FDTD_ERR_UNSUPPORTED, "nonlinear media with poles need the ADE pass");
   h->ade_pass = on != 0;
   return 0;
 }
@@ -2334,6 +2531,7 @@ int fdtd_engine_adjoint_init(fdtd_engine* h, const int* design_boxes, int max_se
   if (h->storage != kStoreF32) return fail(FDTD_ERR_UNSUPPORTED, "the adjoint runs on FP32 field storage only");
   if (h->wrap) return fail(FDTD_ERR_UNSUPPORTED, "the adjoint of periodic and Bloch faces is not supported");
   if (h->pmc) return fail(FDTD_ERR_UNSUPPORTED, "the adjoint of PMC faces is not supported");
+  if (h->nl_general >= 0) return fail(FDTD_ERR_UNSUPPORTED, "the adjoint of nonlinear media is not supported");
   if (h->adj.ready) return fail(FDTD_ERR_STATE, "adjoint already initialised");
   AdjointHost& a = h->adj;
   a.q = AdjParams{};
@@ -2996,6 +3194,8 @@ int fdtd_bloch_create(fdtd_engine* re, fdtd_engine* im, const float* phase_cos, 
   if (!re->finalized || !im->finalized) return fail(FDTD_ERR_STATE, "both engines must be finalized");
   if (re->in_pair || im->in_pair) return fail(FDTD_ERR_STATE, "an engine is already in a Bloch pair");
   if (!re->wrap) return fail(FDTD_ERR_INVALID_ARG, "the engines have no periodic or Bloch face");
+  if (re->nl_general >= 0 || im->nl_general >= 0)
+    return fail(FDTD_ERR_UNSUPPORTED, "nonlinear media on Bloch (complex) fields");
   const fdtd_grid_desc &a = re->desc, &b = im->desc;
   bool same = a.nx == b.nx && a.ny == b.ny && a.nz == b.nz && a.dt == b.dt && re->stream == im->stream && re->M == im->M;
   for (int f = 0; f < 6; ++f) same = same && a.boundary[f] == b.boundary[f];

@@ -152,6 +152,11 @@ struct StepParams {
   // witwin/maxwell/fdtd/runtime/stepping.py:2316-2318); with TFSF the
   // corrections and sources added after the update stay (0).
   int pec_clamp;
+  // Bounding box [nl_lo, nl_hi) (node indices) of the cells whose E
+  // coefficients an instantaneous nonlinearity rewrites before every step:
+  // warp tasks whose footprint meets it read the coefficient arrays whatever
+  // the values at classification time (empty: nl_lo[0] >= nl_hi[0]).
+  int nl_lo[3], nl_hi[3];
 };
 
 // A warp task needs the CPML code (some cell of its footprint lies in a slab)
@@ -193,6 +198,10 @@ struct AdeParams {
   // PEC faces (bit f for face f) whose tangential E stays zero after the pass
   // (StepParams::pec_clamp), and the grid extents the face test needs
   int pec_faces, NX, NZ;
+  // Scenes with an instantaneous nonlinearity subtract J times the E curl
+  // coefficient of this step (dt 1) instead of dt J / eps
+  // (witwin/maxwell/fdtd/runtime/materials.py:751-773); nullptr otherwise.
+  const float* nl_curl[3];
   AdePole poles[kAdeMaxPoles];
 };
 // ADE pass after the step kernel: tiles are int4 {i * NY + j, k0, k1, pole

@@ -504,6 +504,82 @@ bool cpml_args_ok(int mode, float* psi_a, float* psi_b, const float* ika, const 
   return mode == 1 || slab != nullptr;
 }
 
+// Instantaneous nonlinear coefficients of E component comp (kernels/
+// dispersive.cu:165-400): E collocated onto comp's Yee edge (own component
+// direct, the other two 4-point averaged with clamped indices), then the Kerr
+// curl (general = 0: curl = dt / eps_eff * decay) or the general decay / curl
+// pair (general = 1; dec is then the external decay).
+struct NlShapes {
+  int s[3][3];  // Ex, Ey, Ez array shapes
+};
+
+__device__ __forceinline__ float nl_at(const float* f, const NlShapes& sh, int c, int i, int j, int k) {
+  i = min(max(i, 0), sh.s[c][0] - 1);
+  j = min(max(j, 0), sh.s[c][1] - 1);
+  k = min(max(k, 0), sh.s[c][2] - 1);
+  return f[off3(i, j, k, sh.s[c][1], sh.s[c][2])];
+}
+
+__global__ void op_nonlinear_kernel(int comp, int general, NlShapes sh, const float* ex, const float* ey,
+                                    const float* ez, const float* eps, const float* dec, const float* sig_s,
+                                    const float* chi2, const float* chi3, const float* tpa, float dt, float eps0,
+                                    float* out_decay, float* out_curl) {
+  const int dx = sh.s[comp][0], dy = sh.s[comp][1], dz = sh.s[comp][2];
+  const int64_t n = static_cast<int64_t>(dx) * dy * dz;
+  for (int64_t x = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; x < n;
+       x += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    int i, j, k;
+    unflatten(x, dy, dz, i, j, k);
+    float vx, vy, vz;
+    if (comp == 0) {
+      vx = ex[x];
+      vy = 0.25f * (nl_at(ey, sh, 1, i, j - 1, k) + nl_at(ey, sh, 1, i, j, k) + nl_at(ey, sh, 1, i + 1, j - 1, k) +
+                    nl_at(ey, sh, 1, i + 1, j, k));
+      vz = 0.25f * (nl_at(ez, sh, 2, i, j, k - 1) + nl_at(ez, sh, 2, i, j, k) + nl_at(ez, sh, 2, i + 1, j, k - 1) +
+                    nl_at(ez, sh, 2, i + 1, j, k));
+    } else if (comp == 1) {
+      vx = 0.25f * (nl_at(ex, sh, 0, i - 1, j, k) + nl_at(ex, sh, 0, i, j, k) + nl_at(ex, sh, 0, i - 1, j + 1, k) +
+                    nl_at(ex, sh, 0, i, j + 1, k));
+      vy = ey[x];
+      vz = 0.25f * (nl_at(ez, sh, 2, i, j, k - 1) + nl_at(ez, sh, 2, i, j, k) + nl_at(ez, sh, 2, i, j + 1, k - 1) +
+                    nl_at(ez, sh, 2, i, j + 1, k));
+    } else {
+      vx = 0.25f * (nl_at(ex, sh, 0, i - 1, j, k) + nl_at(ex, sh, 0, i, j, k) + nl_at(ex, sh, 0, i - 1, j, k + 1) +
+                    nl_at(ex, sh, 0, i, j, k + 1));
+      vy = 0.25f * (nl_at(ey, sh, 1, i, j - 1, k) + nl_at(ey, sh, 1, i, j, k) + nl_at(ey, sh, 1, i, j - 1, k + 1) +
+                    nl_at(ey, sh, 1, i, j, k + 1));
+      vz = ez[x];
+    }
+    const float fsq = vx * vx + vy * vy + vz * vz;
+    const float floor_eps = 1.0e-12f * eps0;
+    if (!general) {
+      float eff = eps[x] + eps0 * chi3[x] * fsq;
+      if (eff < floor_eps) eff = floor_eps;
+      out_curl[x] = (dt / eff) * dec[x];
+    } else {
+      const float own = comp == 0 ? vx : (comp == 1 ? vy : vz);
+      float eff = eps[x] + eps0 * (chi2[x] * own + chi3[x] * fsq);
+      if (eff < floor_eps) eff = floor_eps;
+      float sigma = sig_s[x] + tpa[x] * fsq;
+      if (sigma < 0.0f) sigma = 0.0f;
+      const float half = 0.5f * sigma * dt / eff;
+      const float inv_denom = 1.0f / (1.0f + half);
+      out_decay[x] = dec[x] * (1.0f - half) * inv_denom;
+      out_curl[x] = dec[x] * (dt / eff) * inv_denom;
+    }
+  }
+}
+
+bool nl_shapes(const int* shapes, NlShapes& sh) {
+  if (!shapes) return false;
+  for (int c = 0; c < 3; ++c)
+    for (int a = 0; a < 3; ++a) {
+      sh.s[c][a] = shapes[3 * c + a];
+      if (sh.s[c][a] <= 0) return false;
+    }
+  return true;
+}
+
 }  // namespace
 
 extern "C" {
@@ -734,6 +810,32 @@ int fdtd_op_clamp_face(float* field, const int* fshape, int axis, int side, void
   op_clamp_kernel<<<blocks_for(static_cast<int64_t>(da) * db), kThreads, 0, static_cast<cudaStream_t>(stream)>>>(
       field, fshape[0], fshape[1], fshape[2], axis, side);
   return op_launch_check("clamp_face");
+}
+
+int fdtd_op_update_kerr_curl(int comp, const int* shapes, const float* ex, const float* ey, const float* ez,
+                             const float* eps, const float* decay, const float* chi3, float dt, float eps0,
+                             float* curl, void* stream) {
+  NlShapes sh;
+  if (comp < 0 || comp > 2 || !nl_shapes(shapes, sh) || !ex || !ey || !ez || !eps || !decay || !chi3 || !curl)
+    return op_fail(FDTD_ERR_INVALID_ARG, "update_kerr_curl: bad arguments");
+  const int64_t n = static_cast<int64_t>(sh.s[comp][0]) * sh.s[comp][1] * sh.s[comp][2];
+  op_nonlinear_kernel<<<blocks_for(n), kThreads, 0, static_cast<cudaStream_t>(stream)>>>(
+      comp, 0, sh, ex, ey, ez, eps, decay, nullptr, nullptr, chi3, nullptr, dt, eps0, nullptr, curl);
+  return op_launch_check("update_kerr_curl");
+}
+
+int fdtd_op_update_nonlinear_coefficients(int comp, const int* shapes, const float* ex, const float* ey,
+                                          const float* ez, const float* eps, const float* external_decay,
+                                          const float* sigma, const float* chi2, const float* chi3, const float* tpa,
+                                          float dt, float eps0, float* decay, float* curl, void* stream) {
+  NlShapes sh;
+  if (comp < 0 || comp > 2 || !nl_shapes(shapes, sh) || !ex || !ey || !ez || !eps || !external_decay || !sigma ||
+      !chi2 || !chi3 || !tpa || !decay || !curl)
+    return op_fail(FDTD_ERR_INVALID_ARG, "update_nonlinear_coefficients: bad arguments");
+  const int64_t n = static_cast<int64_t>(sh.s[comp][0]) * sh.s[comp][1] * sh.s[comp][2];
+  op_nonlinear_kernel<<<blocks_for(n), kThreads, 0, static_cast<cudaStream_t>(stream)>>>(
+      comp, 1, sh, ex, ey, ez, eps, external_decay, sigma, chi2, chi3, tpa, dt, eps0, decay, curl);
+  return op_launch_check("update_nonlinear_coefficients");
 }
 
 }  // extern "C"

@@ -878,6 +878,10 @@ __global__ void classify_vec_kernel(const StepParams p, int n_kblocks, int n_chu
       }
     }
   }
+  // cells whose coefficients an instantaneous nonlinearity rewrites every step
+  if (p.nl_lo[0] < p.nl_hi[0] && istart < p.nl_hi[0] && i1 > p.nl_lo[0] && kb < p.nl_hi[2] &&
+      kb + V > p.nl_lo[2] && ((jm >= p.nl_lo[1] && jm < p.nl_hi[1]) || (j >= p.nl_lo[1] && j < p.nl_hi[1])))
+    coef = true;
   const unsigned any_cpml = __any_sync(kFull, cpml), any_coef = __any_sync(kFull, coef);
   if (lane == 0) out[task] = static_cast<unsigned char>((any_cpml ? kClassCpml : 0u) | (any_coef ? kClassCoef : 0u));
 }

@@ -169,6 +169,12 @@ def slice_scene(cs: CompiledScene, x0: int, x1: int) -> tuple[CompiledScene, lis
             continue
         regions.append(CompiledRegion(reg.monitor, reg.component, (c[0] - lx0, c[1] - lx0) + tuple(c[2:])))
         placement.append((g, c[0] - reg.box[0]))
+    nonlinear = cs.nonlinear
+    if nonlinear is not None:
+        # the collocation of a cell next to a cut reads the ghost plane, which
+        # the exchange fills: owned cells see the single-domain values
+        nonlinear = dataclasses.replace(
+            nonlinear, channels={n: {k: cut(n, v) for k, v in ch.items()} for n, ch in nonlinear.channels.items()})
     local = dataclasses.replace(
         cs, nodes=(nl, cs.nodes[1], cs.nodes[2]), boundary=tuple(boundary), pml_lo=pml_lo, pml_hi=pml_hi,
         inv_e=inv_e, inv_h=inv_h, cpml=cpml,
@@ -176,6 +182,7 @@ def slice_scene(cs: CompiledScene, x0: int, x1: int) -> tuple[CompiledScene, lis
         decay={n: cut(n, a) for n, a in cs.decay.items()},
         curl={n: cut(n, a) for n, a in cs.curl.items()},
         poles=poles, patches=patches, line_patches=line_patches, regions=regions, shifted=shifted,
+        nonlinear=nonlinear,
     )
     return local, placement
 

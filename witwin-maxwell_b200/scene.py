@@ -170,9 +170,28 @@ class LorentzPole:
 
 @dataclass(frozen=True)
 class Medium:
+    """A material (witwin/maxwell/media.py): relative permittivity, dispersive
+    poles, diagonal anisotropy, static conductivity ``sigma`` (S/m) and the
+    instantaneous nonlinear channels: Kerr ``kerr_chi3`` (m^2/V^2), ``chi2``
+    (m/V) and two-photon absorption ``tpa_beta`` (m/W; conductivity
+    tpa_sigma |E|^2, media.py:395-423)."""
+
     eps_r: float = 1.0
     poles: tuple = ()
     eps_diag: tuple[float, float, float] | None = None  # diagonal anisotropy (eps_xx, eps_yy, eps_zz)
+    sigma: float = 0.0
+    kerr_chi3: float = 0.0
+    chi2: float = 0.0
+    tpa_beta: float = 0.0
+    tpa_index: float | None = None  # n0 of the TPA scale; sqrt(eps_r) when None
+
+    @property
+    def tpa_sigma(self) -> float:
+        """sigma_NL / |E|^2 = (4/3) beta (n0 eps0 c0)^2 (media.py:420-423, 884-893)."""
+        if self.tpa_beta == 0.0:
+            return 0.0
+        n0 = float(self.tpa_index) if self.tpa_index is not None else math.sqrt(float(self.eps_r))
+        return (4.0 / 3.0) * float(self.tpa_beta) * (n0 * EPSILON_0 * C_0) ** 2
 
     @staticmethod
     def debye(eps_inf: float, delta_eps: float, tau: float) -> "Medium":
@@ -484,10 +503,34 @@ class CompiledScene:
     bloch_cos: tuple[float, float, float] = (1.0, 1.0, 1.0)
     bloch_sin: tuple[float, float, float] = (0.0, 0.0, 0.0)
     shifted: list = field(default_factory=list)  # CompiledShiftedPatch
+    nonlinear: "CompiledNonlinear | None" = None
 
     @property
     def cells(self) -> int:
         return int(np.prod([n - 1 for n in self.nodes]))
+
+
+@dataclass
+class CompiledNonlinear:
+    """Instantaneous nonlinear channels on the E components
+    (witwin/maxwell/fdtd/runtime/materials.py:164-217): per component the
+    static decay (Kerr form) or external decay (general form, ones here: CPML is
+    not folded into the coefficients), the static conductivity and the chi2,
+    chi3 and TPA channels, averaged onto the Yee edges (float32, Yee shapes).
+    general: some chi2 or TPA channel is nonzero, and both the decay and the
+    curl coefficients are recomposed every step; else only the Kerr curl."""
+
+    general: bool
+    eps0: float
+    channels: dict  # component -> {"decay", "sigma", "chi2", "chi3", "tpa"}
+
+    def active(self, name: str) -> np.ndarray:
+        """Cells whose coefficients change with the field."""
+        ch = self.channels[name]
+        m = ch["chi3"] != 0
+        if self.general:
+            m = m | (ch["chi2"] != 0) | (ch["tpa"] != 0)
+        return m
 
 
 def _avg_node_to_component(node: np.ndarray, name: str) -> np.ndarray:
@@ -723,11 +766,17 @@ def compile_scene(scene: Scene, time_steps: int) -> CompiledScene:
     inv_h = [np.full(n - 1, 1.0 / d, dtype=np.float64).astype(np.float32) for n in nodes]
     # --- materials: node rasterisation, then node -> component averaging ---
     eps_node = [np.ones(nodes, dtype=np.float64) for _ in range(3)]
+    # conductivity and nonlinear channels blend like the static eps
+    # (compiler/materials.py:740-756): the last structure covering a node wins
+    chan_node = {k: np.zeros(nodes, dtype=np.float64) for k in ("sigma", "chi2", "chi3", "tpa")}
     pole_weights = []  # list of (pole, node weight array)
     for st in scene.structures:
         mask = st.geometry.node_mask(nodes)
         for a in range(3):
             eps_node[a][mask] = st.medium.axis_eps(a)
+        med = st.medium
+        for key, value in (("sigma", med.sigma), ("chi2", med.chi2), ("chi3", med.kerr_chi3), ("tpa", med.tpa_sigma)):
+            chan_node[key][mask] = float(value)
         for entry in pole_weights:
             entry[1][mask] = 0.0
         for pole in st.medium.poles:
@@ -744,17 +793,57 @@ def compile_scene(scene: Scene, time_steps: int) -> CompiledScene:
     eps = {}
     for a, name in enumerate(("Ex", "Ey", "Ez")):
         eps[name] = (EPSILON_0 * _avg_node_to_component(eps_node[a], name)).astype(np.float32)
-    # --- update coefficients (materials.py:942-1008): lossless, CPML not folded ---
+    # --- update coefficients (materials.py:942-1008): semi-implicit lossy fold, CPML not folded ---
+    chan = {k: {name: _avg_node_to_component(v, name).astype(np.float32) for name in ("Ex", "Ey", "Ez")}
+            for k, v in chan_node.items()}
+    conductive = bool(np.any(chan_node["sigma"] != 0))
+    is_nonlinear = any(bool(np.any(chan_node[k] != 0)) for k in ("chi2", "chi3", "tpa"))
+    general = bool(np.any(chan_node["chi2"] != 0) or np.any(chan_node["tpa"] != 0))
+    dt32 = np.float32(dt)
+    one32 = np.float32(1.0)
     decay, curl, uniform = {}, {}, {}
+    nl_channels = {}
+    static_curl = {}  # the static curl coefficients, from which the source terms are built
     for name in ("Ex", "Ey", "Ez"):
-        c = (np.float32(dt) / eps[name]).astype(np.float32)
-        decay[name] = None
-        if float(c.min()) == float(c.max()):
+        e = eps[name]
+        if conductive:
+            half = (np.float32(0.5) * chan["sigma"][name] * dt32) / e
+            denom = one32 + half
+            mdecay = ((one32 - half) / denom).astype(np.float32)
+            c = ((dt32 / e) / denom).astype(np.float32)
+        else:
+            mdecay = None
+            c = (dt32 / e).astype(np.float32)
+        static_curl[name] = np.float32(c.flat[0]) if float(c.min()) == float(c.max()) else c
+        if is_nonlinear:
+            # the field-dependent coefficients with every nonlinear channel at
+            # rest: constant on the cells without one (materials.py:1664-1770);
+            # the engine rewrites the others before every step
+            if general:
+                ext = np.ones_like(e)
+                sig = np.maximum(chan["sigma"][name], np.float32(0.0))
+                half = (np.float32(0.5) * sig * dt32) / e
+                inv_denom = one32 / (one32 + half)
+                decay[name] = (ext * (one32 - half) * inv_denom).astype(np.float32)
+                curl[name] = (ext * (dt32 / e) * inv_denom).astype(np.float32)
+                dparam = ext
+            else:
+                static = mdecay if mdecay is not None else np.ones_like(e)
+                decay[name] = mdecay
+                curl[name] = ((dt32 / e) * static).astype(np.float32)
+                dparam = static
+            uniform[name] = (1.0 if decay[name] is None else None, None)
+            nl_channels[name] = {"decay": dparam, "sigma": chan["sigma"][name], "chi2": chan["chi2"][name],
+                                 "chi3": chan["chi3"][name], "tpa": chan["tpa"][name]}
+            continue
+        decay[name] = mdecay
+        if mdecay is None and float(c.min()) == float(c.max()):
             curl[name] = None
             uniform[name] = (1.0, float(c.flat[0]))
         else:
             curl[name] = c
-            uniform[name] = (1.0, None)
+            uniform[name] = (1.0 if mdecay is None else None, None)
+    nonlinear = CompiledNonlinear(general, EPSILON_0, nl_channels) if is_nonlinear else None
     h_curl = float(np.float32(dt) / np.float32(MU_0))
     for name in ("Hx", "Hy", "Hz"):
         decay[name] = None
@@ -824,8 +913,7 @@ def compile_scene(scene: Scene, time_steps: int) -> CompiledScene:
         elif isinstance(src, PlaneSource):
             patches.extend(_plane_source_patches(scene, src, eps, dt, time_steps))
         elif isinstance(src, GaussianBeam):
-            curl_full = {name: curl[name] if curl[name] is not None else np.float32(uniform[name][1])
-                         for name in COMPONENTS}
+            curl_full = {name: static_curl.get(name, np.float32(uniform[name][1])) for name in COMPONENTS}
             beam_patches, beam_shifted = _beam_patches(scene, src, curl_full, dt, time_steps)
             patches.extend(beam_patches)
             shifted.extend(beam_shifted)
@@ -834,9 +922,7 @@ def compile_scene(scene: Scene, time_steps: int) -> CompiledScene:
                 raise ValueError("TFSF sources with Bloch faces are not supported; use PlaneSource")
             if aux_line is not None:
                 raise ValueError("one TFSF source per scene")
-            curl_full = {}
-            for name in COMPONENTS:
-                curl_full[name] = curl[name] if curl[name] is not None else np.float32(uniform[name][1])
+            curl_full = {name: static_curl.get(name, np.float32(uniform[name][1])) for name in COMPONENTS}
             aux_line, line_patches = _compile_tfsf(scene, src, curl_full, dt, time_steps)
         else:
             raise TypeError(f"unsupported source {type(src).__name__}")
@@ -882,6 +968,7 @@ def compile_scene(scene: Scene, time_steps: int) -> CompiledScene:
         poles=poles, patches=patches, aux_line=aux_line, line_patches=line_patches, regions=regions,
         frequencies=tuple(freq_list), monitor_frequencies=mon_freqs, window=window, design=design,
         complex_fields=complex_fields, bloch_cos=tuple(bcos), bloch_sin=tuple(bsin), shifted=shifted,
+        nonlinear=nonlinear,
     )
 
 

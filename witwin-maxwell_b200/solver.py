@@ -164,6 +164,23 @@ class B200FDTD:
                     ),
                     "set_coefficients",
                 )
+            nl = getattr(cs, "nonlinear", None)
+            if nl is not None:
+                # the nonlinear cells' parameters (materials.py:1664-1770); the
+                # coefficient arrays above hold the formula with the channels at rest
+                for name in ("Ex", "Ey", "Ez"):
+                    m = nl.active(name)
+                    ijk = np.ascontiguousarray(np.argwhere(m), dtype=np.int32)
+                    ch = nl.channels[name]
+                    prm = np.ascontiguousarray(np.stack(
+                        [cs.eps[name][m], ch["decay"][m], ch["sigma"][m], ch["chi2"][m], ch["chi3"][m], ch["tpa"][m]],
+                        axis=1), dtype=np.float32)
+                    _lib.check(
+                        lib.fdtd_engine_set_nonlinear(h, COMP_INDEX[name], int(len(ijk)), ctypes.c_void_p(ijk.ctypes.data),
+                                                      ctypes.c_void_p(prm.ctypes.data), int(nl.general),
+                                                      float(np.float32(nl.eps0))),
+                        "set_nonlinear",
+                    )
             self.pole_ids = []
             for pole in cs.poles:
                 pid = ctypes.c_int()
