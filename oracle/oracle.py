@@ -347,7 +347,8 @@ class OracleSimulation:
     def update_nonlinear(self):
         F = self.fields
         nl = self.nl
-        dt, eps0 = self.cs.dt, nl["eps0"]
+        # the reference's kernels take dt and eps0 as float (dispersive.cu:284-285)
+        dt, eps0 = float(np.float32(self.cs.dt)), float(np.float32(nl["eps0"]))
         out = {}
         for n in ("Ex", "Ey", "Ez"):
             ch, eps = nl["ch"][n], nl["eps"][n]

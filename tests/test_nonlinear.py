@@ -56,11 +56,11 @@ def test_oracle_nonlinear_coefficients_match_reference():
 def _scene(wm, kind: str, cells=(24, 20, 18)):
     sc = wm.Scene(cells=cells, spacing=25e-9, pml_cells=5)
     if kind == "kerr":
-        med = wm.Medium(eps_r=2.25, kerr_chi3=0.02)
+        med = wm.Medium(eps_r=2.25, kerr_chi3=1e-4)
     elif kind == "general":
-        med = wm.Medium(eps_r=2.25, kerr_chi3=0.02, chi2=0.09, tpa_beta=8e7, sigma=2e4)
+        med = wm.Medium(eps_r=2.25, kerr_chi3=1e-4, chi2=0.005, tpa_beta=5e6, sigma=2e4)
     elif kind == "kerr_lorentz":
-        med = wm.Medium(eps_r=2.0, poles=(wm.scene.LorentzPole(1.5, 250e12, 20e12),), kerr_chi3=0.03)
+        med = wm.Medium(eps_r=2.0, poles=(wm.scene.LorentzPole(1.5, 250e12, 20e12),), kerr_chi3=1.5e-4)
     else:  # lossy: conductivity only (no nonlinear channel)
         med = wm.Medium(eps_r=2.25, sigma=3e4)
     sc.structures.append(wm.Structure(wm.Box((8, 6, 5), (16, 14, 13)), med))
@@ -117,7 +117,7 @@ def test_nonlinearity_changes_the_oracle_run(kind):
     from oracle import oracle as orc
 
     wm = load_package()
-    steps = 120
+    steps = 240
     a = orc.OracleSimulation(wm.compile_scene(_scene(wm, kind), steps), "f64", threads=4).run(steps)
     linear = {"kerr": wm.Medium(eps_r=2.25), "general": wm.Medium(eps_r=2.25, sigma=2e4),
               "kerr_lorentz": wm.Medium(eps_r=2.0, poles=(wm.scene.LorentzPole(1.5, 250e12, 20e12),))}[kind]
@@ -192,7 +192,7 @@ def test_engine_nonlinear_every_launch_variant():
     from test_engine_parity import assert_fields_close
 
     wm = load_package()
-    steps = 120
+    steps = 240
     cs = wm.compile_scene(_scene(wm, "general"), steps)
     ref = orc.OracleSimulation(cs, "f64", threads=4).run(steps)
     for variant in range(1, 11):

@@ -28,7 +28,7 @@ def _scene(wm, nonlinear=False):
     if nonlinear:
         # Kerr, chi2 and TPA channels across the cut of two ranks (node plane 16)
         sc.structures.append(wm.Structure(wm.Box((12, 3, 3), (21, 12, 11)),
-                                          wm.Medium(eps_r=2.0, kerr_chi3=0.02, chi2=0.05, tpa_beta=5e7, sigma=1e4)))
+                                          wm.Medium(eps_r=2.0, kerr_chi3=1e-4, chi2=0.005, tpa_beta=5e6, sigma=1e4)))
     sc.structures.append(wm.Structure(wm.Box((10, 4, 4), (20, 12, 10)), wm.Medium(eps_r=3.0)))
     sc.structures.append(wm.Structure(wm.Sphere((15, 8, 7), 3.0), wm.Medium.lorentz(2.0, 3.0, 250e12, 20e12)))
     sc.structures.append(wm.Structure(wm.Box((18, 3, 3), (21, 13, 11)),
