@@ -183,6 +183,11 @@ int fdtd_engine_add_sample_region(fdtd_engine* h, int comp, const int* box, int6
  * window weight per step (n_steps entries, FP64).  Phases are reduced in FP64
  * on the GPU; H regions carry the -omega*dt/2 retard (spectral.py:197-220). */
 int fdtd_engine_set_dft(fdtd_engine* h, int n_freq, const double* omega, int n_steps, const double* window);
+/* The same with one window per frequency: window holds n_steps x n_freq FP64
+ * weights, [step][frequency] (the per-frequency spectral start steps of
+ * witwin/maxwell/fdtd/runtime/spectral.py:250-298: CW runs start each
+ * frequency's Hanning / ramp window after its own transient). */
+int fdtd_engine_set_dft_windows(fdtd_engine* h, int n_freq, const double* omega, int n_steps, const double* window);
 /* Read the accumulated DFT: re/im device arrays of n_freq * n_samples floats,
  * [freq][slot] order, unscaled (scale 2/sum(window) is applied by the caller). */
 int fdtd_engine_read_dft(fdtd_engine* h, float* re, float* im);

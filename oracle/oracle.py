@@ -430,7 +430,8 @@ class OracleSimulation:
         cs = self.cs
         if self.freqs.size == 0 or not cs.regions:
             return
-        w = float(cs.window[n])
+        # one weight per step, or one per (step, frequency)
+        w = np.broadcast_to(np.asarray(cs.window[n], dtype=np.float64), self.phase_cos.shape)
         wc = w * self.phase_cos
         ws = w * self.phase_sin
         hc = wc * self.h_off_cos - ws * self.h_off_sin
@@ -455,11 +456,14 @@ class OracleSimulation:
 
     def monitor_results(self) -> dict:
         cs = self.cs
-        scale = 2.0 / self.window_sum if self.window_sum > 0 else 0.0
+        total = np.broadcast_to(np.asarray(self.window_sum, dtype=np.float64), self.freqs.shape)
+        scale = np.zeros(self.freqs.shape)
+        np.divide(2.0, total, out=scale, where=total > 0)
         out: dict = {}
         for reg, (re, im) in zip(cs.regions, self.acc):
             fidx = [cs.frequencies.index(f) for f in cs.monitor_frequencies[reg.monitor]]
-            data = (re[fidx].astype(np.float64) + 1j * im[fidx].astype(np.float64)) * scale
+            sc = scale[fidx].reshape((-1,) + (1,) * (re.ndim - 1))
+            data = (re[fidx].astype(np.float64) + 1j * im[fidx].astype(np.float64)) * sc
             out.setdefault(reg.monitor, {})[reg.component] = data
         return out
 

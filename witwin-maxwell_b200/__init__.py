@@ -56,8 +56,8 @@ def __getattr__(name):
         from .solver import B200Batch
 
         return B200Batch
-    if name == "Simulation":
-        from .simulation import Simulation
+    if name in ("Simulation", "TimeConfig", "SpectralSampler"):
+        from . import simulation
 
-        return Simulation
+        return getattr(simulation, name)
     raise AttributeError(name)

@@ -70,6 +70,7 @@ _SIGNATURES = {
     "fdtd_engine_add_line_patch": ([_vp, _i, _c_int_p, _vp, _i, _i, _vp, _i, _f], _i),
     "fdtd_engine_add_sample_region": ([_vp, _i, _c_int_p, _c_i64_p], _i),
     "fdtd_engine_set_dft": ([_vp, _i, ctypes.POINTER(_d), _i, ctypes.POINTER(_d)], _i),
+    "fdtd_engine_set_dft_windows": ([_vp, _i, ctypes.POINTER(_d), _i, ctypes.POINTER(_d)], _i),
     "fdtd_engine_read_dft": ([_vp, _vp, _vp], _i),
     "fdtd_engine_finalize": ([_vp], _i),
     "fdtd_engine_step_range": ([_vp, _i, _i], _i),

@@ -29,7 +29,7 @@ import numpy as np
 import torch
 
 from . import _lib
-from .scene import EPSILON_0, MaterialRegion, Scene, compile_scene
+from .scene import EPSILON_0, MaterialRegion, Scene, compile_scene, window_scales
 from .solver import B200FDTD
 
 
@@ -157,8 +157,7 @@ class DesignProblem:
         nf = len(cs.frequencies)
         g_re = torch.zeros((nf, solver.n_samples), device=solver.device)
         g_im = torch.zeros((nf, solver.n_samples), device=solver.device)
-        norm = float(np.sum(cs.window[: solver.steps_done]))
-        scale = 2.0 / norm if norm > 0 else 0.0
+        scales = window_scales(cs.window, solver.steps_done, nf)
         for reg, base in zip(cs.regions, solver.region_base):
             g = grad.get(reg.monitor, {}).get(reg.component)
             if g is None:
@@ -168,8 +167,9 @@ class DesignProblem:
             count = (b[1] - b[0]) * (b[3] - b[2]) * (b[5] - b[4])
             fidx = [cs.frequencies.index(f) for f in cs.monitor_frequencies[reg.monitor]]
             flat = g.reshape(len(fidx), count)
-            g_re[fidx, base:base + count] += scale * flat.real
-            g_im[fidx, base:base + count] += scale * flat.imag
+            sc = torch.as_tensor(scales[fidx], dtype=torch.float32, device=solver.device)[:, None]
+            g_re[fidx, base:base + count] += sc * flat.real
+            g_im[fidx, base:base + count] += sc * flat.imag
         return g_re, g_im
 
     def backward(self, grad: dict) -> np.ndarray:

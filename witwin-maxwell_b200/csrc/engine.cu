@@ -193,15 +193,16 @@ __global__ void aux_history_kernel(int ne, const float* e_decay, const float* e_
 
 // DFT weights in FP64: phase = omega * (n [- 1/2]) * dt reduced modulo 2*pi in
 // double precision, window applied, stored as float2 (cos, sin).
-__global__ void dft_weight_kernel(int n_freq, int n_steps, const double* omega, const double* window, double dt,
-                                  float2* w_e, float2* w_h) {
+// window: one weight per step (per_freq 0) or per (step, frequency) (1).
+__global__ void dft_weight_kernel(int n_freq, int n_steps, const double* omega, const double* window, int per_freq,
+                                  double dt, float2* w_e, float2* w_h) {
   const int64_t total = static_cast<int64_t>(n_freq) * n_steps;
   const double two_pi = 6.283185307179586476925286766559;
   for (int64_t x = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; x < total;
        x += static_cast<int64_t>(gridDim.x) * blockDim.x) {
     const int n = static_cast<int>(x / n_freq);
     const int f = static_cast<int>(x % n_freq);
-    const double w = window[n];
+    const double w = per_freq ? window[x] : window[n];
     double pe = fmod(omega[f] * dt * static_cast<double>(n), two_pi);
     double ph = fmod(omega[f] * dt * (static_cast<double>(n) - 0.5), two_pi);
     double se, ce, sh, ch;
@@ -1829,7 +1830,9 @@ int fdtd_engine_add_sample_region(fdtd_engine* h, int comp, const int* box, int6
   return 0;
 }
 
-int fdtd_engine_set_dft(fdtd_engine* h, int n_freq, const double* omega, int n_steps, const double* window) {
+namespace {
+
+int set_dft_impl(fdtd_engine* h, int n_freq, const double* omega, int n_steps, const double* window, int per_freq) {
   if (!h || n_freq <= 0 || n_freq > 256 || !omega || n_steps <= 0 || !window)
     return fail(FDTD_ERR_INVALID_ARG, "bad DFT arguments");
   h->n_freq = n_freq;
@@ -1838,17 +1841,29 @@ int fdtd_engine_set_dft(fdtd_engine* h, int n_freq, const double* omega, int n_s
   cudaFree(h->w_h);
   CUDA_TRY(cudaMalloc(&h->w_e, sizeof(float2) * static_cast<size_t>(n_freq) * n_steps));
   CUDA_TRY(cudaMalloc(&h->w_h, sizeof(float2) * static_cast<size_t>(n_freq) * n_steps));
+  const size_t n_window = static_cast<size_t>(n_steps) * (per_freq ? n_freq : 1);
   double *d_omega = nullptr, *d_window = nullptr;
   CUDA_TRY(cudaMalloc(&d_omega, sizeof(double) * n_freq));
-  CUDA_TRY(cudaMalloc(&d_window, sizeof(double) * n_steps));
+  CUDA_TRY(cudaMalloc(&d_window, sizeof(double) * n_window));
   CUDA_TRY(cudaMemcpyAsync(d_omega, omega, sizeof(double) * n_freq, cudaMemcpyHostToDevice, h->stream));
-  CUDA_TRY(cudaMemcpyAsync(d_window, window, sizeof(double) * n_steps, cudaMemcpyHostToDevice, h->stream));
-  dft_weight_kernel<<<256, 256, 0, h->stream>>>(n_freq, n_steps, d_omega, d_window, h->desc.dt, h->w_e, h->w_h);
+  CUDA_TRY(cudaMemcpyAsync(d_window, window, sizeof(double) * n_window, cudaMemcpyHostToDevice, h->stream));
+  dft_weight_kernel<<<256, 256, 0, h->stream>>>(n_freq, n_steps, d_omega, d_window, per_freq, h->desc.dt, h->w_e,
+                                                h->w_h);
   CUDA_TRY(cudaGetLastError());
   CUDA_TRY(cudaStreamSynchronize(h->stream));
   cudaFree(d_omega);
   cudaFree(d_window);
   return 0;
+}
+
+}  // namespace
+
+int fdtd_engine_set_dft(fdtd_engine* h, int n_freq, const double* omega, int n_steps, const double* window) {
+  return set_dft_impl(h, n_freq, omega, n_steps, window, 0);
+}
+
+int fdtd_engine_set_dft_windows(fdtd_engine* h, int n_freq, const double* omega, int n_steps, const double* window) {
+  return set_dft_impl(h, n_freq, omega, n_steps, window, 1);
 }
 
 namespace {

@@ -533,6 +533,17 @@ class CompiledNonlinear:
         return m
 
 
+def window_scales(window: np.ndarray, steps: int, n_freq: int) -> np.ndarray:
+    """Per-frequency spectrum scale 2 / sum(window) over the first ``steps`` steps
+    (witwin/maxwell/fdtd/observers.py:236-241); ``window`` is one weight per step
+    or one per (step, frequency); 0 where nothing was sampled."""
+    w = np.asarray(window, dtype=np.float64)[: int(steps)]
+    total = np.broadcast_to(w.sum(axis=0), (n_freq,)).astype(np.float64)
+    out = np.zeros(n_freq, dtype=np.float64)
+    np.divide(2.0, total, out=out, where=total > 0)
+    return out
+
+
 def _avg_node_to_component(node: np.ndarray, name: str) -> np.ndarray:
     """witwin/maxwell/fdtd/runtime/materials.py:399-407."""
     if name == "Ex":

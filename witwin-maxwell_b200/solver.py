@@ -19,7 +19,7 @@ import numpy as np
 import torch
 
 from . import _lib
-from .scene import COMP_INDEX, CompiledScene, GaussianPulse, component_shape
+from .scene import COMP_INDEX, CompiledScene, GaussianPulse, component_shape, window_scales
 
 
 def _require_cuda(device: torch.device) -> None:
@@ -250,9 +250,11 @@ class B200FDTD:
             if cs.regions and cs.frequencies:
                 omega = (ctypes.c_double * len(cs.frequencies))(*[2.0 * np.pi * f for f in cs.frequencies])
                 window = np.ascontiguousarray(cs.window, dtype=np.float64)
+                # one weight per step, or per (step, frequency)
+                setter = lib.fdtd_engine_set_dft_windows if window.ndim == 2 else lib.fdtd_engine_set_dft
                 _lib.check(
-                    lib.fdtd_engine_set_dft(
-                        h, len(cs.frequencies), omega, int(window.size),
+                    setter(
+                        h, len(cs.frequencies), omega, int(window.shape[0]),
                         window.ctypes.data_as(ctypes.POINTER(ctypes.c_double)),
                     ),
                     "set_dft",
@@ -385,15 +387,15 @@ class B200FDTD:
             # complex field F = A + iB: DFT(F) = DFT(A) + i DFT(B)
             re_b, im_b = self.raw_dft(imag=True)
             re, im = re - im_b, im + re_b
-        norm = float(np.sum(cs.window[: self.steps_done]))
-        scale = 2.0 / norm if norm > 0 else 0.0
+        scales = torch.as_tensor(window_scales(cs.window, self.steps_done, len(cs.frequencies)),
+                                 dtype=torch.float32, device=self.device)
         out: dict = {}
         for reg, base in zip(cs.regions, self.region_base):
             b = reg.box
             shape = (b[1] - b[0], b[3] - b[2], b[5] - b[4])
             count = shape[0] * shape[1] * shape[2]
             fidx = [cs.frequencies.index(f) for f in cs.monitor_frequencies[reg.monitor]]
-            data = torch.complex(re[fidx, base:base + count], im[fidx, base:base + count]) * scale
+            data = torch.complex(re[fidx, base:base + count], im[fidx, base:base + count]) * scales[fidx, None]
             out.setdefault(reg.monitor, {})[reg.component] = data.reshape((len(fidx),) + shape)
         if host:
             staged: dict = {}
