@@ -144,6 +144,20 @@ int fdtd_engine_set_pole_state(fdtd_engine* h, int pole_id, const float* pol, co
 int fdtd_engine_set_nonlinear(fdtd_engine* h, int comp, int n_cells, const int* cells, const float* params,
                               int general, float eps0);
 
+/* Full (off-diagonal) anisotropy of E component comp (0..2) over box (Yee
+ * indices): after the step kernel the engine adds
+ *   E_c += (coeff_a <curlH_a> + coeff_b <curlH_b>) / 4
+ * (witwin/maxwell/fdtd/cuda/kernels/aniso.cu:26-580, applied right after the
+ * E update, runtime/stepping.py:1808-1811), a < b the two other axes,
+ * <curlH_d> the sum of curl(H)_d over the four d-edges around the cell and
+ * coeff = dt inv_cd / eps0 from the per-edge inverse permittivity tensor
+ * (runtime/materials.py:1421-1440); coeff_a / coeff_b are box-dense (host or
+ * device).  The base curl coefficient of the component carries the inverse
+ * tensor's diagonal.  One box per component; the box stays a cell clear of the
+ * CPML slabs; not with periodic / Bloch faces, poles, nonlinear media,
+ * reduced storage or the adjoint. */
+int fdtd_engine_set_full_aniso(fdtd_engine* h, int comp, const int* box, const float* coeff_a, const float* coeff_b);
+
 /* Soft source patch: comp gets coeff[cell] * signal[n] added at step n
  * (witwin/maxwell/fdtd/cuda/kernels/sources.cu:135-154; the signal table
  * holds the host-evaluated waveform, excitation/temporal.py:408-491). */
@@ -440,6 +454,14 @@ int fdtd_op_apply_polarization(int64_t n, const float* cur, const float* inv_eps
  * eps_eff = eps + eps0 (chi2 E_comp + chi3 |E|^2), sigma = max(sigma + tpa |E|^2, 0),
  * half = sigma dt / (2 eps_eff), decay = ext (1 - half) / (1 + half),
  * curl = ext dt / eps_eff / (1 + half). */
+/* Off-diagonal anisotropic coupling of E component comp (update_electric_e{x,y,z}_full_aniso,
+ * extension.cpp:2113-2115; kernels/aniso.cu:26-580): e has comp's Yee shape on a grid of nx x ny x nz nodes;
+ * coeff_a / coeff_b (comp's shape) weight the two other curl(H) components, lower axis first;
+ * inv_d* are the per-node inverse spacings; periodic axes wrap the stencils. */
+int fdtd_op_update_electric_full_aniso(int comp, int nx, int ny, int nz, float* e, const float* hx, const float* hy,
+                                       const float* hz, const float* coeff_a, const float* coeff_b,
+                                       const float* inv_dx, const float* inv_dy, const float* inv_dz, int periodic_x,
+                                       int periodic_y, int periodic_z, void* stream);
 int fdtd_op_update_kerr_curl(int comp, const int* shapes, const float* ex, const float* ey, const float* ez,
                              const float* eps, const float* decay, const float* chi3, float dt, float eps0,
                              float* curl, void* stream);

@@ -13,6 +13,7 @@ in ``fdtd_oracle.c`` on full Yee-shaped arrays:
     soft sources                       sources.cu:135-154, temporal.py:408-491
     ADE subtraction E -= dt J / eps    dispersive.cu:72-83, materials.py:911
     nonlinear E coefficients           dispersive.cu:165-400, materials.py:1664-1770
+    full-anisotropy coupling           aniso.cu:26-580, stepping.py:1808-1811
     monitor running DFT                observers.py:577-659, spectral.py:165-232
 
 The DFT phase follows the reference's observer path: a float64 rotation
@@ -133,6 +134,76 @@ def collocate_e(comp, ex, ey, ez):
     return vx, vy, ez
 
 
+def _aniso_curl_at(d, s, h, inv, periodic):
+    """curl(H)_d at the d-edges with index arrays s = (s0, s1, s2) (kernels/
+    aniso.cu:105-215): s_d an edge coordinate, the other two node coordinates;
+    returns (value, valid) with the sample skipped where a stencil leaves a
+    non-periodic axis (periodic axes wrap, the last node duplicating node 0)."""
+    n = [h[0].shape[0], h[1].shape[1], h[2].shape[2]]  # node counts
+    s = [np.array(v) for v in s]
+    valid = np.ones(np.broadcast(*s).shape, dtype=bool)
+    cnt = n[d] - 1
+    if periodic[d]:
+        s[d] = np.where(s[d] < 0, s[d] + cnt, np.where(s[d] >= cnt, s[d] - cnt, s[d]))
+    else:
+        valid &= (s[d] >= 0) & (s[d] < cnt)
+    pairs = {}
+    for ax in range(3):
+        if ax == d:
+            continue
+        if periodic[ax]:
+            s[ax] = np.where(s[ax] == n[ax] - 1, 0, s[ax])
+        hi, lo = s[ax].copy(), s[ax] - 1
+        if periodic[ax]:
+            hi = np.where(hi > n[ax] - 2, hi - (n[ax] - 1), hi)
+            lo = np.where(lo < 0, lo + (n[ax] - 1), lo)
+        else:
+            valid &= (hi <= n[ax] - 2) & (lo >= 0)
+        pairs[ax] = (lo, hi)
+    s = [np.where(valid, v, 0) for v in s]
+    pairs = {ax: (np.where(valid, lo, 0), np.where(valid, hi, 0)) for ax, (lo, hi) in pairs.items()}
+
+    def diff(comp, ax):
+        lo, hi = pairs[ax]
+        a = [s[0], s[1], s[2]]
+        b = [s[0], s[1], s[2]]
+        a[ax], b[ax] = hi, lo
+        return (h[comp][tuple(a)] - h[comp][tuple(b)]) * inv[ax][s[ax]]
+
+    if d == 0:
+        value = diff(2, 1) - diff(1, 2)  # dHz/dy - dHy/dz
+    elif d == 1:
+        value = diff(0, 2) - diff(2, 0)  # dHx/dz - dHz/dx
+    else:
+        value = diff(1, 0) - diff(0, 1)  # dHy/dx - dHx/dy
+    return np.where(valid, value, 0.0), valid
+
+
+def full_aniso_correction(comp, e, h, coeff_a, coeff_b, inv, periodic=(False, False, False)):
+    """E_c += (coeff_a <curlH_a> + coeff_b <curlH_b>) / 4 (kernels/aniso.cu:373-580):
+    <curlH_d> sums curl(H)_d over the four d-edges around each E_c edge (own
+    axis offsets {0, 1}, curl axis {-1, 0}, the lower axis outermost), skipped
+    samples contributing nothing; cells with both coefficients zero unchanged.
+    ``h`` = (Hx, Hy, Hz), ``inv`` = per-node inverse spacings; updates e in place."""
+    idx = np.meshgrid(*(np.arange(v) for v in e.shape), indexing="ij")
+    da, db = (1, 2) if comp == 0 else ((0, 2) if comp == 1 else (0, 1))
+    active = (coeff_a != 0) | (coeff_b != 0)
+    total = np.zeros(e.shape, dtype=np.result_type(e, coeff_a))
+    for coeff, d in ((coeff_a, da), (coeff_b, db)):
+        outer, inner = min(comp, d), max(comp, d)
+        acc = np.zeros_like(total)
+        for u in range(2):
+            for v in range(2):
+                s = [idx[0].copy(), idx[1].copy(), idx[2].copy()]
+                s[outer] += u if outer == comp else u - 1
+                s[inner] += v if inner == comp else v - 1
+                value, _ = _aniso_curl_at(d, s, h, inv, periodic)
+                acc = acc + value
+        total = total + coeff * acc
+    e[active] += (0.25 * total)[active]
+    return e
+
+
 def kerr_curl(comp, ex, ey, ez, eps, decay, chi3, dt, eps0):
     """Kerr curl coefficient (dispersive.cu:267-321): dt / max(eps + eps0 chi3 |E|^2,
     1e-12 eps0) * decay."""
@@ -212,6 +283,14 @@ class OracleSimulation:
                 "comp": pole.component, "kind": pole.kind, "decay": pole.decay, "restoring": pole.restoring,
                 "drive": drive, "inv_eps": inv_eps, "P": np.zeros(shape, dt), "J": np.zeros(shape, dt),
             })
+        # full anisotropy: the off-diagonal coupling after the E update
+        self.aniso = []
+        for name, (box, ca, cb) in (getattr(cs, "aniso", None) or {}).items():
+            shape = component_shape(name, nodes)
+            fa, fb = np.zeros(shape, dt), np.zeros(shape, dt)
+            sl = (slice(box[0], box[1]), slice(box[2], box[3]), slice(box[4], box[5]))
+            fa[sl], fb[sl] = ca, cb
+            self.aniso.append((name, fa, fb))
         # instantaneous nonlinear channels: the E coefficients are recomposed
         # from E^n over every cell before each E update (materials.py:1664-1770)
         self.nl = None
@@ -404,6 +483,9 @@ class OracleSimulation:
         if self.nl is not None:
             self.update_nonlinear()
         self.update_e()
+        for name, fa, fb in self.aniso:  # stepping.py:1808-1811
+            full_aniso_correction("xyz".index(name[1]), self.fields[name],
+                                  (self.fields["Hx"], self.fields["Hy"], self.fields["Hz"]), fa, fb, self.inv_e)
         if self.aux is not None:
             self._line_corrections(False)
             a = self.aux

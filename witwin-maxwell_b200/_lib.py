@@ -66,6 +66,7 @@ _SIGNATURES = {
     "fdtd_engine_add_patch": ([_vp, _i, _c_int_p, _vp, _vp, _i, _f], _i),
     "fdtd_engine_add_shifted_patch": ([_vp, _i, _c_int_p, _vp, _vp, _d, _i, _d, _d, _d, _d, _d, _i], _i),
     "fdtd_engine_set_nonlinear": ([_vp, _i, _i, _vp, _vp, _i, _f], _i),
+    "fdtd_engine_set_full_aniso": ([_vp, _i, _c_int_p, _vp, _vp], _i),
     "fdtd_engine_add_aux_line": ([_vp, _i, _vp, _vp, _vp, _vp, _i, _vp, _i, _c_int_p], _i),
     "fdtd_engine_add_line_patch": ([_vp, _i, _c_int_p, _vp, _i, _i, _vp, _i, _f], _i),
     "fdtd_engine_add_sample_region": ([_vp, _i, _c_int_p, _c_i64_p], _i),
@@ -111,6 +112,8 @@ _SIGNATURES = {
     "fdtd_op_update_drude": ([_i64, _vp, _vp, _f, _vp, _vp], _i),
     "fdtd_op_update_lorentz": ([_i64, _vp, _vp, _f, _f, _f, _vp, _vp, _vp], _i),
     "fdtd_op_apply_polarization": ([_i64, _vp, _vp, _f, _vp, _vp], _i),
+    "fdtd_op_update_electric_full_aniso": ([_i, _i, _i, _i, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _i, _i, _i,
+                                            _vp], _i),
     "fdtd_op_update_kerr_curl": ([_i, _c_int_p, _vp, _vp, _vp, _vp, _vp, _vp, _f, _f, _vp, _vp], _i),
     "fdtd_op_update_nonlinear_coefficients": ([_i, _c_int_p, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _f, _f,
                                                _vp, _vp, _vp], _i),

@@ -150,6 +150,30 @@ def _full(t, like, n=None):
     return t
 
 
+# (curl component of the first coefficient, of the second) per E component
+_ANISO = {"Ex": ("Y", "Z"), "Ey": ("X", "Z"), "Ez": ("X", "Y")}
+
+
+def _full_aniso(comp: str):
+    """updateElectricField{Ex,Ey,Ez}FullAniso3D (witwin/maxwell/fdtd/cuda/backend.py,
+    update_electric_e*_full_aniso; kernels/aniso.cu:26-580)."""
+    c = "xyz".index(comp[1].lower())
+    first, second = _ANISO[comp]
+
+    def run(*, Hx, Hy, Hz, invDx, invDy, invDz, periodicX=0, periodicY=0, periodicZ=0, **kw):
+        e = kw[comp]
+        ca, cb = kw[f"Coeff{first}"], kw[f"Coeff{second}"]
+        for name, t in ((comp, e), ("Hx", Hx), ("Hy", Hy), ("Hz", Hz), (f"Coeff{first}", ca), (f"Coeff{second}", cb)):
+            _check_tensor(t, name)
+        nodes = [Hx.shape[0], Hy.shape[1], Hz.shape[2]]
+        inv = [_full(t, e, n) for t, n in zip((invDx, invDy, invDz), nodes)]
+        _lib.check(_lib.load().fdtd_op_update_electric_full_aniso(
+            c, *nodes, _lib.ptr(e), _lib.ptr(Hx), _lib.ptr(Hy), _lib.ptr(Hz), _lib.ptr(ca), _lib.ptr(cb),
+            *(_lib.ptr(t) for t in inv), int(periodicX), int(periodicY), int(periodicZ), _stream(e)), "full aniso")
+
+    return run
+
+
 def _nl_shapes(ex, ey, ez):
     return (ctypes.c_int * 9)(*ex.shape, *ey.shape, *ez.shape)
 
@@ -355,6 +379,9 @@ _KERNELS.update({
     "updateDrudeCurrent3D": _drude,
     "updateLorentzCurrent3D": _lorentz,
     "applyPolarizationCurrent3D": _apply_polarization,
+    "updateElectricFieldExFullAniso3D": _full_aniso("Ex"),
+    "updateElectricFieldEyFullAniso3D": _full_aniso("Ey"),
+    "updateElectricFieldEzFullAniso3D": _full_aniso("Ez"),
     "updateKerrElectricFieldExCurl3D": _kerr_curl("Ex"),
     "updateKerrElectricFieldEyCurl3D": _kerr_curl("Ey"),
     "updateKerrElectricFieldEzCurl3D": _kerr_curl("Ez"),

@@ -492,6 +492,109 @@ __global__ void __launch_bounds__(256) nonlinear_kernel(const __grid_constant__ 
   }
 }
 
+// Off-diagonal anisotropic coupling (witwin/maxwell/fdtd/cuda/kernels/
+// aniso.cu:26-580, applied right after the E update, runtime/stepping.py:
+// 1808-1811): after the step kernel, every E cell of an anisotropic box gets
+//   E_c += (coeff_a <curlH_a> + coeff_b <curlH_b>) / 4
+// from the new H, <curlH_d> the sum of curl(H)_d (backward differences) over
+// the four d-edges around the cell; a sample whose stencil leaves the grid is
+// skipped.  Boxes stay clear of the CPML slabs and of wrapped faces (the host
+// checks), so plain differences are exact there.
+constexpr int kMaxAniso = 3;
+struct AnisoHost {
+  int comp;
+  int box[6];
+  float* ca;  // box-dense coefficients of the two off-axis curl components (lower axis first)
+  float* cb;
+};
+
+struct AnisoLaunch {
+  int count;
+  int comp[kMaxAniso];
+  int box[kMaxAniso][6];
+  const float* ca[kMaxAniso];
+  const float* cb[kMaxAniso];
+  const float* H[3];  // H^{n+1/2} (padded)
+  float* E[3];        // E^{n+1} (padded)
+  const float* inv[3];
+  float inv_u[3];
+  int uniform;
+  int n[3];
+  int NY, P;
+  int pec_faces;  // PEC faces (bit f) whose tangential E stays zero (scenes without TFSF)
+};
+
+__device__ __forceinline__ float an_h(const AnisoLaunch& a, int c, int i, int j, int k) {
+  return __ldg(a.H[c] + (static_cast<int64_t>(i) * a.NY + j) * a.P + k);
+}
+
+__device__ __forceinline__ float an_inv(const AnisoLaunch& a, int axis, int idx) {
+  return a.uniform ? a.inv_u[axis] : __ldg(a.inv[axis] + idx);
+}
+
+// curl(H)_d at the d-edge s (non-periodic axes): false when the stencil leaves the grid
+__device__ __forceinline__ bool an_curl(const AnisoLaunch& a, int d, const int* s, float& value) {
+  if (s[d] < 0 || s[d] > a.n[d] - 2) return false;
+  const int x = d == 0 ? 1 : 0, y = d == 2 ? 1 : 2;  // derivative axes, lower first
+  if (s[x] < 1 || s[x] > a.n[x] - 2 || s[y] < 1 || s[y] > a.n[y] - 2) return false;
+  if (d == 0) {  // dHz/dy - dHy/dz
+    value = (an_h(a, 2, s[0], s[1], s[2]) - an_h(a, 2, s[0], s[1] - 1, s[2])) * an_inv(a, 1, s[1]) -
+            (an_h(a, 1, s[0], s[1], s[2]) - an_h(a, 1, s[0], s[1], s[2] - 1)) * an_inv(a, 2, s[2]);
+  } else if (d == 1) {  // dHx/dz - dHz/dx
+    value = (an_h(a, 0, s[0], s[1], s[2]) - an_h(a, 0, s[0], s[1], s[2] - 1)) * an_inv(a, 2, s[2]) -
+            (an_h(a, 2, s[0], s[1], s[2]) - an_h(a, 2, s[0] - 1, s[1], s[2])) * an_inv(a, 0, s[0]);
+  } else {  // dHy/dx - dHx/dy
+    value = (an_h(a, 1, s[0], s[1], s[2]) - an_h(a, 1, s[0] - 1, s[1], s[2])) * an_inv(a, 0, s[0]) -
+            (an_h(a, 0, s[0], s[1], s[2]) - an_h(a, 0, s[0], s[1] - 1, s[2])) * an_inv(a, 1, s[1]);
+  }
+  return true;
+}
+
+__global__ void __launch_bounds__(256) aniso_pass_kernel(const __grid_constant__ AnisoLaunch a) {
+  const int t = blockIdx.y;
+  const int comp = a.comp[t];
+  const int* b = a.box[t];
+  const int n1 = b[3] - b[2], n2 = b[5] - b[4];
+  const int64_t cells = static_cast<int64_t>(b[1] - b[0]) * n1 * n2;
+  const int da = comp == 0 ? 1 : 0, db = comp == 2 ? 1 : 2;
+  for (int64_t c = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; c < cells;
+       c += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    const float c_a = __ldg(a.ca[t] + c), c_b = __ldg(a.cb[t] + c);
+    if (c_a == 0.0f && c_b == 0.0f) continue;
+    const int k = b[4] + static_cast<int>(c % n2);
+    const int j = b[2] + static_cast<int>((c / n2) % n1);
+    const int i = b[0] + static_cast<int>(c / (static_cast<int64_t>(n1) * n2));
+    const int pos[3] = {i, j, k};
+    if (a.pec_faces) {
+      // tangential E on a PEC face stays zero
+      bool face = false;
+      for (int ax = 0; ax < 3; ++ax) {
+        if (ax == comp) continue;
+        face = face || (pos[ax] == 0 && (a.pec_faces >> (2 * ax) & 1)) ||
+               (pos[ax] == a.n[ax] - 1 && (a.pec_faces >> (2 * ax + 1) & 1));
+      }
+      if (face) continue;
+    }
+    float acc[2] = {0.0f, 0.0f};
+    for (int q = 0; q < 2; ++q) {
+      const int d = q == 0 ? da : db;
+      if ((q == 0 ? c_a : c_b) == 0.0f) continue;
+      // own axis offsets {0, +1}, curl axis {-1, 0}; the lower axis outermost
+      const int outer = min(comp, d), inner = max(comp, d);
+      for (int u = 0; u < 2; ++u)
+        for (int v = 0; v < 2; ++v) {
+          int s[3] = {i, j, k};
+          s[outer] += outer == comp ? u : u - 1;
+          s[inner] += inner == comp ? v : v - 1;
+          float sample;
+          if (an_curl(a, d, s, sample)) acc[q] += sample;
+        }
+    }
+    float* e = a.E[comp] + (static_cast<int64_t>(i) * a.NY + j) * a.P + k;
+    *e += 0.25f * (c_a * acc[0] + c_b * acc[1]);
+  }
+}
+
 struct AdjointHost {
   bool ready = false;
   AdjParams q{};
@@ -539,6 +642,7 @@ struct fdtd_engine {
   int4* d_nl_cells = nullptr;
   float* d_nl_prm = nullptr;
   int nl_lo[3] = {0, 0, 0}, nl_hi[3] = {0, 0, 0};
+  std::vector<AnisoHost> aniso;  // full-anisotropy boxes (fdtd_engine_set_full_aniso)
   bool bloch = false;
   bool in_pair = false;
   int64_t plane = 0, vol = 0;
@@ -945,6 +1049,43 @@ int launch_nonlinear(fdtd_engine* h) {
   return 0;
 }
 
+int launch_aniso(fdtd_engine* h, const StepParams& p) {
+  AnisoLaunch a{};
+  a.count = static_cast<int>(h->aniso.size());
+  int64_t most = 0;
+  for (int t = 0; t < a.count; ++t) {
+    const AnisoHost& x = h->aniso[t];
+    a.comp[t] = x.comp;
+    for (int q = 0; q < 6; ++q) a.box[t][q] = x.box[q];
+    a.ca[t] = x.ca;
+    a.cb[t] = x.cb;
+    most = std::max<int64_t>(most, static_cast<int64_t>(x.box[1] - x.box[0]) * (x.box[3] - x.box[2]) *
+                                       (x.box[5] - x.box[4]));
+  }
+  for (int c = 0; c < 3; ++c) {
+    a.H[c] = p.Hout[c];
+    a.E[c] = p.Eout[c];
+    a.inv[c] = h->inv_e[c];
+    a.inv_u[c] = h->inv_e_u[c];
+  }
+  a.uniform = h->uniform_grid ? 1 : 0;
+  a.n[0] = h->NX;
+  a.n[1] = h->NY;
+  a.n[2] = h->NZ;
+  a.NY = h->NY;
+  a.P = h->P;
+  a.pec_faces = 0;
+  if (h->lines.empty())
+    for (int f = 0; f < 6; ++f)
+      if (h->desc.boundary[f] == FDTD_BND_PEC) a.pec_faces |= 1 << f;
+  const int gx = static_cast<int>(std::min<int64_t>((most + 255) / 256, 4 * 148));
+  aniso_pass_kernel<<<dim3(gx, a.count), 256, 0, h->stream>>>(a);
+  const cudaError_t err = cudaGetLastError();
+  if (err != cudaSuccess) return cuda_fail(err, "aniso_pass_kernel launch");
+  ++h->launches;
+  return 0;
+}
+
 int launch_step(fdtd_engine* h, int n, int slot) {
   if (!h->shifted.empty()) {
     const int rc = launch_shifted(h, n);
@@ -1033,6 +1174,10 @@ int launch_step(fdtd_engine* h, int n, int slot) {
   cudaError_t err = cudaGetLastError();
   if (err != cudaSuccess) return cuda_fail(err, "warp_step_kernel launch");
   ++h->launches;
+  if (!h->aniso.empty()) {
+    const int rc = launch_aniso(h, p);
+    if (rc) return rc;
+  }
   if (ade_pass) {
     for (int c = 0; c < 3; ++c) {
       h->ade.Ein[c] = p.Ein[c];
@@ -1738,6 +1883,36 @@ int fdtd_engine_set_nonlinear(fdtd_engine* h, int comp, int n_cells, const int* 
   return 0;
 }
 
+int fdtd_engine_set_full_aniso(fdtd_engine* h, int comp, const int* box, const float* coeff_a, const float* coeff_b) {
+  if (!h || comp < 0 || comp > 2 || !box || !coeff_a || !coeff_b)
+    return fail(FDTD_ERR_INVALID_ARG, "bad full-anisotropy arguments");
+  if (h->finalized) return fail(FDTD_ERR_STATE, "engine already finalized");
+  if (static_cast<int>(h->aniso.size()) >= kMaxAniso) return fail(FDTD_ERR_UNSUPPORTED, "one anisotropic box per component");
+  for (const auto& x : h->aniso)
+    if (x.comp == comp) return fail(FDTD_ERR_UNSUPPORTED, "one anisotropic box per component");
+  if (!box_ok(h, comp, box)) return fail(FDTD_ERR_INVALID_ARG, "anisotropic box outside the component extent");
+  if (h->wrap) return fail(FDTD_ERR_UNSUPPORTED, "full anisotropy with periodic or Bloch faces");
+  if (h->storage != kStoreF32) return fail(FDTD_ERR_UNSUPPORTED, "full anisotropy with reduced field storage");
+  const int n[3] = {h->NX, h->NY, h->NZ};
+  for (int ax = 0; ax < 3; ++ax) {
+    // the box and its curl stencils (one cell around it) stay clear of the CPML slabs
+    if (h->desc.pml_lo[ax] > 0 && box[2 * ax] < h->desc.pml_lo[ax] + 1)
+      return fail(FDTD_ERR_UNSUPPORTED, "anisotropic box within a cell of a CPML slab");
+    if (h->desc.pml_hi[ax] > 0 && box[2 * ax + 1] > n[ax] - 1 - h->desc.pml_hi[ax] - 1)
+      return fail(FDTD_ERR_UNSUPPORTED, "anisotropic box within a cell of a CPML slab");
+  }
+  const int64_t cnt = static_cast<int64_t>(box[1] - box[0]) * (box[3] - box[2]) * (box[5] - box[4]);
+  AnisoHost x{};
+  x.comp = comp;
+  for (int q = 0; q < 6; ++q) x.box[q] = box[q];
+  int rc = dev_copy(h, &x.ca, coeff_a, cnt);
+  if (!rc) rc = dev_copy(h, &x.cb, coeff_b, cnt);
+  if (!rc) CUDA_TRY(cudaStreamSynchronize(h->stream));
+  if (rc) return rc;
+  h->aniso.push_back(x);
+  return 0;
+}
+
 int fdtd_engine_add_aux_line(fdtd_engine* h, int n_e, const float* e_decay, const float* e_curl,
                              const float* h_decay, const float* h_curl, int source_index, const float* source,
                              int n_steps, int* line_id) {
@@ -1957,6 +2132,8 @@ int fdtd_engine_finalize(fdtd_engine* h) {
     rc = build_box_index(h, h->terms, sel, h->term_ix[ph]);
     if (rc) return rc;
   }
+  if (!h->aniso.empty() && (!h->poles.empty() || h->nl_general >= 0))
+    return fail(FDTD_ERR_UNSUPPORTED, "full anisotropy with dispersive or nonlinear media");
   if (h->nl_general >= 0) {
     // nonlinear cells: their coefficient arrays must exist (the host passes
     // arrays, not uniform values), poles run in the ADE pass, FP32 storage
@@ -2547,6 +2724,7 @@ int fdtd_engine_adjoint_init(fdtd_engine* h, const int* design_boxes, int max_se
   if (h->wrap) return fail(FDTD_ERR_UNSUPPORTED, "the adjoint of periodic and Bloch faces is not supported");
   if (h->pmc) return fail(FDTD_ERR_UNSUPPORTED, "the adjoint of PMC faces is not supported");
   if (h->nl_general >= 0) return fail(FDTD_ERR_UNSUPPORTED, "the adjoint of nonlinear media is not supported");
+  if (!h->aniso.empty()) return fail(FDTD_ERR_UNSUPPORTED, "the adjoint of full anisotropy is not supported");
   if (h->adj.ready) return fail(FDTD_ERR_STATE, "adjoint already initialised");
   AdjointHost& a = h->adj;
   a.q = AdjParams{};

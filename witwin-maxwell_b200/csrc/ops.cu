@@ -570,6 +570,115 @@ __global__ void op_nonlinear_kernel(int comp, int general, NlShapes sh, const fl
   }
 }
 
+// Off-diagonal (full-tensor) anisotropic coupling of E component comp
+// (kernels/aniso.cu:26-580): E_c += coeff_a <curlH_a> / 4 + coeff_b <curlH_b> / 4,
+// with <curlH_d> the sum of curl(H)_d over the four d-edges around the E_c edge
+// (curl from H with backward differences at each d-edge).  A sample whose
+// stencil leaves a non-periodic axis is skipped; periodic axes wrap (the last
+// node duplicates node 0).  Cells with both coefficients zero are untouched.
+struct AnisoGrid {
+  int n[3];      // node counts
+  int per[3];    // periodic flags
+  const float* h[3];
+  const float* inv[3];
+};
+
+// Edge coordinate (array length n - 1) wrapped on a periodic axis; -1 = skip.
+__device__ __forceinline__ int aniso_edge(int c, int n, int per) {
+  if (c >= 0 && c < n - 1) return c;
+  if (!per) return -1;
+  return c < 0 ? c + (n - 1) : c - (n - 1);
+}
+
+// Backward edge pair (c - 1, c) at node coordinate c (after the periodic node map).
+__device__ __forceinline__ bool aniso_pair(int& c, int n, int per, int& lo, int& hi) {
+  if (per && c == n - 1) c = 0;
+  hi = c;
+  lo = c - 1;
+  if (hi > n - 2) {
+    if (!per) return false;
+    hi -= n - 1;
+  }
+  if (lo < 0) {
+    if (!per) return false;
+    lo += n - 1;
+  }
+  return true;
+}
+
+__device__ __forceinline__ float aniso_h(const AnisoGrid& g, int c, int i, int j, int k) {
+  // H shapes: Hx (n0, n1 - 1, n2 - 1), Hy (n0 - 1, n1, n2 - 1), Hz (n0 - 1, n1 - 1, n2)
+  const int ny = c == 1 ? g.n[1] : g.n[1] - 1;
+  const int nz = c == 2 ? g.n[2] : g.n[2] - 1;
+  return __ldg(g.h[c] + off3(i, j, k, ny, nz));
+}
+
+// curl(H)_d at the d-edge (s0, s1, s2) (s_d an edge coordinate, the others
+// node coordinates); false when the sample is skipped.
+__device__ bool aniso_curl(const AnisoGrid& g, int d, int s0, int s1, int s2, float& value) {
+  int s[3] = {s0, s1, s2};
+  s[d] = aniso_edge(s[d], g.n[d], g.per[d]);
+  if (s[d] < 0) return false;
+  const int a = d == 0 ? 1 : 0, b = d == 2 ? 1 : 2;  // the two derivative axes, a < b
+  int alo, ahi, blo, bhi;
+  if (!aniso_pair(s[a], g.n[a], g.per[a], alo, ahi) || !aniso_pair(s[b], g.n[b], g.per[b], blo, bhi)) return false;
+  // curl_d = d(H_b')/da - d(H_a')/db with the cyclic pairs of (d, a, b):
+  //   x: dHz/dy - dHy/dz;  y: dHx/dz - dHz/dx;  z: dHy/dx - dHx/dy
+  if (d == 1) {
+    // dHx/dz (Hx at (s0, s1, z)) - dHz/dx (Hz at (x, s1, s2))
+    const float d_z = (aniso_h(g, 0, s[0], s[1], bhi) - aniso_h(g, 0, s[0], s[1], blo)) * __ldg(g.inv[2] + s[2]);
+    const float d_x = (aniso_h(g, 2, ahi, s[1], s[2]) - aniso_h(g, 2, alo, s[1], s[2])) * __ldg(g.inv[0] + s[0]);
+    value = d_z - d_x;
+  } else if (d == 0) {
+    // dHz/dy (Hz at (s0, y, s2)) - dHy/dz (Hy at (s0, s1, z))
+    const float d_y = (aniso_h(g, 2, s[0], ahi, s[2]) - aniso_h(g, 2, s[0], alo, s[2])) * __ldg(g.inv[1] + s[1]);
+    const float d_z = (aniso_h(g, 1, s[0], s[1], bhi) - aniso_h(g, 1, s[0], s[1], blo)) * __ldg(g.inv[2] + s[2]);
+    value = d_y - d_z;
+  } else {
+    // dHy/dx (Hy at (x, s1, s2)) - dHx/dy (Hx at (s0, y, s2))
+    const float d_x = (aniso_h(g, 1, ahi, s[1], s[2]) - aniso_h(g, 1, alo, s[1], s[2])) * __ldg(g.inv[0] + s[0]);
+    const float d_y = (aniso_h(g, 0, s[0], bhi, s[2]) - aniso_h(g, 0, s[0], blo, s[2])) * __ldg(g.inv[1] + s[1]);
+    value = d_x - d_y;
+  }
+  return true;
+}
+
+__global__ void op_full_aniso_kernel(int comp, AnisoGrid g, const float* __restrict__ ca, const float* __restrict__ cb,
+                                     float* __restrict__ e) {
+  const int ex = comp == 0 ? g.n[0] - 1 : g.n[0], ey = comp == 1 ? g.n[1] - 1 : g.n[1];
+  const int ez = comp == 2 ? g.n[2] - 1 : g.n[2];
+  const int64_t total = static_cast<int64_t>(ex) * ey * ez;
+  // the two off-axis curl components (a < b) and, per axis, the offsets of the
+  // four neighbouring edges: the own axis spans {c, c + 1} (node positions
+  // around the half-index edge), the curl's axis spans {c - 1, c}
+  const int da = comp == 0 ? 1 : 0, db = comp == 2 ? 1 : 2;
+  for (int64_t x = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; x < total;
+       x += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    const float c_a = ca[x], c_b = cb[x];
+    if (c_a == 0.0f && c_b == 0.0f) continue;
+    int i, j, k;
+    unflatten(x, ey, ez, i, j, k);
+    const int pos[3] = {i, j, k};
+    float acc[2] = {0.0f, 0.0f};
+    for (int t = 0; t < 2; ++t) {
+      const int d = t == 0 ? da : db;
+      if ((t == 0 ? c_a : c_b) == 0.0f) continue;
+      // own axis offsets {0, +1}, curl axis d offsets {-1, 0}; the lower of the
+      // two axes is the outer loop (the reference's summation order)
+      const int outer = min(comp, d), inner = max(comp, d);
+      for (int u = 0; u < 2; ++u)
+        for (int v = 0; v < 2; ++v) {
+          int s[3] = {pos[0], pos[1], pos[2]};
+          s[outer] += outer == comp ? u : u - 1;
+          s[inner] += inner == comp ? v : v - 1;
+          float sample;
+          if (aniso_curl(g, d, s[0], s[1], s[2], sample)) acc[t] += sample;
+        }
+    }
+    e[x] += 0.25f * (c_a * acc[0] + c_b * acc[1]);
+  }
+}
+
 bool nl_shapes(const int* shapes, NlShapes& sh) {
   if (!shapes) return false;
   for (int c = 0; c < 3; ++c)
@@ -836,6 +945,31 @@ int fdtd_op_update_nonlinear_coefficients(int comp, const int* shapes, const flo
   op_nonlinear_kernel<<<blocks_for(n), kThreads, 0, static_cast<cudaStream_t>(stream)>>>(
       comp, 1, sh, ex, ey, ez, eps, external_decay, sigma, chi2, chi3, tpa, dt, eps0, decay, curl);
   return op_launch_check("update_nonlinear_coefficients");
+}
+
+int fdtd_op_update_electric_full_aniso(int comp, int nx, int ny, int nz, float* e, const float* hx, const float* hy,
+                                       const float* hz, const float* coeff_a, const float* coeff_b,
+                                       const float* inv_dx, const float* inv_dy, const float* inv_dz, int periodic_x,
+                                       int periodic_y, int periodic_z, void* stream) {
+  if (comp < 0 || comp > 2 || nx < 2 || ny < 2 || nz < 2 || !e || !hx || !hy || !hz || !coeff_a || !coeff_b ||
+      !inv_dx || !inv_dy || !inv_dz)
+    return op_fail(FDTD_ERR_INVALID_ARG, "update_electric_full_aniso: bad arguments");
+  AnisoGrid g;
+  g.n[0] = nx;
+  g.n[1] = ny;
+  g.n[2] = nz;
+  g.per[0] = periodic_x != 0;
+  g.per[1] = periodic_y != 0;
+  g.per[2] = periodic_z != 0;
+  g.h[0] = hx;
+  g.h[1] = hy;
+  g.h[2] = hz;
+  g.inv[0] = inv_dx;
+  g.inv[1] = inv_dy;
+  g.inv[2] = inv_dz;
+  const int64_t n = static_cast<int64_t>(comp == 0 ? nx - 1 : nx) * (comp == 1 ? ny - 1 : ny) * (comp == 2 ? nz - 1 : nz);
+  op_full_aniso_kernel<<<blocks_for(n), kThreads, 0, static_cast<cudaStream_t>(stream)>>>(comp, g, coeff_a, coeff_b, e);
+  return op_launch_check("update_electric_full_aniso");
 }
 
 }  // extern "C"

@@ -171,7 +171,7 @@ class LorentzPole:
 @dataclass(frozen=True)
 class Medium:
     """A material (witwin/maxwell/media.py): relative permittivity, dispersive
-    poles, diagonal anisotropy, static conductivity ``sigma`` (S/m) and the
+    poles, diagonal or full (symmetric) anisotropy, static conductivity ``sigma`` (S/m) and the
     instantaneous nonlinear channels: Kerr ``kerr_chi3`` (m^2/V^2), ``chi2``
     (m/V) and two-photon absorption ``tpa_beta`` (m/W; conductivity
     tpa_sigma |E|^2, media.py:395-423)."""
@@ -179,6 +179,8 @@ class Medium:
     eps_r: float = 1.0
     poles: tuple = ()
     eps_diag: tuple[float, float, float] | None = None  # diagonal anisotropy (eps_xx, eps_yy, eps_zz)
+    # off-diagonal relative permittivity (eps_xy, eps_xz, eps_yz) of a full symmetric tensor
+    eps_offdiag: tuple[float, float, float] | None = None
     sigma: float = 0.0
     kerr_chi3: float = 0.0
     chi2: float = 0.0
@@ -504,6 +506,9 @@ class CompiledScene:
     bloch_sin: tuple[float, float, float] = (0.0, 0.0, 0.0)
     shifted: list = field(default_factory=list)  # CompiledShiftedPatch
     nonlinear: "CompiledNonlinear | None" = None
+    # full anisotropy: component -> (box, coeff_a, coeff_b), box-dense
+    # off-diagonal coupling coefficients dt inv_cd / eps0 (lower axis first)
+    aniso: dict | None = None
 
     @property
     def cells(self) -> int:
@@ -531,6 +536,51 @@ class CompiledNonlinear:
         if self.general:
             m = m | (ch["chi2"] != 0) | (ch["tpa"] != 0)
         return m
+
+
+_ANISO_ROWS = {"Ex": ("xy", "xz"), "Ey": ("xy", "yz"), "Ez": ("xz", "yz")}
+_ANISO_DIAG = {"Ex": "xx", "Ey": "yy", "Ez": "zz"}
+
+
+def _full_aniso(eps_node, offdiag_node, dt):
+    """Per-edge inverse permittivity tensors (witwin/maxwell/fdtd/runtime/
+    materials.py:272-398, 1421-1440), in float32 like the reference: the six
+    relative node tensors averaged onto each E component's edges, inverted in
+    closed form; the diagonal entry gives the effective permittivity of the
+    base curl coefficient (eps0 / inv_ii), the two off-diagonal entries of the
+    component's row the coupling coefficients dt inv / eps0.  Returns
+    ({component: eps_eff}, {component: (box, coeff_a, coeff_b)}) with the box
+    the bounding box of the nonzero coefficients."""
+    f32 = np.float32
+    node = {"xx": eps_node[0], "yy": eps_node[1], "zz": eps_node[2], **offdiag_node}
+    node = {k: v.astype(f32) for k, v in node.items()}
+    scale = f32(dt / EPSILON_0)
+    eps_eff, aniso = {}, {}
+    for name in ("Ex", "Ey", "Ez"):
+        axis = "xyz".index(name[1])
+        sl0 = [slice(None)] * 3
+        sl1 = [slice(None)] * 3
+        sl0[axis], sl1[axis] = slice(None, -1), slice(1, None)
+        e = {k: (f32(0.5) * (v[tuple(sl0)] + v[tuple(sl1)])).astype(f32) for k, v in node.items()}
+        a, b, c, d, ee, f = e["xx"], e["yy"], e["zz"], e["xy"], e["xz"], e["yz"]
+        det = a * (b * c - f * f) - d * (d * c - f * ee) + ee * (d * f - b * ee)
+        inv_det = f32(1.0) / det
+        inv = {"xx": (b * c - f * f) * inv_det, "yy": (a * c - ee * ee) * inv_det, "zz": (a * b - d * d) * inv_det,
+               "xy": (ee * f - d * c) * inv_det, "xz": (d * f - b * ee) * inv_det, "yz": (d * ee - a * f) * inv_det}
+        diag = inv[_ANISO_DIAG[name]]
+        if np.any(det <= 0) or np.any(diag <= 0):
+            raise ValueError(f"the anisotropic permittivity tensor is not positive-definite on the {name} edges")
+        eps_eff[name] = (f32(EPSILON_0) / diag).astype(f32)
+        ca = (scale * inv[_ANISO_ROWS[name][0]]).astype(f32)
+        cb = (scale * inv[_ANISO_ROWS[name][1]]).astype(f32)
+        nz = np.argwhere((ca != 0) | (cb != 0))
+        if nz.size == 0:
+            continue
+        lo, hi = nz.min(axis=0), nz.max(axis=0) + 1
+        box = (int(lo[0]), int(hi[0]), int(lo[1]), int(hi[1]), int(lo[2]), int(hi[2]))
+        sl = (slice(box[0], box[1]), slice(box[2], box[3]), slice(box[4], box[5]))
+        aniso[name] = (box, np.ascontiguousarray(ca[sl]), np.ascontiguousarray(cb[sl]))
+    return eps_eff, aniso
 
 
 def window_scales(window: np.ndarray, steps: int, n_freq: int) -> np.ndarray:
@@ -780,6 +830,7 @@ def compile_scene(scene: Scene, time_steps: int) -> CompiledScene:
     # conductivity and nonlinear channels blend like the static eps
     # (compiler/materials.py:740-756): the last structure covering a node wins
     chan_node = {k: np.zeros(nodes, dtype=np.float64) for k in ("sigma", "chi2", "chi3", "tpa")}
+    offdiag_node = {k: np.zeros(nodes, dtype=np.float64) for k in ("xy", "xz", "yz")}
     pole_weights = []  # list of (pole, node weight array)
     for st in scene.structures:
         mask = st.geometry.node_mask(nodes)
@@ -788,6 +839,8 @@ def compile_scene(scene: Scene, time_steps: int) -> CompiledScene:
         med = st.medium
         for key, value in (("sigma", med.sigma), ("chi2", med.chi2), ("chi3", med.kerr_chi3), ("tpa", med.tpa_sigma)):
             chan_node[key][mask] = float(value)
+        for key, value in zip(("xy", "xz", "yz"), med.eps_offdiag or (0.0, 0.0, 0.0)):
+            offdiag_node[key][mask] = float(value)
         for entry in pole_weights:
             entry[1][mask] = 0.0
         for pole in st.medium.poles:
@@ -815,8 +868,14 @@ def compile_scene(scene: Scene, time_steps: int) -> CompiledScene:
     decay, curl, uniform = {}, {}, {}
     nl_channels = {}
     static_curl = {}  # the static curl coefficients, from which the source terms are built
+    aniso = None
+    eps_curl = eps  # the permittivity of the curl coefficients
+    if any(bool(np.any(v != 0)) for v in offdiag_node.values()):
+        if any(bool(np.any(chan_node[k] != 0)) for k in ("sigma", "chi2", "chi3", "tpa")) or pole_weights:
+            raise ValueError("full anisotropy with conductive, nonlinear or dispersive media is not supported")
+        eps_curl, aniso = _full_aniso(eps_node, offdiag_node, dt)
     for name in ("Ex", "Ey", "Ez"):
-        e = eps[name]
+        e = eps_curl[name]
         if conductive:
             half = (np.float32(0.5) * chan["sigma"][name] * dt32) / e
             denom = one32 + half
@@ -979,7 +1038,7 @@ def compile_scene(scene: Scene, time_steps: int) -> CompiledScene:
         poles=poles, patches=patches, aux_line=aux_line, line_patches=line_patches, regions=regions,
         frequencies=tuple(freq_list), monitor_frequencies=mon_freqs, window=window, design=design,
         complex_fields=complex_fields, bloch_cos=tuple(bcos), bloch_sin=tuple(bsin), shifted=shifted,
-        nonlinear=nonlinear,
+        nonlinear=nonlinear, aniso=aniso,
     )
 
 

@@ -181,6 +181,12 @@ class B200FDTD:
                                                       float(np.float32(nl.eps0))),
                         "set_nonlinear",
                     )
+            for name, (box, ca, cb) in (getattr(cs, "aniso", None) or {}).items():
+                _lib.check(
+                    lib.fdtd_engine_set_full_aniso(h, COMP_INDEX[name], _lib.int_array(box), _lib.ptr(self._dev(ca)),
+                                                   _lib.ptr(self._dev(cb))),
+                    "set_full_aniso",
+                )
             self.pole_ids = []
             for pole in cs.poles:
                 pid = ctypes.c_int()
