@@ -87,13 +87,13 @@ def test_facade_cw_run_with_hanning_windows_matches_oracle():
 
     wm = load_package()
     sim = wm.Simulation.fdtd(_cw_scene(wm, with_freqs=False), frequencies=[300e12, 280e12],
-                             run_time=wm.TimeConfig(time_steps=900), spectral_sampler=wm.SpectralSampler("hanning"))
+                             run_time=wm.TimeConfig(time_steps=1500), spectral_sampler=wm.SpectralSampler("hanning"))
     result = sim.run()
     cs = sim.solver.compiled
-    assert cs.window.shape == (900, 2)
+    assert cs.window.shape == (1500, 2)
     starts = [int(np.argmax(cs.window[:, f] > 0)) for f in range(2)]
     assert starts[0] != starts[1] and min(starts) > 0  # per-frequency transients
-    ref = orc.OracleSimulation(cs, "f64", threads=4).run(900)
+    ref = orc.OracleSimulation(cs, "f64", threads=4).run(1500)
     want = ref.monitor_results()
     got = {name: {c: v.cpu().numpy() for c, v in result.monitor(name)["components"].items()} for name in want}
     assert_monitors_close(got, want)
