@@ -366,6 +366,13 @@ int fdtd_engine_adjoint_range(fdtd_engine* h, int n1, int n0);
  * segment (the reference's segment replay, witwin/maxwell/fdtd/adjoint/
  * core.py:3527-3565, with its checkpoints, checkpoint.py:365-568). */
 int fdtd_engine_backward_replay(fdtd_engine* h, int n_steps, int stride);
+/* Region replay (on by default): inside fdtd_engine_backward_replay, step t
+ * of a T-step segment updates only the warp tasks over the design boxes grown
+ * by T - t + 2 cells (the domain of dependence of the recorded design-box E:
+ * one cell per step), with the scalar warp kernels; the history, and so the
+ * gradient, is the full replay's bit for bit.  Applies to FP32 engines without
+ * periodic / Bloch faces on launch variants 1-3 or 10; 0 replays whole steps. */
+int fdtd_engine_set_replay_region(fdtd_engine* h, int on);
 /* Accumulated dL/deps (absolute permittivity) of the design box of E
  * component comp (0..2), box-dense [i][j][k]. */
 int fdtd_engine_adjoint_grad(fdtd_engine* h, int comp, float* out);

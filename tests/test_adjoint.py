@@ -291,3 +291,38 @@ def test_design_workload_gradient_against_fp64_finite_differences():
     scale = np.abs(fds).max()
     assert scale > 0
     np.testing.assert_allclose(gs, fds, rtol=0, atol=2e-3 * scale)
+
+
+@pytest.mark.parametrize("dispersive", [False, True])
+def test_region_replay_equals_full_replay(dispersive):
+    """Region replay (each replayed step restricted to the design boxes' domain
+    of dependence) records the full replay's design history bit for bit, so the
+    gradients are identical; both agree with the stored-history gradient."""
+    wm = load_package()
+    adj = wm.adjoint
+    rng = np.random.default_rng(21)
+    eps_r = 2.0 + 2.0 * rng.random((4, 4, 3))
+
+    def scene(e):
+        sc = wm.Scene(cells=(72, 64, 56), spacing=25e-9, pml_cells=6)
+        if dispersive:
+            sc.structures.append(wm.Structure(wm.Box((40, 26, 22), (43, 38, 34)),
+                                              wm.Medium.lorentz(2.0, 3.0, 250e12, 20e12)))
+            sc.structures.append(wm.Structure(wm.Box((20, 10, 10), (22, 54, 46)),
+                                              wm.Medium.drude(2e15 / (2 * np.pi), 1e14 / (2 * np.pi))))
+        sc.sources.append(wm.PointDipole((30, 32, 28), "Ez", wm.GaussianPulse(300e12, 100e12), width=25e-9))
+        sc.material_regions.append(wm.MaterialRegion((34, 30, 26), (38, 34, 29), e))
+        sc.monitors.append(wm.PointMonitor("probe", (46, 32, 28), frequencies=(300e12,)))
+        return sc
+
+    steps, stride = 240, 24
+    grads = {}
+    for key, kw in (("region", {"history": "replay", "replay_region": True}),
+                    ("full", {"history": "replay", "replay_region": False}), ("store", {"history": "store"})):
+        problem = adj.DesignProblem(scene(eps_r), steps, stride=stride, **kw)
+        mons = problem.forward(eps_r)
+        grads[key] = problem.backward({"probe": {c: 2.0 * v for c, v in mons["probe"].items()}})
+        problem.close()
+    assert np.abs(grads["full"]).max() > 0
+    np.testing.assert_array_equal(grads["region"], grads["full"])
+    np.testing.assert_allclose(grads["region"], grads["store"], rtol=0, atol=1e-5 * np.abs(grads["store"]).max())

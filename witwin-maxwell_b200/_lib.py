@@ -94,6 +94,7 @@ _SIGNATURES = {
     "fdtd_engine_step_range_recorded": ([_vp, _i, _i], _i),
     "fdtd_engine_adjoint_range": ([_vp, _i, _i], _i),
     "fdtd_engine_backward_replay": ([_vp, _i, _i], _i),
+    "fdtd_engine_set_replay_region": ([_vp, _i], _i),
     "fdtd_engine_set_range_flush": ([_vp, _i], _i),
     "fdtd_engine_get_plane": ([_vp, _i, _i, _vp], _i),
     "fdtd_engine_set_plane": ([_vp, _i, _i, _vp], _i),

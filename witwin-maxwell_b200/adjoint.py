@@ -85,10 +85,13 @@ class DesignProblem:
     bytes of HBM, no replay), "replay" keeps a full-state checkpoint every
     ``stride`` steps and re-runs each segment during the backward pass (the
     reference's scheme, for histories too large to keep), "auto" stores when
-    the history fits in ``history_budget`` bytes."""
+    the history fits in ``history_budget`` bytes.  ``replay_region`` (replay
+    only): each replayed step updates only the domain of dependence of the
+    design boxes (``fdtd_engine_set_replay_region``; the gradient is the full
+    replay's bit for bit)."""
 
     def __init__(self, scene: Scene, steps: int, stride: int = 100, device: str = "cuda", history: str = "auto",
-                 history_budget: int = 16 << 30):
+                 history_budget: int = 16 << 30, replay_region: bool = True):
         if not scene.material_regions:
             raise ValueError("the scene has no MaterialRegion to differentiate")
         if history not in ("auto", "store", "replay"):
@@ -99,6 +102,7 @@ class DesignProblem:
         self.device = device
         self.history = history
         self.history_budget = int(history_budget)
+        self.replay_region = bool(replay_region)
         self.stored = False
         self.solver: B200FDTD | None = None
         self.boxes = None
@@ -131,6 +135,7 @@ class DesignProblem:
         if not self.stored:
             n_slots = (self.steps + self.stride - 1) // self.stride
             _lib.check(lib.fdtd_engine_checkpoint_reserve(h, n_slots), "checkpoint_reserve")
+            _lib.check(lib.fdtd_engine_set_replay_region(h, 1 if self.replay_region else 0), "set_replay_region")
         self.solver = solver
         return solver
 

@@ -643,6 +643,7 @@ struct fdtd_engine {
   float* d_nl_prm = nullptr;
   int nl_lo[3] = {0, 0, 0}, nl_hi[3] = {0, 0, 0};
   std::vector<AnisoHost> aniso;  // full-anisotropy boxes (fdtd_engine_set_full_aniso)
+  bool replay_region = true;     // fdtd_engine_set_replay_region
   bool bloch = false;
   bool in_pair = false;
   int64_t plane = 0, vol = 0;
@@ -818,6 +819,8 @@ int background_value(fdtd_engine* h, int comp, const float* arr, float* out) {
   return 0;
 }
 
+int z_blocks(const fdtd_engine* h);
+
 void fill_params(const fdtd_engine* h, StepParams& p) {
   std::memset(&p, 0, sizeof(p));
   p.NX = h->NX;
@@ -887,6 +890,7 @@ void fill_params(const fdtd_engine* h, StepParams& p) {
   for (int f = 0; f < 6; ++f)
     if (h->desc.boundary[f] == FDTD_BND_PMC) p.pmc |= 1 << f;
   p.pec_clamp = h->lines.empty() ? 1 : 0;
+  p.n_kb = z_blocks(h);
   for (int a = 0; a < 3; ++a) {
     p.nl_lo[a] = h->nl_lo[a];
     p.nl_hi[a] = h->nl_hi[a];
@@ -1086,7 +1090,11 @@ int launch_aniso(fdtd_engine* h, const StepParams& p) {
   return 0;
 }
 
-int launch_step(fdtd_engine* h, int n, int slot) {
+// region: node box (x0, x1, y0, y1, z0, z1) to which the warp kernel's task
+// grid is restricted (a sub-grid of whole row blocks, z blocks and chunks that
+// covers it), or nullptr for the full step.  Only the scalar warp kernels take
+// a region (region_ok); cells outside it keep stale values.
+int launch_step(fdtd_engine* h, int n, int slot, const int* region = nullptr) {
   if (!h->shifted.empty()) {
     const int rc = launch_shifted(h, n);
     if (rc) return rc;
@@ -1097,7 +1105,19 @@ int launch_step(fdtd_engine* h, int n, int slot) {
   }
   StepParams p;
   fill_params(h, p);
-  const dim3 grid = step_grid(h);
+  dim3 grid = step_grid(h);
+  if (region) {
+    const unsigned rb0 = static_cast<unsigned>(region[2] / kWarpRows), kb0 = static_cast<unsigned>(region[4] / kWarpOut);
+    const unsigned ch0 = static_cast<unsigned>(region[0] / h->CX);
+    const unsigned rb1 = std::min<unsigned>(grid.x, static_cast<unsigned>((region[3] + kWarpRows - 1) / kWarpRows));
+    const unsigned kb1 = std::min<unsigned>(grid.y, static_cast<unsigned>((region[5] + kWarpOut - 1) / kWarpOut));
+    const unsigned ch1 = std::min<unsigned>(grid.z, static_cast<unsigned>((region[1] + h->CX - 1) / h->CX));
+    if (rb1 <= rb0 || kb1 <= kb0 || ch1 <= ch0) return fail(FDTD_ERR_INVALID_ARG, "empty step region");
+    p.rb0 = static_cast<int>(rb0);
+    p.kb0 = static_cast<int>(kb0);
+    p.ch0 = static_cast<int>(ch0);
+    grid = dim3(rb1 - rb0, kb1 - kb0, ch1 - ch0);
+  }
   const bool ade_pass = ade_pass_active(h);
   bool coef = false;
   for (int c = 0; c < 6; ++c) coef = coef || h->ecoef[c][0] || h->ecoef[c][1];
@@ -1117,7 +1137,7 @@ int launch_step(fdtd_engine* h, int n, int slot) {
   if (h->storage != kStoreF32) {
     const int err = launch_step_reduced(p, n, grid, h->cpml, coef, h->uniform_grid, h->stream);
     if (err != 0) return cuda_fail(static_cast<cudaError_t>(err), "warp_step_kernel_rs launch");
-  } else if (tile_runs(h)) {
+  } else if (!region && tile_runs(h)) {
     // the row-tile kernel, then (scenes with CPML) the warp kernel over the
     // CTAs that meet a slab, which the row-tile kernel leaves alone
     const int err = launch_tile_step(p, h->maps[h->cur], n, grid, h->cpml, coef, h->uniform_grid, h->stream);
@@ -1138,7 +1158,7 @@ int launch_step(fdtd_engine* h, int n, int slot) {
       const cudaError_t e2 = cudaGetLastError();
       if (e2 != cudaSuccess) return cuda_fail(e2, "warp_step_kernel (CPML shell) launch");
     }
-  } else if (VecLauncher vl = vec_launcher(h->variant)) {
+  } else if (VecLauncher vl = region ? nullptr : vec_launcher(h->variant)) {
     const int err = vl(p, n, grid, h->cpml, coef, h->uniform_grid, h->stream);
     if (err != 0) return cuda_fail(static_cast<cudaError_t>(err), "vec_step_kernel launch");
   } else {
@@ -2658,6 +2678,12 @@ int fdtd_engine_set_ade_pass(fdtd_engine* h, int on) {
   return 0;
 }
 
+int fdtd_engine_set_replay_region(fdtd_engine* h, int on) {
+  if (!h) return fail(FDTD_ERR_INVALID_ARG, "null engine");
+  h->replay_region = on != 0;
+  return 0;
+}
+
 int fdtd_engine_set_range_flush(fdtd_engine* h, int on) {
   if (!h) return fail(FDTD_ERR_INVALID_ARG, "null engine");
   h->range_flush = on != 0;
@@ -2921,6 +2947,25 @@ int fdtd_engine_backward_replay(fdtd_engine* h, int n_steps, int stride) {
         if (q.design[c].grad) q.design[c].hist = a.hist2[c];
     return q;
   };
+  // Region replay: the segment only has to reproduce E in the design boxes.
+  // One step moves information by at most one cell, so step t of a T-step
+  // segment (t = 1..T) updates only the tasks over the design boxes' bounding
+  // box grown by T - t cells (+2 for the half-cell component offsets): every
+  // cell of that region reads inputs from the previous step's larger region,
+  // which were exact, so the recorded design history is the full replay's
+  // (same kernel bodies per task, bit for bit).  Cells outside the region
+  // keep stale values, which nothing reads before the next checkpoint load.
+  const bool region_ok = h->replay_region && design && h->storage == kStoreF32 && !h->wrap &&
+                         ((h->variant >= 1 && h->variant <= 3) || h->variant == kTileVariant);
+  int dbox[6] = {INT_MAX, -1, INT_MAX, -1, INT_MAX, -1};
+  for (int c = 0; c < 3; ++c) {
+    const DesignBox& d = a.q.design[c];
+    if (!d.grad) continue;
+    for (int ax = 0; ax < 3; ++ax) {
+      dbox[2 * ax] = std::min(dbox[2 * ax], d.lo[ax]);
+      dbox[2 * ax + 1] = std::max(dbox[2 * ax + 1], d.hi[ax]);
+    }
+  }
   auto replay = [&](int s) -> int {
     const int n0 = s * stride, n1 = std::min(n_steps, n0 + stride);
     int r = fdtd_engine_checkpoint_load(h, s);
@@ -2930,8 +2975,19 @@ int fdtd_engine_backward_replay(fdtd_engine* h, int n_steps, int stride) {
     fill_params(h, p);
     int err = design ? launch_design_record(p, q, 0, h->stream) : 0;
     if (err) return cuda_fail(static_cast<cudaError_t>(err), "design record");
+    const int nn[3] = {h->NX, h->NY, h->NZ};
     for (int n = n0; n < n1; ++n) {
-      r = launch_step(h, n, -1);
+      if (region_ok) {
+        const int m = (n1 - 1 - n) + 2;  // cells of dependence left after this step, plus the offsets
+        int box[6];
+        for (int ax = 0; ax < 3; ++ax) {
+          box[2 * ax] = std::max(0, dbox[2 * ax] - m);
+          box[2 * ax + 1] = std::min(nn[ax], dbox[2 * ax + 1] + m);
+        }
+        r = launch_step(h, n, -1, box);
+      } else {
+        r = launch_step(h, n, -1);
+      }
       if (r) return r;
       if (design) {
         fill_params(h, p);

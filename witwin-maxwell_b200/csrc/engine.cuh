@@ -157,6 +157,10 @@ struct StepParams {
   // warp tasks whose footprint meets it read the coefficient arrays whatever
   // the values at classification time (empty: nl_lo[0] >= nl_hi[0]).
   int nl_lo[3], nl_hi[3];
+  // Warp kernels: the launch grid covers row blocks, z blocks and x chunks
+  // starting at (rb0, kb0, ch0) of the full task grid, whose z-block count is
+  // n_kb (the class table's layout); 0, 0, 0 and gridDim.y for a full launch.
+  int rb0, kb0, ch0, n_kb;
 };
 
 // A warp task needs the CPML code (some cell of its footprint lies in a slab)

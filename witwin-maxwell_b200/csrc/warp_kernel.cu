@@ -44,7 +44,7 @@ __device__ __forceinline__ void prefetch_row(const StepParams& p, int ip, int i1
   }
 }
 
-// The march of one warp task (row j, z block blockIdx.y, x chunk blockIdx.z).
+// The march of one warp task (row j, z block kb, x chunk ch).
 // kCpml: run the CPML psi code (the task's footprint touches a slab).  kCoef:
 // read the per-cell decay/curl arrays (some coefficient of the footprint
 // differs from the background scalars p.*_u).  kUniform: every axis has
@@ -56,13 +56,13 @@ __device__ __forceinline__ void prefetch_row(const StepParams& p, int ip, int i1
 // ahead of the march.  kAde: the ADE poles run here (false when the ADE pass
 // after the step kernel advances them; the pole code is then not compiled).
 template <typename TS, bool kCpml, bool kCoef, bool kUniform, bool kPf = false, bool kAde = true>
-__device__ __forceinline__ void march(const StepParams& p, int n, int lane, int j) {
+__device__ __forceinline__ void march(const StepParams& p, int n, int lane, int j, int kb, int ch) {
   using TA = typename std::conditional<std::is_same<TS, __nv_bfloat16>::value, __nv_bfloat16, float>::type;
   const int NX = p.NX, NY = p.NY, NZ = p.NZ, P = p.P;
-  const int k = blockIdx.y * kOut - 1 + lane;
+  const int k = kb * kOut - 1 + lane;
   const bool kok = k >= 0 && k < P;
   const bool out_lane = lane >= 1 && lane <= kOut && k < P;
-  const int i0 = blockIdx.z * p.CX;
+  const int i0 = ch * p.CX;
   const int i1 = min(i0 + p.CX, NX);
   const int istart = max(i0 - 1, 0);
   const bool jm_ok = j >= 1, jp_ok = j + 1 < NY;
@@ -382,20 +382,22 @@ __global__ void __launch_bounds__(256, kMinBlocks) warp_step_kernel(const StepPa
   constexpr bool kPlainPrefetch = !(kAnyCpml && kAnyCoef) || !kAde;
   if (p.step_base) n += __ldg(p.step_base);
   const int lane = threadIdx.x & 31;
-  const int j = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  // task of this warp in the full grid (a region launch covers a sub-grid)
+  const int j = (blockIdx.x + p.rb0) * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  const int kb = blockIdx.y + p.kb0, ch = blockIdx.z + p.ch0;
   unsigned cls = 0;
   if ((kAnyCpml || kAnyCoef) && j < p.NY)
-    cls = __ldg(p.warp_class + (static_cast<int64_t>(blockIdx.z) * gridDim.y + blockIdx.y) * p.NY + j);
+    cls = __ldg(p.warp_class + (static_cast<int64_t>(ch) * p.n_kb + kb) * p.NY + j);
   // shell_only: the CTAs without a CPML warp belong to the row-tile kernel
   // (its CTAs cover the same rows, z block and chunk)
   if (kAnyCpml && p.shell_only && !__syncthreads_or(cls & kClassCpml)) return;
   if (j >= p.NY) return;  // whole warp; no block-level barrier follows
   if (kAnyCpml && (cls & kClassCpml)) {
-    if (kAnyCoef && (cls & kClassCoef)) march<float, true, true, kUniform, false, kAde>(p, n, lane, j);
-    else march<float, true, false, kUniform, false, kAde>(p, n, lane, j);
+    if (kAnyCoef && (cls & kClassCoef)) march<float, true, true, kUniform, false, kAde>(p, n, lane, j, kb, ch);
+    else march<float, true, false, kUniform, false, kAde>(p, n, lane, j, kb, ch);
   } else {
-    if (kAnyCoef && (cls & kClassCoef)) march<float, false, true, kUniform, false, kAde>(p, n, lane, j);
-    else march<float, false, false, kUniform, kPlainPrefetch, kAde>(p, n, lane, j);
+    if (kAnyCoef && (cls & kClassCoef)) march<float, false, true, kUniform, false, kAde>(p, n, lane, j, kb, ch);
+    else march<float, false, false, kUniform, kPlainPrefetch, kAde>(p, n, lane, j, kb, ch);
   }
 }
 
@@ -411,11 +413,11 @@ __global__ void __launch_bounds__(256, 4) warp_step_kernel_rs(const StepParams p
   if (kAnyCpml || kAnyCoef)
     cls = __ldg(p.warp_class + (static_cast<int64_t>(blockIdx.z) * gridDim.y + blockIdx.y) * p.NY + j);
   if (kAnyCpml && (cls & kClassCpml)) {
-    if (kAnyCoef && (cls & kClassCoef)) march<TS, true, true, kUniform>(p, n, lane, j);
-    else march<TS, true, false, kUniform>(p, n, lane, j);
+    if (kAnyCoef && (cls & kClassCoef)) march<TS, true, true, kUniform>(p, n, lane, j, blockIdx.y, blockIdx.z);
+    else march<TS, true, false, kUniform>(p, n, lane, j, blockIdx.y, blockIdx.z);
   } else {
-    if (kAnyCoef && (cls & kClassCoef)) march<TS, false, true, kUniform>(p, n, lane, j);
-    else march<TS, false, false, kUniform>(p, n, lane, j);
+    if (kAnyCoef && (cls & kClassCoef)) march<TS, false, true, kUniform>(p, n, lane, j, blockIdx.y, blockIdx.z);
+    else march<TS, false, false, kUniform>(p, n, lane, j, blockIdx.y, blockIdx.z);
   }
 }
 
