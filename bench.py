@@ -580,10 +580,16 @@ def run_adjoint_bench(wm, device):
     against a plain forward solve of the same scene, device time on the engine's
     stream.  Two history modes: "store" keeps the design-box E history of every
     step in HBM (2.4 GB here, no replay); "replay" keeps a full-state checkpoint
-    every 100 steps and re-runs each segment during the backward pass."""
+    every 100 steps and re-runs each segment during the backward pass, each
+    replayed step restricted to the design block's domain of dependence
+    ("replay_full_steps": whole replayed steps, for comparison; "replay_stride_50":
+    a checkpoint every 50 steps)."""
     import torch
 
     steps, stride = 3000, 100
+    modes = {"store": {"history": "store"}, "replay": {"history": "replay"},
+             "replay_full_steps": {"history": "replay", "replay_region": False},
+             "replay_stride_50": {"history": "replay", "stride": 50}}
     scene = wm.workloads.adjoint_160(steps)
     eps_r = scene.material_regions[0].eps_r
     out = {
@@ -595,14 +601,16 @@ def run_adjoint_bench(wm, device):
     }
     cs = None
     grads = {}
-    for mode in ("store", "replay"):
-        problem = wm.adjoint.DesignProblem(scene, steps, stride=stride, device=str(device), history=mode)
+    for mode, kw in modes.items():
+        kw = dict(kw)
+        st = kw.pop("stride", stride)
+        problem = wm.adjoint.DesignProblem(scene, steps, stride=st, device=str(device), **kw)
         mons = problem.forward(eps_r)
         g = problem.backward({"patch": {c: 2.0 * v for c, v in mons["patch"].items()}})
         grads[mode] = g
         out[mode] = {"forward_ms": problem.timings["forward_ms"], "backward_ms": problem.timings["backward_ms"]}
-        if mode == "replay":
-            out[mode]["checkpoint_stride"] = stride
+        if kw["history"] == "replay":
+            out[mode]["checkpoint_stride"] = st
         cs = problem.solver.compiled
         problem.close()
         torch.cuda.empty_cache()
@@ -611,11 +619,12 @@ def run_adjoint_bench(wm, device):
     plain.close()
     torch.cuda.empty_cache()
     out["forward_plain_ms"] = plain_ms
-    for mode in ("store", "replay"):
+    for mode in modes:
         out[mode]["fwd_adj_over_fwd"] = (out[mode]["forward_ms"] + out[mode]["backward_ms"]) / plain_ms
     out["fwd_adj_over_fwd"] = out["store"]["fwd_adj_over_fwd"]
     den = float(np.abs(grads["replay"]).max())
     out["store_vs_replay_max_rel_diff"] = float(np.abs(grads["store"] - grads["replay"]).max() / den) if den else 0.0
+    out["region_replay_equals_full_replay"] = bool(np.array_equal(grads["replay"], grads["replay_full_steps"]))
     return out
 
 
