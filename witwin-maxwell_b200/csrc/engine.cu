@@ -18,6 +18,8 @@
 #include <string>
 #include <vector>
 
+#include <nvtx3/nvToolsExt.h>
+
 #include "../../include/fdtd_b200.h"
 #include "engine.cuh"
 #include "tma_step.cuh"
@@ -45,6 +47,16 @@ using namespace fdtdb200;
 namespace {
 
 thread_local std::string g_last_error;
+
+// An NVTX range over a host entry point (step ranges, replay, reverse,
+// checkpoints, autotune): names the enqueue span on a profiler's timeline;
+// without an attached tool the calls return at once.
+struct NvtxRange {
+  explicit NvtxRange(const char* name) { nvtxRangePushA(name); }
+  ~NvtxRange() { nvtxRangePop(); }
+  NvtxRange(const NvtxRange&) = delete;
+  NvtxRange& operator=(const NvtxRange&) = delete;
+};
 
 int fail(int code, const std::string& msg) {
   g_last_error = msg;
@@ -2405,9 +2417,13 @@ struct AsyncGather {
   ~AsyncGather() { join(); }
 };
 
-int fdtd_engine_step_range(fdtd_engine* h, int n0, int n1) { return step_range_impl(h, n0, n1, false); }
+int fdtd_engine_step_range(fdtd_engine* h, int n0, int n1) {
+  NvtxRange r("fdtd_engine_step_range");
+  return step_range_impl(h, n0, n1, false);
+}
 
 int fdtd_engine_step_range_recorded(fdtd_engine* h, int n0, int n1) {
+  NvtxRange nvtx_range("fdtd_engine_step_range_recorded");
   if (!h || !h->adj.ready) return fail(FDTD_ERR_STATE, "adjoint not initialised");
   if (n0 < 0 || n1 < n0 || n1 - n0 > h->adj.max_segment) return fail(FDTD_ERR_INVALID_ARG, "bad recorded range");
   return step_range_impl(h, n0, n1, true);
@@ -2549,6 +2565,7 @@ int fdtd_engine_checkpoint_reserve(fdtd_engine* h, int n_slots) {
 }
 
 int fdtd_engine_checkpoint_save(fdtd_engine* h, int slot) {
+  NvtxRange nvtx_range("fdtd_engine_checkpoint_save");
   if (!h || slot < 0 || slot > 1 << 20) return fail(FDTD_ERR_INVALID_ARG, "bad checkpoint slot");
   if (static_cast<int>(h->checkpoints.size()) <= slot) h->checkpoints.resize(slot + 1);
   std::vector<std::pair<float*, size_t>> bufs;
@@ -2564,6 +2581,7 @@ int fdtd_engine_checkpoint_save(fdtd_engine* h, int slot) {
 }
 
 int fdtd_engine_checkpoint_load(fdtd_engine* h, int slot) {
+  NvtxRange nvtx_range("fdtd_engine_checkpoint_load");
   if (!h || slot < 0 || slot >= static_cast<int>(h->checkpoints.size()) || !h->checkpoints[slot].valid)
     return fail(FDTD_ERR_INVALID_ARG, "no checkpoint in that slot");
   std::vector<std::pair<float*, size_t>> bufs;
@@ -2576,6 +2594,7 @@ int fdtd_engine_checkpoint_load(fdtd_engine* h, int slot) {
 }
 
 int fdtd_engine_autotune(fdtd_engine* h, int* tile_rows, int* chunk_planes) {
+  NvtxRange nvtx_range("fdtd_engine_autotune");
   if (!h || !h->finalized) return fail(FDTD_ERR_STATE, "engine not finalized");
   int rc = flush_samples(h);
   if (rc) return rc;
@@ -2873,6 +2892,7 @@ int fdtd_engine_replay_range(fdtd_engine* h, int n0, int n1) {
 }
 
 int fdtd_engine_adjoint_range(fdtd_engine* h, int n1, int n0) {
+  NvtxRange nvtx_range("fdtd_engine_adjoint_range");
   if (!h || !h->adj.ready) return fail(FDTD_ERR_STATE, "adjoint not initialised");
   if (n0 < 0 || n1 < n0) return fail(FDTD_ERR_INVALID_ARG, "bad adjoint range");
   AdjointHost& a = h->adj;
@@ -2904,6 +2924,7 @@ int fdtd_engine_adjoint_range(fdtd_engine* h, int n1, int n0) {
 // the same time: each is latency-bound well below the HBM roof, and together
 // they use it better than one after the other.
 int fdtd_engine_backward_replay(fdtd_engine* h, int n_steps, int stride) {
+  NvtxRange nvtx_range("fdtd_engine_backward_replay");
   if (!h || !h->adj.ready) return fail(FDTD_ERR_STATE, "adjoint not initialised");
   AdjointHost& a = h->adj;
   if (n_steps < 1 || stride < 1 || stride > a.max_segment)
@@ -2967,6 +2988,7 @@ int fdtd_engine_backward_replay(fdtd_engine* h, int n_steps, int stride) {
     }
   }
   auto replay = [&](int s) -> int {
+    NvtxRange seg("replay segment");
     const int n0 = s * stride, n1 = std::min(n_steps, n0 + stride);
     int r = fdtd_engine_checkpoint_load(h, s);
     if (r) return r;
@@ -3008,6 +3030,7 @@ int fdtd_engine_backward_replay(fdtd_engine* h, int n_steps, int stride) {
   for (int s = S - 1; s >= 0; --s) {
     const int n0 = s * stride, n1 = std::min(n_steps, n0 + stride);
     CUDA_TRY(cudaStreamWaitEvent(a.rev, a.ev_rep[s & 1], 0));
+    NvtxRange seg("reverse segment");
     const AdjParams qs = with_hist(s);
     for (int n = n1 - 1; n >= n0; --n) {
       AdjParams q = qs;
@@ -3314,6 +3337,7 @@ int fdtd_batch_autotune(fdtd_batch* b) {
 }
 
 int fdtd_batch_step_range(fdtd_batch* b, int n0, int n1) {
+  NvtxRange nvtx_range("fdtd_batch_step_range");
   if (!b) return fail(FDTD_ERR_INVALID_ARG, "null batch");
   if (n1 < n0 || n0 < 0) return fail(FDTD_ERR_INVALID_ARG, "bad step range");
   for (fdtd_engine* h : b->eng) {
@@ -3482,6 +3506,7 @@ int fdtd_bloch_destroy(fdtd_bloch* p) {
 }
 
 int fdtd_bloch_step_range(fdtd_bloch* p, int n0, int n1) {
+  NvtxRange nvtx_range("fdtd_bloch_step_range");
   if (!p) return fail(FDTD_ERR_INVALID_ARG, "null Bloch pair");
   if (n1 < n0 || n0 < 0) return fail(FDTD_ERR_INVALID_ARG, "bad step range");
   fdtd_engine* hs[2] = {p->re, p->im};
