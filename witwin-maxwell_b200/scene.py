@@ -583,6 +583,18 @@ def _full_aniso(eps_node, offdiag_node, dt):
     return eps_eff, aniso
 
 
+def _node_bbox(mask: np.ndarray):
+    """Inclusive (lo, hi) node index range per axis of the nonzero entries, or None."""
+    out = []
+    for a in range(3):
+        other = tuple(b for b in range(3) if b != a)
+        idx = np.flatnonzero(np.any(mask != 0, axis=other))
+        if idx.size == 0:
+            return None
+        out.append((int(idx[0]), int(idx[-1])))
+    return out
+
+
 def window_scales(window: np.ndarray, steps: int, n_freq: int) -> np.ndarray:
     """Per-frequency spectrum scale 2 / sum(window) over the first ``steps`` steps
     (witwin/maxwell/fdtd/observers.py:236-241); ``window`` is one weight per step
@@ -858,7 +870,9 @@ def compile_scene(scene: Scene, time_steps: int) -> CompiledScene:
     for a, name in enumerate(("Ex", "Ey", "Ez")):
         eps[name] = (EPSILON_0 * _avg_node_to_component(eps_node[a], name)).astype(np.float32)
     # --- update coefficients (materials.py:942-1008): semi-implicit lossy fold, CPML not folded ---
-    chan = {k: {name: _avg_node_to_component(v, name).astype(np.float32) for name in ("Ex", "Ey", "Ez")}
+    # averaged channels; an all-zero channel stays zero (np.zeros: no pass over the grid)
+    chan = {k: {name: (_avg_node_to_component(v, name).astype(np.float32) if np.any(v != 0)
+                       else np.zeros(component_shape(name, nodes), np.float32)) for name in ("Ex", "Ey", "Ez")}
             for k, v in chan_node.items()}
     conductive = bool(np.any(chan_node["sigma"] != 0))
     is_nonlinear = any(bool(np.any(chan_node[k] != 0)) for k in ("chi2", "chi3", "tpa"))
@@ -963,14 +977,26 @@ def compile_scene(scene: Scene, time_steps: int) -> CompiledScene:
             decay_v = (2.0 - g * dt) / denom
             restoring = 2.0 * w0 * w0 * dt / denom
             base = 2.0 * EPSILON_0 * pole.delta_eps * w0 * w0 * dt / denom
+        node_box = _node_bbox(w_node)
+        if node_box is None:
+            continue
         for name in ("Ex", "Ey", "Ez"):
-            weight = _avg_node_to_component(w_node, name).astype(np.float32)
-            nzi = np.nonzero(weight)
-            if nzi[0].size == 0:
-                continue
-            box = tuple(int(v) for a in range(3) for v in (nzi[a].min(), nzi[a].max() + 1))
+            # the component cells whose two averaged nodes meet the pole's nodes:
+            # the bounding box of the nonzero averaged weights, without a pass
+            # over the whole grid
+            axis = "xyz".index(name[1])
+            box = []
+            for a in range(3):
+                lo, hi = node_box[a]
+                if a == axis:
+                    lo, hi = max(lo - 1, 0), min(hi, nodes[a] - 2)
+                box += [lo, hi + 1]
+            box = tuple(box)
             sl = (slice(box[0], box[1]), slice(box[2], box[3]), slice(box[4], box[5]))
-            drive = (weight[sl] * np.float32(base)).astype(np.float32)
+            nsl = [slice(box[0], box[1]), slice(box[2], box[3]), slice(box[4], box[5])]
+            nsl[axis] = slice(box[2 * axis], box[2 * axis + 1] + 1)
+            weight = _avg_node_to_component(w_node[tuple(nsl)], name).astype(np.float32)
+            drive = (weight * np.float32(base)).astype(np.float32)
             inv_eps = (np.float32(1.0) / eps[name][sl]).astype(np.float32)
             poles.append(CompiledPole(name, kind, float(decay_v), float(restoring), box,
                                       np.ascontiguousarray(drive), np.ascontiguousarray(inv_eps)))
