@@ -251,9 +251,18 @@ class RefGpuSimulation:
         self.pc, self.ps = (self.pc * self.step_c - self.ps * self.step_s,
                             self.ps * self.step_c + self.pc * self.step_s)
 
+    def _add_patches(self, n: int, magnetic: bool):
+        """Soft patches of one phase: H components right after the H update
+        (witwin/maxwell/fdtd/runtime/stepping.py:1773-1777), E components after
+        the E update (:2296-2308)."""
+        for comp, box, coeff, signal in self.patches:
+            if (comp[0] == "H") == magnetic:
+                self.op.add_source_patch(self.F[comp], coeff, box[0], box[2], box[4], float(signal[n]))
+
     def step_once(self):
         n = self.step
         self._update_h()
+        self._add_patches(n, magnetic=True)
         if self.aux is not None:
             self._line_corrections(True)
             self.op.update_auxiliary_magnetic(self.aux["h"], self.aux["e"], self.aux["hd"], self.aux["hc"])
@@ -263,8 +272,7 @@ class RefGpuSimulation:
             self._line_corrections(False)
             self.op.update_auxiliary_electric(self.aux["e"], self.aux["h"], self.aux["ed"], self.aux["ec"],
                                               self.aux["src"], float(self.aux["signal"][n]))
-        for comp, box, coeff, signal in self.patches:
-            self.op.add_source_patch(self.F[comp], coeff, box[0], box[2], box[4], float(signal[n]))
+        self._add_patches(n, magnetic=False)
         self._apply_ade()
         if self.aux is None:
             self._clamp_pec()
@@ -319,7 +327,12 @@ class RefGpuBloch:
     cuda/backend.py:54-70).  Monitors are the complex DFT A + iB of the two
     channels' spectra."""
 
-    def __init__(self, compiled, device: str = "cuda"):
+    def __init__(self, compiled, device: str = "cuda", bloch_terms=None, term_phases=None):
+        """``bloch_terms``: CW Bloch face terms (component, box, cos_patch,
+        sin_patch, signal_cos, signal_sin) injected through the reference's own
+        add_source_patch_bloch, real and imaginary values launched separately as
+        cuda/backend.py:1817-1854 does, in place of the compiled patches;
+        ``term_phases[component]``: the two tangential (wrap, cos kL, sin kL)."""
         cs = compiled
         if cs.cpml and (any(cs.pml_lo[:2]) or any(cs.pml_hi[:2])):
             raise ValueError("the Bloch checker covers CPML on z only")
@@ -328,6 +341,29 @@ class RefGpuBloch:
         self.im = RefGpuSimulation(cs, device, channel=1)
         self.op = self.re.op
         self.z_cpml = bool(cs.cpml and (cs.pml_lo[2] or cs.pml_hi[2]))
+        self.terms = None
+        if bloch_terms is not None:
+            dev = self.re.dev
+            self.re.patches, self.im.patches = [], []
+            self.terms = [(t.component, t.box, torch.as_tensor(t.cos_patch, device=dev),
+                           torch.as_tensor(t.sin_patch, device=dev), np.asarray(t.signal_cos, np.float32),
+                           np.asarray(t.signal_sin, np.float32), term_phases[t.component]) for t in bloch_terms]
+
+    def _bloch_terms(self, n: int, magnetic: bool):
+        if not self.terms:
+            return
+        R, I = self.re.F, self.im.F
+        for comp, box, cp, sp, sc, ss, ph in self.terms:
+            if (comp[0] == "H") != magnetic:
+                continue
+            names = ("Hx", "Hy", "Hz") if magnetic else ("Ex", "Ey", "Ez")
+            triplet = [t for nm in names for t in (R[nm], I[nm])]
+            (wa, ca, sa), (wb, cb, sb) = ph
+            c, s = float(sc[n]), float(ss[n])
+            for values, sr, si in ((cp * c + sp * s, 1.0, 0.0), (cp * s - sp * c, 0.0, 1.0)):
+                self.op.add_source_patch_bloch(*triplet, values.contiguous(), box[0], box[2], box[4], sr, si,
+                                               "xyz".index(comp[1]), float(ca), float(sa), float(cb), float(sb),
+                                               int(wa), int(wb))
 
     def _z_cpml_corrections(self, sim):
         bnd = self.cs.boundary
@@ -371,12 +407,16 @@ class RefGpuBloch:
         n = re.step
         re._update_h()
         im._update_h()
+        re._add_patches(n, magnetic=True)
+        im._add_patches(n, magnetic=True)
+        self._bloch_terms(n, magnetic=True)
         re._advance_ade()
         im._advance_ade()
         self._update_e()
+        re._add_patches(n, magnetic=False)
+        im._add_patches(n, magnetic=False)
+        self._bloch_terms(n, magnetic=False)
         for sim in (re, im):
-            for comp, box, coeff, signal in sim.patches:
-                self.op.add_source_patch(sim.F[comp], coeff, box[0], box[2], box[4], float(signal[n]))
             sim._apply_ade()
             sim._clamp_pec()
             sim._accumulate(n)

@@ -1013,9 +1013,11 @@ def compile_scene(scene: Scene, time_steps: int) -> CompiledScene:
             beam_patches, beam_shifted = _beam_patches(scene, src, curl_full, dt, time_steps)
             patches.extend(beam_patches)
             shifted.extend(beam_shifted)
+        elif isinstance(src, PlaneWaveTFSF) and any(b == BOUNDARY_BLOCH for b in scene.boundary):
+            # CW plane wave through a TFSF slab on the complex Bloch field
+            patches.extend(_grating_slab_patches(scene, src, {n: static_curl.get(n, np.float32(uniform[n][1]))
+                                                              for n in COMPONENTS}, dt, time_steps))
         elif isinstance(src, PlaneWaveTFSF):
-            if any(b == BOUNDARY_BLOCH for b in scene.boundary):
-                raise ValueError("TFSF sources with Bloch faces are not supported; use PlaneSource")
             if aux_line is not None:
                 raise ValueError("one TFSF source per scene")
             curl_full = {name: static_curl.get(name, np.float32(uniform[name][1])) for name in COMPONENTS}
@@ -1169,6 +1171,194 @@ def _beam_launch_plane(scene: Scene, axis: int, forward: bool) -> int:
     target = lo + 0.05 * (hi - lo) if forward else hi - 0.05 * (hi - lo)
     below = int(math.floor(target))
     return below if target - below <= (below + 1) - target else below + 1
+
+
+def _discrete_plane_wave_vectors(direction, polarization, k_num: float, d: float):
+    """Unit E and H vectors of the discrete plane wave (witwin/maxwell/fdtd/excitation/
+    tfsf_specs.py:369-386): the polarisation made transverse to the effective
+    wavevector sin(k u_a d / 2) / d, H along -(kappa x E)."""
+    eff = np.array([math.sin(0.5 * k_num * float(c) * d) / d for c in direction])
+    kh = eff / np.linalg.norm(eff)
+    p = np.asarray(polarization, dtype=np.float64)
+    e = p - float(p @ kh) * kh
+    e = e / np.linalg.norm(e)
+    m = -np.cross(kh, e)
+    m = m / np.linalg.norm(m)
+    return ({n: float(v) for n, v in zip(("Ex", "Ey", "Ez"), e)},
+            {n: float(v) for n, v in zip(("Hx", "Hy", "Hz"), m)})
+
+
+def tfsf_bloch_wavevector(scene: Scene, src: PlaneWaveTFSF) -> tuple[float, float, float]:
+    """The Bloch wavevector (rad/m per axis) a TFSF slab's CW plane wave needs on the
+    scene's grid: the numerical wavenumber of the discrete dispersion relation along
+    the direction, projected on each axis (the normal axis entry is unused)."""
+    dvec = np.asarray(src.direction, dtype=np.float64)
+    dvec = dvec / np.linalg.norm(dvec)
+    omega = 2.0 * math.pi * float(src.source_time.frequency)
+    k_num = _numerical_wavenumber(omega, scene.resolve_dt(), dvec, float(scene.spacing))
+    return tuple(float(k_num * c) for c in dvec)
+
+
+@dataclass(frozen=True)
+class GratingSlabTerm:
+    """One CW face term of a TFSF slab on Bloch faces, as the reference's
+    addCwPhasedSourcePatchBloch3D receives it (witwin/maxwell/fdtd/cuda/backend.py:
+    1817-1854): at step n the complex delta of the cells of ``box`` is
+    (cos_patch s_c + sin_patch s_s) + i (cos_patch s_s - sin_patch s_c) with
+    (s_c, s_s) = (signal_cos[n], signal_sin[n])."""
+
+    component: str
+    box: tuple
+    cos_patch: np.ndarray
+    sin_patch: np.ndarray
+    signal_cos: np.ndarray
+    signal_sin: np.ndarray
+
+
+def grating_slab_terms(scene: Scene, src: PlaneWaveTFSF, curl: dict, dt: float, steps: int) -> list:
+    """CW plane wave through a TFSF slab on a Bloch scene (the reference's grating-slab
+    provider, witwin/maxwell/fdtd/excitation/tfsf_state.py:202-279): the two faces
+    normal to the injection axis over the whole transverse extent (tfsf_specs.py:
+    322-332), the E faces driven by the discrete magnetic vector / eta0 and the H
+    faces by the electric one, each term the curl coefficient over the spacing times
+    the face sign, with the CW phase omega (r - r0).u / v of the numerical phase speed
+    v (tfsf_common.py:354-421); (s_c, s_s) = A (cos, sin)(omega t + phase)
+    (temporal.py:71-74), E terms at (n + 1/2) dt and H terms at n dt
+    (tfsf_apply.py:226-242)."""
+    st = src.source_time
+    if not isinstance(st, CW):
+        raise ValueError("a TFSF slab on Bloch faces takes a CW source time")
+    dvec = np.asarray(src.direction, dtype=np.float64)
+    dvec = dvec / np.linalg.norm(dvec)
+    pvec = np.asarray(src.polarization, dtype=np.float64)
+    pvec = pvec / np.linalg.norm(pvec)
+    axis = int(np.argmax(np.abs(dvec)))
+    transverse = [a for a in range(3) if a != axis]
+    for a in transverse:
+        if scene.boundary[2 * a] not in (BOUNDARY_BLOCH, BOUNDARY_PERIODIC):
+            raise ValueError("a TFSF slab on Bloch faces needs Bloch or periodic transverse axes")
+    if scene.boundary[2 * axis] in (BOUNDARY_BLOCH, BOUNDARY_PERIODIC):
+        raise ValueError("the injection axis of a TFSF slab cannot be periodic")
+    d = float(scene.spacing)
+    nodes = scene.nodes
+    freq = float(st.frequency)
+    omega = 2.0 * math.pi * freq
+    k_num = _numerical_wavenumber(omega, dt, dvec, d)
+    for a in transverse:
+        need = k_num * dvec[a]
+        have = float(scene.bloch_k[a]) if scene.boundary[2 * a] == BOUNDARY_BLOCH else 0.0
+        if abs(need - have) > 1e-6 * max(k_num, 1.0):
+            raise ValueError(f"Bloch wavevector {have:.9g} on axis {'xyz'[a]} does not match the TFSF plane wave "
+                             f"({need:.9g} rad/m, scene.tfsf_bloch_wavevector)")
+    speed = omega / k_num if k_num > 1e-12 else C_0
+    e_unit, h_unit = _discrete_plane_wave_vectors(dvec, pvec, k_num, d)
+    h_vec = {n: v / ETA_0 for n, v in h_unit.items()}
+    lower = [0, 0, 0]
+    upper = [n - 1 for n in nodes]
+    lower[axis], upper[axis] = int(src.lower[axis]), int(src.upper[axis])
+    ele, mag = _tfsf_specs(lower, upper)
+    ele, mag = ele[4 * axis:4 * axis + 4], mag[4 * axis:4 * axis + 4]  # the low and the high face
+    ref = np.array([0.5 * (src.lower[a] + src.upper[a]) * d for a in range(3)])
+    terms = []
+    for specs, vector, t_off in ((ele, h_vec, 0.5 * dt), (mag, e_unit, 0.0)):
+        times = np.arange(steps, dtype=np.float64) * dt + t_off
+        ramp = np.array([st.ramp(t) for t in times])
+        sc = (st.amplitude * ramp * np.cos(omega * times + st.phase)).astype(np.float32)
+        ss = (st.amplitude * ramp * np.sin(omega * times + st.phase)).astype(np.float32)
+        for fname, iname, offs, shape, soffs, _delta_axis, sgn in specs:
+            comp_scale = float(vector[iname])
+            if abs(sgn * comp_scale) <= 1e-12:
+                continue
+            box = (offs[0], offs[0] + shape[0], offs[1], offs[1] + shape[1], offs[2], offs[2] + shape[2])
+            c = curl[fname]
+            c_arr = np.broadcast_to(c, component_shape(fname, nodes)) if np.ndim(c) == 0 else c
+            coeff = c_arr[box[0]:box[1], box[2]:box[3], box[4]:box[5]].astype(np.float64) / d
+            delay = ((_component_positions(iname, soffs, shape, d) - ref) @ dvec) / speed
+            scale = sgn * comp_scale * coeff
+            terms.append(GratingSlabTerm(fname, box, np.ascontiguousarray((scale * np.cos(omega * delay)).astype(np.float32)),
+                                         np.ascontiguousarray((scale * np.sin(omega * delay)).astype(np.float32)), sc, ss))
+    return terms
+
+
+def bloch_patch_phases(scene: Scene, component: str):
+    """Per tangential axis of a field component (the two axes other than its own,
+    in increasing order): whether a Bloch patch wraps there and the face phase
+    (cos kL, sin kL), 1 on a periodic axis (witwin/maxwell/fdtd/excitation/
+    temporal.py:126-205)."""
+    own = "xyz".index(component[1])
+    out = []
+    for a in (x for x in range(3) if x != own):
+        kind = scene.boundary[2 * a]
+        if kind == BOUNDARY_BLOCH:
+            ang = float(scene.bloch_k[a]) * (scene.nodes[a] - 1) * float(scene.spacing)
+            out.append((a, True, math.cos(ang), math.sin(ang)))
+        else:
+            out.append((a, kind == BOUNDARY_PERIODIC, 1.0, 0.0))
+    return out
+
+
+def _fold_bloch_wrap_copies(scene: Scene, term: GratingSlabTerm):
+    """Per-channel coefficients of a CW Bloch term with the reference's wrap copies
+    folded in (witwin/maxwell/fdtd/cuda/kernels/sources.cu:368-440): a cell on the
+    first plane of a wrapped tangential axis also adds e^{+ikL} times its delta to
+    the last plane, a cell on the last plane e^{-ikL} times its delta to the first,
+    and a cell on both wrapped axes' boundaries the doubly rotated delta to the
+    opposite corner.  Returns (real s_c, real s_s, imag s_c, imag s_s) coefficient
+    arrays over the term's box, which must span every wrapped axis whole."""
+    shape = component_shape(term.component, scene.nodes)
+    cp, sp = term.cos_patch.astype(np.float64), term.sin_patch.astype(np.float64)
+    # delta = (Ac sc + As ss) + i (Bc sc + Bs ss)
+    src = [cp, sp, -sp, cp]
+    out = [x.copy() for x in src]
+    wraps = []
+    for a, wrap, c, s in bloch_patch_phases(scene, term.component):
+        if not wrap:
+            continue
+        lo, hi = term.box[2 * a], term.box[2 * a + 1]
+        if lo != 0 or hi != shape[a] or shape[a] < 2:
+            raise ValueError("a Bloch slab term must span the wrapped axes whole")
+        wraps.append((a, c, s))
+
+    def rotate(vals, c, s):  # e^{i theta} on (Ac, As, Bc, Bs)
+        ac, as_, bc, bs = vals
+        return [c * ac - s * bc, c * as_ - s * bs, s * ac + c * bc, s * as_ + c * bs]
+
+    def take(vals, a, idx):
+        return [np.take(v, [idx], axis=a) for v in vals]
+
+    def add_at(a_list, idx_list, vals):
+        sl = [slice(None)] * 3
+        for a, idx in zip(a_list, idx_list):
+            sl[a] = slice(idx, idx + 1)
+        for o, v in zip(out, vals):
+            o[tuple(sl)] += v
+
+    for a, c, s in wraps:
+        n = shape[a]
+        add_at([a], [n - 1], rotate(take(src, a, 0), c, s))
+        add_at([a], [0], rotate(take(src, a, n - 1), c, -s))
+    if len(wraps) == 2:
+        (a, ca, sa), (b, cb, sb) = wraps
+        na, nb = shape[a], shape[b]
+        for ia, ra in ((0, 1.0), (na - 1, -1.0)):
+            for ib, rb in ((0, 1.0), (nb - 1, -1.0)):
+                corner = take(take(src, a, ia), b, ib)
+                add_at([a, b], [na - 1 - ia, nb - 1 - ib], rotate(rotate(corner, ca, ra * sa), cb, rb * sb))
+    return tuple(np.ascontiguousarray(o.astype(np.float32)) for o in out)
+
+
+def _grating_slab_patches(scene: Scene, src: PlaneWaveTFSF, curl: dict, dt: float, steps: int) -> list:
+    """The grating-slab terms as per-channel patches of the complex field: real
+    channel (A_c s_c + A_s s_s), imaginary channel (B_c s_c + B_s s_s) with the
+    reference kernel's wrap copies folded into A and B."""
+    patches = []
+    for t in grating_slab_terms(scene, src, curl, dt, steps):
+        ac, as_, bc, bs = _fold_bloch_wrap_copies(scene, t)
+        patches += [CompiledPatch(t.component, t.box, ac, t.signal_cos, 0),
+                    CompiledPatch(t.component, t.box, as_, t.signal_sin, 0),
+                    CompiledPatch(t.component, t.box, bc, t.signal_cos, 1),
+                    CompiledPatch(t.component, t.box, bs, t.signal_sin, 1)]
+    return patches
 
 
 def _beam_patches(scene: Scene, src: GaussianBeam, curl: dict, dt: float, steps: int):
