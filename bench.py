@@ -564,8 +564,8 @@ def run_grating_bench(wm, device, steps: int = 64, warmup: int = 8):
     torch.cuda.empty_cache()
     return {
         "workload": "bloch_grating: 512x512x384 cells, Bloch x/y (k_x = 0.1 * 2 pi / L_x), 16-cell CPML on z, "
-                    "Debye grating layer (64-cell period, 50 % duty), Ex plane source with the Bloch phase, "
-                    "32-frequency diffraction plane",
+                    "Debye grating layer (64-cell period, 50 % duty), pulsed Ex plane wave through a TFSF slab on z "
+                    "(the reference's grating slab), 32-frequency diffraction plane",
         "cells": int(cs.cells),
         "steps": steps,
         "ms_per_step": ms / steps,

@@ -328,10 +328,12 @@ class RefGpuBloch:
     channels' spectra."""
 
     def __init__(self, compiled, device: str = "cuda", bloch_terms=None, term_phases=None):
-        """``bloch_terms``: CW Bloch face terms (component, box, cos_patch,
-        sin_patch, signal_cos, signal_sin) injected through the reference's own
-        add_source_patch_bloch, real and imaginary values launched separately as
-        cuda/backend.py:1817-1854 does, in place of the compiled patches;
+        """``bloch_terms``: Bloch face terms injected through the reference's own
+        add_source_patch_bloch in place of the compiled patches: a CW term
+        (component, box, cos_patch, sin_patch, signal_cos, signal_sin) as its real
+        and imaginary values in two launches (cuda/backend.py:1817-1854), a pulsed
+        term (scale, delay, t_offset, source_time) as the real values scale * w(n dt
+        + t_offset - delay) (excitation/temporal.py:229-247, 395-405);
         ``term_phases[component]``: the two tangential (wrap, cos kL, sin kL)."""
         cs = compiled
         if cs.cpml and (any(cs.pml_lo[:2]) or any(cs.pml_hi[:2])):
@@ -343,24 +345,31 @@ class RefGpuBloch:
         self.z_cpml = bool(cs.cpml and (cs.pml_lo[2] or cs.pml_hi[2]))
         self.terms = None
         if bloch_terms is not None:
-            dev = self.re.dev
             self.re.patches, self.im.patches = [], []
-            self.terms = [(t.component, t.box, torch.as_tensor(t.cos_patch, device=dev),
-                           torch.as_tensor(t.sin_patch, device=dev), np.asarray(t.signal_cos, np.float32),
-                           np.asarray(t.signal_sin, np.float32), term_phases[t.component]) for t in bloch_terms]
+            self.terms = [(t, term_phases[t.component]) for t in bloch_terms]
 
     def _bloch_terms(self, n: int, magnetic: bool):
         if not self.terms:
             return
+        from oracle.oracle import shifted_waveform
+
         R, I = self.re.F, self.im.F
-        for comp, box, cp, sp, sc, ss, ph in self.terms:
+        dev = self.re.dev
+        for t, ph in self.terms:
+            comp, box = t.component, t.box
             if (comp[0] == "H") != magnetic:
                 continue
             names = ("Hx", "Hy", "Hz") if magnetic else ("Ex", "Ey", "Ez")
-            triplet = [t for nm in names for t in (R[nm], I[nm])]
+            triplet = [f for nm in names for f in (R[nm], I[nm])]
             (wa, ca, sa), (wb, cb, sb) = ph
-            c, s = float(sc[n]), float(ss[n])
-            for values, sr, si in ((cp * c + sp * s, 1.0, 0.0), (cp * s - sp * c, 0.0, 1.0)):
+            if t.cos_patch is None:
+                w = shifted_waveform(t.source_time, n * self.cs.dt + t.t_offset - t.delay.astype(np.float64))
+                launches = ((torch.as_tensor((t.scale * w).astype(np.float32), device=dev), 1.0, 0.0),)
+            else:
+                cp, sp = torch.as_tensor(t.cos_patch, device=dev), torch.as_tensor(t.sin_patch, device=dev)
+                c, s = float(t.signal_cos[n]), float(t.signal_sin[n])
+                launches = ((cp * c + sp * s, 1.0, 0.0), (cp * s - sp * c, 0.0, 1.0))
+            for values, sr, si in launches:
                 self.op.add_source_patch_bloch(*triplet, values.contiguous(), box[0], box[2], box[4], sr, si,
                                                "xyz".index(comp[1]), float(ca), float(sa), float(cb), float(sb),
                                                int(wa), int(wb))

@@ -118,12 +118,14 @@ def test_bloch_matches_reference_bloch_kernels():
 def test_bloch_grating_shape_with_z_cpml_matches_reference_kernels():
     """The large grating's boundary set on a small copy: Bloch x / y faces
     (k_x = 0.1 * 2 pi / L_x), 8-cell CPML on z only, the Debye grating layer
-    and the phased current sheet (64 x 64 x 48 cells, 4 frequencies, 300
-    steps), against the reference's Bloch-xy / standard-z E kernels followed by
-    its z-CPML corrections of Ex and Ey on both channels."""
+    and a phased current sheet in place of its TFSF slab (64 x 64 x 48 cells,
+    4 frequencies, 300 steps), against the reference's Bloch-xy / standard-z E
+    kernels followed by its z-CPML corrections of Ex and Ey on both channels."""
     wm = load_package()
     steps = 300
-    cs = wm.compile_scene(wm.workloads.bloch_grating(cells=(64, 64, 48), pml=8, n_freq=4), steps)
+    sc = wm.workloads.bloch_grating(cells=(64, 64, 48), pml=8, n_freq=4)
+    sc.sources[:] = [wm.PlaneSource(2, 48 - 8 - 5, "Ex", wm.GaussianPulse(300e12, 120e12))]
+    cs = wm.compile_scene(sc, steps)
     assert cs.complex_fields and cs.pml_lo[2] == 8 and cs.pml_lo[0] == 0
     assert {p.kind for p in cs.poles} == {0}
     solver = wm.solver.B200FDTD(cs).init_field()

@@ -40,9 +40,14 @@ def _terms(wm, sc, cs, steps):
     return wm.scene.grating_slab_terms(sc, sc.sources[0], curl, cs.dt, steps)
 
 
-def _kernel_restatement(wm, sc, term, sig_c, sig_s):
+def _cw_delta(term, sig_c, sig_s):
+    cp, sp = term.cos_patch.astype(np.float64), term.sin_patch.astype(np.float64)
+    return (cp * sig_c + sp * sig_s) + 1j * (cp * sig_s - sp * sig_c)
+
+
+def _kernel_restatement(wm, sc, term, delta_box):
     """Per-cell add_bloch_source_patch_kernel (sources.cu:368-440) for one term and
-    one (s_c, s_s): the complex field increment over the component's extent."""
+    its complex delta over the box: the field increment over the component's extent."""
     shape = wm.scene.component_shape(term.component, sc.nodes)
     out = np.zeros(shape, np.complex128)
     ph = wm.scene.bloch_patch_phases(sc, term.component)
@@ -51,8 +56,7 @@ def _kernel_restatement(wm, sc, term, sig_c, sig_s):
     for i in range(b[1] - b[0]):
         for j in range(b[3] - b[2]):
             for k in range(b[5] - b[4]):
-                cp, sp = float(term.cos_patch[i, j, k]), float(term.sin_patch[i, j, k])
-                delta = complex(cp * sig_c + sp * sig_s, cp * sig_s - sp * sig_c)
+                delta = complex(delta_box[i, j, k])
                 cell = [b[0] + i, b[2] + j, b[4] + k]
                 out[tuple(cell)] += delta
                 ca_, cb_ = cell[ax_a], cell[ax_b]
@@ -106,23 +110,23 @@ def test_face_terms_and_checks():
         comp_patches = [p for p in cs.patches if p.component == t.component and p.box == t.box]
         assert len(comp_patches) == 4
         for sig_c, sig_s in rng.normal(size=(2, 2)):
-            want = _kernel_restatement(wm, sc, t, sig_c, sig_s)
+            want = _kernel_restatement(wm, sc, t, _cw_delta(t, sig_c, sig_s))
             got = np.zeros_like(want)
             b = t.box
             for p in comp_patches:
                 sig = sig_c if np.array_equal(p.signal, t.signal_cos) else sig_s
                 got[b[0]:b[1], b[2]:b[3], b[4]:b[5]] += (1 if p.channel == 0 else 1j) * p.coeff.astype(np.float64) * sig
             np.testing.assert_allclose(got, want, rtol=1e-5, atol=1e-6 * np.abs(want).max())
-    # a Bloch wavevector that does not match the plane wave, a pulse
+    # a CW wave whose Bloch wavevector does not match it, an injection along a Bloch axis
     bad = _scene(wm)
     bad.bloch_k = (0.5 * bad.bloch_k[0], 0.0, 0.0)
     with pytest.raises(ValueError):
         wm.compile_scene(bad, 10)
-    pulsed = _scene(wm)
-    pulsed.sources[0] = wm.PlaneWaveTFSF(pulsed.sources[0].direction, pulsed.sources[0].polarization,
-                                         wm.GaussianPulse(300e12, 100e12), (0, 0, 20), (24, 20, 40))
+    along_x = _scene(wm)
+    along_x.sources[0] = wm.PlaneWaveTFSF((1.0, 0.0, 0.0), (0.0, 1.0, 0.0), wm.GaussianPulse(300e12, 100e12),
+                                          (4, 0, 0), (20, 20, 60))
     with pytest.raises(ValueError):
-        wm.compile_scene(pulsed, 10)
+        wm.compile_scene(along_x, 10)
 
 
 @pytest.mark.gpu
@@ -171,3 +175,74 @@ def test_bloch_tfsf_slab_confines_total_field(pol):
     print(f"TFSF slab on Bloch faces ({pol}): inside {inside:.3e}, outside {outside:.3e}, ratio {outside / inside:.2e}")
     assert inside > 0.1
     assert outside < inside
+
+
+def _grating(wm):
+    """The large grating's shape on a small copy: Bloch x / y (k_x = 0.1 * 2 pi / L_x),
+    8-cell CPML on z, the Debye layer and the pulsed TFSF slab, 64 x 64 x 48 cells."""
+    return wm.workloads.bloch_grating(cells=(64, 64, 48), pml=8, n_freq=4)
+
+
+def test_pulsed_slab_terms_fold():
+    from oracle.oracle import shifted_waveform
+
+    wm = load_package()
+    sc = _grating(wm)
+    steps = 60
+    cs = wm.compile_scene(sc, steps)
+    assert cs.complex_fields and not cs.patches
+    # Ex and Hy terms on both faces; the x copies of Hy carry the Bloch phase into
+    # the imaginary channel, the y copies of Ex (k_y = 0) stay real
+    assert sorted((p.component, p.channel) for p in cs.shifted) == [
+        ("Ex", 0), ("Ex", 0), ("Hy", 0), ("Hy", 0), ("Hy", 1), ("Hy", 1)]
+    terms = _terms(wm, sc, cs, steps)
+    assert [t.component for t in terms] == ["Ex", "Ex", "Hy", "Hy"]
+    for t in terms:
+        for n in (7, 31):
+            w = shifted_waveform(t.source_time, n * cs.dt + t.t_offset - t.delay.astype(np.float64))
+            want = _kernel_restatement(wm, sc, t, t.scale.astype(np.float64) * w)
+            got = np.zeros_like(want)
+            for p in cs.shifted:
+                if p.component != t.component or p.t_offset != t.t_offset:
+                    continue
+                b = p.box
+                if not (b[4] == t.box[4] and b[5] == t.box[5]):
+                    continue
+                wp = shifted_waveform(p.source_time, n * cs.dt + p.t_offset - p.delay.astype(np.float64))
+                got[b[0]:b[1], b[2]:b[3], b[4]:b[5]] += (1 if p.channel == 0 else 1j) * p.scale.astype(np.float64) * wp
+            np.testing.assert_allclose(got, want, rtol=1e-5, atol=1e-6 * max(np.abs(want).max(), 1e-30))
+
+
+@pytest.mark.gpu
+def test_grating_workload_slab_matches_reference_ops():
+    """The pulsed TFSF slab of the grating workload (small copy, 300 steps) with
+    the Debye layer and z CPML, against the reference's ops with its own Bloch
+    patch kernel."""
+    from oracle import ref_gpu
+    from test_bloch import FIELDS, TOL, joint
+
+    if not ref_gpu.available():
+        pytest.skip("oracle/_ref not built")
+    wm = load_package()
+    steps = 300
+    sc = _grating(wm)
+    cs = wm.compile_scene(sc, steps)
+    solver = wm.solver.B200FDTD(cs).init_field()
+    solver.step_range(0, steps)
+    got = {**{f"re_{n}": solver.field(n).cpu().numpy() for n in FIELDS},
+           **{f"im_{n}": solver.field(n, imag=True).cpu().numpy() for n in FIELDS}}
+    mons = {k: {c: v.cpu().numpy() for c, v in d.items()} for k, d in solver.monitor_results().items()}
+    solver.close()
+    phases = {c: [(w, co, si) for _a, w, co, si in wm.scene.bloch_patch_phases(sc, c)] for c in COMPONENTS}
+    ref = ref_gpu.RefGpuBloch(cs, bloch_terms=_terms(wm, sc, cs, steps), term_phases=phases)
+    assert ref.z_cpml
+    ref.run(steps)
+    ref_re, ref_im = ref.fields()
+    want = {**{f"re_{n}": ref_re[n] for n in FIELDS}, **{f"im_{n}": ref_im[n] for n in FIELDS}}
+    assert np.linalg.norm(want["re_Ex"]) > 0 and np.linalg.norm(want["im_Ex"]) > 1e-3 * np.linalg.norm(want["re_Ex"])
+    err = joint(got, want)
+    print(f"grating workload TFSF slab vs the reference's ops: joint relative L2 {err:.2e}")
+    assert err < TOL
+    refm = ref.monitor_results()
+    for m in refm:
+        assert joint(mons[m], refm[m]) < TOL, m

@@ -444,6 +444,7 @@ class CompiledShiftedPatch:
     delay: np.ndarray  # box-dense float32, seconds
     t_offset: float  # 0 for H components, dt / 2 for E components
     source_time: object
+    channel: int = 0  # 0 real, 1 imaginary part of a complex (Bloch) field
 
 
 @dataclass
@@ -1015,8 +1016,10 @@ def compile_scene(scene: Scene, time_steps: int) -> CompiledScene:
             shifted.extend(beam_shifted)
         elif isinstance(src, PlaneWaveTFSF) and any(b == BOUNDARY_BLOCH for b in scene.boundary):
             # CW plane wave through a TFSF slab on the complex Bloch field
-            patches.extend(_grating_slab_patches(scene, src, {n: static_curl.get(n, np.float32(uniform[n][1]))
-                                                              for n in COMPONENTS}, dt, time_steps))
+            slab_patches, slab_shifted = _grating_slab_patches(
+                scene, src, {n: static_curl.get(n, np.float32(uniform[n][1])) for n in COMPONENTS}, dt, time_steps)
+            patches.extend(slab_patches)
+            shifted.extend(slab_shifted)
         elif isinstance(src, PlaneWaveTFSF):
             if aux_line is not None:
                 raise ValueError("one TFSF source per scene")
@@ -1201,18 +1204,23 @@ def tfsf_bloch_wavevector(scene: Scene, src: PlaneWaveTFSF) -> tuple[float, floa
 
 @dataclass(frozen=True)
 class GratingSlabTerm:
-    """One CW face term of a TFSF slab on Bloch faces, as the reference's
-    addCwPhasedSourcePatchBloch3D receives it (witwin/maxwell/fdtd/cuda/backend.py:
-    1817-1854): at step n the complex delta of the cells of ``box`` is
-    (cos_patch s_c + sin_patch s_s) + i (cos_patch s_s - sin_patch s_c) with
-    (s_c, s_s) = (signal_cos[n], signal_sin[n])."""
+    """One face term of a TFSF slab on Bloch faces, as the reference's Bloch patch
+    launchers receive it.  CW (witwin/maxwell/fdtd/cuda/backend.py:1817-1854): at
+    step n the complex delta of the cells of ``box`` is (cos_patch s_c + sin_patch
+    s_s) + i (cos_patch s_s - sin_patch s_c), (s_c, s_s) = (signal_cos[n],
+    signal_sin[n]).  Pulsed (witwin/maxwell/fdtd/excitation/temporal.py:229-247,
+    395-405): the real delta scale * w(n dt + t_offset - delay) per cell."""
 
     component: str
     box: tuple
-    cos_patch: np.ndarray
-    sin_patch: np.ndarray
-    signal_cos: np.ndarray
-    signal_sin: np.ndarray
+    cos_patch: np.ndarray | None = None
+    sin_patch: np.ndarray | None = None
+    signal_cos: np.ndarray | None = None
+    signal_sin: np.ndarray | None = None
+    scale: np.ndarray | None = None
+    delay: np.ndarray | None = None
+    t_offset: float = 0.0
+    source_time: object = None
 
 
 def grating_slab_terms(scene: Scene, src: PlaneWaveTFSF, curl: dict, dt: float, steps: int) -> list:
@@ -1226,8 +1234,9 @@ def grating_slab_terms(scene: Scene, src: PlaneWaveTFSF, curl: dict, dt: float, 
     (temporal.py:71-74), E terms at (n + 1/2) dt and H terms at n dt
     (tfsf_apply.py:226-242)."""
     st = src.source_time
-    if not isinstance(st, CW):
-        raise ValueError("a TFSF slab on Bloch faces takes a CW source time")
+    cw = isinstance(st, CW)
+    if not cw and not isinstance(st, GaussianPulse):
+        raise ValueError("a TFSF slab on Bloch faces takes a CW or GaussianPulse source time")
     dvec = np.asarray(src.direction, dtype=np.float64)
     dvec = dvec / np.linalg.norm(dvec)
     pvec = np.asarray(src.polarization, dtype=np.float64)
@@ -1244,7 +1253,7 @@ def grating_slab_terms(scene: Scene, src: PlaneWaveTFSF, curl: dict, dt: float, 
     freq = float(st.frequency)
     omega = 2.0 * math.pi * freq
     k_num = _numerical_wavenumber(omega, dt, dvec, d)
-    for a in transverse:
+    for a in transverse if cw else ():  # a pulse keeps the scene's fixed Bloch wavevector
         need = k_num * dvec[a]
         have = float(scene.bloch_k[a]) if scene.boundary[2 * a] == BOUNDARY_BLOCH else 0.0
         if abs(need - have) > 1e-6 * max(k_num, 1.0):
@@ -1261,10 +1270,11 @@ def grating_slab_terms(scene: Scene, src: PlaneWaveTFSF, curl: dict, dt: float, 
     ref = np.array([0.5 * (src.lower[a] + src.upper[a]) * d for a in range(3)])
     terms = []
     for specs, vector, t_off in ((ele, h_vec, 0.5 * dt), (mag, e_unit, 0.0)):
-        times = np.arange(steps, dtype=np.float64) * dt + t_off
-        ramp = np.array([st.ramp(t) for t in times])
-        sc = (st.amplitude * ramp * np.cos(omega * times + st.phase)).astype(np.float32)
-        ss = (st.amplitude * ramp * np.sin(omega * times + st.phase)).astype(np.float32)
+        if cw:
+            times = np.arange(steps, dtype=np.float64) * dt + t_off
+            ramp = np.array([st.ramp(t) for t in times])
+            sc = (st.amplitude * ramp * np.cos(omega * times + st.phase)).astype(np.float32)
+            ss = (st.amplitude * ramp * np.sin(omega * times + st.phase)).astype(np.float32)
         for fname, iname, offs, shape, soffs, _delta_axis, sgn in specs:
             comp_scale = float(vector[iname])
             if abs(sgn * comp_scale) <= 1e-12:
@@ -1275,6 +1285,11 @@ def grating_slab_terms(scene: Scene, src: PlaneWaveTFSF, curl: dict, dt: float, 
             coeff = c_arr[box[0]:box[1], box[2]:box[3], box[4]:box[5]].astype(np.float64) / d
             delay = ((_component_positions(iname, soffs, shape, d) - ref) @ dvec) / speed
             scale = sgn * comp_scale * coeff
+            if not cw:
+                terms.append(GratingSlabTerm(fname, box, scale=np.ascontiguousarray(scale.astype(np.float32)),
+                                             delay=np.ascontiguousarray(delay.astype(np.float32)), t_offset=t_off,
+                                             source_time=st))
+                continue
             terms.append(GratingSlabTerm(fname, box, np.ascontiguousarray((scale * np.cos(omega * delay)).astype(np.float32)),
                                          np.ascontiguousarray((scale * np.sin(omega * delay)).astype(np.float32)), sc, ss))
     return terms
@@ -1347,18 +1362,67 @@ def _fold_bloch_wrap_copies(scene: Scene, term: GratingSlabTerm):
     return tuple(np.ascontiguousarray(o.astype(np.float32)) for o in out)
 
 
-def _grating_slab_patches(scene: Scene, src: PlaneWaveTFSF, curl: dict, dt: float, steps: int) -> list:
-    """The grating-slab terms as per-channel patches of the complex field: real
-    channel (A_c s_c + A_s s_s), imaginary channel (B_c s_c + B_s s_s) with the
-    reference kernel's wrap copies folded into A and B."""
-    patches = []
+def _fold_shifted_wrap_copies(scene: Scene, term: GratingSlabTerm) -> list:
+    """Time-shifted patches of a pulsed Bloch term with the reference kernel's wrap
+    copies (sources.cu:368-440): the real delta scale * w(t - delay) on channel 0,
+    and each wrapped axis' first / last plane copied to the opposite plane rotated
+    by e^{+ikL} / e^{-ikL} (real part to channel 0, imaginary part to channel 1).
+    A copy whose delays equal the target plane's (a wave without a phase along
+    that axis) is folded into the target's scale; otherwise it is a patch of its
+    own over that plane."""
+    shape = component_shape(term.component, scene.nodes)
+    scale = term.scale.astype(np.float64)
+    main_re, main_im = scale.copy(), np.zeros_like(scale)
+    extra = []
+    wraps = [(a, c, s) for a, w, c, s in bloch_patch_phases(scene, term.component) if w]
+    if len(wraps) > 1:
+        raise ValueError("a pulsed Bloch slab term wraps on one tangential axis at most")
+    for a, c, s in wraps:
+        lo, hi = term.box[2 * a], term.box[2 * a + 1]
+        n = shape[a]
+        if lo != 0 or hi != n or n < 2:
+            raise ValueError("a Bloch slab term must span the wrapped axes whole")
+        for src, dst, sn in ((0, n - 1, s), (n - 1, 0, -s)):
+            sl_src = [slice(None)] * 3
+            sl_dst = [slice(None)] * 3
+            sl_src[a], sl_dst[a] = slice(src, src + 1), slice(dst, dst + 1)
+            sl_src, sl_dst = tuple(sl_src), tuple(sl_dst)
+            if np.array_equal(term.delay[sl_src], term.delay[sl_dst]):
+                main_re[sl_dst] += c * scale[sl_src]
+                main_im[sl_dst] += sn * scale[sl_src]
+                continue
+            box = list(term.box)
+            box[2 * a], box[2 * a + 1] = dst, dst + 1
+            dly = np.ascontiguousarray(term.delay[sl_src])
+            for ch, f in ((0, c), (1, sn)):
+                if f != 0.0:
+                    extra.append(CompiledShiftedPatch(term.component, tuple(box),
+                                                      np.ascontiguousarray((f * scale[sl_src]).astype(np.float32)), dly,
+                                                      term.t_offset, term.source_time, ch))
+    out = [CompiledShiftedPatch(term.component, term.box, np.ascontiguousarray(main_re.astype(np.float32)), term.delay,
+                                term.t_offset, term.source_time, 0)]
+    if np.any(main_im != 0.0):
+        out.append(CompiledShiftedPatch(term.component, term.box, np.ascontiguousarray(main_im.astype(np.float32)),
+                                        term.delay, term.t_offset, term.source_time, 1))
+    return out + extra
+
+
+def _grating_slab_patches(scene: Scene, src: PlaneWaveTFSF, curl: dict, dt: float, steps: int):
+    """The grating-slab terms on the complex field: a CW term as per-channel patches,
+    real channel (A_c s_c + A_s s_s), imaginary channel (B_c s_c + B_s s_s) with the
+    reference kernel's wrap copies folded into A and B; a pulsed term as
+    time-shifted patches (_fold_shifted_wrap_copies).  Returns (patches, shifted)."""
+    patches, shifted = [], []
     for t in grating_slab_terms(scene, src, curl, dt, steps):
+        if t.cos_patch is None:
+            shifted += _fold_shifted_wrap_copies(scene, t)
+            continue
         ac, as_, bc, bs = _fold_bloch_wrap_copies(scene, t)
         patches += [CompiledPatch(t.component, t.box, ac, t.signal_cos, 0),
                     CompiledPatch(t.component, t.box, as_, t.signal_sin, 0),
                     CompiledPatch(t.component, t.box, bc, t.signal_cos, 1),
                     CompiledPatch(t.component, t.box, bs, t.signal_sin, 1)]
-    return patches
+    return patches, shifted
 
 
 def _beam_patches(scene: Scene, src: GaussianBeam, curl: dict, dt: float, steps: int):

@@ -209,7 +209,7 @@ class B200FDTD:
                     ),
                     "add_patch",
                 )
-            for sp in getattr(cs, "shifted", []) if channel == 0 else []:
+            for sp in (sp for sp in getattr(cs, "shifted", []) if getattr(sp, "channel", 0) == channel):
                 st = sp.source_time
                 pulse = isinstance(st, GaussianPulse)
                 _lib.check(

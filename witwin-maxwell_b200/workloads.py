@@ -16,7 +16,6 @@ from .scene import (
     MaterialRegion,
     Medium,
     PlaneMonitor,
-    PlaneSource,
     PlaneWaveTFSF,
     PointDipole,
     PointMonitor,
@@ -144,10 +143,10 @@ def bloch_grating(cells: tuple[int, int, int] = (512, 512, 384), pml: int = 16, 
     """Large grating workload: Bloch-periodic x / y faces with k_x = kx_fraction * 2 pi / L_x
     (k_y = 0) and a 16-cell CPML on z; a Debye grating layer (eps_inf 2.5, delta_eps 3.5,
     tau 1e-14 s) 32 cells high at z in [176, 208) with a 64-cell period in x and 50 % duty
-    (scaled with the grid); a z-normal Ex plane source (300 THz, fwidth 120 THz) 40 cells
-    below the top CPML carrying the Bloch phase e^{i k_x x}; a 32-frequency diffraction
-    plane (all components) at z = 320.  The reference drives this scene with a TFSF slab;
-    here a soft current sheet with the same phase profile stands in for it."""
+    (scaled with the grid); an Ex-polarised plane wave (300 THz, fwidth 120 THz) heading
+    down z through a TFSF slab from 40 cells below the top CPML to 16 cells above the
+    bottom one (the reference's grating slab, witwin/maxwell/fdtd/excitation/
+    tfsf_state.py:202-279); a 32-frequency diffraction plane (Ex, Ey, Hx, Hy) at z = 320."""
     nx, ny, nz = cells
     sz = nz / 384.0
     L = nx * SPACING
@@ -158,7 +157,9 @@ def bloch_grating(cells: tuple[int, int, int] = (512, 512, 384), pml: int = 16, 
     for x0 in range(0, nx, period):
         x1 = min(nx, x0 + period // 2)
         sc.structures.append(Structure(Box((x0, 0, z0), (x1, ny, z1)), Medium.debye(2.5, 3.5, 1e-14)))
-    sc.sources.append(PlaneSource(2, nz - pml - int(round(40 * sz)), "Ex", GaussianPulse(300e12, 120e12)))
+    sc.sources.append(PlaneWaveTFSF((0.0, 0.0, -1.0), (1.0, 0.0, 0.0), GaussianPulse(300e12, 120e12),
+                                    (0, 0, pml + int(round(16 * sz))), (nx, ny, nz - pml - int(round(40 * sz))),
+                                    slab=True))
     freqs = tuple(np.linspace(250e12, 350e12, n_freq))
     sc.monitors.append(PlaneMonitor("diffraction", 2, int(round(320 * sz)) if nz >= 384 else nz - pml - 2,
                                     ("Ex", "Ey", "Hx", "Hy"), freqs))
