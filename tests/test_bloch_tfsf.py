@@ -246,3 +246,21 @@ def test_grating_workload_slab_matches_reference_ops():
     refm = ref.monitor_results()
     for m in refm:
         assert joint(mons[m], refm[m]) < TOL, m
+
+
+def test_auto_bloch_wavevector():
+    """bloch_k = "auto" resolves to the CW plane wave's wavevector on the Bloch axes
+    (witwin/maxwell/fdtd/boundary/bloch.py:60-78) and compiles the same patches."""
+    wm = load_package()
+    sc = _scene(wm)
+    auto = _scene(wm)
+    auto.bloch_k = "auto"
+    assert wm.scene.resolve_bloch_wavevector(auto) == (sc.bloch_k[0], sc.bloch_k[1], 0.0)
+    a, b = wm.compile_scene(auto, 20), wm.compile_scene(sc, 20)
+    assert a.bloch_cos == b.bloch_cos and a.bloch_sin == b.bloch_sin
+    for p, q in zip(a.patches, b.patches):
+        np.testing.assert_array_equal(p.coeff, q.coeff)
+    pulsed = _grating(wm)
+    pulsed.bloch_k = "auto"
+    with pytest.raises(ValueError):
+        wm.compile_scene(pulsed, 10)

@@ -20,7 +20,7 @@ reference.  Cell-index coordinates are node indices of the full grid
 from __future__ import annotations
 
 import math
-from dataclasses import dataclass, field
+from dataclasses import dataclass, field, replace
 from typing import Sequence
 
 import numpy as np
@@ -390,7 +390,7 @@ class Scene:
     # Bloch wavevector (rad/m) of the x / y Bloch faces: the field on the high
     # face is e^{i k L} times the field on the low face
     # (witwin/maxwell/fdtd/boundary/bloch.py:79-90).
-    bloch_k: tuple[float, float, float] = (0.0, 0.0, 0.0)
+    bloch_k: tuple[float, float, float] | str = (0.0, 0.0, 0.0)  # or "auto": from the CW TFSF plane wave
 
     @property
     def nodes(self) -> tuple[int, int, int]:
@@ -829,8 +829,28 @@ def _compile_tfsf(scene: Scene, src: PlaneWaveTFSF, curl: dict, dt: float, steps
     return aux, out
 
 
+def resolve_bloch_wavevector(scene: Scene) -> tuple[float, float, float]:
+    """``scene.bloch_k``, or for ``"auto"`` the wavevector of the scene's one CW
+    TFSF plane wave on its Bloch axes (k_num times the direction there, 0
+    elsewhere; witwin/maxwell/fdtd/boundary/bloch.py:32-78, which also requires a
+    TFSF slab whose normal axis is not Bloch)."""
+    if not isinstance(scene.bloch_k, str):
+        return tuple(float(v) for v in scene.bloch_k)
+    if scene.bloch_k != "auto":
+        raise ValueError(f"bloch_k must be three numbers or 'auto', not {scene.bloch_k!r}")
+    waves = [s for s in scene.sources if isinstance(s, PlaneWaveTFSF)]
+    if len(scene.sources) != 1 or len(waves) != 1:
+        raise ValueError("an automatic Bloch wavevector needs exactly one source, a TFSF plane wave")
+    if not isinstance(waves[0].source_time, CW):
+        raise ValueError("an automatic Bloch wavevector needs a CW plane wave")
+    k = tfsf_bloch_wavevector(scene, waves[0])
+    return tuple(k[a] if scene.boundary[2 * a] == BOUNDARY_BLOCH else 0.0 for a in range(3))
+
+
 def compile_scene(scene: Scene, time_steps: int) -> CompiledScene:
     """Compile a scene into the solver tensors consumed by the FDTD step path."""
+    if isinstance(scene.bloch_k, str):
+        scene = replace(scene, bloch_k=resolve_bloch_wavevector(scene))
     nodes = scene.nodes
     d = float(scene.spacing)
     dt = scene.resolve_dt()
