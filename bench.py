@@ -557,11 +557,15 @@ def run_grating_bench(wm, device, steps: int = 64, warmup: int = 8):
     t0 = time.perf_counter()
     cs = wm.compile_scene(wm.workloads.bloch_grating(), warmup + steps + 4)
     compile_s = time.perf_counter() - t0
-    solver = wm.solver.B200FDTD(cs, device=device).init_field()
-    solver.step_range(0, warmup)
-    ms = solver.step_range(warmup, warmup + steps)
-    solver.close()
-    torch.cuda.empty_cache()
+    timed = {}
+    for storage in ("fp32", "bf16"):
+        solver = wm.solver.B200FDTD(cs, device=device, storage=storage).init_field()
+        solver.step_range(0, warmup)
+        timed[storage] = solver.step_range(warmup, warmup + steps)
+        solver.close()
+        del solver
+        torch.cuda.empty_cache()
+    ms = timed["fp32"]
     return {
         "workload": "bloch_grating: 512x512x384 cells, Bloch x/y (k_x = 0.1 * 2 pi / L_x), 16-cell CPML on z, "
                     "Debye grating layer (64-cell period, 50 % duty), pulsed Ex plane wave through a TFSF slab on z "
@@ -571,6 +575,8 @@ def run_grating_bench(wm, device, steps: int = 64, warmup: int = 8):
         "ms_per_step": ms / steps,
         "gcell_updates_per_s": cs.cells * steps / (ms * 1e-3) / 1e9,
         "channels": 2,
+        "bf16_storage": {"ms_per_step": timed["bf16"] / steps,
+                         "gcell_updates_per_s": cs.cells * steps / (timed["bf16"] * 1e-3) / 1e9},
         "compile_s": compile_s,
     }
 

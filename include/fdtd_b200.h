@@ -82,7 +82,9 @@ int fdtd_engine_destroy(fdtd_engine* h);
  * uses 1.  No counterpart in the reference (its fields are FP32 only,
  * stepping.py:1625-1630).  Call right after fdtd_engine_create (the field
  * buffers are re-allocated and zeroed).  Reduced storage runs launch variant 2
- * only, and the adjoint needs FP32.  FP16 values above 65504 * scale overflow
+ * only, and the adjoint needs FP32.  Engines with periodic or Bloch faces take
+ * FP32 or BF16 (FDTD_ERR_UNSUPPORTED for FP16); both engines of a Bloch pair
+ * need the same kind.  FP16 values above 65504 * scale overflow
  * to infinity: give explicit scales when the sources do not bound the field. */
 #define FDTD_STORE_F32 0
 #define FDTD_STORE_F16 1

@@ -264,3 +264,26 @@ def test_auto_bloch_wavevector():
     pulsed.bloch_k = "auto"
     with pytest.raises(ValueError):
         wm.compile_scene(pulsed, 10)
+
+
+@pytest.mark.gpu
+def test_grating_bf16_storage_tracks_fp32():
+    """BF16 field storage on the Bloch pair (wrap faces included, Debye pole state
+    in BF16): the grating copy's diffraction monitor within the BF16 bound of the
+    FP32 pair; FP16 storage on Bloch faces is refused."""
+    from test_precision import BF16_TOL, joint_rel_l2
+
+    wm = load_package()
+    steps = 300
+    cs = wm.compile_scene(_grating(wm), steps)
+    mons = {}
+    for storage in ("fp32", "bf16"):
+        solver = wm.solver.B200FDTD(cs, storage=storage).init_field()
+        solver.step_range(0, steps)
+        mons[storage] = {f"{m}_{c}": v.cpu().numpy() for m, d in solver.monitor_results().items() for c, v in d.items()}
+        solver.close()
+    err = joint_rel_l2(mons["bf16"], mons["fp32"])
+    print(f"grating copy, BF16 storage on the Bloch pair: monitor joint relative L2 {err:.2e}")
+    assert 0.0 < err <= BF16_TOL
+    with pytest.raises(Exception):
+        wm.solver.B200FDTD(cs, storage="fp16").init_field()

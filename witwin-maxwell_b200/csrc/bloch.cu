@@ -33,9 +33,11 @@ __device__ __forceinline__ float inv_e_at(const StepParams& p, int axis, int idx
 }
 
 // Backward difference of H component hc along `axis` for the E cell (i, j, k),
-// both channels (im ignored when !cplx).
-__device__ Cplx bdiff(const StepParams& p, const WrapFields& fr, const WrapFields& fi, bool cplx, int hc, int axis,
-                      int i, int j, int k, float pc, float ps) {
+// both channels (im ignored when !cplx); TS: the stored field type, each channel
+// read with its own scale (p: real channel, q: imaginary channel).
+template <typename TS>
+__device__ Cplx bdiff(const StepParams& p, const StepParams& q, const WrapFields& fr, const WrapFields& fi, bool cplx,
+                      int hc, int axis, int i, int j, int k, float pc, float ps) {
   const int N = axis == 0 ? p.NX : (axis == 1 ? p.NY : p.NZ);
   const int coord = axis == 0 ? i : (axis == 1 ? j : k);
   const float inv = inv_e_at(p, axis, coord);
@@ -44,7 +46,8 @@ __device__ Cplx bdiff(const StepParams& p, const WrapFields& fr, const WrapField
   };
   const float* hr = fr.hnew[hc];
   const float* hi = cplx ? fi.hnew[hc] : nullptr;
-  auto val = [&](int c) { return Cplx{__ldg(hr + at(c)), hi ? __ldg(hi + at(c)) : 0.0f}; };
+  const float sr = p.fscale[3 + hc], si = q.fscale[3 + hc];
+  auto val = [&](int c) { return Cplx{ldf<TS>(hr, at(c), true, sr), hi ? ldf<TS>(hi, at(c), true, si) : 0.0f}; };
   if (wraps(p.bnd[2 * axis])) {
     if (coord == 0) {
       const Cplx lo = val(0), h = val(N - 2);
@@ -80,13 +83,15 @@ __device__ float psi_term(const StepParams& p, int c, int which, int axis, int i
 
 __device__ __forceinline__ float coef_at(const float* arr, float u, int64_t x) { return arr ? __ldg(arr + x) : u; }
 
-// The E update of the deferred components at (i, j, k) for one channel.
+// The E update of the deferred components at (i, j, k) for one channel; TS the
+// stored field type, TA the ADE pole state type.
+template <typename TS, typename TA>
 __device__ void wrap_cell_channel(const StepParams& p, const WrapFields& f, const Cplx (&d)[3][2], const int (&m)[3],
                                   int n, int i, int j, int k, bool imag) {
   const int64_t x = wcell(p, i, j, k);
   float v[3] = {0.f, 0.f, 0.f};
   float eo[3];
-  for (int c = 0; c < 3; ++c) eo[c] = __ldg(f.eold[c] + x);
+  for (int c = 0; c < 3; ++c) eo[c] = ldf<TS>(f.eold[c], x, true, p.fscale[c]);
   unsigned mask = 0;
   // component c: its two derivative terms a (which 0) and b (which 1) along
   // Ex: y, z; Ey: x, z; Ez: x, y; Ex = (a - b), Ey = (b - a), Ez = (a - b)
@@ -110,7 +115,7 @@ __device__ void wrap_cell_channel(const StepParams& p, const WrapFields& f, cons
       const PoleTerm& pt = p.poles[b];
       if (j >= pt.j0 && j < pt.j1 && k >= pt.k0 && k < pt.k1) lane_poles |= 1u << b;
     }
-    ade<float>(p, lane_poles, i, j, k, eo[0], eo[1], eo[2], v[0], v[1], v[2], mask);
+    ade<TA>(p, lane_poles, i, j, k, eo[0], eo[1], eo[2], v[0], v[1], v[2], mask);
   }
   if (p.n_terms[0]) {
     const bool sx = __ldg(p.plane_bits + i) & kPlaneETerms;
@@ -119,11 +124,12 @@ __device__ void wrap_cell_channel(const StepParams& p, const WrapFields& f, cons
     if (sx || sy || sz) add_terms(p, 0, 0, n, i, j, k, sx, sy, sz, v[0], v[1], v[2]);
   }
   for (int c = 0; c < 3; ++c)
-    if ((mask >> c) & 1u) f.enew[c][x] = v[c];
+    if ((mask >> c) & 1u) stf<TS>(f.enew[c], x, v[c], p.finv[c]);
 }
 
 // One thread per cell of the wrap faces: the two x faces (whole planes) when x
 // wraps, then the two y faces (rows, without the x-face cells already counted).
+template <typename TS, typename TA>
 __global__ void wrap_fixup_kernel(const StepParams pr, const StepParams pim, const WrapFields fr, const WrapFields fi,
                                   int cplx, float pcx, float psx, float pcy, float psy, int n) {
   const StepParams& p = pr;
@@ -167,12 +173,12 @@ __global__ void wrap_fixup_kernel(const StepParams pr, const StepParams pim, con
       d[c][w] = {0.0f, 0.0f};
       if (m[c] == kModeDeferred) {
         const int a = ax[c][w];
-        d[c][w] = bdiff(p, fr, fi, cx, hsrc[c][w], a, i, j, k, pc[a], ps[a]);
+        d[c][w] = bdiff<TS>(p, pim, fr, fi, cx, hsrc[c][w], a, i, j, k, pc[a], ps[a]);
       }
     }
   }
-  wrap_cell_channel(pr, fr, d, m, n, i, j, k, false);
-  if (cx) wrap_cell_channel(pim, fi, d, m, n, i, j, k, true);
+  wrap_cell_channel<TS, TA>(pr, fr, d, m, n, i, j, k, false);
+  if (cx) wrap_cell_channel<TS, TA>(pim, fi, d, m, n, i, j, k, true);
 }
 
 }  // namespace
@@ -186,13 +192,20 @@ int64_t wrap_cell_count(const StepParams& p) {
 }
 
 int launch_wrap_fixup(const StepParams& pr, const StepParams* pim, const WrapFields& fr, const WrapFields* fi,
-                      const float* phase_cos, const float* phase_sin, int n, cudaStream_t stream) {
+                      const float* phase_cos, const float* phase_sin, int n, cudaStream_t stream, int storage) {
   const int64_t cells = wrap_cell_count(pr);
   if (cells == 0) return 0;
+  if (storage != kStoreF32 && storage != kStoreBF16) return static_cast<int>(cudaErrorInvalidValue);
   const unsigned blocks = static_cast<unsigned>((cells + 255) / 256);
   const bool cplx = pim != nullptr && fi != nullptr;
-  wrap_fixup_kernel<<<blocks, 256, 0, stream>>>(pr, cplx ? *pim : pr, fr, cplx ? *fi : fr, cplx ? 1 : 0,
-                                                  phase_cos[0], phase_sin[0], phase_cos[1], phase_sin[1], n);
+  if (storage == kStoreBF16)
+    wrap_fixup_kernel<__nv_bfloat16, __nv_bfloat16><<<blocks, 256, 0, stream>>>(
+        pr, cplx ? *pim : pr, fr, cplx ? *fi : fr, cplx ? 1 : 0, phase_cos[0], phase_sin[0], phase_cos[1],
+        phase_sin[1], n);
+  else
+    wrap_fixup_kernel<float, float><<<blocks, 256, 0, stream>>>(pr, cplx ? *pim : pr, fr, cplx ? *fi : fr,
+                                                                cplx ? 1 : 0, phase_cos[0], phase_sin[0],
+                                                                phase_cos[1], phase_sin[1], n);
   return static_cast<int>(cudaGetLastError());
 }
 

@@ -1239,7 +1239,7 @@ int launch_wrap_single(fdtd_engine* h, int n) {
     f.hnew[c] = h->H[h->cur][c];
   }
   const float pc[3] = {1.0f, 1.0f, 1.0f}, ps[3] = {0.0f, 0.0f, 0.0f};
-  const int err = launch_wrap_fixup(p, nullptr, f, nullptr, pc, ps, n, h->stream);
+  const int err = launch_wrap_fixup(p, nullptr, f, nullptr, pc, ps, n, h->stream, h->storage);
   if (err != 0) return cuda_fail(static_cast<cudaError_t>(err), "wrap_fixup_kernel launch");
   ++h->launches;
   return 0;
@@ -1544,7 +1544,8 @@ int fdtd_engine_set_storage(fdtd_engine* h, int kind, const float* scales) {
   if (!h || kind < kStoreF32 || kind > kStoreBF16) return fail(FDTD_ERR_INVALID_ARG, "bad storage kind");
   if (h->finalized || !h->poles.empty() || !h->checkpoints.empty())
     return fail(FDTD_ERR_STATE, "storage must be chosen right after fdtd_engine_create");
-  if (h->wrap && kind != kStoreF32) return fail(FDTD_ERR_UNSUPPORTED, "periodic and Bloch faces need FP32 storage");
+  if (h->wrap && kind == kStoreF16)
+    return fail(FDTD_ERR_UNSUPPORTED, "periodic and Bloch faces need FP32 or BF16 storage");
   if (scales) {
     for (int c = 0; c < 6; ++c) {
       int e = 0;
@@ -3470,7 +3471,8 @@ int fdtd_bloch_create(fdtd_engine* re, fdtd_engine* im, const float* phase_cos, 
   if (re->nl_general >= 0 || im->nl_general >= 0)
     return fail(FDTD_ERR_UNSUPPORTED, "nonlinear media on Bloch (complex) fields");
   const fdtd_grid_desc &a = re->desc, &b = im->desc;
-  bool same = a.nx == b.nx && a.ny == b.ny && a.nz == b.nz && a.dt == b.dt && re->stream == im->stream && re->M == im->M;
+  bool same = a.nx == b.nx && a.ny == b.ny && a.nz == b.nz && a.dt == b.dt && re->stream == im->stream && re->M == im->M &&
+              re->storage == im->storage;
   for (int f = 0; f < 6; ++f) same = same && a.boundary[f] == b.boundary[f];
   for (int x = 0; x < 3; ++x) same = same && a.pml_lo[x] == b.pml_lo[x] && a.pml_hi[x] == b.pml_hi[x];
   if (!same) return fail(FDTD_ERR_INVALID_ARG, "the two channels need the same grid, boundaries, stream and sample block");
@@ -3543,7 +3545,7 @@ int fdtd_bloch_step_range(fdtd_bloch* p, int n0, int n1) {
       fi.enew[c] = p->im->E[p->im->cur][c];
       fi.hnew[c] = p->im->H[p->im->cur][c];
     }
-    const int err = launch_wrap_fixup(pr, &pim, fr, &fi, p->pc, p->ps, n, st);
+    const int err = launch_wrap_fixup(pr, &pim, fr, &fi, p->pc, p->ps, n, st, p->re->storage);
     if (err != 0) return cuda_fail(static_cast<cudaError_t>(err), "wrap_fixup_kernel launch");
     for (fdtd_engine* h : hs) {
       int rc = launch_gather(h, h->n_samples > 0 ? h->pending : -1);

@@ -212,8 +212,9 @@ struct AdeParams {
 // mask}, one warp each.
 int launch_ade_pass(const AdeParams& a, const int* tiles, int n_tiles, cudaStream_t stream);
 // pim / fi: the imaginary channel of a Bloch pair, or nullptr (real periodic).
+// storage: kStoreF32 or kStoreBF16 (the stored field type of both channels).
 int launch_wrap_fixup(const StepParams& pr, const StepParams* pim, const WrapFields& fr, const WrapFields* fi,
-                      const float* phase_cos, const float* phase_sin, int n, cudaStream_t stream);
+                      const float* phase_cos, const float* phase_sin, int n, cudaStream_t stream, int storage);
 
 constexpr int kStoreF32 = 0;
 constexpr int kStoreF16 = 1;
