@@ -127,6 +127,20 @@ def test_face_terms_and_checks():
                                           (4, 0, 0), (20, 20, 60))
     with pytest.raises(ValueError):
         wm.compile_scene(along_x, 10)
+    # the reference's slab checks (tfsf_state.py:171-199): faces inside the non-CPML
+    # region, in vacuum
+    in_pml = _scene(wm)
+    w = in_pml.sources[0]
+    in_pml.sources[0] = wm.PlaneWaveTFSF(w.direction, w.polarization, w.source_time, (0, 0, 4), (24, 20, 40))
+    with pytest.raises(ValueError):
+        wm.compile_scene(in_pml, 10)
+    dielectric_face = _scene(wm)
+    dielectric_face.structures.append(wm.Structure(wm.Box((0, 0, 38), (24, 20, 44)), wm.Medium(2.0)))
+    with pytest.raises(ValueError):
+        wm.compile_scene(dielectric_face, 10)
+    inside = _scene(wm)
+    inside.structures.append(wm.Structure(wm.Box((0, 0, 26), (24, 20, 32)), wm.Medium(2.0)))
+    wm.compile_scene(inside, 10)
 
 
 @pytest.mark.gpu

@@ -1036,6 +1036,7 @@ def compile_scene(scene: Scene, time_steps: int) -> CompiledScene:
             shifted.extend(beam_shifted)
         elif isinstance(src, PlaneWaveTFSF) and any(b == BOUNDARY_BLOCH for b in scene.boundary):
             # CW plane wave through a TFSF slab on the complex Bloch field
+            _validate_grating_slab(scene, src, eps_node)
             slab_patches, slab_shifted = _grating_slab_patches(
                 scene, src, {n: static_curl.get(n, np.float32(uniform[n][1])) for n in COMPONENTS}, dt, time_steps)
             patches.extend(slab_patches)
@@ -1241,6 +1242,26 @@ class GratingSlabTerm:
     delay: np.ndarray | None = None
     t_offset: float = 0.0
     source_time: object = None
+
+
+def _validate_grating_slab(scene: Scene, src: PlaneWaveTFSF, eps_node) -> None:
+    """The reference's checks of a TFSF slab (witwin/maxwell/fdtd/excitation/
+    tfsf_state.py:171-199): at least two cells along the injection axis, both faces
+    inside the non-CPML region, and vacuum (relative permittivity 1 within 1e-5)
+    on the two face planes."""
+    dvec = np.asarray(src.direction, dtype=np.float64)
+    axis = int(np.argmax(np.abs(dvec)))
+    lo, hi = int(src.lower[axis]), int(src.upper[axis])
+    pml_lo, pml_hi = scene.pml_lengths()
+    if hi <= lo + 1:
+        raise ValueError(f"TFSF slab bounds must span at least two cells along {'xyz'[axis]}")
+    if lo < pml_lo[axis] or hi > scene.nodes[axis] - pml_hi[axis] - 1:
+        raise ValueError("TFSF slab bounds must lie strictly inside the non-PML simulation region")
+    for face in (lo, hi):
+        for arr in eps_node:
+            plane = np.take(arr, face, axis=axis)
+            if np.max(np.abs(plane - 1.0)) > 1e-5:
+                raise ValueError("TFSF slab interfaces must remain in vacuum")
 
 
 def grating_slab_terms(scene: Scene, src: PlaneWaveTFSF, curl: dict, dt: float, steps: int) -> list:
